@@ -1,0 +1,543 @@
+// ORACLE / TEST INFRASTRUCTURE ONLY.
+//
+// Drives the reference's own CUDA kernels (Tracking/Pyrdown.cu,
+// Tracking/Reduction.cu, Mapping/DeviceMap.cu, Mapping/FuseMap.cu,
+// Mapping/RenderScene.cu, compiled unmodified from the reference tree by
+// oracle/Makefile) through their public free functions (Tracking/Reduction.h,
+// Mapping/RenderScene.h), in the order the reference's host classes call
+// them.  The host classes themselves (Core/Frame.cc, Tracking/Tracking.cc,
+// Mapping/Mapping.cc, Core/System.cc) need OpenCV, Eigen and Sophus, none of
+// which exist here, so their per-frame logic is restated below with the FP64
+// helpers of oracle/se3.hpp.  The result is the reference's CUDA path, used
+// to produce golden vectors that pin the CPU oracle.
+//
+// Buffers are allocated with padding (16 extra rows per 2-D image, voxel pool
+// rounded up to a multiple of 1024 blocks) and zero-filled, so that three
+// out-of-bounds accesses of the reference land inside owned memory:
+//   - ResizeMapKernel bounds-checks against the source size
+//     (Tracking/Pyrdown.cu:256), writing up to 7 rows past a destination whose
+//     height is not a multiple of 8;
+//   - ResetSdfBlockKernel releases voxels without an index bound
+//     (Mapping/FuseMap.cu:341-344), past the pool when NumSdfBlocks is not a
+//     multiple of 1024 (700000 is not);
+//   - fillBlocksKernel reads up to 3 list entries past the tile count
+//     (Mapping/RenderScene.cu:161-165, 269); zero-filling keeps them in range.
+//   - the raycast's per-thread entry cache starts as HashEntry() with ptr -1
+//     and pos (0,0,0) (Mapping/DeviceMap.h:22-24), and FindVoxel trusts a
+//     cache hit without checking ptr (Mapping/DeviceMap.cu:97-103), so a first
+//     probe inside block (0,0,0) reads voxel index -1 + local index; the pool
+//     view starts one block into the allocation so that index stays owned.
+// The hash table is zero-filled before ResetMap because ResetHashKernel only
+// clears ptr (Mapping/FuseMap.cu:321-332, DeviceMap.h:36-38).
+#include "Reduction.h"
+#include "RenderScene.h"
+#include "../se3.hpp"
+
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+constexpr int kPyr = 3;        // Frame::NUM_PYRS (Core/Frame.h:20)
+constexpr int kPadRows = 16;
+
+template <class T>
+void make2d(DeviceArray2D<T>& a, int cols, int rows) {
+    a.create(cols, rows + kPadRows);
+    a.rows = rows;
+    SafeCall(cudaMemset2D(a.data, a.step, 0, a.step, rows + kPadRows));
+}
+
+template <class T>
+void make1d(DeviceArray<T>& a, size_t n) {
+    a.create(n);
+    SafeCall(cudaMemset(a.data, 0, sizeof(T) * n));
+}
+
+struct RFrame {
+    DeviceArray2D<unsigned short> temp;
+    DeviceArray2D<float> range;
+    DeviceArray2D<uchar3> color;
+    DeviceArray2D<float4> vmap[kPyr], nmap[kPyr];
+    DeviceArray2D<float> depth[kPyr];
+    DeviceArray2D<unsigned char> image[kPyr];
+    DeviceArray2D<short> dIdx[kPyr], dIdy[kPyr];
+    double pose[16];
+
+    void create(int cols, int rows) {
+        make2d(temp, cols, rows);
+        make2d(range, cols, rows);
+        make2d(color, cols, rows);
+        for (int i = 0; i < kPyr; ++i) {
+            int c = cols / (1 << i), r = rows / (1 << i);
+            make2d(vmap[i], c, r);
+            make2d(nmap[i], c, r);
+            make2d(depth[i], c, r);
+            make2d(image[i], c, r);
+            make2d(dIdx[i], c, r);
+            make2d(dIdy[i], c, r);
+        }
+        for (int i = 0; i < 16; ++i) pose[i] = (i % 5 == 0) ? 1.0 : 0.0;
+    }
+    // Frame::GpuRotation / GpuInvRotation / GpuTranslation (Core/Frame.cc:275-294)
+    Matrix3f rot() const {
+        Matrix3f m;
+        m.rowx = make_float3(pose[0], pose[1], pose[2]);
+        m.rowy = make_float3(pose[4], pose[5], pose[6]);
+        m.rowz = make_float3(pose[8], pose[9], pose[10]);
+        return m;
+    }
+    Matrix3f rot_inv() const {
+        Matrix3f m;
+        m.rowx = make_float3(pose[0], pose[4], pose[8]);
+        m.rowy = make_float3(pose[1], pose[5], pose[9]);
+        m.rowz = make_float3(pose[2], pose[6], pose[10]);
+        return m;
+    }
+    float3 trans() const { return make_float3(pose[3], pose[7], pose[11]); }
+};
+
+struct RefCtx {
+    int cols, rows;
+    float fx, fy, cx, cy;
+    float depthScale, depthCutoff;
+    int iters[kPyr];
+    RFrame frames[2];
+    RFrame* next;
+    RFrame* last;
+
+    DeviceArray2D<float> sumSE3;
+    DeviceArray<float> outSE3;
+    DeviceArray2D<int> sumRes;
+    DeviceArray<int> outRes;
+    int state, lastState, noMissedFrames, numFramesAfterReloc;
+    float lastIcpError, lastRgbError, lastIcpCount, lastRgbCount;
+
+    DeviceArray<int> heap, heapCounter, hashCounter, bucketMutex;
+    DeviceArray<Voxel> sdfBlock;
+    DeviceArray<uint> noVisibleEntries;
+    DeviceArray<HashEntry> hashEntries, visibleEntries;
+    DeviceArray<uint> noRenderingBlocks;
+    DeviceArray<RenderingBlock> renderingBlockList;
+    DeviceArray2D<float> zRangeMin, zRangeMax;
+
+    // Mapping::operator DeviceMap (Mapping/Mapping.cc:311-325)
+    DeviceMap devmap() const {
+        DeviceMap m;
+        m.heapMem = heap;
+        m.heapCounter = heapCounter;
+        m.noVisibleBlocks = noVisibleEntries;
+        m.bucketMutex = bucketMutex;
+        m.hashEntries = hashEntries;
+        m.visibleEntries = visibleEntries;
+        m.voxelBlocks = sdfBlock;
+        m.voxelBlocks.data = (Voxel*)sdfBlock.data + DeviceMap::BlockSize3;  // front pad
+        m.entryPtr = hashCounter;
+        return m;
+    }
+    Intrinsics K(int i) const { return Intrinsics(fx, fy, cx, cy)(i); }
+    // Frame::fx(i) ... (Core/Frame.cc:229-257): K / 2^i in float
+    float fxl(int i) const { return fx / (1 << i); }
+    float fyl(int i) const { return fy / (1 << i); }
+    float cxl(int i) const { return cx / (1 << i); }
+    float cyl(int i) const { return cy / (1 << i); }
+};
+
+// Frame::FillImages (Core/Frame.cc:59-78)
+void fill_images(RefCtx* c, RFrame* f, const uint16_t* depth, const uint8_t* rgb) {
+    f->temp.upload(depth, sizeof(uint16_t) * c->cols);
+    f->color.upload(rgb, 3 * c->cols);
+    FilterDepth(f->temp, f->range, f->depth[0], c->depthScale, c->depthCutoff);
+    ImageToIntensity(f->color, f->image[0]);
+    for (int i = 1; i < kPyr; ++i) {
+        PyrDownGauss(f->depth[i - 1], f->depth[i]);
+        PyrDownGauss(f->image[i - 1], f->image[i]);
+    }
+    for (int i = 0; i < kPyr; ++i) {
+        ComputeVMap(f->depth[i], f->vmap[i], c->fxl(i), c->fyl(i), c->cxl(i), c->cyl(i),
+                    c->depthCutoff);
+        ComputeNMap(f->vmap[i], f->nmap[i]);
+        ComputeDerivativeImage(f->image[i], f->dIdx[i], f->dIdy[i]);
+    }
+}
+
+// Frame::ResizeImages (Core/Frame.cc:80-84)
+void resize_images(RFrame* f) {
+    for (int i = 1; i < kPyr; ++i) ResizeMap(f->vmap[i - 1], f->nmap[i - 1], f->vmap[i], f->nmap[i]);
+}
+
+void rgb_step(RefCtx* c, int i, double* A, double* b, float* res) {
+    RFrame *N = c->next, *L = c->last;
+    RGBStep(N->image[i], L->image[i], N->vmap[i], L->vmap[i], N->dIdx[i], N->dIdy[i], N->rot(),
+            N->rot_inv(), L->rot(), L->rot_inv(), N->trans(), L->trans(), c->K(i), c->sumSE3,
+            c->outSE3, c->sumRes, c->outRes, res, A, b);
+}
+
+void icp_step(RefCtx* c, int i, double* A, double* b, float* res) {
+    RFrame *N = c->next, *L = c->last;
+    ICPStep(N->vmap[i], L->vmap[i], N->nmap[i], L->nmap[i], N->rot(), N->trans(), L->rot(),
+            L->rot_inv(), L->trans(), c->K(i), c->sumSE3, c->outSE3, res, A, b);
+}
+
+// Tracker::ComputeSE3(false, ITERATIONS_SE3, THRESH_ICP_SE3)
+// (Tracking/Tracking.cc:296-409; MIN_ICP_COUNT from Tracking.h:102)
+bool compute_se3(RefCtx* c) {
+    const int minCount[kPyr] = {2000, 1000, 100};
+    const float thresh = 0.0001f;
+    double lastPose[16], pose[16], delta[16];
+    std::memcpy(lastPose, c->last->pose, sizeof lastPose);
+    std::memcpy(pose, c->next->pose, sizeof pose);
+    for (int i = 0; i < 16; ++i) delta[i] = (i % 5 == 0) ? 1.0 : 0.0;
+    float rgbError = 0, icpError = 0;
+    int rgbCount = 0, icpCount = 0;
+    for (int i = kPyr - 1; i >= 0; --i) {
+        for (int j = 0; j < c->iters[i]; ++j) {
+            double Ar[36], br[6], Ai[36], bi[6];
+            float rr[2], ri[2];
+            rgb_step(c, i, Ar, br, rr);
+            rgbError = std::sqrt(rr[0]) / rr[1];
+            rgbCount = (int)rr[1];
+            c->lastRgbError = rgbError;
+            c->lastRgbCount = rr[1];
+            if (std::isnan(rgbError) || rgbCount < minCount[i]) {
+                std::memcpy(c->next->pose, lastPose, sizeof lastPose);
+                return false;
+            }
+            icp_step(c, i, Ai, bi, ri);
+            icpError = std::sqrt(ri[0]) / ri[1];
+            icpCount = (int)ri[1];
+            c->lastIcpError = icpError;
+            c->lastIcpCount = ri[1];
+            if (std::isnan(icpError) || icpCount < minCount[i]) {
+                std::memcpy(c->next->pose, lastPose, sizeof lastPose);
+                return false;
+            }
+            double A[36], b[6], xi[6], dT[16], dinv[16];
+            const float w = 1e-4f;
+            for (int k = 0; k < 36; ++k) A[k] = Ar[k] * w + Ai[k];
+            for (int k = 0; k < 6; ++k) b[k] = br[k] * w + bi[k];
+            fbo::ldlt_solve(A, b, xi);
+            fbo::se3_exp(xi, dT);
+            fbo::mat4_mul(dT, delta, delta);
+            fbo::mat4_inv(delta, dinv);
+            fbo::mat4_mul(lastPose, dinv, c->next->pose);
+        }
+    }
+    double pinv[16], p[16];
+    fbo::mat4_inv(pose, pinv);
+    fbo::mat4_mul(pinv, c->next->pose, p);
+    double tn = std::sqrt(p[3] * p[3] + p[7] * p[7] + p[11] * p[11]);
+    if (icpError < thresh && fbo::euler_sin_norm(p) <= 0.1 && tn <= 0.1) return true;
+    std::memcpy(c->next->pose, lastPose, sizeof lastPose);
+    return false;
+}
+
+void swap_frames(RefCtx* c) { std::swap(c->next, c->last); }
+
+// Tracker::Track with the SURF bootstrap, keyframes and relocalisation absent
+// (Tracking/Tracking.cc:58-112, 150-164): TrackLastFrame fails without key
+// points, so the next pose starts from the last pose; relocalisation fails.
+bool track(RefCtx* c) {
+    std::swap(c->state, c->lastState);
+    switch (c->state) {
+    case 1:
+        // InitTracking -> ResetTracking (Tracking.cc:45-53, 229-234)
+        for (int i = 0; i < 16; ++i) c->next->pose[i] = c->last->pose[i] = (i % 5 == 0);
+        swap_frames(c);
+        c->lastState = 0;
+        return true;
+    case 0: {
+        std::memcpy(c->next->pose, c->last->pose, sizeof c->next->pose);
+        bool valid = compute_se3(c);
+        if (valid) {
+            c->noMissedFrames = 0;
+            if (c->lastState != -1) {
+                c->lastState = 0;
+                swap_frames(c);
+                return true;
+            }
+            c->lastState = 0;
+            return false;
+        }
+        c->lastState = 0;
+        c->noMissedFrames++;
+        if (c->noMissedFrames > 9) c->lastState = -1;
+        return false;
+    }
+    default:
+        c->lastState = -1;
+        return false;
+    }
+}
+
+// Mapping::FuseColor (Mapping/Mapping.cc:76-90)
+void fuse(RefCtx* c, RFrame* f, uint* no) {
+    FuseMapColor(f->range, f->color, f->nmap[0], c->noVisibleEntries, f->rot(), f->rot_inv(),
+                 f->trans(), c->devmap(), c->fxl(0), c->fyl(0), c->cxl(0), c->cyl(0),
+                 DeviceMap::DepthMax, DeviceMap::DepthMin, no);
+}
+
+// Mapping::RayTrace (Mapping/Mapping.cc:92-109)
+void raytrace(RefCtx* c, RFrame* f, uint noVisibleBlocks) {
+    float depthMax = DeviceMap::DepthMax, depthMin = DeviceMap::DepthMin;
+    float fx = c->fxl(0), fy = c->fyl(0), cx = c->cxl(0), cy = c->cyl(0);
+    if (CreateRenderingBlocks(c->visibleEntries, c->zRangeMin, c->zRangeMax, depthMax, depthMin,
+                              c->renderingBlockList, c->noRenderingBlocks, f->rot_inv(),
+                              f->trans(), noVisibleBlocks, fx, fy, cx, cy)) {
+        Raycast(c->devmap(), f->vmap[0], f->nmap[0], c->zRangeMin, c->zRangeMax, f->rot(),
+                f->rot_inv(), f->trans(), 1.0 / fx, 1.0 / fy, cx, cy);
+    }
+}
+
+void reset_map(RefCtx* c) {
+    SafeCall(cudaMemset(c->hashEntries.data, 0, sizeof(HashEntry) * c->hashEntries.size));
+    SafeCall(cudaMemset(c->visibleEntries.data, 0, sizeof(HashEntry) * c->visibleEntries.size));
+    ResetMap(c->devmap());
+}
+
+template <class T>
+void download2d(const DeviceArray2D<T>& a, void* dst) {
+    if (dst) a.download(dst, sizeof(T) * a.cols);
+}
+
+}  // namespace
+
+extern "C" {
+
+// DeviceMap compile-time constants of this reference build
+// (Mapping/DeviceMap.h:135-151).
+void ref_constants(double* out) {
+    out[0] = DeviceMap::VoxelSize;
+    out[1] = DeviceMap::TruncateDist;
+    out[2] = DeviceMap::DepthMin;
+    out[3] = DeviceMap::DepthMax;
+    out[4] = DeviceMap::NumBuckets;
+    out[5] = DeviceMap::NumExcess;
+    out[6] = DeviceMap::NumSdfBlocks;
+    out[7] = DeviceMap::MaxRenderingBlocks;
+    out[8] = DeviceMap::stepScale;
+    out[9] = sizeof(HashEntry);
+    out[10] = sizeof(Voxel);
+    out[11] = sizeof(RenderingBlock);
+}
+
+void* ref_create(int cols, int rows, float fx, float fy, float cx, float cy, float depth_scale,
+                 float depth_cutoff, const int* iters) {
+    RefCtx* c = new RefCtx();
+    c->cols = cols;
+    c->rows = rows;
+    c->fx = fx;
+    c->fy = fy;
+    c->cx = cx;
+    c->cy = cy;
+    c->depthScale = depth_scale;
+    c->depthCutoff = depth_cutoff;
+    for (int i = 0; i < kPyr; ++i) c->iters[i] = iters ? iters[i] : (i == 0 ? 10 : i == 1 ? 5 : 3);
+    c->frames[0].create(cols, rows);
+    c->frames[1].create(cols, rows);
+    c->next = &c->frames[0];
+    c->last = &c->frames[1];
+    // Tracker::Tracker (Tracking/Tracking.cc:29-34)
+    make2d(c->sumSE3, 29, 96);
+    make1d(c->outSE3, 29);
+    make2d(c->sumRes, 2, 96);
+    make1d(c->outRes, 2);
+    c->state = c->lastState = 1;
+    c->noMissedFrames = 0;
+    c->numFramesAfterReloc = 10;  // System::System (Core/System.cc:72)
+    // Mapping::Create (Mapping/Mapping.cc:11-51), hot-path buffers only
+    make1d(c->heapCounter, 1);
+    make1d(c->hashCounter, 1);
+    make1d(c->noVisibleEntries, 1);
+    make1d(c->heap, DeviceMap::NumSdfBlocks);
+    size_t paddedBlocks = (DeviceMap::NumSdfBlocks + 1023) / 1024 * 1024;
+    make1d(c->sdfBlock, (paddedBlocks + 1) * DeviceMap::BlockSize3);
+    c->sdfBlock.size = (size_t)DeviceMap::NumVoxels;
+    make1d(c->bucketMutex, DeviceMap::NumBuckets);
+    make1d(c->hashEntries, DeviceMap::NumEntries);
+    make1d(c->visibleEntries, DeviceMap::NumEntries);
+    make2d(c->zRangeMin, 80, 60);
+    make2d(c->zRangeMax, 80, 60);
+    make1d(c->noRenderingBlocks, 1);
+    make1d(c->renderingBlockList, DeviceMap::MaxRenderingBlocks);
+    reset_map(c);
+    return c;
+}
+
+void ref_destroy(void* h) {
+    RefCtx* c = (RefCtx*)h;
+    c->sdfBlock.size = 0;
+    delete c;
+}
+
+// System::GrabImage (Core/System.cc:92-138) with the viewer-only
+// RenderTopDown and the mesh/key-point requests left out.
+// info: [0] GrabFrame result, [1] tracker state, [2] visible blocks (fused
+// frames), [3] icp error, [4] icp count, [5] rgb error, [6] rgb count,
+// [7] fused (1/0)
+int ref_grab(void* h, const uint16_t* depth, const uint8_t* rgb, double* info) {
+    RefCtx* c = (RefCtx*)h;
+    c->lastIcpError = c->lastRgbError = NAN;
+    c->lastIcpCount = c->lastRgbCount = 0;
+    // Tracker::GrabFrame (Tracking/Tracking.cc:236-243)
+    resize_images(c->last);
+    fill_images(c, c->next, depth, rgb);
+    bool state = track(c);
+    if (c->state == 0) c->numFramesAfterReloc++;
+    if (c->state == -1) c->numFramesAfterReloc = 0;
+    uint noBlocks = 0;
+    int fused = 0;
+    if (state) {
+        if (c->state != -1 && c->numFramesAfterReloc >= 10) {
+            fuse(c, c->last, &noBlocks);
+            fused = 1;
+        }
+        if (c->state != -1) raytrace(c, c->last, noBlocks);
+    }
+    if (info) {
+        info[0] = state;
+        info[1] = c->state;
+        info[2] = noBlocks;
+        info[3] = c->lastIcpError;
+        info[4] = c->lastIcpCount;
+        info[5] = c->lastRgbError;
+        info[6] = c->lastRgbCount;
+        info[7] = fused;
+    }
+    return 0;
+}
+
+static RFrame* pick(RefCtx* c, int which) { return which ? c->next : c->last; }
+
+void ref_get_pose(void* h, int which, double* T) { std::memcpy(T, pick((RefCtx*)h, which)->pose, 128); }
+void ref_set_pose(void* h, int which, const double* T) { std::memcpy(pick((RefCtx*)h, which)->pose, T, 128); }
+void ref_swap(void* h) { swap_frames((RefCtx*)h); }
+
+int ref_fill_images(void* h, int which, const uint16_t* depth, const uint8_t* rgb) {
+    RefCtx* c = (RefCtx*)h;
+    fill_images(c, pick(c, which), depth, rgb);
+    return 0;
+}
+
+int ref_resize_images(void* h, int which) {
+    resize_images(pick((RefCtx*)h, which));
+    return 0;
+}
+
+int ref_download_level(void* h, int which, int level, float* vmap, float* nmap, float* depth,
+                       uint8_t* image, int16_t* dx, int16_t* dy) {
+    RFrame* f = pick((RefCtx*)h, which);
+    download2d(f->vmap[level], vmap);
+    download2d(f->nmap[level], nmap);
+    download2d(f->depth[level], depth);
+    download2d(f->image[level], image);
+    download2d(f->dIdx[level], dx);
+    download2d(f->dIdy[level], dy);
+    return 0;
+}
+
+int ref_download_range(void* h, int which, float* range) {
+    download2d(pick((RefCtx*)h, which)->range, range);
+    return 0;
+}
+
+int ref_upload_maps(void* h, int which, int level, const float* vmap, const float* nmap) {
+    RFrame* f = pick((RefCtx*)h, which);
+    if (vmap) f->vmap[level].upload(vmap, sizeof(float4) * f->vmap[level].cols);
+    if (nmap) f->nmap[level].upload(nmap, sizeof(float4) * f->nmap[level].cols);
+    return 0;
+}
+
+int ref_icp_step(void* h, int level, double* A, double* b, float* res) {
+    icp_step((RefCtx*)h, level, A, b, res);
+    return 0;
+}
+
+int ref_rgb_step(void* h, int level, double* A, double* b, float* res) {
+    rgb_step((RefCtx*)h, level, A, b, res);
+    return 0;
+}
+
+int ref_reset_map(void* h) {
+    reset_map((RefCtx*)h);
+    return 0;
+}
+
+int ref_fuse(void* h, int which, uint32_t* no) {
+    RefCtx* c = (RefCtx*)h;
+    uint n = 0;
+    fuse(c, pick(c, which), &n);
+    *no = n;
+    return 0;
+}
+
+int ref_raytrace(void* h, int which, uint32_t no) {
+    RefCtx* c = (RefCtx*)h;
+    raytrace(c, pick(c, which), no);
+    return 0;
+}
+
+// entries: NumEntries x {pos.x, pos.y, pos.z, ptr, offset}; counters:
+// {heapCounter, entryPtr}
+int ref_download_hash(void* h, int32_t* entries, int32_t* counters) {
+    RefCtx* c = (RefCtx*)h;
+    std::vector<HashEntry> tmp(c->hashEntries.size);
+    c->hashEntries.download(tmp.data());
+    for (size_t i = 0; i < tmp.size(); ++i) {
+        entries[i * 5 + 0] = tmp[i].pos.x;
+        entries[i * 5 + 1] = tmp[i].pos.y;
+        entries[i * 5 + 2] = tmp[i].pos.z;
+        entries[i * 5 + 3] = tmp[i].ptr;
+        entries[i * 5 + 4] = tmp[i].offset;
+    }
+    if (counters) {
+        c->heapCounter.download(&counters[0]);
+        c->hashCounter.download(&counters[1]);
+    }
+    return 0;
+}
+
+int ref_download_visible(void* h, int32_t* entries, uint32_t n) {
+    RefCtx* c = (RefCtx*)h;
+    std::vector<HashEntry> tmp(n);
+    SafeCall(cudaMemcpy(tmp.data(), c->visibleEntries.data, sizeof(HashEntry) * n,
+                        cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) {
+        entries[i * 5 + 0] = tmp[i].pos.x;
+        entries[i * 5 + 1] = tmp[i].pos.y;
+        entries[i * 5 + 2] = tmp[i].pos.z;
+        entries[i * 5 + 3] = tmp[i].ptr;
+        entries[i * 5 + 4] = tmp[i].offset;
+    }
+    return 0;
+}
+
+// Voxels of n blocks given by their entry ptr (voxel index of the block).
+int ref_download_blocks(void* h, const int32_t* ptrs, int n, float* sdf, uint8_t* weight,
+                        uint8_t* rgb) {
+    RefCtx* c = (RefCtx*)h;
+    std::vector<Voxel> tmp(512);
+    for (int i = 0; i < n; ++i) {
+        const Voxel* base = (const Voxel*)c->sdfBlock.data + DeviceMap::BlockSize3;
+        SafeCall(cudaMemcpy(tmp.data(), base + ptrs[i], sizeof(Voxel) * 512,
+                            cudaMemcpyDeviceToHost));
+        for (int v = 0; v < 512; ++v) {
+            sdf[i * 512 + v] = tmp[v].sdf;
+            weight[i * 512 + v] = tmp[v].weight;
+            rgb[(i * 512 + v) * 3 + 0] = tmp[v].color.x;
+            rgb[(i * 512 + v) * 3 + 1] = tmp[v].color.y;
+            rgb[(i * 512 + v) * 3 + 2] = tmp[v].color.z;
+        }
+    }
+    return 0;
+}
+
+int ref_download_zrange(void* h, float* zmin, float* zmax) {
+    RefCtx* c = (RefCtx*)h;
+    download2d(c->zRangeMin, zmin);
+    download2d(c->zRangeMax, zmax);
+    return 0;
+}
+
+}  // extern "C"
