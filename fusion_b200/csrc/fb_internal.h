@@ -1,0 +1,149 @@
+// Internal interfaces between the translation units of libfusion_b200.so.
+#ifndef FB_INTERNAL_H
+#define FB_INTERNAL_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fb_common.cuh"
+
+namespace fb {
+
+// ------------------------------------------------------------------ tracking
+
+constexpr int kTrackMaxBlocks = 592;   // 4 resident blocks of 256 threads per SM
+
+// One pyramid level of the current (next) and last frames.  Pitches in
+// elements: vp for float4 maps, gp for u8 images, sp for i16 derivatives.
+struct TrackLevel {
+    int W, H, vp, gp, sp;
+    Intr k;
+    const float4* vcurr;
+    const float4* ncurr;
+    const float4* vlast;
+    const float4* nlast;
+    const uint8_t* gcurr;
+    const uint8_t* glast;
+    const int16_t* dx;
+    const int16_t* dy;
+};
+
+// Device-resident tracker state of one session (Tracker's poses, residuals).
+struct TrackState {
+    double last_pose[16];   // pose of the last (model) frame
+    double pose[16];        // current estimate of the next frame's pose
+    double init_pose[16];   // the next pose when ComputeSE3 started
+    double delta[16];       // accumulated increment (Tracking.cc:314, 392)
+    DevPose cur, last;      // float views of pose / last_pose
+    int failed;             // tracking of this frame failed (pose rolled back)
+    int pad0;
+    float icp_error, icp_count, rgb_error, rgb_count;
+    float sigma;
+    int pad1;
+    long long rgb_cnt, rgb_sq;
+    double icp_sums[29];
+    double rgb_sums[29];
+    long long scratch_cnt[kTrackMaxBlocks];
+    long long scratch_sq[kTrackMaxBlocks];
+};
+
+int track_grid(int n);
+int launch_track_begin(TrackState* st, cudaStream_t s);
+int launch_track_iter(const TrackLevel& L, TrackState* st, float* partials, unsigned int* tickets, int* residual,
+                       int min_count, bool is_final, cudaStream_t s);
+int launch_step_icp(const TrackLevel& L, const DevPose& cur, const DevPose& last, float* partials,
+                     unsigned int* ticket, double* out, cudaStream_t s);
+int launch_step_rgb(const TrackLevel& L, const DevPose& cur, const DevPose& last, float* partials,
+                     unsigned int* tickets, int* residual, double* out, cudaStream_t s);
+
+// ------------------------------------------------------------- preprocessing
+
+int launch_level0(const uint16_t* depth, int dpitch, const uint8_t* rgb, int rgbpitch, int W, int H,
+                   float depth_scale, float cutoff, float* raw, int rawpitch, float* filt, int fpitch,
+                   uint8_t* gray, int gpitch, cudaStream_t st);
+int launch_pyrdown(const float* sd, int sdp, const uint8_t* sg, int sgp, int SW, int SH, float* dd, int ddp,
+                    uint8_t* dg, int dgp, cudaStream_t st);
+int launch_maps(const float* depth, int dp, const uint8_t* gray, int gp, int W, int H, const Intr& k,
+                 float cutoff, float4* vmap, int vp, float4* nmap, int np, int16_t* dx, int16_t* dy, int sp,
+                 cudaStream_t st);
+int launch_nmap(const float4* vmap, int vp, int W, int H, float4* nmap, int np, cudaStream_t st);
+int launch_resize(const float4* vs, const float4* ns, int sp, int SW, int SH, float4* vd, float4* nd, int dp,
+                   cudaStream_t st);
+
+// ----------------------------------------------------------------------- map
+
+struct MapCounters {
+    int heap_counter;      // top of the free-block stack (DeviceMap heapCounter)
+    int entry_ptr;         // next excess-list slot, 1-based (DeviceMap entryPtr)
+    int holes;             // an entry with ptr -1 was linked (pool exhausted once)
+    int n_alloc;           // entries in the allocated list
+    int n_req;             // new blocks requested this frame
+    int n_new;             // blocks inserted by the last allocation
+    int n_visible;         // visible blocks of the last fusion / visibility pass
+    int n_tiles;           // rendering rectangles of the last z-range pass
+    int excess_total;      // new blocks going to the excess list this frame
+    unsigned int err;      // ErrFlag bits, sticky
+    int seq_path;          // last allocation used the sequential path
+    // snapshot taken before insertion (read by the insert kernel only)
+    int snap_M, snap_hc, snap_ep, snap_na;
+    int fast;              // the parallel insertion path applies
+    int pad;
+};
+
+struct NewBlock {
+    short x, y, z, pad;
+    uint32_t bucket;
+    int setslot;           // slot in the request set (cleared after insertion)
+    int j;                 // arrival index inside the bucket
+    int rank;              // canonical rank: order by (bucket, x, y, z)
+    int pad2;
+};
+
+// Geometry of the map (runtime form of DeviceMap's constants).
+struct MapGeom {
+    float voxel_size, voxel_size_inv, trunc_dist, step_scale, block_width;
+    float depth_min, depth_max;
+};
+
+struct MapView {
+    HEntry* entries;
+    int NB, NE, NS;
+    int* heap;
+    Voxel* voxels;
+    MapCounters* ctr;
+    int* alloc_list;            // slots of allocated entries, allocation order (NS)
+    int* visible;               // slots of visible entries (NS)
+    unsigned long long* reqset; // request set, open addressing (reqcap, power of 2)
+    int reqcap;
+    NewBlock* newblk;           // this frame's new blocks (newcap)
+    int newcap;
+    int* order;                 // canonical order -> newblk index (newcap)
+    int* arrival;               // bucket segment -> newblk index (newcap)
+    int* bucket_cnt;            // NB, zero between frames
+    int* bucket_start;          // NB
+    int* bucket_x;              // NB: excess start << 1 | head-was-empty
+    int* chunk_sums;            // 2 * nchunks
+    int nchunks;
+    float* zmin;                // z-range image, zc x zr
+    float* zmax;
+    int zc, zr;
+    MapGeom g;
+};
+
+constexpr int kScanChunk = 4096;
+
+int launch_map_reset(const MapView& m, cudaStream_t s);
+// pose: device pointer; skip: device flag (nonzero: do nothing), may be null
+int launch_allocate(const MapView& m, const float* raw, int rp, int W, int H, const Intr& k, const DevPose* pose,
+                     const int* skip, cudaStream_t s);
+int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
+                       cudaStream_t s);
+int launch_integrate(const MapView& m, const float* raw, int rp, const uint8_t* rgb, int cp, const float4* nmap,
+                      int np, int W, int H, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s);
+int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s);
+int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,
+                    const DevPose* pose, const int* skip, cudaStream_t s);
+
+}  // namespace fb
+
+#endif

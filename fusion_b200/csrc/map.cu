@@ -1,0 +1,647 @@
+// Voxel-block hash map: block allocation, visibility and TSDF/colour
+// integration (the reference's Mapping/DeviceMap.cu, Mapping/FuseMap.cu).
+//
+// Allocation is deterministic.  The reference lets every pixel's probes race
+// for a per-bucket try-lock (DeviceMap.cu:23-62): requests that lose the lock
+// are dropped and entries can be duplicated.  Here one frame's requests are
+// collected first and then inserted as if one at a time, without contention,
+// in canonical order -- ascending (bucket, x, y, z) -- so the resulting hash
+// state (slot, voxel block and chain link of every entry) depends only on the
+// inputs.  The kernels:
+//   requests : per pixel, the reference's probe walk along the truncation band
+//              (Fusion::CreateBlocks, FuseMap.cu:80-111); blocks that are not in
+//              the map go into a per-frame open-addressing request set (CAS on
+//              64-bit keys); the first insert of a key appends it to the list
+//              of new blocks.
+//   count / scan / place / rank : a counting sort of the new blocks by bucket
+//              (per-bucket counters, a two-level scan over all buckets), then
+//              the rank of each block inside its bucket by coordinates.
+//   insert   : each new block computes from its rank alone where the
+//              sequential insertion would put it: free-stack position, head
+//              slot or excess slot, and its chain link; the one block per
+//              bucket that extends an existing chain links the old tail.  If
+//              the pool or the excess list would run out, or an earlier
+//              exhaustion left empty entries inside chains, a single thread
+//              performs the same insertions one by one with the reference's
+//              exact CreateBlock rules instead.
+// Visibility walks the list of allocated entries rather than every slot of
+// the table (CheckVisibleBlockKernel, FuseMap.cu:113-138, scans all of them).
+// Integration processes one visible block per CTA iteration: 256 threads, two
+// voxels each, one 16-byte load and at most one 16-byte store per thread.
+#include "fb_internal.h"
+
+namespace fb {
+
+// FindEntry (DeviceMap.cu:122-135): slot of the live entry for a block, or -1.
+__device__ __forceinline__ int find_slot(const MapView& m, int x, int y, int z) {
+    int b = (int)bucket_of(x, y, z, (uint32_t)m.NB);
+    HEntry e = m.entries[b];
+    if (e.ptr != -1 && e.x == x && e.y == y && e.z == z) return b;
+    for (int guard = 0; e.offset > 0 && e.offset <= m.NE && guard <= m.NE; ++guard) {
+        int s = m.NB + e.offset - 1;
+        e = m.entries[s];
+        if (e.x == x && e.y == y && e.z == z && e.ptr != -1) return s;
+    }
+    return -1;
+}
+
+__device__ __forceinline__ unsigned long long block_key(int x, int y, int z) {
+    return (1ull << 63) | ((unsigned long long)(x & 0xFFFF) << 32) | ((unsigned long long)(y & 0xFFFF) << 16) |
+           (unsigned long long)(z & 0xFFFF);
+}
+
+__device__ __forceinline__ uint32_t mix64(unsigned long long k) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return (uint32_t)k;
+}
+
+__device__ __forceinline__ void request_block(const MapView& m, int x, int y, int z) {
+    if (x < -kCoordLimit || x > kCoordLimit || y < -kCoordLimit || y > kCoordLimit || z < -kCoordLimit ||
+        z > kCoordLimit) {
+        atomicOr(&m.ctr->err, kErrCoordRange);
+        return;
+    }
+    if (find_slot(m, x, y, z) >= 0) return;
+    const unsigned long long key = block_key(x, y, z);
+    uint32_t h = mix64(key) & (uint32_t)(m.reqcap - 1);
+    for (int probe = 0; probe < 64; ++probe) {
+        unsigned long long old = atomicCAS(&m.reqset[h], 0ull, key);
+        if (old == 0ull) {
+            int idx = atomicAdd(&m.ctr->n_req, 1);
+            if (idx < m.newcap) {
+                NewBlock nb;
+                nb.x = (short)x;
+                nb.y = (short)y;
+                nb.z = (short)z;
+                nb.pad = 0;
+                nb.bucket = bucket_of(x, y, z, (uint32_t)m.NB);
+                nb.setslot = (int)h;
+                nb.j = 0;
+                nb.rank = 0;
+                nb.pad2 = 0;
+                m.newblk[idx] = nb;
+            } else {
+                atomicOr(&m.ctr->err, kErrNewListFull);
+                atomicExch(&m.reqset[h], 0ull);
+            }
+            return;
+        }
+        if (old == key) return;
+        h = (h + 1) & (uint32_t)(m.reqcap - 1);
+    }
+    atomicOr(&m.ctr->err, kErrRequestSetFull);
+}
+
+// Fusion::CreateBlocks (FuseMap.cu:80-111) for one pixel of the raw depth map.
+__global__ void __launch_bounds__(256) k_alloc_requests(MapView m, const float* __restrict__ raw, int rp, int W,
+                                                        int H, Intr k, const DevPose* __restrict__ posep,
+                                                        const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const float z = raw[(size_t)y * rp + x];
+    const float dmin = m.g.depth_min, dmax = m.g.depth_max;
+    if (isnan(z) || z < dmin || z > dmax) return;
+    const DevPose P = *posep;
+    const float thresh = m.g.trunc_dist / 2;
+    const float zn = fminf(dmax, fs(z, thresh));
+    const float zf = fminf(dmax, fa(z, thresh));
+    if (zn >= zf) return;
+    const float vinv = m.g.voxel_size_inv;
+    const float ux = fs((float)x, k.cx), uy = fs((float)y, k.cy);
+    f3 pn = mul3(add3(mv(P.R, mk3(fm(fm(zn, ux), k.invfx), fm(fm(zn, uy), k.invfy), zn)), P.t), vinv);
+    f3 pf = mul3(add3(mv(P.R, mk3(fm(fm(zf, ux), k.invfx), fm(fm(zf, uy), k.invfy), zf)), P.t), vinv);
+    f3 dir = sub3(pf, pn);
+    const float len = norm3(dir);
+    const int nSteps = (int)ceil(2.0 * (double)len);
+    dir = div3(dir, (float)(nSteps - 1));
+    int px = 0, py = 0, pz = 0;
+    bool have = false;
+    for (int i = 0; i < nSteps; ++i) {
+        // make_int3(float3) truncates toward zero (VectorMath.h:36-38)
+        int bx = block_of(__float2int_rz(pn.x)), by = block_of(__float2int_rz(pn.y)),
+            bz = block_of(__float2int_rz(pn.z));
+        if (!have || bx != px || by != py || bz != pz) {
+            request_block(m, bx, by, bz);
+            px = bx;
+            py = by;
+            pz = bz;
+            have = true;
+        }
+        pn = add3(pn, dir);
+    }
+}
+
+__global__ void k_alloc_count(MapView m) {
+    const int M = min(m.ctr->n_req, m.newcap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x)
+        m.newblk[i].j = atomicAdd(&m.bucket_cnt[m.newblk[i].bucket], 1);
+}
+
+// Per chunk of kScanChunk buckets: number of new blocks, and of those that go
+// to the excess list (all but the first when the bucket's head slot is empty).
+__global__ void __launch_bounds__(256) k_scan_chunks(MapView m) {
+    if (m.ctr->n_req == 0) return;
+    __shared__ int s_c[256], s_x[256];
+    const int base = blockIdx.x * kScanChunk;
+    int c = 0, xs = 0;
+    for (int q = threadIdx.x; q < kScanChunk; q += 256) {
+        int b = base + q;
+        if (b >= m.NB) break;
+        int n = m.bucket_cnt[b];
+        if (n) {
+            int he = m.entries[b].ptr == -1 ? 1 : 0;
+            c += n;
+            xs += n - he;
+        }
+    }
+    s_c[threadIdx.x] = c;
+    s_x[threadIdx.x] = xs;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            s_c[threadIdx.x] += s_c[threadIdx.x + o];
+            s_x[threadIdx.x] += s_x[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        m.chunk_sums[2 * blockIdx.x] = s_c[0];
+        m.chunk_sums[2 * blockIdx.x + 1] = s_x[0];
+    }
+}
+
+// Exclusive scan over the chunk sums; snapshot of the counters and choice of
+// the parallel or sequential insertion path.
+__global__ void k_scan_top(MapView m) {
+    MapCounters* c = m.ctr;
+    const int M = min(c->n_req, m.newcap);
+    __shared__ int total_x;
+    if (threadIdx.x == 0) {
+        int a = 0, e = 0;
+        if (M > 0)
+            for (int i = 0; i < m.nchunks; ++i) {
+                int ca = m.chunk_sums[2 * i], cx = m.chunk_sums[2 * i + 1];
+                m.chunk_sums[2 * i] = a;
+                m.chunk_sums[2 * i + 1] = e;
+                a += ca;
+                e += cx;
+            }
+        total_x = e;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        c->excess_total = total_x;
+        c->snap_M = M;
+        c->snap_hc = c->heap_counter;
+        c->snap_ep = c->entry_ptr;
+        c->snap_na = c->n_alloc;
+        // the parallel path reproduces sequential insertion only while the
+        // free stack and the excess list suffice and no chain holds an empty
+        // entry left by an earlier exhaustion
+        c->fast = (M <= c->heap_counter + 1) && (c->entry_ptr - 1 + total_x <= m.NE) && !c->holes;
+    }
+}
+
+// Per chunk: exclusive scan of the per-bucket counts into segment starts and
+// excess starts.
+__global__ void __launch_bounds__(256) k_scan_apply(MapView m) {
+    if (m.ctr->snap_M == 0) return;
+    __shared__ int s_c[256], s_x[256];
+    constexpr int per = kScanChunk / 256;
+    const int base = blockIdx.x * kScanChunk + threadIdx.x * per;
+    int cnt[per], he[per];
+    int c = 0, xs = 0;
+#pragma unroll
+    for (int q = 0; q < per; ++q) {
+        int b = base + q;
+        cnt[q] = 0;
+        he[q] = 0;
+        if (b < m.NB) {
+            cnt[q] = m.bucket_cnt[b];
+            if (cnt[q]) he[q] = m.entries[b].ptr == -1 ? 1 : 0;
+        }
+        c += cnt[q];
+        xs += cnt[q] - he[q];
+    }
+    s_c[threadIdx.x] = c;
+    s_x[threadIdx.x] = xs;
+    __syncthreads();
+    // Hillis-Steele inclusive scan over 256 thread totals
+    for (int o = 1; o < 256; o <<= 1) {
+        int ac = threadIdx.x >= o ? s_c[threadIdx.x - o] : 0;
+        int ax = threadIdx.x >= o ? s_x[threadIdx.x - o] : 0;
+        __syncthreads();
+        s_c[threadIdx.x] += ac;
+        s_x[threadIdx.x] += ax;
+        __syncthreads();
+    }
+    int run_c = m.chunk_sums[2 * blockIdx.x] + s_c[threadIdx.x] - c;
+    int run_x = m.chunk_sums[2 * blockIdx.x + 1] + s_x[threadIdx.x] - xs;
+#pragma unroll
+    for (int q = 0; q < per; ++q) {
+        int b = base + q;
+        if (cnt[q]) {
+            m.bucket_start[b] = run_c;
+            m.bucket_x[b] = (run_x << 1) | he[q];
+        }
+        run_c += cnt[q];
+        run_x += cnt[q] - he[q];
+    }
+}
+
+__global__ void k_alloc_place(MapView m) {
+    const int M = m.ctr->snap_M;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
+        const NewBlock& nb = m.newblk[i];
+        m.arrival[m.bucket_start[nb.bucket] + nb.j] = i;
+    }
+}
+
+__device__ __forceinline__ bool coord_less(const NewBlock& a, const NewBlock& b) {
+    if (a.x != b.x) return a.x < b.x;
+    if (a.y != b.y) return a.y < b.y;
+    return a.z < b.z;
+}
+
+__global__ void k_alloc_rank(MapView m) {
+    const int M = m.ctr->snap_M;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < M; p += gridDim.x * blockDim.x) {
+        const int i = m.arrival[p];
+        const NewBlock me = m.newblk[i];
+        const int s = m.bucket_start[me.bucket], n = m.bucket_cnt[me.bucket];
+        int r = 0;
+        for (int q = s; q < s + n; ++q)
+            if (coord_less(m.newblk[m.arrival[q]], me)) ++r;
+        m.newblk[i].rank = s + r;
+        m.order[s + r] = i;
+    }
+}
+
+// CreateBlock (DeviceMap.cu:23-62) without lock contention, one block at a
+// time, for the sequential path.  Returns the slot written or -1.
+__device__ int create_block_seq(const MapView& m, int x, int y, int z, int& hc, int& ep, int& holes) {
+    const int b = (int)bucket_of(x, y, z, (uint32_t)m.NB);
+    HEntry* e = &m.entries[b];
+    HEntry* eEmpty = nullptr;
+    if (e->x == x && e->y == y && e->z == z && e->ptr != -1) return -1;
+    if (e->ptr == -1) eEmpty = e;
+    for (int guard = 0; e->offset > 0 && e->offset <= m.NE && guard <= m.NE; ++guard) {
+        e = &m.entries[m.NB + e->offset - 1];
+        if (e->x == x && e->y == y && e->z == z && e->ptr != -1) return -1;
+        if (e->ptr == -1 && !eEmpty) eEmpty = e;
+    }
+    // CreateEntry (DeviceMap.cu:12-21)
+    auto create_entry = [&](int offset) {
+        HEntry n;
+        n.x = (short)x;
+        n.y = (short)y;
+        n.z = (short)z;
+        n.pad = 0;
+        int old = hc--;
+        int ptr = old >= 0 ? m.heap[old] : -1;
+        if (ptr != -1) {
+            n.ptr = ptr;
+            n.offset = offset;
+        } else {
+            n.ptr = -1;
+            n.offset = 0;
+        }
+        return n;
+    };
+    if (eEmpty) {
+        *eEmpty = create_entry(e->offset);
+        if (eEmpty->ptr == -1) holes = 1;
+        return (int)(eEmpty - m.entries);
+    }
+    int offset = ep++;
+    if (offset <= m.NE) {
+        HEntry* n = &m.entries[m.NB + offset - 1];
+        *n = create_entry(0);
+        e->offset = offset;
+        if (n->ptr == -1) holes = 1;
+        return (int)(n - m.entries);
+    }
+    return -1;
+}
+
+__global__ void __launch_bounds__(256) k_alloc_insert(MapView m) {
+    MapCounters* c = m.ctr;
+    const int M = c->snap_M;
+    if (M == 0) return;
+    const int hc0 = c->snap_hc, ep0 = c->snap_ep, na0 = c->snap_na;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    if (!c->fast) {
+        if (gtid == 0) {
+            int hc = hc0, ep = ep0, holes = c->holes, na = na0;
+            for (int R = 0; R < M; ++R) {
+                const NewBlock nb = m.newblk[m.order[R]];
+                int slot = create_block_seq(m, nb.x, nb.y, nb.z, hc, ep, holes);
+                if (slot >= 0 && m.entries[slot].ptr != -1) m.alloc_list[na++] = slot;
+            }
+            unsigned err = kErrSequentialInsert;
+            if (hc < -1) err |= kErrHeapExhausted;
+            if (ep - 1 > m.NE) err |= kErrExcessFull;
+            atomicOr(&c->err, err);
+            c->heap_counter = hc;
+            c->entry_ptr = ep;
+            c->holes = holes;
+            c->n_alloc = na;
+            c->seq_path = 1;
+        }
+        for (int R = gtid; R < M; R += gstride) m.reqset[m.newblk[m.order[R]].setslot] = 0ull;
+        return;
+    }
+    for (int R = gtid; R < M; R += gstride) {
+        const int i = m.order[R];
+        const NewBlock nb = m.newblk[i];
+        const int b = (int)nb.bucket;
+        const int s = m.bucket_start[b], n = m.bucket_cnt[b], bx = m.bucket_x[b];
+        const int he = bx & 1, xs = bx >> 1;
+        const int r = R - s;
+        HEntry e;
+        e.x = nb.x;
+        e.y = nb.y;
+        e.z = nb.z;
+        e.pad = 0;
+        e.ptr = m.heap[hc0 - R];
+        int slot;
+        if (he && r == 0) {
+            slot = b;
+            e.offset = n > 1 ? ep0 + xs : 0;
+        } else {
+            const int q = r - he;                 // rank among this bucket's excess blocks
+            const int off = ep0 + xs + q;
+            slot = m.NB + off - 1;
+            e.offset = r + 1 < n ? off + 1 : 0;
+            if (q == 0 && !he) {
+                // link the tail of the existing chain (CreateBlock's e->offset = offset)
+                int t = b;
+                for (int guard = 0; m.entries[t].offset > 0 && m.entries[t].offset <= m.NE && guard <= m.NE;
+                     ++guard)
+                    t = m.NB + m.entries[t].offset - 1;
+                m.entries[t].offset = off;
+            }
+        }
+        m.entries[slot] = e;
+        m.alloc_list[na0 + R] = slot;
+        m.reqset[nb.setslot] = 0ull;
+    }
+}
+
+__global__ void k_alloc_finalize(MapView m) {
+    MapCounters* c = m.ctr;
+    const int M = c->snap_M;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x)
+        m.bucket_cnt[m.newblk[i].bucket] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (M > 0 && c->fast) {
+            c->heap_counter = c->snap_hc - M;
+            c->entry_ptr = c->snap_ep + c->excess_total;
+            c->n_alloc = c->snap_na + M;
+            c->seq_path = 0;
+        }
+        c->n_new = M;
+        c->n_req = 0;
+        c->n_visible = 0;
+        c->n_tiles = 0;
+    }
+}
+
+// ---------------------------------------------------------------- visibility
+
+// Fusion::CheckVertexVisibility / CheckBlockVisibility (FuseMap.cu:36-78);
+// the eight corners are reached by the reference's sequence of float adds.
+__device__ __forceinline__ bool vertex_visible(f3 p, const DevPose& P, const Intr& k, int W, int H,
+                                               const MapGeom& g) {
+    p = mv(P.Rinv, sub3(p, P.t));
+    if (p.z < 1e-3f) return false;
+    float u = fa(fd(fm(k.fx, p.x), p.z), k.cx), v = fa(fd(fm(k.fy, p.y), p.z), k.cy);
+    return u >= 0 && v >= 0 && u < (float)W && v < (float)H && p.z >= g.depth_min && p.z <= g.depth_max;
+}
+
+__device__ bool block_visible(int bx, int by, int bz, const DevPose& P, const Intr& k, int W, int H,
+                              const MapGeom& g) {
+    const float s = g.block_width;
+    f3 c = mk3(fm((float)bx, s), fm((float)by, s), fm((float)bz, s));
+    if (vertex_visible(c, P, k, W, H, g)) return true;
+    c.z = fa(c.z, s);
+    if (vertex_visible(c, P, k, W, H, g)) return true;
+    c.y = fa(c.y, s);
+    if (vertex_visible(c, P, k, W, H, g)) return true;
+    c.x = fa(c.x, s);
+    if (vertex_visible(c, P, k, W, H, g)) return true;
+    c.z = fs(c.z, s);
+    if (vertex_visible(c, P, k, W, H, g)) return true;
+    c.y = fs(c.y, s);
+    if (vertex_visible(c, P, k, W, H, g)) return true;
+    c.x = fs(c.x, s);
+    c.y = fa(c.y, s);
+    if (vertex_visible(c, P, k, W, H, g)) return true;
+    c.x = fa(c.x, s);
+    c.y = fs(c.y, s);
+    c.z = fa(c.z, s);
+    if (vertex_visible(c, P, k, W, H, g)) return true;
+    return false;
+}
+
+__global__ void k_reset_visible(MapCounters* c) {
+    c->n_visible = 0;
+    c->n_tiles = 0;
+}
+
+__global__ void __launch_bounds__(256) k_visibility(MapView m, int W, int H, Intr k, const DevPose* __restrict__ posep,
+                                                    const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const DevPose P = *posep;
+    const int n = m.ctr->n_alloc;
+    const int lane = threadIdx.x & 31;
+    const int nIter = (n + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x);
+    for (int it = 0; it < nIter; ++it) {
+        const int i = (it * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
+        bool vis = false;
+        int slot = -1;
+        if (i < n) {
+            slot = m.alloc_list[i];
+            HEntry e = m.entries[slot];
+            vis = block_visible(e.x, e.y, e.z, P, k, W, H, m.g);
+        }
+        // warp-aggregated append
+        unsigned mask = __ballot_sync(0xffffffffu, vis);
+        if (mask) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&m.ctr->n_visible, __popc(mask));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (vis) {
+                int o = base + __popc(mask & ((1u << lane) - 1));
+                if (o < m.NS) m.visible[o] = slot;
+                else atomicOr(&m.ctr->err, kErrVisibleFull);
+            }
+        }
+    }
+}
+
+// --------------------------------------------------------------- integration
+
+// Fusion::integrateColor (FuseMap.cu:140-191) for one voxel.  Returns true
+// when the voxel changed.
+__device__ __forceinline__ bool integrate_voxel(Voxel& vox, int vx, int vy, int vz, const float* __restrict__ raw,
+                                                int rp, const uint8_t* __restrict__ rgb, int cp,
+                                                const float4* __restrict__ nmap, int np, int W, int H,
+                                                const Intr& k, const DevPose& P, const MapGeom& g) {
+    f3 pos = mk3(fm((float)vx, g.voxel_size), fm((float)vy, g.voxel_size), fm((float)vz, g.voxel_size));
+    pos = mv(P.Rinv, sub3(pos, P.t));
+    const float pu = fa(fd(fm(k.fx, pos.x), pos.z), k.cx), pv = fa(fd(fm(k.fy, pos.y), pos.z), k.cy);
+    const int u = __float2int_rz(pu), v = __float2int_rz(pv);  // make_int2(float2)
+    if (u < 0 || v < 0 || u >= W || v >= H) return false;
+    const float dp = raw[(size_t)v * rp + u];
+    if (isnan(dp) || dp > g.depth_max || dp < g.depth_min) return false;
+    const float thresh = g.trunc_dist;
+    float sdf = fs(dp, pos.z);
+    if (!(sdf >= -thresh)) return false;
+    sdf = fminf(1.0f, fd(sdf, thresh));
+    const float4 nl = nmap[(size_t)v * np + u];
+    if (isnan(nl.x)) return false;
+    // w = nl * normalised(float4(pos, 1)): the dot runs over all four lanes
+    const float nrm = fsq(fa(fa(fa(fm(pos.x, pos.x), fm(pos.y, pos.y)), fm(pos.z, pos.z)), 1.0f));
+    const float w = fa(fa(fa(fm(nl.x, fd(pos.x, nrm)), fm(nl.y, fd(pos.y, nrm))), fm(nl.z, fd(pos.z, nrm))),
+                       fm(nl.w, fd(1.0f, nrm)));
+    const uint8_t* px = rgb + (size_t)v * cp + 3 * u;
+    if (vox.weight == 0) {
+        vox.sdf = sdf;
+        vox.weight = 1;
+        vox.r = px[0];
+        vox.g = px[1];
+        vox.b = px[2];
+        return true;
+    }
+    const float a = fm(w, 0.2f), oa = fs(1.0f, a);
+    const float W0 = (float)vox.weight;
+    float rr = fm(fa(fm(a, fd((float)px[0], 255.f)), fm(oa, fd((float)vox.r, 255.f))), 255.f);
+    float gg = fm(fa(fm(a, fd((float)px[1], 255.f)), fm(oa, fd((float)vox.g, 255.f))), 255.f);
+    float bb = fm(fa(fm(a, fd((float)px[2], 255.f)), fm(oa, fd((float)vox.b, 255.f))), 255.f);
+    vox.sdf = fd(fa(fm(vox.sdf, W0), fm(w, sdf)), fa(W0, w));
+    vox.weight = (unsigned char)min(255, (int)vox.weight + 1);
+    // make_uchar3(float3): truncate to int, then to the low byte
+    vox.r = (unsigned char)__float2int_rz(rr);
+    vox.g = (unsigned char)__float2int_rz(gg);
+    vox.b = (unsigned char)__float2int_rz(bb);
+    return true;
+}
+
+__global__ void __launch_bounds__(256) k_integrate(MapView m, const float* __restrict__ raw, int rp,
+                                                   const uint8_t* __restrict__ rgb, int cp,
+                                                   const float4* __restrict__ nmap, int np, int W, int H, Intr k,
+                                                   const DevPose* __restrict__ posep, const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const DevPose P = *posep;
+    const int n = min(m.ctr->n_visible, m.NS);
+    const int t = threadIdx.x;
+    const int lx = (2 * t) & 7, ly = (t >> 2) & 7, lz = t >> 5;
+    for (int b = blockIdx.x; b < n; b += gridDim.x) {
+        const HEntry e = m.entries[m.visible[b]];
+        const int vx = e.x * 8 + lx, vy = e.y * 8 + ly, vz = e.z * 8 + lz;
+        uint4* base = (uint4*)(m.voxels + (size_t)e.ptr * 512) + t;
+        uint4 raw2 = *base;
+        Voxel v0 = *(Voxel*)&raw2.x, v1 = *(Voxel*)&raw2.z;
+        bool c0 = integrate_voxel(v0, vx, vy, vz, raw, rp, rgb, cp, nmap, np, W, H, k, P, m.g);
+        bool c1 = integrate_voxel(v1, vx + 1, vy, vz, raw, rp, rgb, cp, nmap, np, W, H, k, P, m.g);
+        if (c0 || c1) {
+            uint4 o;
+            *(Voxel*)&o.x = v0;
+            *(Voxel*)&o.z = v1;
+            *base = o;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------- reset
+
+// ResetHashKernel / ResetSdfBlockKernel (FuseMap.cu:321-350) on all of the
+// table (the reference leaves pos and offset of released entries in place).
+__global__ void k_map_reset(MapView m) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t ne = (size_t)m.NB + m.NE;
+    for (size_t i = tid; i < ne; i += stride) {
+        HEntry e;
+        e.x = e.y = e.z = e.pad = 0;
+        e.ptr = -1;
+        e.offset = 0;
+        m.entries[i] = e;
+    }
+    for (size_t i = tid; i < (size_t)m.NS; i += stride) m.heap[i] = m.NS - (int)i - 1;
+    const uint4 released = make_uint4(0x7fffffffu, 0u, 0x7fffffffu, 0u);  // {NaN, w 0, rgb 0} x 2
+    uint4* vv = (uint4*)m.voxels;
+    for (size_t i = tid; i < (size_t)m.NS * 256; i += stride) vv[i] = released;
+    for (size_t i = tid; i < (size_t)m.NB; i += stride) m.bucket_cnt[i] = 0;
+    for (size_t i = tid; i < (size_t)m.reqcap; i += stride) m.reqset[i] = 0ull;
+    if (tid == 0) {
+        MapCounters* c = m.ctr;
+        c->heap_counter = m.NS - 1;
+        c->entry_ptr = 1;
+        c->holes = 0;
+        c->n_alloc = 0;
+        c->n_req = 0;
+        c->n_new = 0;
+        c->n_visible = 0;
+        c->n_tiles = 0;
+        c->excess_total = 0;
+        c->err = 0;
+        c->seq_path = 0;
+        c->snap_M = 0;
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+
+static int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+int launch_map_reset(const MapView& m, cudaStream_t s) { k_map_reset<<<sm_count() * 8, 256, 0, s>>>(m);
+    return 1;
+}
+
+int launch_allocate(const MapView& m, const float* raw, int rp, int W, int H, const Intr& k, const DevPose* pose,
+                     const int* skip, cudaStream_t s) {
+    dim3 b(32, 8), g((W + 31) / 32, (H + 7) / 8);
+    k_alloc_requests<<<g, b, 0, s>>>(m, raw, rp, W, H, k, pose, skip);
+    const int gs = sm_count() * 4;
+    k_alloc_count<<<gs, 256, 0, s>>>(m);
+    k_scan_chunks<<<m.nchunks, 256, 0, s>>>(m);
+    k_scan_top<<<1, 32, 0, s>>>(m);
+    k_scan_apply<<<m.nchunks, 256, 0, s>>>(m);
+    k_alloc_place<<<gs, 256, 0, s>>>(m);
+    k_alloc_rank<<<gs, 256, 0, s>>>(m);
+    k_alloc_insert<<<gs, 256, 0, s>>>(m);
+    k_alloc_finalize<<<gs, 256, 0, s>>>(m);
+    return 9;
+}
+
+int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
+                       cudaStream_t s) {
+    k_reset_visible<<<1, 1, 0, s>>>(m.ctr);
+    k_visibility<<<sm_count() * 4, 256, 0, s>>>(m, W, H, k, pose, skip);
+    return 2;
+}
+
+int launch_integrate(const MapView& m, const float* raw, int rp, const uint8_t* rgb, int cp, const float4* nmap,
+                      int np, int W, int H, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s) {
+    k_integrate<<<sm_count() * 8, 256, 0, s>>>(m, raw, rp, rgb, cp, nmap, np, W, H, k, pose, skip);
+    return 1;
+}
+
+}  // namespace fb

@@ -1,0 +1,247 @@
+// Model raycasting (the reference's Mapping/RenderScene.cu): per-pixel depth
+// intervals from the visible blocks, then sphere tracing of the TSDF through
+// the voxel-block hash with trilinear refinement and a central-difference
+// normal.
+//
+// z ranges: each visible block is projected once (8 corners) and its
+// rectangle at 1/8 resolution is min/max-ed into the z-range images with
+// integer atomics on the float bits (all values are positive, so integer order
+// is float order).  In the reference each block's rectangle is first split
+// into 16x16 tiles appended to a list (Projection::createRenderingBlockList,
+// RenderScene.cu:106-124) and filled by a second kernel; because every tile's
+// lower-right corner is taken from the block's upper-left corner
+// (RenderScene.cu:115-116), only the first tile of a block ever covers
+// pixels: [ul, min(ul + 15, lr)].  That is the rectangle filled here.
+#include "fb_internal.h"
+
+namespace fb {
+
+__global__ void k_zrange_init(MapView m, const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const int n = m.zc * m.zr;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        m.zmin[i] = 100.f;   // CreateRenderingBlocks uploads 100 (RenderScene.cu:245-251)
+        m.zmax[i] = 0.f;     // and clears zRangeY (RenderScene.cu:244)
+    }
+}
+
+// Projection::projectBlock (RenderScene.cu:54-104) + the first tile's fill
+// (fillBlocks, RenderScene.cu:156-179).
+__global__ void __launch_bounds__(256) k_zrange(MapView m, Intr k, const DevPose* __restrict__ posep,
+                                                const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const DevPose P = *posep;
+    const int n = min(m.ctr->n_visible, m.NS);
+    const int zc = m.zc, zr = m.zr;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const HEntry e = m.entries[m.visible[i]];
+        int ulx = zc, uly = zr, lrx = -1, lry = -1;
+        float zx = m.g.depth_max, zy = m.g.depth_min;
+        for (int c = 0; c < 8; ++c) {
+            const int tx = e.x + ((c & 1) ? 1 : 0), ty = e.y + ((c & 2) ? 1 : 0), tz = e.z + ((c & 4) ? 1 : 0);
+            f3 p = mk3(fm((float)(tx * 8), m.g.voxel_size), fm((float)(ty * 8), m.g.voxel_size),
+                       fm((float)(tz * 8), m.g.voxel_size));
+            p = mv(P.Rinv, sub3(p, P.t));
+            if ((double)p.z < 2e-1) continue;
+            const float qx = fd(fa(fd(fm(k.fx, p.x), p.z), k.cx), 8.0f);
+            const float qy = fd(fa(fd(fm(k.fy, p.y), p.z), k.cy), 8.0f);
+            // upperLeft / lowerRight are short2 (DeviceMap.h:11-18)
+            if ((float)ulx > floorf(qx)) ulx = (short)(int)floorf(qx);
+            if ((float)lrx < ceilf(qx)) lrx = (short)(int)ceilf(qx);
+            if ((float)uly > floorf(qy)) uly = (short)(int)floorf(qy);
+            if ((float)lry < ceilf(qy)) lry = (short)(int)ceilf(qy);
+            if (zx > p.z) zx = p.z;
+            if (zy < p.z) zy = p.z;
+        }
+        if (ulx < 0) ulx = 0;
+        if (uly < 0) uly = 0;
+        if (lrx >= zc) lrx = zc - 1;
+        if (lry >= zr) lry = zr - 1;
+        if (ulx > lrx || uly > lry) continue;
+        if (zx < m.g.depth_min) zx = m.g.depth_min;
+        if (zy < m.g.depth_min) continue;
+        atomicAdd(&m.ctr->n_tiles, 1);
+        const int ex = min(ulx + 15, lrx), ey = min(uly + 15, lry);
+        const int bzx = __float_as_int(zx), bzy = __float_as_int(zy);
+        for (int y = uly; y <= ey; ++y)
+            for (int x = ulx; x <= ex; ++x) {
+                atomicMin((int*)&m.zmin[y * zc + x], bzx);
+                atomicMax((int*)&m.zmax[y * zc + x], bzy);
+            }
+    }
+}
+
+// ----------------------------------------------------------------- raycast
+
+struct EntryCache {
+    int x, y, z, ptr;
+    bool set;
+};
+
+// FindVoxel(float3, cache, valid) (DeviceMap.cu:97-114).  The reference's
+// cache starts as HashEntry() -- position (0,0,0), ptr -1 -- and a first probe
+// inside block (0,0,0) then reads voxel index -1 + local index; here the cache
+// starts empty.  Returns nullptr for a missing block.
+__device__ __forceinline__ const Voxel* find_voxel(const MapView& m, f3 p, EntryCache& c, bool& valid) {
+    const int vx = __float2int_rz(p.x), vy = __float2int_rz(p.y), vz = __float2int_rz(p.z);
+    const int bx = block_of(vx), by = block_of(vy), bz = block_of(vz);
+    const int idx = local_of(vz) * 64 + local_of(vy) * 8 + local_of(vx);
+    if (c.set && bx == c.x && by == c.y && bz == c.z) {
+        valid = true;
+        return m.voxels + (size_t)c.ptr * 512 + idx;
+    }
+    int b = (int)bucket_of(bx, by, bz, (uint32_t)m.NB);
+    HEntry e = m.entries[b];
+    bool found = e.ptr != -1 && e.x == bx && e.y == by && e.z == bz;
+    for (int guard = 0; !found && e.offset > 0 && e.offset <= m.NE && guard <= m.NE; ++guard) {
+        e = m.entries[m.NB + e.offset - 1];
+        found = e.x == bx && e.y == by && e.z == bz && e.ptr != -1;
+    }
+    if (!found) {
+        valid = false;
+        return nullptr;
+    }
+    valid = true;
+    c.x = bx;
+    c.y = by;
+    c.z = bz;
+    c.ptr = e.ptr;
+    c.set = true;
+    return m.voxels + (size_t)e.ptr * 512 + idx;
+}
+
+__device__ __forceinline__ float vsdf(const Voxel* v) { return v ? v->sdf : qnan(); }
+
+// Rendering::readSdf (RenderScene.cu:290-295)
+__device__ __forceinline__ float read_sdf(const MapView& m, f3 p, EntryCache& c, bool& valid) {
+    const Voxel* v = find_voxel(m, p, c, valid);
+    if (!v) return qnan();
+    Voxel vv = *v;
+    if (vv.weight == 0) valid = false;
+    return vv.sdf;
+}
+
+// Rendering::readSdfInterped (RenderScene.cu:297-319)
+__device__ float read_sdf_interp(const MapView& m, f3 pt, EntryCache& c, bool& valid) {
+    const f3 f = mk3(fs(pt.x, floorf(pt.x)), fs(pt.y, floorf(pt.y)), fs(pt.z, floorf(pt.z)));
+    auto lerp = [](float a, float b, float t) { return fa(fm(fs(1.0f, t), a), fm(t, b)); };
+    float s0 = vsdf(find_voxel(m, pt, c, valid));
+    float s1 = vsdf(find_voxel(m, mk3(fa(pt.x, 1.f), pt.y, pt.z), c, valid));
+    float r0 = lerp(s0, s1, f.x);
+    s0 = vsdf(find_voxel(m, mk3(pt.x, fa(pt.y, 1.f), pt.z), c, valid));
+    s1 = vsdf(find_voxel(m, mk3(fa(pt.x, 1.f), fa(pt.y, 1.f), pt.z), c, valid));
+    float r1 = lerp(s0, s1, f.x);
+    float r2 = lerp(r0, r1, f.y);
+    s0 = vsdf(find_voxel(m, mk3(pt.x, pt.y, fa(pt.z, 1.f)), c, valid));
+    s1 = vsdf(find_voxel(m, mk3(fa(pt.x, 1.f), pt.y, fa(pt.z, 1.f)), c, valid));
+    r0 = lerp(s0, s1, f.x);
+    s0 = vsdf(find_voxel(m, mk3(pt.x, fa(pt.y, 1.f), fa(pt.z, 1.f)), c, valid));
+    s1 = vsdf(find_voxel(m, mk3(fa(pt.x, 1.f), fa(pt.y, 1.f), fa(pt.z, 1.f)), c, valid));
+    r1 = lerp(s0, s1, f.x);
+    float r3 = lerp(r0, r1, f.y);
+    return lerp(r2, r3, f.z);
+}
+
+// Rendering::readNormal (RenderScene.cu:321-352)
+__device__ bool read_normal(const MapView& m, f3 pt, EntryCache& c, const M3& Rinv, f3& n) {
+    bool valid;
+    float s[6];
+    const float off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    for (int q = 0; q < 6; ++q) {
+        s[q] = read_sdf_interp(m, mk3(fa(pt.x, off[q][0]), fa(pt.y, off[q][1]), fa(pt.z, off[q][2])), c, valid);
+        if (isnan(s[q]) || s[q] == 1.0f || !valid) return false;
+    }
+    n = normalised3(mv(Rinv, mk3(fs(s[0], s[1]), fs(s[2], s[3]), fs(s[4], s[5]))));
+    return true;
+}
+
+// Rendering::operator() (RenderScene.cu:354-440)
+__global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__ vmap, float4* __restrict__ nmap,
+                                                 int vp, int W, int H, Intr k, const DevPose* __restrict__ posep,
+                                                 const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    if (m.ctr->n_tiles == 0) return;   // CreateRenderingBlocks returned false: maps untouched
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const DevPose P = *posep;
+    const size_t o = (size_t)y * vp + x;
+    const float4 nan4 = make_float4(qnan(), qnan(), qnan(), qnan());
+    float4 vout = nan4, nout = nan4;
+    const int lx = (int)floorf(fd((float)x, 8.f)), ly = (int)floorf(fd((float)y, 8.f));
+    const float zrx = m.zmin[ly * m.zc + lx], zry = m.zmax[ly * m.zc + lx];
+    if (!((double)zry < 1e-3 || (double)zrx < 1e-3 || isnan(zrx) || isnan(zry))) {
+        const float vinv = m.g.voxel_size_inv, stepScale = m.g.step_scale;
+        f3 p;
+        p.z = zrx;
+        p.x = fm(fm(p.z, fs((float)x, k.cx)), k.invfx);
+        p.y = fm(fm(p.z, fs((float)y, k.cy)), k.invfy);
+        float dist_s = fm(norm3(p), vinv);
+        const f3 block_s = mul3(add3(mv(P.R, p), P.t), vinv);
+        p.z = zry;
+        p.x = fm(fm(p.z, fs((float)x, k.cx)), k.invfx);
+        p.y = fm(fm(p.z, fs((float)y, k.cy)), k.invfy);
+        const float dist_e = fm(norm3(p), vinv);
+        const f3 block_e = mul3(add3(mv(P.R, p), P.t), vinv);
+        const f3 dir = normalised3(sub3(block_e, block_s));
+        f3 result = block_s;
+        float sdf = 1.0f, step;
+        bool valid = false, found = false;
+        EntryCache c;
+        c.set = false;
+        while (dist_s < dist_e) {
+            sdf = read_sdf(m, result, c, valid);
+            if (!valid) {
+                step = 8.0f;
+            } else {
+                if (sdf <= 0.1f && sdf >= -0.5f) sdf = read_sdf_interp(m, result, c, valid);
+                if (sdf <= 0.0f) break;
+                step = !isnan(sdf) ? fmaxf(fm(sdf, stepScale), 1.0f) : 8.0f;
+            }
+            result = add3(result, smul3(step, dir));
+            dist_s = fa(dist_s, step);
+        }
+        if (sdf <= 0.0f) {
+            step = fm(sdf, stepScale);
+            result = add3(result, smul3(step, dir));
+            sdf = read_sdf_interp(m, result, c, valid);
+            step = fm(sdf, stepScale);
+            result = add3(result, smul3(step, dir));
+            found = true;
+        }
+        f3 n;
+        if (found && read_normal(m, result, c, P.Rinv, n)) {
+            const f3 r = mv(P.Rinv, sub3(mul3(result, m.g.voxel_size), P.t));
+            vout = make_float4(r.x, r.y, r.z, 1.0f);
+            nout = make_float4(n.x, n.y, n.z, 1.0f);
+        }
+    }
+    vmap[o] = vout;
+    nmap[o] = nout;
+}
+
+static int sm_count_rc() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s) {
+    k_zrange_init<<<(m.zc * m.zr + 255) / 256, 256, 0, s>>>(m, skip);
+    k_zrange<<<sm_count_rc() * 2, 256, 0, s>>>(m, k, pose, skip);
+    return 2;
+}
+
+int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,
+                    const DevPose* pose, const int* skip, cudaStream_t s) {
+    dim3 b(16, 8), g((W + 15) / 16, (H + 7) / 8);
+    k_raycast<<<g, b, 0, s>>>(m, vmap, nmap, p, W, H, k, pose, skip);
+    return 1;
+}
+
+}  // namespace fb

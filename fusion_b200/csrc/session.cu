@@ -1,0 +1,976 @@
+// Session objects and the C ABI of libfusion_b200.so (include/fusion_b200.h).
+//
+// A session holds, in device memory, the two frames the reference's Tracker
+// swaps (NextFrame / LastFrame, Core/Frame.h:61-70), the tracker state and the
+// voxel-block map (Mapping::Create, Mapping/Mapping.cc:11-51).  fb_grab_frame
+// issues the whole frame -- pyramid, 19 Gauss-Newton iterations with their
+// on-device solves, allocation, visibility, integration, z ranges and raycast
+// -- as one stream of kernels with no host round trip in between; the kernels
+// after tracking read the device's tracking verdict and do nothing when the
+// frame was not tracked.  One small device-to-host copy at the end returns the
+// frame result, and the host then advances the reference's tracking state
+// machine (Tracking/Tracking.cc:58-112) and swaps the frames.
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/fusion_b200.h"
+#include "fb_internal.h"
+
+using namespace fb;
+
+namespace {
+
+thread_local char g_last_error[256] = "";
+
+bool cuda_ok(cudaError_t e) {
+    if (e == cudaSuccess) return true;
+    snprintf(g_last_error, sizeof g_last_error, "%s", cudaGetErrorString(e));
+    return false;
+}
+
+#define FB_CUDA(call)                          \
+    do {                                       \
+        if (!cuda_ok(call)) return FB_ECUDA;   \
+    } while (0)
+
+// Kernels launched through the launchers report errors here.
+int check_launch() {
+    cudaError_t e = cudaGetLastError();
+    return cuda_ok(e) ? FB_OK : FB_ECUDA;
+}
+
+// Compact result gathered on the device at the end of a frame.
+struct FrameOut {
+    double pose[16];
+    int failed;
+    float icp_error, icp_count, rgb_error, rgb_count;
+    int n_alloc, n_visible, n_new, n_tiles;
+    unsigned err;
+    int heap_counter, entry_ptr, seq_path;
+};
+
+__global__ void k_init_poses(TrackState* st) {
+    for (int i = 0; i < 16; ++i) st->pose[i] = st->last_pose[i] = st->init_pose[i] = (i % 5 == 0) ? 1.0 : 0.0;
+    st->cur = make_dev_pose_d(st->pose);
+    st->last = st->cur;
+    st->failed = 0;
+    st->icp_error = st->rgb_error = qnan();
+    st->icp_count = st->rgb_count = 0;
+}
+
+// After the frame: a tracked frame becomes the last frame (SwapFrame).
+__global__ void k_commit(TrackState* st, MapCounters* c, FrameOut* out, int tracked_path) {
+    if (tracked_path && !st->failed) {
+        for (int i = 0; i < 16; ++i) st->last_pose[i] = st->pose[i];
+        st->last = st->cur;
+    }
+    for (int i = 0; i < 16; ++i) out->pose[i] = st->pose[i];
+    out->failed = st->failed;
+    out->icp_error = st->icp_error;
+    out->icp_count = st->icp_count;
+    out->rgb_error = st->rgb_error;
+    out->rgb_count = st->rgb_count;
+    out->n_alloc = c->n_alloc;
+    out->n_visible = c->n_visible;
+    out->n_new = c->n_new;
+    out->n_tiles = c->n_tiles;
+    out->err = c->err;
+    out->heap_counter = c->heap_counter;
+    out->entry_ptr = c->entry_ptr;
+    out->seq_path = c->seq_path;
+}
+
+__global__ void k_set_pose(DevPose* dst, DevPose p) { *dst = p; }
+
+// Export of the hash table in the reference's field order, ptr as voxel index.
+__global__ void k_export_entries(const HEntry* e, int n, int* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        HEntry h = e[i];
+        out[5 * i + 0] = h.x;
+        out[5 * i + 1] = h.y;
+        out[5 * i + 2] = h.z;
+        out[5 * i + 3] = h.ptr >= 0 ? h.ptr * 512 : -1;
+        out[5 * i + 4] = h.offset;
+    }
+}
+
+struct FrameBuf {
+    uint16_t* depth_in;
+    uint8_t* rgb;
+    float* raw;
+    float* depth[3];
+    float4* vmap[3];
+    float4* nmap[3];
+    uint8_t* gray[3];
+    int16_t* dx[3];
+    int16_t* dy[3];
+};
+
+}  // namespace
+
+constexpr int kStages = 8;   // resize, pyramid, tracking, allocation, visibility, integration, z ranges, raycast
+
+struct fb_session {
+    fb_config cfg;
+    cudaStream_t stream;
+    bool own_stream;
+    int W[3], H[3];
+    Intr K[3];
+    FrameBuf fr[2];
+    int next;                  // index of NextFrame in fr
+    TrackState* st;
+    float* partials;
+    unsigned int* tickets;
+    int* residual;
+    MapView map;
+    MapCounters* ctr;
+    DevPose* scratch_pose;
+    FrameOut* d_out;
+    FrameOut* h_out;           // pinned
+    std::vector<void*> allocs;
+    // Tracker / System host state (Tracking.cc:19-23, System.cc:72)
+    int state, last_state, no_missed, frames_after_reloc;
+    uint64_t frame_id;
+    double pose[16];
+    // tracing: CUDA events around each stage (off by default)
+    bool profile;
+    cudaEvent_t ev[kStages + 1];
+    double stage_ms[kStages];
+    uint64_t stage_calls[kStages];
+    uint64_t launches;          // kernels launched by this session
+};
+
+namespace {
+
+template <class T>
+bool dalloc(fb_session* s, T** p, size_t n) {
+    void* q = nullptr;
+    if (!cuda_ok(cudaMalloc(&q, sizeof(T) * (n ? n : 1)))) return false;
+    s->allocs.push_back(q);
+    *p = (T*)q;
+    return true;
+}
+
+size_t next_pow2(size_t v) {
+    size_t p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+bool valid_config(const fb_config* c) {
+    if (!c || c->width < 16 || c->height < 16 || c->width > 4096 || c->height > 2048) return false;
+    if ((size_t)c->width * c->height >= (1u << 22)) return false;  // packed RGB correspondences
+    if (!(c->fx > 0) || !(c->fy > 0) || !(c->depth_scale > 0) || !(c->voxel_size > 0) || !(c->trunc_dist > 0))
+        return false;
+    if (c->num_buckets <= 0 || c->num_excess < 0 || c->num_blocks <= 0) return false;
+    if ((size_t)c->num_blocks * 512 >= ((size_t)1 << 40)) return false;
+    for (int i = 0; i < 3; ++i)
+        if (c->iters[i] < 0 || c->iters[i] > 1000) return false;
+    return true;
+}
+
+MapGeom make_geom(const fb_config& c) {
+    MapGeom g;
+    g.voxel_size = c.voxel_size;
+    // the reference's constexpr expressions (Mapping/DeviceMap.h:148-151)
+    g.voxel_size_inv = (float)(1.0 / (double)c.voxel_size);
+    g.trunc_dist = c.trunc_dist;
+    g.step_scale = (float)(0.5 * (double)c.trunc_dist * (double)g.voxel_size_inv);
+    g.block_width = c.voxel_size * 8.0f;
+    g.depth_min = c.depth_min;
+    g.depth_max = c.depth_max;
+    return g;
+}
+
+TrackLevel level_view(const fb_session* s, int l) {
+    const FrameBuf& N = s->fr[s->next];
+    const FrameBuf& L = s->fr[1 - s->next];
+    TrackLevel t;
+    t.W = s->W[l];
+    t.H = s->H[l];
+    t.vp = t.gp = t.sp = t.W;
+    t.k = s->K[l];
+    t.vcurr = N.vmap[l];
+    t.ncurr = N.nmap[l];
+    t.vlast = L.vmap[l];
+    t.nlast = L.nmap[l];
+    t.gcurr = N.gray[l];
+    t.glast = L.gray[l];
+    t.dx = N.dx[l];
+    t.dy = N.dy[l];
+    return t;
+}
+
+void free_session(fb_session* s) {
+    for (int i = 0; i <= kStages; ++i)
+        if (s->ev[i]) cudaEventDestroy(s->ev[i]);
+    for (void* p : s->allocs) cudaFree(p);
+    if (s->h_out) cudaFreeHost(s->h_out);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+int reset_session(fb_session* s) {
+    launch_map_reset(s->map, s->stream);
+    k_init_poses<<<1, 1, 0, s->stream>>>(s->st);
+    FB_CUDA(cudaMemsetAsync(s->tickets, 0, 4 * sizeof(unsigned), s->stream));
+    for (int f = 0; f < 2; ++f)
+        for (int l = 0; l < 3; ++l) {
+            size_t n = (size_t)s->W[l] * s->H[l];
+            FB_CUDA(cudaMemsetAsync(s->fr[f].vmap[l], 0xff, n * sizeof(float4), s->stream));
+            FB_CUDA(cudaMemsetAsync(s->fr[f].nmap[l], 0xff, n * sizeof(float4), s->stream));
+        }
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    if (check_launch()) return FB_ECUDA;
+    s->state = s->last_state = 1;
+    s->no_missed = 0;
+    s->frames_after_reloc = 10;
+    s->frame_id = 0;
+    s->next = 0;
+    for (int i = 0; i < 16; ++i) s->pose[i] = (i % 5 == 0);
+    return FB_OK;
+}
+
+// The frame's kernels after the input has reached fr[next].  Returns the
+// number of kernels launched and which stages ran (bit k = stage k).
+int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, unsigned* ran) {
+    cudaStream_t st = s->stream;
+    FrameBuf& N = s->fr[s->next];
+    FrameBuf& L = s->fr[1 - s->next];
+    const fb_config& c = s->cfg;
+    int n = 0;
+    *ran = 0;
+    auto mark = [&](int k) {
+        if (s->profile) cudaEventRecord(s->ev[k], st);
+    };
+    // Tracker::GrabFrame (Tracking.cc:236-243): LastFrame->ResizeImages ...
+    mark(0);
+    for (int l = 1; l < 3; ++l)
+        n += launch_resize(L.vmap[l - 1], L.nmap[l - 1], s->W[l - 1], s->W[l - 1], s->H[l - 1], L.vmap[l], L.nmap[l],
+                           s->W[l], st);
+    *ran |= 1u << 0;
+    // ... NextFrame->FillImages (Core/Frame.cc:59-78)
+    mark(1);
+    n += launch_level0(N.depth_in, s->W[0], N.rgb, 3 * s->W[0], s->W[0], s->H[0], c.depth_scale, c.depth_cutoff,
+                       N.raw, s->W[0], N.depth[0], s->W[0], N.gray[0], s->W[0], st);
+    for (int l = 1; l < 3; ++l)
+        n += launch_pyrdown(N.depth[l - 1], s->W[l - 1], N.gray[l - 1], s->W[l - 1], s->W[l - 1], s->H[l - 1],
+                            N.depth[l], s->W[l], N.gray[l], s->W[l], st);
+    for (int l = 0; l < 3; ++l)
+        n += launch_maps(N.depth[l], s->W[l], N.gray[l], s->W[l], s->W[l], s->H[l], s->K[l], c.depth_cutoff,
+                         N.vmap[l], s->W[l], N.nmap[l], s->W[l], N.dx[l], N.dy[l], s->W[l], st);
+    *ran |= 1u << 1;
+    mark(2);
+    const int* skip = nullptr;
+    if (init) {
+        k_init_poses<<<1, 1, 0, st>>>(s->st);
+        n += 1;
+    } else if (track) {
+        // Tracker::ComputeSE3 (Tracking.cc:296-409)
+        static const int min_count[3] = {2000, 1000, 100};   // MIN_ICP_COUNT, Tracking.h:102
+        n += launch_track_begin(s->st, st);
+        int last_level = -1;
+        for (int l = 2; l >= 0; --l)
+            if (c.iters[l] > 0) last_level = l;
+        for (int l = 2; l >= 0; --l) {
+            TrackLevel lv = level_view(s, l);
+            for (int it = 0; it < c.iters[l]; ++it)
+                n += launch_track_iter(lv, s->st, s->partials, s->tickets, s->residual, min_count[l],
+                                       l == last_level && it == c.iters[l] - 1, st);
+        }
+        skip = &s->st->failed;
+        *ran |= 1u << 2;
+    }
+    const DevPose* pose = &s->st->cur;
+    mark(3);
+    if (fuse) {
+        // Mapping::FuseColor(LastFrame) after the swap (Mapping.cc:76-90):
+        // raw depth, colour and level-0 normals of the frame just tracked
+        n += launch_allocate(s->map, N.raw, s->W[0], s->W[0], s->H[0], s->K[0], pose, skip, st);
+        mark(4);
+        n += launch_visibility(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st);
+        mark(5);
+        n += launch_integrate(s->map, N.raw, s->W[0], N.rgb, 3 * s->W[0], N.nmap[0], s->W[0], s->W[0], s->H[0],
+                              s->K[0], pose, skip, st);
+        *ran |= 7u << 3;
+    } else {
+        mark(4);
+        mark(5);
+    }
+    mark(6);
+    if (render) {
+        // Mapping::RayTrace (Mapping.cc:92-109) into the frame's level-0 maps
+        n += launch_zrange(s->map, s->K[0], pose, skip, st);
+        mark(7);
+        n += launch_raycast(s->map, N.vmap[0], N.nmap[0], s->W[0], s->W[0], s->H[0], s->K[0], pose, skip, st);
+        *ran |= 3u << 6;
+    } else {
+        mark(7);
+    }
+    mark(8);
+    k_commit<<<1, 1, 0, st>>>(s->st, s->ctr, s->d_out, track || init);
+    return n + 1;
+}
+
+int image_ok(const fb_image* im, size_t elem) {
+    return im && im->data && im->cols > 0 && im->rows > 0 && im->pitch >= elem * (size_t)im->cols &&
+           im->pitch % elem == 0;
+}
+
+cudaStream_t as_stream(void* s) { return (cudaStream_t)s; }
+
+DevPose pose_from(const float R[9], const float Rinv[9], const float t[3]) {
+    DevPose p;
+    p.R.r0 = {R[0], R[1], R[2]};
+    p.R.r1 = {R[3], R[4], R[5]};
+    p.R.r2 = {R[6], R[7], R[8]};
+    p.Rinv.r0 = {Rinv[0], Rinv[1], Rinv[2]};
+    p.Rinv.r1 = {Rinv[3], Rinv[4], Rinv[5]};
+    p.Rinv.r2 = {Rinv[6], Rinv[7], Rinv[8]};
+    p.t = {t[0], t[1], t[2]};
+    p.pad = 0;
+    return p;
+}
+
+Intr intr_from(const float K[4]) {
+    Intr k;
+    k.fx = K[0];
+    k.fy = K[1];
+    k.cx = K[2];
+    k.cy = K[3];
+    k.invfx = (float)(1.0 / (double)k.fx);
+    k.invfy = (float)(1.0 / (double)k.fy);
+    return k;
+}
+
+}  // namespace
+
+extern "C" {
+
+void fb_default_config(fb_config* c, int width, int height) {
+    std::memset(c, 0, sizeof *c);
+    c->width = width;
+    c->height = height;
+    c->fx = c->fy = 525.0f * width / 640.0f;
+    c->cx = width * 0.5f;
+    c->cy = height * 0.5f;
+    c->depth_scale = 1000.0f;
+    c->depth_cutoff = 3.0f;
+    c->voxel_size = 0.006f;
+    c->trunc_dist = 0.006f * 8;
+    c->depth_min = 0.1f;
+    c->depth_max = 3.0f;
+    c->num_buckets = 1000000;
+    c->num_excess = 500000;
+    c->num_blocks = 700000;
+    c->iters[0] = 10;
+    c->iters[1] = 5;
+    c->iters[2] = 3;
+}
+
+const char* fb_status_string(int st) {
+    switch (st) {
+    case FB_OK: return "ok";
+    case FB_EINVAL: return "invalid argument";
+    case FB_ENOMEM: return "out of memory";
+    case FB_ECUDA: return "CUDA error";
+    case FB_ETRACK_LOST: return "frame not tracked";
+    default: return "unknown status";
+    }
+}
+
+const char* fb_last_error(void) { return g_last_error; }
+
+size_t fb_session_bytes(const fb_config* c) {
+    if (!valid_config(c)) return 0;
+    size_t px = (size_t)c->width * c->height, frame = 0;
+    for (int l = 0; l < 3; ++l) {
+        size_t n = (size_t)(c->width >> l) * (c->height >> l);
+        frame += n * (4 + 16 + 16 + 1 + 2 + 2);
+    }
+    frame += px * (2 + 3 + 4);
+    size_t NS = c->num_blocks, NB = c->num_buckets, NE = c->num_excess;
+    size_t reqcap = next_pow2(2 * NS > 4096 ? 2 * NS : 4096);
+    size_t map = (NB + NE) * sizeof(HEntry) + NS * 4 + NS * 512 * sizeof(Voxel) + 2 * NS * 4 + reqcap * 8 +
+                 NS * sizeof(NewBlock) + 2 * NS * 4 + 3 * NB * 4;
+    return 2 * frame + map + px * 4 + kTrackMaxBlocks * 32 * 4 + sizeof(TrackState);
+}
+
+int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
+    if (!out || !valid_config(cfg)) return FB_EINVAL;
+    *out = nullptr;
+    fb_session* s = new (std::nothrow) fb_session();
+    if (!s) return FB_ENOMEM;
+    s->cfg = *cfg;
+    s->h_out = nullptr;
+    s->profile = false;
+    for (int i = 0; i <= kStages; ++i) s->ev[i] = nullptr;
+    for (int i = 0; i < kStages; ++i) {
+        s->stage_ms[i] = 0;
+        s->stage_calls[i] = 0;
+    }
+    s->launches = 0;
+    s->own_stream = stream == nullptr;
+    s->stream = (cudaStream_t)stream;
+    // an owned stream is a blocking one: it orders after work the caller put
+    // on the legacy default stream (e.g. the copies that filled its inputs)
+    if (s->own_stream && !cuda_ok(cudaStreamCreate(&s->stream))) {
+        s->stream = nullptr;
+        free_session(s);
+        return FB_ECUDA;
+    }
+    for (int l = 0; l < 3; ++l) {
+        s->W[l] = cfg->width >> l;
+        s->H[l] = cfg->height >> l;
+        s->K[l] = make_intr(cfg->fx, cfg->fy, cfg->cx, cfg->cy, l);
+    }
+    bool ok = true;
+    for (int f = 0; f < 2 && ok; ++f) {
+        FrameBuf& F = s->fr[f];
+        size_t n0 = (size_t)s->W[0] * s->H[0];
+        ok = ok && dalloc(s, &F.depth_in, n0) && dalloc(s, &F.rgb, 3 * n0) && dalloc(s, &F.raw, n0);
+        for (int l = 0; l < 3 && ok; ++l) {
+            size_t n = (size_t)s->W[l] * s->H[l];
+            ok = dalloc(s, &F.depth[l], n) && dalloc(s, &F.vmap[l], n) && dalloc(s, &F.nmap[l], n) &&
+                 dalloc(s, &F.gray[l], n) && dalloc(s, &F.dx[l], n) && dalloc(s, &F.dy[l], n);
+        }
+    }
+    ok = ok && dalloc(s, &s->st, 1) && dalloc(s, &s->partials, (size_t)kTrackMaxBlocks * 32) &&
+         dalloc(s, &s->tickets, 4) && dalloc(s, &s->residual, (size_t)s->W[0] * s->H[0]) &&
+         dalloc(s, &s->scratch_pose, 1) && dalloc(s, &s->d_out, 1);
+    MapView& m = s->map;
+    if (ok) {
+        m.NB = cfg->num_buckets;
+        m.NE = cfg->num_excess;
+        m.NS = cfg->num_blocks;
+        m.reqcap = (int)next_pow2((size_t)2 * m.NS > 4096 ? (size_t)2 * m.NS : 4096);
+        m.newcap = m.NS;
+        m.nchunks = (m.NB + kScanChunk - 1) / kScanChunk;
+        m.zc = (cfg->width + 7) / 8;
+        m.zr = (cfg->height + 7) / 8;
+        m.g = make_geom(*cfg);
+        ok = dalloc(s, &m.entries, (size_t)m.NB + m.NE) && dalloc(s, &m.heap, m.NS) &&
+             dalloc(s, &m.voxels, (size_t)m.NS * 512) && dalloc(s, &m.ctr, 1) && dalloc(s, &m.alloc_list, m.NS) &&
+             dalloc(s, &m.visible, m.NS) && dalloc(s, &m.reqset, m.reqcap) && dalloc(s, &m.newblk, m.newcap) &&
+             dalloc(s, &m.order, m.newcap) && dalloc(s, &m.arrival, m.newcap) &&
+             dalloc(s, &m.bucket_cnt, m.NB) && dalloc(s, &m.bucket_start, m.NB) && dalloc(s, &m.bucket_x, m.NB) &&
+             dalloc(s, &m.chunk_sums, 2 * (size_t)m.nchunks) && dalloc(s, &m.zmin, (size_t)m.zc * m.zr) &&
+             dalloc(s, &m.zmax, (size_t)m.zc * m.zr);
+        s->ctr = m.ctr;
+    }
+    if (ok) ok = cuda_ok(cudaMallocHost((void**)&s->h_out, sizeof(FrameOut)));
+    for (int i = 0; i <= kStages && ok; ++i) ok = cuda_ok(cudaEventCreate(&s->ev[i]));
+    if (!ok) {
+        free_session(s);
+        return FB_ENOMEM;
+    }
+    int rc = reset_session(s);
+    if (rc) {
+        free_session(s);
+        return rc;
+    }
+    *out = s;
+    return FB_OK;
+}
+
+int fb_session_destroy(fb_session* s) {
+    if (!s) return FB_EINVAL;
+    cudaStreamSynchronize(s->stream);
+    free_session(s);
+    return FB_OK;
+}
+
+int fb_session_reset(fb_session* s) {
+    if (!s) return FB_EINVAL;
+    return reset_session(s);
+}
+
+int fb_grab_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, const uint8_t* rgb, size_t rgb_pitch,
+                  int on_device, fb_frame_result* out) {
+    if (!s || !depth || !rgb) return FB_EINVAL;
+    const int W = s->W[0], H = s->H[0];
+    if (depth_pitch < (size_t)W * 2 || rgb_pitch < (size_t)W * 3) return FB_EINVAL;
+    FrameBuf& N = s->fr[s->next];
+    cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    FB_CUDA(cudaMemcpy2DAsync(N.depth_in, (size_t)W * 2, depth, depth_pitch, (size_t)W * 2, H, kind, s->stream));
+    FB_CUDA(cudaMemcpy2DAsync(N.rgb, (size_t)W * 3, rgb, rgb_pitch, (size_t)W * 3, H, kind, s->stream));
+    // Tracker::Track (Tracking.cc:58-112): the state is known on the host;
+    // whether tracking succeeds is decided on the device.
+    std::swap(s->state, s->last_state);
+    const int state = s->state;
+    const bool init = state == 1;
+    const bool track = state == 0;
+    // System::GrabImage (System.cc:98-115): frames_after_reloc is updated from
+    // the tracker state, which does not depend on this frame's outcome
+    int after = s->frames_after_reloc;
+    if (state == 0) after++;
+    if (state == -1) after = 0;
+    const bool fuse = (init || track) && after >= 10;
+    const bool render = init || track;
+    unsigned ran = 0;
+    s->launches += (uint64_t)issue_frame(s, track, fuse, render, init, &ran);
+    if (check_launch()) return FB_ECUDA;
+    FB_CUDA(cudaMemcpyAsync(s->h_out, s->d_out, sizeof(FrameOut), cudaMemcpyDeviceToHost, s->stream));
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    if (s->profile)
+        for (int k = 0; k < kStages; ++k) {
+            if (!(ran & (1u << k))) continue;
+            float ms = 0;
+            FB_CUDA(cudaEventElapsedTime(&ms, s->ev[k], s->ev[k + 1]));
+            s->stage_ms[k] += ms;
+            s->stage_calls[k] += 1;
+        }
+    const FrameOut& o = *s->h_out;
+    bool valid = false;
+    if (init) {
+        s->next = 1 - s->next;  // SwapFrame
+        s->last_state = 0;
+        valid = true;
+    } else if (track) {
+        if (!o.failed) {
+            s->no_missed = 0;
+            if (s->last_state != -1) {
+                s->last_state = 0;
+                s->next = 1 - s->next;
+                valid = true;
+            } else {
+                s->last_state = 0;
+            }
+        } else {
+            s->last_state = 0;
+            if (++s->no_missed > 9) s->last_state = -1;
+        }
+    } else {
+        s->last_state = -1;
+    }
+    s->frames_after_reloc = after;
+    std::memcpy(s->pose, o.pose, sizeof s->pose);
+    if (out) {
+        out->status = valid ? FB_OK : FB_ETRACK_LOST;
+        out->tracked = valid;
+        out->tracker_state = state;
+        out->fused = fuse && valid;
+        out->no_visible = (fuse && valid) ? (uint32_t)o.n_visible : 0;
+        out->no_allocated = (uint32_t)o.n_alloc;
+        out->no_new = (fuse && valid) ? (uint32_t)o.n_new : 0;
+        out->error_flags = o.err;
+        out->icp_error = o.icp_error;
+        out->icp_count = o.icp_count;
+        out->rgb_error = o.rgb_error;
+        out->rgb_count = o.rgb_count;
+        std::memcpy(out->pose, o.pose, sizeof out->pose);
+        out->frame_id = s->frame_id;
+    }
+    s->frame_id++;
+    return FB_OK;
+}
+
+int fb_session_set_profiling(fb_session* s, int on) {
+    if (!s) return FB_EINVAL;
+    s->profile = on != 0;
+    for (int i = 0; i < kStages; ++i) {
+        s->stage_ms[i] = 0;
+        s->stage_calls[i] = 0;
+    }
+    return FB_OK;
+}
+
+int fb_session_stage_times(fb_session* s, double* ms, uint64_t* calls, int n) {
+    if (!s || n < 0) return FB_EINVAL;
+    for (int i = 0; i < n && i < kStages; ++i) {
+        if (ms) ms[i] = s->stage_ms[i];
+        if (calls) calls[i] = s->stage_calls[i];
+    }
+    return FB_OK;
+}
+
+int fb_session_launch_count(fb_session* s, uint64_t* launches) {
+    if (!s || !launches) return FB_EINVAL;
+    *launches = s->launches;
+    return FB_OK;
+}
+
+int fb_frame_transfer_bytes(const fb_config* c, size_t* h2d, size_t* d2h) {
+    if (!valid_config(c)) return FB_EINVAL;
+    if (h2d) *h2d = (size_t)c->width * c->height * (sizeof(uint16_t) + 3);
+    if (d2h) *d2h = sizeof(FrameOut);
+    return FB_OK;
+}
+
+int fb_get_pose(fb_session* s, double pose[16]) {
+    if (!s || !pose) return FB_EINVAL;
+    std::memcpy(pose, s->pose, sizeof s->pose);
+    return FB_OK;
+}
+
+int fb_download_level(fb_session* s, int which, int l, float* vmap, float* nmap, float* depth, uint8_t* gray,
+                      int16_t* dx, int16_t* dy) {
+    if (!s || which < 0 || which > 1 || l < 0 || l > 2) return FB_EINVAL;
+    const FrameBuf& F = s->fr[which ? s->next : 1 - s->next];
+    size_t n = (size_t)s->W[l] * s->H[l];
+    cudaStream_t st = s->stream;
+    if (vmap) FB_CUDA(cudaMemcpyAsync(vmap, F.vmap[l], 16 * n, cudaMemcpyDeviceToHost, st));
+    if (nmap) FB_CUDA(cudaMemcpyAsync(nmap, F.nmap[l], 16 * n, cudaMemcpyDeviceToHost, st));
+    if (depth) FB_CUDA(cudaMemcpyAsync(depth, F.depth[l], 4 * n, cudaMemcpyDeviceToHost, st));
+    if (gray) FB_CUDA(cudaMemcpyAsync(gray, F.gray[l], n, cudaMemcpyDeviceToHost, st));
+    if (dx) FB_CUDA(cudaMemcpyAsync(dx, F.dx[l], 2 * n, cudaMemcpyDeviceToHost, st));
+    if (dy) FB_CUDA(cudaMemcpyAsync(dy, F.dy[l], 2 * n, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    return FB_OK;
+}
+
+int fb_download_raw(fb_session* s, int which, float* raw) {
+    if (!s || !raw || which < 0 || which > 1) return FB_EINVAL;
+    const FrameBuf& F = s->fr[which ? s->next : 1 - s->next];
+    FB_CUDA(cudaMemcpyAsync(raw, F.raw, 4 * (size_t)s->W[0] * s->H[0], cudaMemcpyDeviceToHost, s->stream));
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    return FB_OK;
+}
+
+int fb_map_get_stats(fb_session* s, fb_map_stats* out) {
+    if (!s || !out) return FB_EINVAL;
+    MapCounters c;
+    FB_CUDA(cudaMemcpyAsync(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost, s->stream));
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    out->heap_counter = c.heap_counter;
+    out->entry_ptr = c.entry_ptr;
+    out->no_allocated = (uint32_t)c.n_alloc;
+    out->no_visible = (uint32_t)c.n_visible;
+    out->no_new = (uint32_t)c.n_new;
+    out->no_tiles = (uint32_t)c.n_tiles;
+    out->error_flags = c.err;
+    out->sequential = c.seq_path;
+    return FB_OK;
+}
+
+int fb_map_download_entries(fb_session* s, int32_t* entries) {
+    if (!s || !entries) return FB_EINVAL;
+    const int n = s->map.NB + s->map.NE;
+    int* tmp = nullptr;
+    FB_CUDA(cudaMallocAsync((void**)&tmp, sizeof(int) * 5 * (size_t)n, s->stream));
+    k_export_entries<<<592, 256, 0, s->stream>>>(s->map.entries, n, tmp);
+    cudaError_t e = cudaMemcpyAsync(entries, tmp, sizeof(int) * 5 * (size_t)n, cudaMemcpyDeviceToHost, s->stream);
+    cudaFreeAsync(tmp, s->stream);
+    FB_CUDA(e);
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    return FB_OK;
+}
+
+int fb_map_download_blocks(fb_session* s, const int32_t* ptrs, int n, float* sdf, uint8_t* weight, uint8_t* rgb) {
+    if (!s || (n > 0 && !ptrs) || n < 0) return FB_EINVAL;
+    std::vector<Voxel> tmp(512);
+    for (int i = 0; i < n; ++i) {
+        if (ptrs[i] < 0 || ptrs[i] % 512 || ptrs[i] / 512 >= s->map.NS) return FB_EINVAL;
+        FB_CUDA(cudaMemcpyAsync(tmp.data(), s->map.voxels + ptrs[i], 512 * sizeof(Voxel), cudaMemcpyDeviceToHost,
+                                s->stream));
+        FB_CUDA(cudaStreamSynchronize(s->stream));
+        for (int v = 0; v < 512; ++v) {
+            size_t o = (size_t)i * 512 + v;
+            if (sdf) sdf[o] = tmp[v].sdf;
+            if (weight) weight[o] = tmp[v].weight;
+            if (rgb) {
+                rgb[3 * o] = tmp[v].r;
+                rgb[3 * o + 1] = tmp[v].g;
+                rgb[3 * o + 2] = tmp[v].b;
+            }
+        }
+    }
+    return FB_OK;
+}
+
+int fb_map_download_visible(fb_session* s, int32_t* slots, uint32_t capacity, uint32_t* n) {
+    if (!s || !n) return FB_EINVAL;
+    MapCounters c;
+    FB_CUDA(cudaMemcpyAsync(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost, s->stream));
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    uint32_t nv = (uint32_t)(c.n_visible < s->map.NS ? c.n_visible : s->map.NS);
+    *n = nv;
+    if (slots && capacity) {
+        uint32_t k = nv < capacity ? nv : capacity;
+        FB_CUDA(cudaMemcpyAsync(slots, s->map.visible, 4 * (size_t)k, cudaMemcpyDeviceToHost, s->stream));
+        FB_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    return FB_OK;
+}
+
+// ---------------------------------------------------------- per-stage entries
+
+int fb_filter_depth(const fb_image* depth, fb_image* raw, fb_image* filtered, float depth_scale, float depth_cutoff,
+                    void* stream) {
+    if (!image_ok(depth, 2) || !image_ok(raw, 4) || !image_ok(filtered, 4)) return FB_EINVAL;
+    if (raw->cols < depth->cols || raw->rows < depth->rows || filtered->cols < depth->cols ||
+        filtered->rows < depth->rows || !(depth_scale > 0))
+        return FB_EINVAL;
+    launch_level0((const uint16_t*)depth->data, (int)(depth->pitch / 2), nullptr, 0, depth->cols, depth->rows,
+                  depth_scale, depth_cutoff, (float*)raw->data, (int)(raw->pitch / 4), (float*)filtered->data,
+                  (int)(filtered->pitch / 4), nullptr, 0, as_stream(stream));
+    return check_launch();
+}
+
+int fb_image_to_intensity(const fb_image* rgb, fb_image* gray, void* stream) {
+    if (!image_ok(rgb, 3) || !image_ok(gray, 1) || gray->cols < rgb->cols || gray->rows < rgb->rows) return FB_EINVAL;
+    // gray only: the level-0 kernel with no depth outputs reads no depth
+    launch_level0(nullptr, 0, (const uint8_t*)rgb->data, (int)rgb->pitch, rgb->cols, rgb->rows, 1.0f, 0.0f,
+                  nullptr, 0, nullptr, 0, (uint8_t*)gray->data, (int)gray->pitch, as_stream(stream));
+    return check_launch();
+}
+
+int fb_pyrdown_gauss_f32(const fb_image* src, fb_image* dst, void* stream) {
+    if (!image_ok(src, 4) || !image_ok(dst, 4) || dst->cols < src->cols / 2 || dst->rows < src->rows / 2)
+        return FB_EINVAL;
+    launch_pyrdown((const float*)src->data, (int)(src->pitch / 4), nullptr, 0, src->cols, src->rows,
+                   (float*)dst->data, (int)(dst->pitch / 4), nullptr, 0, as_stream(stream));
+    return check_launch();
+}
+
+int fb_pyrdown_gauss_u8(const fb_image* src, fb_image* dst, void* stream) {
+    if (!image_ok(src, 1) || !image_ok(dst, 1) || dst->cols < src->cols / 2 || dst->rows < src->rows / 2)
+        return FB_EINVAL;
+    launch_pyrdown(nullptr, 0, (const uint8_t*)src->data, (int)src->pitch, src->cols, src->rows, nullptr, 0,
+                   (uint8_t*)dst->data, (int)dst->pitch, as_stream(stream));
+    return check_launch();
+}
+
+int fb_compute_vmap(const fb_image* depth, fb_image* vmap, float fx, float fy, float cx, float cy, float depth_cutoff,
+                    void* stream) {
+    if (!image_ok(depth, 4) || !image_ok(vmap, 16) || vmap->cols < depth->cols || vmap->rows < depth->rows)
+        return FB_EINVAL;
+    if (!(fx > 0) || !(fy > 0)) return FB_EINVAL;
+    Intr k;
+    k.fx = fx;
+    k.fy = fy;
+    k.cx = cx;
+    k.cy = cy;
+    k.invfx = (float)(1.0 / (double)fx);
+    k.invfy = (float)(1.0 / (double)fy);
+    launch_maps((const float*)depth->data, (int)(depth->pitch / 4), nullptr, 0, depth->cols, depth->rows, k,
+                depth_cutoff, (float4*)vmap->data, (int)(vmap->pitch / 16), nullptr, 0, nullptr, nullptr, 0,
+                as_stream(stream));
+    return check_launch();
+}
+
+int fb_compute_nmap(const fb_image* vmap, fb_image* nmap, void* stream) {
+    if (!image_ok(vmap, 16) || !image_ok(nmap, 16) || nmap->cols < vmap->cols || nmap->rows < vmap->rows)
+        return FB_EINVAL;
+    launch_nmap((const float4*)vmap->data, (int)(vmap->pitch / 16), vmap->cols, vmap->rows, (float4*)nmap->data,
+                (int)(nmap->pitch / 16), as_stream(stream));
+    return check_launch();
+}
+
+int fb_compute_derivative_image(const fb_image* gray, fb_image* dx, fb_image* dy, void* stream) {
+    if (!image_ok(gray, 1) || !image_ok(dx, 2) || !image_ok(dy, 2) || dx->pitch != dy->pitch ||
+        dx->cols < gray->cols || dx->rows < gray->rows)
+        return FB_EINVAL;
+    Intr k{};
+    launch_maps(nullptr, 0, (const uint8_t*)gray->data, (int)gray->pitch, gray->cols, gray->rows, k, 0.f, nullptr, 0,
+                nullptr, 0, (int16_t*)dx->data, (int16_t*)dy->data, (int)(dx->pitch / 2), as_stream(stream));
+    return check_launch();
+}
+
+int fb_resize_map(const fb_image* vsrc, const fb_image* nsrc, fb_image* vdst, fb_image* ndst, void* stream) {
+    if (!image_ok(vsrc, 16) || !image_ok(nsrc, 16) || !image_ok(vdst, 16) || !image_ok(ndst, 16)) return FB_EINVAL;
+    if (vsrc->pitch != nsrc->pitch || vdst->pitch != ndst->pitch || vdst->cols < vsrc->cols / 2 ||
+        vdst->rows < vsrc->rows / 2)
+        return FB_EINVAL;
+    launch_resize((const float4*)vsrc->data, (const float4*)nsrc->data, (int)(vsrc->pitch / 16), vsrc->cols,
+                  vsrc->rows, (float4*)vdst->data, (float4*)ndst->data, (int)(vdst->pitch / 16), as_stream(stream));
+    return check_launch();
+}
+
+size_t fb_step_scratch_bytes(int cols, int rows) {
+    if (cols <= 0 || rows <= 0) return 0;
+    // partials | tickets | out sums (32 doubles) | per-pixel correspondences
+    return (size_t)kTrackMaxBlocks * 32 * 4 + 256 + 32 * 8 + (size_t)cols * rows * 4;
+}
+
+namespace {
+struct StepScratch {
+    float* partials;
+    unsigned int* tickets;
+    double* out;
+    int* residual;
+};
+bool carve(void* scratch, size_t bytes, int cols, int rows, StepScratch& s) {
+    if (!scratch || bytes < fb_step_scratch_bytes(cols, rows) || ((uintptr_t)scratch & 15)) return false;
+    char* p = (char*)scratch;
+    s.partials = (float*)p;
+    p += (size_t)kTrackMaxBlocks * 32 * 4;
+    s.tickets = (unsigned int*)p;
+    p += 256;
+    s.out = (double*)p;
+    p += 32 * 8;
+    s.residual = (int*)p;
+    return true;
+}
+void unpack(const double* s, double* A, double* b) {
+    int n = 0;
+    for (int i = 0; i < 6; ++i)
+        for (int j = i; j < 7; ++j) {
+            double v = (double)(float)s[n++];  // the reference's sums are floats (Reduction.cu:369-371)
+            if (j == 6)
+                b[i] = v;
+            else
+                A[j * 6 + i] = A[i * 6 + j] = v;
+        }
+}
+}  // namespace
+
+int fb_icp_step(const fb_image* vcurr, const fb_image* vlast, const fb_image* ncurr, const fb_image* nlast,
+                const float Rcurr[9], const float tcurr[3], const float Rlast[9], const float RlastInv[9],
+                const float tlast[3], const float K[4], void* scratch, size_t scratch_bytes, float residual[2],
+                double A[36], double b[6], void* stream) {
+    if (!image_ok(vcurr, 16) || !image_ok(vlast, 16) || !image_ok(ncurr, 16) || !image_ok(nlast, 16)) return FB_EINVAL;
+    if (!Rcurr || !tcurr || !Rlast || !RlastInv || !tlast || !K || !residual || !A || !b) return FB_EINVAL;
+    const int W = vcurr->cols, H = vcurr->rows;
+    if (vlast->cols != W || vlast->rows != H || ncurr->cols != W || nlast->cols != W || ncurr->rows != H ||
+        nlast->rows != H || vcurr->pitch != vlast->pitch || vcurr->pitch != ncurr->pitch ||
+        vcurr->pitch != nlast->pitch)
+        return FB_EINVAL;
+    StepScratch sc;
+    if (!carve(scratch, scratch_bytes, W, H, sc)) return FB_EINVAL;
+    cudaStream_t st = as_stream(stream);
+    TrackLevel L{};
+    L.W = W;
+    L.H = H;
+    L.vp = (int)(vcurr->pitch / 16);
+    L.k = intr_from(K);
+    L.vcurr = (const float4*)vcurr->data;
+    L.vlast = (const float4*)vlast->data;
+    L.ncurr = (const float4*)ncurr->data;
+    L.nlast = (const float4*)nlast->data;
+    float Rt[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Rt[i * 3 + j] = Rcurr[j * 3 + i];
+    DevPose cur = pose_from(Rcurr, Rt, tcurr), last = pose_from(Rlast, RlastInv, tlast);
+    FB_CUDA(cudaMemsetAsync(sc.tickets, 0, 16, st));
+    launch_step_icp(L, cur, last, sc.partials, sc.tickets, sc.out, st);
+    if (check_launch()) return FB_ECUDA;
+    double host[32];
+    FB_CUDA(cudaMemcpyAsync(host, sc.out, 29 * 8, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    unpack(host, A, b);
+    residual[0] = (float)host[27];
+    residual[1] = (float)host[28];
+    return FB_OK;
+}
+
+int fb_rgb_step(const fb_image* gcurr, const fb_image* glast, const fb_image* vcurr, const fb_image* vlast,
+                const fb_image* dx, const fb_image* dy, const float Rcurr[9], const float RcurrInv[9],
+                const float Rlast[9], const float RlastInv[9], const float tcurr[3], const float tlast[3],
+                const float K[4], void* scratch, size_t scratch_bytes, float residual[2], double A[36], double b[6],
+                void* stream) {
+    if (!image_ok(gcurr, 1) || !image_ok(glast, 1) || !image_ok(vcurr, 16) || !image_ok(vlast, 16) ||
+        !image_ok(dx, 2) || !image_ok(dy, 2))
+        return FB_EINVAL;
+    if (!Rcurr || !RcurrInv || !Rlast || !RlastInv || !tcurr || !tlast || !K || !residual || !A || !b)
+        return FB_EINVAL;
+    const int W = gcurr->cols, H = gcurr->rows;
+    if (glast->cols != W || glast->rows != H || vcurr->cols != W || vcurr->rows != H || vlast->cols != W ||
+        vlast->rows != H || dx->cols != W || dy->cols != W || dx->rows != H || dy->rows != H ||
+        gcurr->pitch != glast->pitch || vcurr->pitch != vlast->pitch || dx->pitch != dy->pitch)
+        return FB_EINVAL;
+    StepScratch sc;
+    if (!carve(scratch, scratch_bytes, W, H, sc)) return FB_EINVAL;
+    cudaStream_t st = as_stream(stream);
+    TrackLevel L{};
+    L.W = W;
+    L.H = H;
+    L.vp = (int)(vcurr->pitch / 16);
+    L.gp = (int)gcurr->pitch;
+    L.sp = (int)(dx->pitch / 2);
+    L.k = intr_from(K);
+    L.vcurr = (const float4*)vcurr->data;
+    L.vlast = (const float4*)vlast->data;
+    L.gcurr = (const uint8_t*)gcurr->data;
+    L.glast = (const uint8_t*)glast->data;
+    L.dx = (const int16_t*)dx->data;
+    L.dy = (const int16_t*)dy->data;
+    DevPose cur = pose_from(Rcurr, RcurrInv, tcurr), last = pose_from(Rlast, RlastInv, tlast);
+    FB_CUDA(cudaMemsetAsync(sc.tickets, 0, 16, st));
+    launch_step_rgb(L, cur, last, sc.partials, sc.tickets, sc.residual, sc.out, st);
+    if (check_launch()) return FB_ECUDA;
+    double host[32];
+    FB_CUDA(cudaMemcpyAsync(host, sc.out, 32 * 8, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    unpack(host, A, b);
+    residual[0] = (float)host[27];
+    residual[1] = (float)host[28];
+    return FB_OK;
+}
+
+int fb_reset_map(fb_session* s) {
+    if (!s) return FB_EINVAL;
+    launch_map_reset(s->map, s->stream);
+    if (check_launch()) return FB_ECUDA;
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    return FB_OK;
+}
+
+int fb_fuse_map_color(fb_session* s, const fb_image* depth, const fb_image* rgb, const fb_image* nmap,
+                      const float Rview[9], const float RviewInv[9], const float tview[3], const float K[4],
+                      uint32_t* no_visible, void* stream) {
+    if (!s || !image_ok(depth, 4) || !image_ok(rgb, 3) || !image_ok(nmap, 16) || !Rview || !RviewInv || !tview || !K)
+        return FB_EINVAL;
+    const int W = depth->cols, H = depth->rows;
+    if (rgb->cols < W || rgb->rows < H || nmap->cols < W || nmap->rows < H) return FB_EINVAL;
+    if ((W + 7) / 8 > s->map.zc || (H + 7) / 8 > s->map.zr) return FB_EINVAL;
+    cudaStream_t st = stream ? as_stream(stream) : s->stream;
+    k_set_pose<<<1, 1, 0, st>>>(s->scratch_pose, pose_from(Rview, RviewInv, tview));
+    const Intr k = intr_from(K);
+    launch_allocate(s->map, (const float*)depth->data, (int)(depth->pitch / 4), W, H, k, s->scratch_pose, nullptr, st);
+    launch_visibility(s->map, W, H, k, s->scratch_pose, nullptr, st);
+    launch_integrate(s->map, (const float*)depth->data, (int)(depth->pitch / 4), (const uint8_t*)rgb->data,
+                     (int)rgb->pitch, (const float4*)nmap->data, (int)(nmap->pitch / 16), W, H, k, s->scratch_pose,
+                     nullptr, st);
+    if (check_launch()) return FB_ECUDA;
+    FB_CUDA(cudaStreamSynchronize(st));
+    if (no_visible) {
+        MapCounters c;
+        FB_CUDA(cudaMemcpy(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost));
+        *no_visible = (uint32_t)c.n_visible;
+    }
+    return FB_OK;
+}
+
+int fb_check_block_visibility(fb_session* s, const float Rview[9], const float RviewInv[9], const float tview[3],
+                              int cols, int rows, const float K[4], uint32_t* no_visible, void* stream) {
+    if (!s || !Rview || !RviewInv || !tview || !K || cols <= 0 || rows <= 0) return FB_EINVAL;
+    cudaStream_t st = stream ? as_stream(stream) : s->stream;
+    k_set_pose<<<1, 1, 0, st>>>(s->scratch_pose, pose_from(Rview, RviewInv, tview));
+    launch_visibility(s->map, cols, rows, intr_from(K), s->scratch_pose, nullptr, st);
+    if (check_launch()) return FB_ECUDA;
+    FB_CUDA(cudaStreamSynchronize(st));
+    if (no_visible) {
+        MapCounters c;
+        FB_CUDA(cudaMemcpy(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost));
+        *no_visible = (uint32_t)c.n_visible;
+    }
+    return FB_OK;
+}
+
+int fb_raycast(fb_session* s, fb_image* vmap, fb_image* nmap, const float Rview[9], const float RviewInv[9],
+               const float tview[3], const float K[4], int* rendered, void* stream) {
+    if (!s || !image_ok(vmap, 16) || !image_ok(nmap, 16) || vmap->pitch != nmap->pitch || !Rview || !RviewInv ||
+        !tview || !K)
+        return FB_EINVAL;
+    const int W = vmap->cols, H = vmap->rows;
+    if (nmap->cols != W || nmap->rows != H || (W + 7) / 8 > s->map.zc || (H + 7) / 8 > s->map.zr) return FB_EINVAL;
+    cudaStream_t st = stream ? as_stream(stream) : s->stream;
+    k_set_pose<<<1, 1, 0, st>>>(s->scratch_pose, pose_from(Rview, RviewInv, tview));
+    const Intr k = intr_from(K);
+    launch_zrange(s->map, k, s->scratch_pose, nullptr, st);
+    launch_raycast(s->map, (float4*)vmap->data, (float4*)nmap->data, (int)(vmap->pitch / 16), W, H, k,
+                   s->scratch_pose, nullptr, st);
+    if (check_launch()) return FB_ECUDA;
+    FB_CUDA(cudaStreamSynchronize(st));
+    if (rendered) {
+        MapCounters c;
+        FB_CUDA(cudaMemcpy(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost));
+        *rendered = c.n_tiles > 0;
+    }
+    return FB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,597 @@
+// Frame-to-model tracking: projective ICP + photometric normal equations
+// (Tracking/Reduction.cu: ICPReduce 212-375, RGBReduction 377-627) and the
+// coarse-to-fine Gauss-Newton loop of Tracker::ComputeSE3
+// (Tracking/Tracking.cc:296-409), kept entirely on the device.
+//
+// One iteration is two kernels:
+//   pass A: per pixel, the ICP row (point-to-plane, 7 wide) and the RGB
+//           correspondence search; ICP products and the RGB count / sum of
+//           squared differences are reduced.  The RGB correspondence of each
+//           pixel is kept as one packed int (last-frame pixel + difference).
+//   pass B: per pixel with a correspondence, the photometric row weighted by
+//           the robust scale sigma from pass A; products reduced.  The last
+//           block to finish also solves A x = b in FP64 (LDL^T), applies the
+//           SE(3) exponential and writes the next pose for the following
+//           iteration, with the reference's failure and acceptance tests.
+// Reductions are deterministic: fixed per-thread pixel sets, warp shuffles,
+// block sums in shared memory, then the blocks' partial sums are added in
+// block order in FP64 by the last block (no atomics on values).
+#include "fb_internal.h"
+
+namespace fb {
+
+// ------------------------------------------------------------ row builders
+
+// ICPReduce::searchPoint + getRow (Reduction.cu:227-286).  Returns false when
+// the pixel has no correspondence.  Decisions use the order-exact float ops.
+__device__ __forceinline__ bool icp_row(const TrackLevel& L, const DevPose& cur, const DevPose& last, int x,
+                                        int y, float row[7]) {
+    const size_t i = (size_t)y * L.vp + x;
+    float4 vc4 = L.vcurr[i];
+    f3 vcurr_c = xyz(vc4);
+    if (isnan(vcurr_c.x) || (double)vcurr_c.z < 1e-3) return false;
+    f3 vcurr_g = add3(mv(cur.R, vcurr_c), cur.t);
+    f3 vcurr_p = mv(last.Rinv, sub3(vcurr_g, last.t));
+    float invz = (float)(1.0 / (double)vcurr_p.z);
+    int u = (int)((double)fa(fm(fm(vcurr_p.x, invz), L.k.fx), L.k.cx) + 0.5);
+    int v = (int)((double)fa(fm(fm(vcurr_p.y, invz), L.k.fy), L.k.cy) + 0.5);
+    if (u < 0 || v < 0 || u >= L.W || v >= L.H) return false;
+    const size_t j = (size_t)v * L.vp + u;
+    f3 vlast_c = xyz(L.vlast[j]);
+    f3 vlast_g = add3(mv(last.R, vlast_c), last.t);
+    f3 ncurr_c = xyz(L.ncurr[i]);
+    f3 ncurr_g = mv(cur.R, ncurr_c);
+    f3 nlast_c = xyz(L.nlast[j]);
+    f3 nlast_g = mv(last.R, nlast_c);
+    float dist = norm3(sub3(vlast_g, vcurr_g));
+    float sine = norm3(cross3(ncurr_g, nlast_g));
+    if (!(sine < 0.6f && dist <= 0.1f && !isnan(ncurr_c.x) && !isnan(nlast_c.x))) return false;
+    f3 nl = mv(last.Rinv, nlast_g);
+    f3 vcl = mv(last.Rinv, sub3(vcurr_g, last.t));
+    f3 vll = mv(last.Rinv, sub3(vlast_g, last.t));
+    f3 c = cross3(nl, vll);
+    row[0] = -nl.x;
+    row[1] = -nl.y;
+    row[2] = -nl.z;
+    row[3] = c.x;
+    row[4] = c.y;
+    row[5] = c.z;
+    row[6] = dot3(neg3(nl), sub3(vcl, vll));
+    return true;
+}
+
+// RGBReduction::FindCorresp (Reduction.cu:404-451).  Returns the packed
+// correspondence ((v * W + u) << 9 | (diff + 255)) of last-frame pixel (u, v),
+// or -1.
+__device__ __forceinline__ int rgb_corresp(const TrackLevel& L, const DevPose& cur, const DevPose& last, int x,
+                                           int y) {
+    const int W = L.W, H = L.H;
+    if (!(x >= 5 && x < W - 5 && y >= 5 && y < H - 5)) return -1;
+    // the window is y-2..y+1, x-2..x+1 (Reduction.cu:416-417)
+    for (int u = y - 2; u < y + 2; ++u)
+        for (int v = x - 2; v < x + 2; ++v)
+            if (L.gcurr[(size_t)u * L.gp + v] == 0) return -1;
+    int gx = L.dx[(size_t)y * L.sp + x], gy = L.dy[(size_t)y * L.sp + x];
+    if (gx == 0 && gy == 0) return -1;  // sqrtf(gx*gx + gy*gy) > 0
+    float4 vcurr = L.vcurr[(size_t)y * L.vp + x];
+    if (isnan(vcurr.x)) return -1;
+    f3 vcurr_g = add3(mv(cur.R, xyz(vcurr)), cur.t);
+    f3 vcl = mv(last.Rinv, sub3(vcurr_g, last.t));
+    float pu = fa(fd(fm(L.k.fx, vcl.x), vcl.z), L.k.cx);
+    float pv = fa(fd(fm(L.k.fy, vcl.y), vcl.z), L.k.cy);
+    int u = (int)floorf((float)((double)pu + 0.5));
+    int v = (int)floorf((float)((double)pv + 0.5));
+    if (!(u >= 0 && v >= 0 && u < W && v < H)) return -1;
+    float4 vlast = L.vlast[(size_t)v * L.vp + u];
+    if (isnan(vlast.x)) return -1;
+    float ddx = fs(vlast.x, vcurr.x), ddy = fs(vlast.y, vcurr.y), ddz = fs(vlast.z, vcurr.z),
+          ddw = fs(vlast.w, vcurr.w);
+    float nd = fsq(fa(fa(fa(fm(ddx, ddx), fm(ddy, ddy)), fm(ddz, ddz)), fm(ddw, ddw)));
+    if (!((double)nd < 0.1)) return -1;
+    int gl = L.glast[(size_t)v * L.gp + u];
+    if (gl == 0) return -1;
+    int diff = (int)L.gcurr[(size_t)y * L.gp + x] - gl;
+    return ((v * W + u) << 9) | (diff + 255);
+}
+
+// RGBReduction::GetRow (Reduction.cu:471-508)
+__device__ __forceinline__ void rgb_row(const TrackLevel& L, const DevPose& cur, const DevPose& last, int x, int y,
+                                        int packed, float sigma, float row[7]) {
+    const int j = packed >> 9;
+    const int v = j / L.W, u = j - v * L.W;
+    const int diff = (packed & 511) - 255;
+    float w = sigma + (float)abs(diff);
+    w = (double)w < 1e-3 ? 1.0f : 1.0f / w;
+    if ((double)sigma < 1e-6) w = 1.0f;
+    f3 vlast = xyz(L.vlast[(size_t)v * L.vp + u]);
+    f3 point = mv(cur.Rinv, sub3(add3(mv(last.R, vlast), last.t), cur.t));
+    const size_t k = (size_t)y * L.sp + x;
+    float gx = (float)((double)(float)L.dx[k] / 9.0);
+    float gy = (float)((double)(float)L.dy[k] / 9.0);
+    float invz = 1.0f / point.z;
+    f3 left;
+    left.x = gx * L.k.fx * invz;
+    left.y = gy * L.k.fy * invz;
+    left.z = -(left.x * point.x + left.y * point.y) * invz;
+    f3 c = cross3(point, left);
+    row[0] = w * left.x;
+    row[1] = w * left.y;
+    row[2] = w * left.z;
+    row[3] = w * c.x;
+    row[4] = w * c.y;
+    row[5] = w * c.z;
+    row[6] = -w * (float)diff;
+}
+
+__device__ __forceinline__ void add_products(const float row[7], float acc[29]) {
+    int n = 0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i)
+#pragma unroll
+        for (int j = i; j < 7; ++j) acc[n++] += row[i] * row[j];
+    acc[28] += 1.0f;
+}
+
+// ------------------------------------------------------------- reductions
+
+// Block-wide sum of NV floats (deterministic).  Result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void block_sum(float v[NV], float* smem /* [32][NV] */) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) smem[wid * NV + k] = v[k];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) v[k] = lane < nw ? smem[lane * NV + k] : 0.f;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+        }
+    }
+}
+
+__device__ __forceinline__ long long block_sum_ll(long long v, long long* smem) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) smem[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        v = lane < nw ? smem[lane] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+// Last-block-done: returns true in every thread of the last block to finish.
+__device__ __forceinline__ bool last_block(unsigned int* ticket) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int t = atomicAdd(ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+// ----------------------------------------------------------- FP64 solver
+
+// LDL^T with symmetric diagonal pivoting on a 6x6 SPD system (restates the
+// effect of Eigen's ldlt().solve used at Tracking.cc:388).
+__device__ void ldlt6(const double* Ain, const double* bin, double* x) {
+    double A[36], L[36], D[6], b[6];
+    int perm[6];
+    for (int i = 0; i < 36; ++i) { A[i] = Ain[i]; L[i] = 0; }
+    for (int i = 0; i < 6; ++i) { b[i] = bin[i]; perm[i] = i; }
+    for (int k = 0; k < 6; ++k) {
+        int p = k;
+        for (int i = k + 1; i < 6; ++i)
+            if (fabs(A[i * 6 + i]) > fabs(A[p * 6 + p])) p = i;
+        if (p != k) {
+            for (int j = 0; j < 6; ++j) { double t = A[k * 6 + j]; A[k * 6 + j] = A[p * 6 + j]; A[p * 6 + j] = t; }
+            for (int i = 0; i < 6; ++i) { double t = A[i * 6 + k]; A[i * 6 + k] = A[i * 6 + p]; A[i * 6 + p] = t; }
+            for (int j = 0; j < k; ++j) { double t = L[k * 6 + j]; L[k * 6 + j] = L[p * 6 + j]; L[p * 6 + j] = t; }
+            int t = perm[k]; perm[k] = perm[p]; perm[p] = t;
+        }
+        double d = A[k * 6 + k];
+        for (int j = 0; j < k; ++j) d -= L[k * 6 + j] * L[k * 6 + j] * D[j];
+        D[k] = d;
+        L[k * 6 + k] = 1;
+        for (int i = k + 1; i < 6; ++i) {
+            double s = A[i * 6 + k];
+            for (int j = 0; j < k; ++j) s -= L[i * 6 + j] * L[k * 6 + j] * D[j];
+            L[i * 6 + k] = s / d;
+        }
+    }
+    double y[6], z[6];
+    for (int i = 0; i < 6; ++i) {
+        double s = b[perm[i]];
+        for (int j = 0; j < i; ++j) s -= L[i * 6 + j] * y[j];
+        y[i] = s;
+    }
+    for (int i = 0; i < 6; ++i) y[i] /= D[i];
+    for (int i = 5; i >= 0; --i) {
+        double s = y[i];
+        for (int j = i + 1; j < 6; ++j) s -= L[j * 6 + i] * z[j];
+        z[i] = s;
+    }
+    for (int i = 0; i < 6; ++i) x[perm[i]] = z[i];
+}
+
+// exp of the se(3) tangent (upsilon, omega) -- the Sophus::SE3d::exp of
+// Tracking.cc:389 restated from the mathematics (Rodrigues rotation, left
+// Jacobian for the translation, Taylor series near zero).
+__device__ void se3_exp(const double* xi, double* T) {
+    const double* u = xi;
+    const double* w = xi + 3;
+    double th2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+    double th = sqrt(th2);
+    double W[9] = {0, -w[2], w[1], w[2], 0, -w[0], -w[1], w[0], 0};
+    double W2[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s = 0;
+            for (int k = 0; k < 3; ++k) s += W[i * 3 + k] * W[k * 3 + j];
+            W2[i * 3 + j] = s;
+        }
+    double a, b, c;
+    if (th < 1e-5) {
+        a = 1 - th2 / 6 + th2 * th2 / 120;
+        b = 0.5 - th2 / 24 + th2 * th2 / 720;
+        c = 1.0 / 6 - th2 / 120 + th2 * th2 / 5040;
+    } else {
+        double s = sin(th), co = cos(th);
+        a = s / th;
+        b = (1 - co) / th2;
+        c = (th - s) / (th2 * th);
+    }
+    for (int i = 0; i < 3; ++i) {
+        double vi[3];
+        for (int j = 0; j < 3; ++j) {
+            double I = (i == j) ? 1.0 : 0.0;
+            T[i * 4 + j] = I + a * W[i * 3 + j] + b * W2[i * 3 + j];
+            vi[j] = I + b * W[i * 3 + j] + c * W2[i * 3 + j];
+        }
+        T[i * 4 + 3] = vi[0] * u[0] + vi[1] * u[1] + vi[2] * u[2];
+    }
+    T[12] = T[13] = T[14] = 0;
+    T[15] = 1;
+}
+
+__device__ void mat4_mul(const double* A, const double* B, double* C) {
+    double T[16];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            double s = 0;
+            for (int k = 0; k < 4; ++k) s += A[i * 4 + k] * B[k * 4 + j];
+            T[i * 4 + j] = s;
+        }
+    for (int i = 0; i < 16; ++i) C[i] = T[i];
+}
+
+__device__ void mat4_rigid_inv(const double* A, double* B) {
+    double T[16];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) T[i * 4 + j] = A[j * 4 + i];
+    for (int i = 0; i < 3; ++i)
+        T[i * 4 + 3] = -(T[i * 4 + 0] * A[3] + T[i * 4 + 1] * A[7] + T[i * 4 + 2] * A[11]);
+    T[12] = T[13] = T[14] = 0;
+    T[15] = 1;
+    for (int i = 0; i < 16; ++i) B[i] = T[i];
+}
+
+__device__ double euler_sin_norm(const double* T) {
+    double a = atan2(-T[6], T[10]);
+    double b = atan2(T[2], sqrt(T[0] * T[0] + T[1] * T[1]));
+    double c = atan2(-T[1], T[0]);
+    double sa = sin(a), sb = sin(b), sc = sin(c);
+    return sqrt(sa * sa + sb * sb + sc * sc);
+}
+
+__device__ void unpack29(const double* s, double* A, double* b) {
+    int n = 0;
+    for (int i = 0; i < 6; ++i)
+        for (int j = i; j < 7; ++j) {
+            double v = s[n++];
+            if (j == 6)
+                b[i] = v;
+            else
+                A[j * 6 + i] = A[i * 6 + j] = v;
+        }
+}
+
+// ------------------------------------------------------------------ kernels
+
+// Frame start: the next pose starts from the last pose (TrackFrame's
+// bootstrap fallback, Tracking.cc:156-159) and delta is the identity.
+__global__ void k_track_begin(TrackState* st) {
+    for (int i = 0; i < 16; ++i) {
+        st->pose[i] = st->last_pose[i];
+        st->init_pose[i] = st->last_pose[i];
+        st->delta[i] = (i % 5 == 0) ? 1.0 : 0.0;
+    }
+    st->cur = make_dev_pose_d(st->pose);
+    st->last = make_dev_pose_d(st->last_pose);
+    st->failed = 0;
+    st->icp_error = st->rgb_error = qnan();
+    st->icp_count = st->rgb_count = 0;
+}
+
+// pass A
+__global__ void __launch_bounds__(256) k_track_a(TrackLevel L, TrackState* st, float* partials,
+                                                 unsigned int* ticket, int* residual, int do_icp, int do_rgb) {
+    if (st->failed) return;
+    __shared__ float sm[32 * 29];
+    __shared__ long long smll[32];
+    const DevPose cur = st->cur, last = st->last;
+    float acc[29];
+#pragma unroll
+    for (int k = 0; k < 29; ++k) acc[k] = 0.f;
+    long long rc = 0, rsq = 0;
+    const int N = L.W * L.H;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        const int y = p / L.W, x = p - y * L.W;
+        if (do_icp) {
+            float row[7];
+            if (icp_row(L, cur, last, x, y, row)) add_products(row, acc);
+        }
+        if (do_rgb) {
+            int r = rgb_corresp(L, cur, last, x, y);
+            residual[p] = r;
+            if (r >= 0) {
+                int d = (r & 511) - 255;
+                rc += 1;
+                rsq += d * d;
+            }
+        }
+    }
+    block_sum<29>(acc, sm);
+    long long bc = block_sum_ll(rc, smll);
+    long long bs = block_sum_ll(rsq, smll);
+    float* out = partials + (size_t)blockIdx.x * 32;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 29; ++k) out[k] = acc[k];
+        st->scratch_cnt[blockIdx.x] = bc;
+        st->scratch_sq[blockIdx.x] = bs;
+    }
+    if (!last_block(ticket)) return;
+    // final sums in FP64, block order
+    if (threadIdx.x < 29) {
+        double s = 0;
+        for (int b = 0; b < gridDim.x; ++b) s += (double)partials[(size_t)b * 32 + threadIdx.x];
+        st->icp_sums[threadIdx.x] = s;
+    }
+    if (threadIdx.x == 32) {
+        long long c = 0, q = 0;
+        for (int b = 0; b < gridDim.x; ++b) { c += st->scratch_cnt[b]; q += st->scratch_sq[b]; }
+        st->rgb_cnt = c;
+        st->rgb_sq = q;
+        // sigma = sqrt((float) sum / count) on the host in the reference (Reduction.cu:608)
+        st->sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
+        *ticket = 0;
+    }
+}
+
+// pass B + solve
+__global__ void __launch_bounds__(256) k_track_b(TrackLevel L, TrackState* st, float* partials,
+                                                 unsigned int* ticket, const int* residual, int min_count,
+                                                 int do_icp, int do_rgb, int is_final) {
+    if (st->failed) return;
+    __shared__ float sm[32 * 29];
+    const DevPose cur = st->cur, last = st->last;
+    const float sigma = st->sigma;
+    float acc[29];
+#pragma unroll
+    for (int k = 0; k < 29; ++k) acc[k] = 0.f;
+    const int N = L.W * L.H;
+    if (do_rgb) {
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+            int r = residual[p];
+            if (r < 0) continue;
+            const int y = p / L.W, x = p - y * L.W;
+            float row[7];
+            rgb_row(L, cur, last, x, y, r, sigma, row);
+            add_products(row, acc);
+        }
+    }
+    block_sum<29>(acc, sm);
+    float* out = partials + (size_t)blockIdx.x * 32;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < 29; ++k) out[k] = acc[k];
+    if (!last_block(ticket)) return;
+    __shared__ double sums[29];
+    if (threadIdx.x < 29) {
+        double s = 0;
+        for (int b = 0; b < gridDim.x; ++b) s += (double)partials[(size_t)b * 32 + threadIdx.x];
+        sums[threadIdx.x] = s;
+        st->rgb_sums[threadIdx.x] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    *ticket = 0;
+    // Tracking.cc:319-394
+    bool fail = false;
+    if (do_rgb) {
+        float r0 = (float)sums[27], r1 = (float)sums[28];
+        float err = sqrtf(r0) / r1;
+        st->rgb_error = err;
+        st->rgb_count = r1;
+        if (isnan(err) || (int)r1 < min_count) fail = true;
+    }
+    float icp_err = st->icp_error;
+    if (!fail && do_icp) {
+        float q0 = (float)st->icp_sums[27], q1 = (float)st->icp_sums[28];
+        icp_err = sqrtf(q0) / q1;
+        st->icp_error = icp_err;
+        st->icp_count = q1;
+        if (isnan(icp_err) || (int)q1 < min_count) fail = true;
+    }
+    if (fail) {
+        for (int i = 0; i < 16; ++i) st->pose[i] = st->last_pose[i];
+        st->failed = 1;
+        return;
+    }
+    double Ar[36], br[6], Ai[36], bi[6], A[36], b[6], x[6], dT[16], dinv[16];
+    for (int i = 0; i < 36; ++i) Ar[i] = Ai[i] = 0;
+    for (int i = 0; i < 6; ++i) br[i] = bi[i] = 0;
+    if (do_rgb) unpack29(sums, Ar, br);
+    if (do_icp) unpack29(st->icp_sums, Ai, bi);
+    const float w = 1e-4f;
+    for (int i = 0; i < 36; ++i) A[i] = Ar[i] * (double)w + Ai[i];
+    for (int i = 0; i < 6; ++i) b[i] = br[i] * (double)w + bi[i];
+    ldlt6(A, b, x);
+    se3_exp(x, dT);
+    mat4_mul(dT, st->delta, st->delta);
+    mat4_rigid_inv(st->delta, dinv);
+    mat4_mul(st->last_pose, dinv, st->pose);
+    st->cur = make_dev_pose_d(st->pose);
+    if (is_final) {
+        // acceptance test (Tracking.cc:398-408)
+        double pinv[16], p[16];
+        mat4_rigid_inv(st->init_pose, pinv);
+        mat4_mul(pinv, st->pose, p);
+        double tn = sqrt(p[3] * p[3] + p[7] * p[7] + p[11] * p[11]);
+        if (!(icp_err < 0.0001f && euler_sin_norm(p) <= 0.1 && tn <= 0.1)) {
+            for (int i = 0; i < 16; ++i) st->pose[i] = st->last_pose[i];
+            st->failed = 1;
+        }
+    }
+}
+
+// Single-step entry points (the reference's ICPStep / RGBStep): reduce the
+// sums of one pass into out[29] (+ rgb count / sum of squares) in FP64.
+__global__ void __launch_bounds__(256) k_step_icp(TrackLevel L, DevPose cur, DevPose last, float* partials,
+                                                  unsigned int* ticket, double* out) {
+    __shared__ float sm[32 * 29];
+    float acc[29];
+#pragma unroll
+    for (int k = 0; k < 29; ++k) acc[k] = 0.f;
+    const int N = L.W * L.H;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        const int y = p / L.W, x = p - y * L.W;
+        float row[7];
+        if (icp_row(L, cur, last, x, y, row)) add_products(row, acc);
+    }
+    block_sum<29>(acc, sm);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < 29; ++k) partials[(size_t)blockIdx.x * 32 + k] = acc[k];
+    if (!last_block(ticket)) return;
+    if (threadIdx.x < 29) {
+        double s = 0;
+        for (int b = 0; b < gridDim.x; ++b) s += (double)partials[(size_t)b * 32 + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+    if (threadIdx.x == 0) *ticket = 0;
+}
+
+__global__ void __launch_bounds__(256) k_step_rgb_a(TrackLevel L, DevPose cur, DevPose last, long long* partials,
+                                                    unsigned int* ticket, int* residual, double* out) {
+    __shared__ long long smll[32];
+    long long rc = 0, rsq = 0;
+    const int N = L.W * L.H;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        const int y = p / L.W, x = p - y * L.W;
+        int r = rgb_corresp(L, cur, last, x, y);
+        residual[p] = r;
+        if (r >= 0) {
+            int d = (r & 511) - 255;
+            rc += 1;
+            rsq += d * d;
+        }
+    }
+    long long bc = block_sum_ll(rc, smll);
+    long long bs = block_sum_ll(rsq, smll);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = bc;
+        partials[2 * blockIdx.x + 1] = bs;
+    }
+    if (!last_block(ticket)) return;
+    if (threadIdx.x == 0) {
+        long long c = 0, q = 0;
+        for (int b = 0; b < gridDim.x; ++b) { c += partials[2 * b]; q += partials[2 * b + 1]; }
+        out[29] = (double)c;
+        out[30] = (double)q;
+        out[31] = sqrtf((float)q / (float)(c == 0 ? 1 : c));
+        *ticket = 0;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_step_rgb_b(TrackLevel L, DevPose cur, DevPose last, float* partials,
+                                                    unsigned int* ticket, const int* residual, double* out) {
+    __shared__ float sm[32 * 29];
+    const float sigma = (float)out[31];
+    float acc[29];
+#pragma unroll
+    for (int k = 0; k < 29; ++k) acc[k] = 0.f;
+    const int N = L.W * L.H;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        int r = residual[p];
+        if (r < 0) continue;
+        const int y = p / L.W, x = p - y * L.W;
+        float row[7];
+        rgb_row(L, cur, last, x, y, r, sigma, row);
+        add_products(row, acc);
+    }
+    block_sum<29>(acc, sm);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < 29; ++k) partials[(size_t)blockIdx.x * 32 + k] = acc[k];
+    if (!last_block(ticket)) return;
+    if (threadIdx.x < 29) {
+        double s = 0;
+        for (int b = 0; b < gridDim.x; ++b) s += (double)partials[(size_t)b * 32 + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+    if (threadIdx.x == 0) *ticket = 0;
+}
+
+// ---------------------------------------------------------------- launchers
+
+int track_grid(int n) {
+    int g = (n + 255) / 256;
+    return g < kTrackMaxBlocks ? g : kTrackMaxBlocks;
+}
+
+int launch_track_begin(TrackState* st, cudaStream_t s) { k_track_begin<<<1, 1, 0, s>>>(st);
+    return 1;
+}
+
+int launch_track_iter(const TrackLevel& L, TrackState* st, float* partials, unsigned int* tickets, int* residual,
+                       int min_count, bool is_final, cudaStream_t s) {
+    const int g = track_grid(L.W * L.H);
+    k_track_a<<<g, 256, 0, s>>>(L, st, partials, tickets + 0, residual, 1, 1);
+    k_track_b<<<g, 256, 0, s>>>(L, st, partials, tickets + 1, residual, min_count, 1, 1, is_final ? 1 : 0);
+    return 2;
+}
+
+int launch_step_icp(const TrackLevel& L, const DevPose& cur, const DevPose& last, float* partials,
+                     unsigned int* ticket, double* out, cudaStream_t s) {
+    k_step_icp<<<track_grid(L.W * L.H), 256, 0, s>>>(L, cur, last, partials, ticket, out);
+    return 1;
+}
+
+int launch_step_rgb(const TrackLevel& L, const DevPose& cur, const DevPose& last, float* partials,
+                     unsigned int* tickets, int* residual, double* out, cudaStream_t s) {
+    const int g = track_grid(L.W * L.H);
+    k_step_rgb_a<<<g, 256, 0, s>>>(L, cur, last, (long long*)partials, tickets + 0, residual, out);
+    k_step_rgb_b<<<g, 256, 0, s>>>(L, cur, last, partials, tickets + 1, residual, out);
+    return 2;
+}
+
+}  // namespace fb

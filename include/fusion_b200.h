@@ -1,0 +1,240 @@
+/*
+ * fusion_b200 -- C ABI of the B200 implementation of the per-frame dense
+ * RGB-D fusion path of cnxyang/Fusion: depth/intensity pyramid, projective
+ * ICP + photometric tracking, voxel-block hash allocation, TSDF/colour
+ * integration and hash-table raycasting.
+ *
+ * Two groups of entry points:
+ *   1. A session API: one session owns the frames, the tracker state and the
+ *      voxel-block map of one camera, and runs the reference's per-frame
+ *      System::GrabImage (Core/System.cc:92-138) on the GPU.
+ *   2. Per-stage entry points with the meaning of the reference's kernel
+ *      free functions (Tracking/Reduction.h:18-83, Mapping/RenderScene.h:3-52)
+ *      over plain device pointers with pitches, so that the reference's host
+ *      classes (Frame, Tracker, Mapping) can call them through a thin shim.
+ *
+ * All functions return a status code (FB_OK = 0) and never terminate the
+ * process (the reference's SafeCall exits, Utility/SafeCall.h:13-21).
+ * Images are row-major; `pitch` is in bytes.  `stream` is a cudaStream_t or
+ * NULL for the session's / the default stream.
+ */
+#ifndef FUSION_B200_H
+#define FUSION_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FB_API __attribute__((visibility("default")))
+#else
+#define FB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FB_OK 0
+#define FB_EINVAL 1        /* bad argument */
+#define FB_ENOMEM 2        /* device or pinned allocation failed */
+#define FB_ECUDA 3         /* a CUDA call failed; see fb_last_error() */
+#define FB_ETRACK_LOST 4   /* frame not tracked (the tracker rolled back) */
+
+/* device-side error flags reported in fb_frame_result.error_flags (sticky) */
+#define FB_ERR_HEAP_EXHAUSTED 0x1u    /* voxel-block pool full: blocks not allocated */
+#define FB_ERR_EXCESS_FULL 0x2u       /* excess list full: blocks not allocated */
+#define FB_ERR_REQUEST_SET_FULL 0x4u  /* per-frame block-request set overflowed */
+#define FB_ERR_COORD_RANGE 0x8u       /* a block beyond +-32767 blocks was skipped */
+#define FB_ERR_NEW_LIST_FULL 0x10u    /* more new blocks in one frame than the pool */
+#define FB_ERR_VISIBLE_FULL 0x20u     /* visible list full */
+#define FB_ERR_SEQUENTIAL_INSERT 0x40u /* pool/excess edge case: exact sequential insert used */
+
+/* Runtime form of the reference's compile-time constants:
+ * Mapping/DeviceMap.h:135-151 (voxel size, truncation, depth range, table
+ * sizes), Tracking/Tracking.h:98-100 (iterations per pyramid level),
+ * Core/Frame.cc:13-14 and Core/System.h:16-27 (depth scale / cutoff, camera). */
+typedef struct fb_config {
+    int width, height;          /* level-0 image size */
+    float fx, fy, cx, cy;       /* level-0 intrinsics */
+    float depth_scale;          /* depth units per metre (Frame::mDepthScale) */
+    float depth_cutoff;         /* pyramid depth cutoff, m (Frame::mDepthCutoff) */
+    float voxel_size;           /* m (DeviceMap::VoxelSize) */
+    float trunc_dist;           /* m (DeviceMap::TruncateDist) */
+    float depth_min, depth_max; /* fusion depth range, m (DeviceMap::DepthMin/Max) */
+    int num_buckets;            /* hash buckets (DeviceMap::NumBuckets) */
+    int num_excess;             /* excess-list entries (DeviceMap::NumExcess) */
+    int num_blocks;             /* voxel blocks of 8^3 in the pool (DeviceMap::NumSdfBlocks) */
+    int iters[3];               /* Gauss-Newton iterations at levels 0, 1, 2 */
+} fb_config;
+
+/* Result of one frame (System::GrabImage). */
+typedef struct fb_frame_result {
+    int status;              /* FB_OK, or FB_ETRACK_LOST when not tracked */
+    int tracked;             /* Tracker::GrabFrame result */
+    int tracker_state;       /* Tracker::state: 1 initialising, 0 tracking, -1 lost */
+    int fused;               /* the frame was integrated into the map */
+    uint32_t no_visible;     /* visible blocks (FuseMapColor's host_data) */
+    uint32_t no_allocated;   /* entries in the map */
+    uint32_t no_new;         /* blocks allocated by this frame */
+    uint32_t error_flags;    /* FB_ERR_* */
+    float icp_error, icp_count, rgb_error, rgb_count;  /* last Gauss-Newton iteration */
+    double pose[16];         /* camera-to-world pose, row-major (Frame::pose) */
+    uint64_t frame_id;
+} fb_frame_result;
+
+typedef struct fb_session fb_session;
+
+/* ---------------------------------------------------------------- session */
+
+/* The reference's defaults for a width x height camera: 6 mm voxels,
+ * truncation 8 voxels, depth 0.1-3.0 m, 1e6 buckets, 5e5 excess entries,
+ * 7e5 blocks, iterations {10, 5, 3}, fx = fy = 525 * width / 640. */
+FB_API void fb_default_config(fb_config* cfg, int width, int height);
+FB_API const char* fb_status_string(int status);
+/* Text of the last CUDA error seen by this library in the calling thread. */
+FB_API const char* fb_last_error(void);
+/* Device bytes a session with this configuration allocates. */
+FB_API size_t fb_session_bytes(const fb_config* cfg);
+
+/* Replaces: System::System (Core/System.cc:16-73) -- Mapping::Create,
+ * Tracker::Tracker, Frame::Create. stream: cudaStream_t or NULL (a stream is
+ * created). */
+FB_API int fb_session_create(const fb_config* cfg, void* stream, fb_session** out);
+FB_API int fb_session_destroy(fb_session* s);
+/* Replaces: System::RebootSystem / Mapping::Reset + Tracker::ResetTracking. */
+FB_API int fb_session_reset(fb_session* s);
+
+/* Replaces: System::GrabImage (Core/System.cc:92-138), without the viewer's
+ * RenderTopDown and the SURF key points.  depth: u16 in 1/depth_scale m;
+ * rgb: packed RGB8.  on_device = 0: host pointers (copied in), 1: device
+ * pointers.  Synchronous: returns when the frame is done. */
+FB_API int fb_grab_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, const uint8_t* rgb,
+                  size_t rgb_pitch, int on_device, fb_frame_result* out);
+
+/* Tracing (the reference has none; Utility/StopWatch.h is never called):
+ * with profiling on, every frame records CUDA events around its stages and
+ * accumulates device milliseconds per stage: 0 resize of the last frame's
+ * maps, 1 pyramid, 2 tracking, 3 block allocation, 4 visibility,
+ * 5 integration, 6 z ranges, 7 raycast.  Switching it on resets the sums. */
+FB_API int fb_session_set_profiling(fb_session* s, int on);
+FB_API int fb_session_stage_times(fb_session* s, double* ms, uint64_t* calls, int n);
+/* Kernels this session has launched so far. */
+FB_API int fb_session_launch_count(fb_session* s, uint64_t* launches);
+/* Bytes fb_grab_frame moves per frame with host inputs: h2d = depth + rgb,
+ * d2h = the frame result read back. */
+FB_API int fb_frame_transfer_bytes(const fb_config* cfg, size_t* h2d, size_t* d2h);
+
+/* Pose of the last tracked frame (LastFrame->pose). */
+FB_API int fb_get_pose(fb_session* s, double pose[16]);
+
+/* Download one pyramid level of the last (which = 0) or next (1) frame to
+ * host memory; any pointer may be NULL.  vmap/nmap: float4 per pixel. */
+FB_API int fb_download_level(fb_session* s, int which, int level, float* vmap, float* nmap, float* depth,
+                      uint8_t* gray, int16_t* dx, int16_t* dy);
+/* Raw (unfiltered) level-0 depth of a frame, metres (Frame::range). */
+FB_API int fb_download_raw(fb_session* s, int which, float* raw);
+
+typedef struct fb_map_stats {
+    int32_t heap_counter;   /* DeviceMap heapCounter */
+    int32_t entry_ptr;      /* DeviceMap entryPtr */
+    uint32_t no_allocated, no_visible, no_new, no_tiles, error_flags;
+    int32_t sequential;     /* last allocation used the exact sequential path */
+} fb_map_stats;
+FB_API int fb_map_get_stats(fb_session* s, fb_map_stats* out);
+/* All hash slots as {x, y, z, ptr, offset} with ptr a voxel index (block *
+ * 512) or -1, in the reference's HashEntry order; entries has room for
+ * (num_buckets + num_excess) * 5 ints. */
+FB_API int fb_map_download_entries(fb_session* s, int32_t* entries);
+/* Voxels of n blocks given by voxel-index ptrs: sdf, weight, rgb (n*512). */
+FB_API int fb_map_download_blocks(fb_session* s, const int32_t* ptrs, int n, float* sdf, uint8_t* weight,
+                           uint8_t* rgb);
+/* Slots of the visible entries of the last fusion / visibility pass. */
+FB_API int fb_map_download_visible(fb_session* s, int32_t* slots, uint32_t capacity, uint32_t* n);
+
+/* -------------------------------------------------------- per-stage entries
+ * Device images with pitches; the meaning of each argument is that of the
+ * reference function named in the comment. */
+
+typedef struct fb_image {
+    void* data;     /* device pointer */
+    size_t pitch;   /* bytes between rows */
+    int cols, rows;
+} fb_image;
+
+/* Replaces: FilterDepth (Tracking/Pyrdown.cu:43-54). depth: u16; raw,
+ * filtered: float. */
+FB_API int fb_filter_depth(const fb_image* depth, fb_image* raw, fb_image* filtered, float depth_scale,
+                    float depth_cutoff, void* stream);
+/* Replaces: ImageToIntensity (Tracking/Pyrdown.cu:195-205). rgb: uchar3; gray: u8. */
+FB_API int fb_image_to_intensity(const fb_image* rgb, fb_image* gray, void* stream);
+/* Replaces: PyrDownGauss(float) (Tracking/Pyrdown.cu:160-169). */
+FB_API int fb_pyrdown_gauss_f32(const fb_image* src, fb_image* dst, void* stream);
+/* Replaces: PyrDownGauss(uchar) (Tracking/Pyrdown.cu:171-181). */
+FB_API int fb_pyrdown_gauss_u8(const fb_image* src, fb_image* dst, void* stream);
+/* Replaces: ComputeVMap (Tracking/Pyrdown.cu:80-91). vmap: float4. */
+FB_API int fb_compute_vmap(const fb_image* depth, fb_image* vmap, float fx, float fy, float cx, float cy,
+                    float depth_cutoff, void* stream);
+/* Replaces: ComputeNMap (Tracking/Pyrdown.cu:116-125). */
+FB_API int fb_compute_nmap(const fb_image* vmap, fb_image* nmap, void* stream);
+/* Replaces: ComputeDerivativeImage (Tracking/Pyrdown.cu:239-249). dx, dy: int16. */
+FB_API int fb_compute_derivative_image(const fb_image* gray, fb_image* dx, fb_image* dy, void* stream);
+/* Replaces: ResizeMap (Tracking/Pyrdown.cu:281-291). */
+FB_API int fb_resize_map(const fb_image* vsrc, const fb_image* nsrc, fb_image* vdst, fb_image* ndst,
+                  void* stream);
+
+/* Scratch the two step functions need, like the reference's sum / out /
+ * sumRes / outRes arrays and the per-call Residual buffer
+ * (Tracking/Tracking.cc:29-34, Reduction.cu:572). */
+FB_API size_t fb_step_scratch_bytes(int cols, int rows);
+
+/* Replaces: ICPStep (Tracking/Reduction.cu:319-375).  R* are row-major 3x3
+ * (Matrix3f), t* 3-vectors, K = {fx, fy, cx, cy} of the level.  Outputs on
+ * the host as the reference's: residual = {sum of squared point-to-plane
+ * residuals, correspondence count}, A (6x6 row-major), b (6).
+ * Synchronous. */
+FB_API int fb_icp_step(const fb_image* vcurr, const fb_image* vlast, const fb_image* ncurr,
+                const fb_image* nlast, const float Rcurr[9], const float tcurr[3], const float Rlast[9],
+                const float RlastInv[9], const float tlast[3], const float K[4], void* scratch,
+                size_t scratch_bytes, float residual[2], double A[36], double b[6], void* stream);
+
+/* Replaces: RGBStep (Tracking/Reduction.cu:547-627).  gray: u8, dx/dy: int16
+ * of the current frame.  Synchronous. */
+FB_API int fb_rgb_step(const fb_image* gcurr, const fb_image* glast, const fb_image* vcurr,
+                const fb_image* vlast, const fb_image* dx, const fb_image* dy, const float Rcurr[9],
+                const float RcurrInv[9], const float Rlast[9], const float RlastInv[9],
+                const float tcurr[3], const float tlast[3], const float K[4], void* scratch,
+                size_t scratch_bytes, float residual[2], double A[36], double b[6], void* stream);
+
+/* Replaces: ResetMap (Mapping/FuseMap.cu:352-364) on the session's map. */
+FB_API int fb_reset_map(fb_session* s);
+
+/* Replaces: FuseMapColor (Mapping/FuseMap.cu:251-319) on the session's map:
+ * block allocation, visibility and integration of one frame.  depth: raw
+ * float depth; rgb: uchar3; nmap: float4; Rview/RviewInv row-major; K =
+ * {fx, fy, cx, cy}; depth range from the session config.  no_visible:
+ * visible block count (host). */
+FB_API int fb_fuse_map_color(fb_session* s, const fb_image* depth, const fb_image* rgb, const fb_image* nmap,
+                      const float Rview[9], const float RviewInv[9], const float tview[3],
+                      const float K[4], uint32_t* no_visible, void* stream);
+
+/* Replaces: CheckBlockVisibility (Mapping/FuseMap.cu:206-249) for a cols x
+ * rows camera. */
+FB_API int fb_check_block_visibility(fb_session* s, const float Rview[9], const float RviewInv[9],
+                              const float tview[3], int cols, int rows, const float K[4],
+                              uint32_t* no_visible, void* stream);
+
+/* Replaces: CreateRenderingBlocks + Raycast (Mapping/RenderScene.cu:199-276,
+ * 447-489) as called by Mapping::RayTrace (Mapping/Mapping.cc:98-109): z
+ * ranges of the visible blocks, then the raycast into vmap/nmap (float4,
+ * camera frame).  Returns with *rendered = 0 and the maps untouched when no
+ * rendering rectangle was produced. */
+FB_API int fb_raycast(fb_session* s, fb_image* vmap, fb_image* nmap, const float Rview[9],
+               const float RviewInv[9], const float tview[3], const float K[4], int* rendered,
+               void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FUSION_B200_H */
