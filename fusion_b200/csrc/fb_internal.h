@@ -131,6 +131,7 @@ struct MapView {
 };
 
 constexpr int kScanChunk = 4096;
+constexpr int kMinNewBlocks = 1 << 16;
 
 int launch_map_reset(const MapView& m, cudaStream_t s);
 // pose: device pointer; skip: device flag (nonzero: do nothing), may be null

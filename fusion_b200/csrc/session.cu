@@ -392,9 +392,10 @@ size_t fb_session_bytes(const fb_config* c) {
     }
     frame += px * (2 + 3 + 4);
     size_t NS = c->num_blocks, NB = c->num_buckets, NE = c->num_excess;
-    size_t reqcap = next_pow2(2 * NS > 4096 ? 2 * NS : 4096);
+    size_t newcap = NS > (size_t)kMinNewBlocks ? NS : (size_t)kMinNewBlocks;
+    size_t reqcap = next_pow2(2 * newcap);
     size_t map = (NB + NE) * sizeof(HEntry) + NS * 4 + NS * 512 * sizeof(Voxel) + 2 * NS * 4 + reqcap * 8 +
-                 NS * sizeof(NewBlock) + 2 * NS * 4 + 3 * NB * 4;
+                 newcap * (sizeof(NewBlock) + 8) + 3 * NB * 4;
     return 2 * frame + map + px * 4 + kTrackMaxBlocks * 32 * 4 + sizeof(TrackState);
 }
 
@@ -445,8 +446,11 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
         m.NB = cfg->num_buckets;
         m.NE = cfg->num_excess;
         m.NS = cfg->num_blocks;
-        m.reqcap = (int)next_pow2((size_t)2 * m.NS > 4096 ? (size_t)2 * m.NS : 4096);
-        m.newcap = m.NS;
+        // new blocks of one frame: at least kMinNewBlocks whatever the pool
+        // size, so that a frame needing more blocks than the pool still lists
+        // all of them and the exhaustion is handled by the exact sequential path
+        m.newcap = m.NS > kMinNewBlocks ? m.NS : kMinNewBlocks;
+        m.reqcap = (int)next_pow2((size_t)2 * m.newcap);
         m.nchunks = (m.NB + kScanChunk - 1) / kScanChunk;
         m.zc = (cfg->width + 7) / 8;
         m.zr = (cfg->height + 7) / 8;

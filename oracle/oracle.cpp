@@ -1206,6 +1206,38 @@ int fbo_system_level(void* sp, int which, int lv, float* vm, float* nm, float* d
     if (dy) std::memcpy(dy, l.dy.data(), 2 * n);
     return 0;
 }
+int fbo_track(const fbo_config* c, const float* const* nv, const float* const* nn,
+              const uint8_t* const* ng, const int16_t* const* ndx, const int16_t* const* ndy,
+              const float* const* lv, const float* const* ln, const uint8_t* const* lg,
+              const double* last_pose, double* out_pose, double* info) {
+    fbo_config cc = *c;
+    cc.num_buckets = 1;
+    cc.num_excess = 0;
+    cc.num_blocks = 1;
+    System s(cc);
+    for (int l = 0; l < 3; ++l) {
+        Level &N = s.next->lv[l], &L = s.last->lv[l];
+        size_t n = (size_t)N.W * N.H;
+        std::memcpy(N.vmap.data(), nv[l], 16 * n);
+        std::memcpy(N.nmap.data(), nn[l], 16 * n);
+        std::memcpy(N.image.data(), ng[l], n);
+        std::memcpy(N.dx.data(), ndx[l], 2 * n);
+        std::memcpy(N.dy.data(), ndy[l], 2 * n);
+        std::memcpy(L.vmap.data(), lv[l], 16 * n);
+        std::memcpy(L.nmap.data(), ln[l], 16 * n);
+        std::memcpy(L.image.data(), lg[l], n);
+    }
+    std::memcpy(s.last->pose, last_pose, 16 * sizeof(double));
+    std::memcpy(s.next->pose, last_pose, 16 * sizeof(double));
+    bool ok = c->precision == 32 ? compute_se3<float>(s) : compute_se3<double>(s);
+    std::memcpy(out_pose, s.next->pose, 16 * sizeof(double));
+    if (info) {
+        info[0] = ok; info[1] = s.lastIcpError; info[2] = s.lastIcpCount; info[3] = s.lastRgbError;
+        info[4] = s.lastRgbCount;
+    }
+    return 0;
+}
+
 int fbo_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

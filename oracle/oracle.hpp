@@ -105,6 +105,16 @@ void* fbo_system_map(void* s);
 // level maps of frame `which` (0 = last, 1 = next); any output may be NULL
 int fbo_system_level(void* s, int which, int level, float* vmap, float* nmap, float* depth,
                      uint8_t* image, int16_t* dx, int16_t* dy);
+// Tracker::ComputeSE3 alone on given inputs (teacher forcing): the next
+// frame's level maps (vertex, normal, gray, Sobel x/y) and the last frame's
+// (vertex, normal, gray), three levels each, and the last pose.  out_pose is
+// the next frame's pose (rolled back to last_pose on failure); info: [0] ok,
+// [1] icp error, [2] icp count, [3] rgb error, [4] rgb count.
+int fbo_track(const fbo_config* cfg, const float* const* next_vmap, const float* const* next_nmap,
+              const uint8_t* const* next_gray, const int16_t* const* next_dx,
+              const int16_t* const* next_dy, const float* const* last_vmap,
+              const float* const* last_nmap, const uint8_t* const* last_gray,
+              const double* last_pose, double* out_pose, double* info);
 int fbo_num_threads(void);
 }
 

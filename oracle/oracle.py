@@ -301,5 +301,27 @@ class System:
         return out
 
 
+def track(cfg, nxt, last, last_pose):
+    """Tracker::ComputeSE3 on given inputs.  nxt / last: lists of three dicts
+    (levels 0-2) with vmap, nmap, image (+ dx, dy for nxt).  Returns
+    (pose, info[ok, icp_err, icp_count, rgb_err, rgb_count])."""
+    keep = []
+
+    def arr(lst, key, dtype):
+        ptrs = (ctypes.c_void_p * 3)()
+        for i in range(3):
+            a = np.ascontiguousarray(lst[i][key], dtype)
+            keep.append(a)
+            ptrs[i] = a.ctypes.data
+        return ptrs
+    out = np.zeros((4, 4), np.float64)
+    info = np.zeros(5, np.float64)
+    lib().fbo_track(ctypes.byref(cfg), arr(nxt, "vmap", np.float32), arr(nxt, "nmap", np.float32),
+                    arr(nxt, "image", np.uint8), arr(nxt, "dx", np.int16), arr(nxt, "dy", np.int16),
+                    arr(last, "vmap", np.float32), arr(last, "nmap", np.float32), arr(last, "image", np.uint8),
+                    _p(np.ascontiguousarray(last_pose, np.float64)), _p(out), _p(info))
+    return out, info
+
+
 def num_threads():
     return int(lib().fbo_num_threads())
