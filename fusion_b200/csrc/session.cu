@@ -438,7 +438,7 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
                  dalloc(s, &F.gray[l], n) && dalloc(s, &F.dx[l], n) && dalloc(s, &F.dy[l], n);
         }
     }
-    ok = ok && dalloc(s, &s->st, 1) && dalloc(s, &s->partials, (size_t)kTrackMaxBlocks * 32) &&
+    ok = ok && dalloc(s, &s->st, 1) && dalloc(s, &s->partials, (size_t)2 * kTrackMaxBlocks * 32) &&
          dalloc(s, &s->tickets, 4) && dalloc(s, &s->residual, (size_t)s->W[0] * s->H[0]) &&
          dalloc(s, &s->scratch_pose, 1) && dalloc(s, &s->d_out, 1);
     MapView& m = s->map;

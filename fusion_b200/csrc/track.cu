@@ -330,9 +330,34 @@ __global__ void k_track_begin(TrackState* st) {
     st->icp_count = st->rgb_count = 0;
 }
 
-// pass A
-__global__ void __launch_bounds__(256) k_track_a(TrackLevel L, TrackState* st, float* partials,
-                                                 unsigned int* ticket, int* residual, int do_icp, int do_rgb) {
+// Fixed-order FP64 sum of nv values over nb block partials laid out as
+// partials[b * stride + v], computed by the whole block: thread t sums value
+// (t % 32) over the block chunk (t / 32), then the 8 chunk sums are added in
+// order.  Deterministic for a given nb.  out: shared array of nv doubles.
+__device__ void reduce_partials(const float* __restrict__ partials, int nb, int stride, int nv, double* out,
+                                double* scratch /* [8][32] shared */) {
+    const int v = threadIdx.x & 31, c = threadIdx.x >> 5, nc = blockDim.x >> 5;
+    const int per = (nb + nc - 1) / nc;
+    for (int v0 = 0; v0 < nv; v0 += 32) {
+        double s = 0;
+        if (v0 + v < nv) {
+            const int b0 = c * per, b1 = min(nb, b0 + per);
+#pragma unroll 8
+            for (int b = b0; b < b1; ++b) s += (double)partials[(size_t)b * stride + v0 + v];
+        }
+        scratch[c * 32 + v] = s;
+        __syncthreads();
+        if (c == 0 && v0 + v < nv) {
+            double t = 0;
+            for (int q = 0; q < nc; ++q) t += scratch[q * 32 + v];
+            out[v0 + v] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// pass A: ICP rows and RGB correspondences; per-block partial sums only.
+__global__ void __launch_bounds__(256) k_track_a(TrackLevel L, TrackState* st, float* partials, int* residual) {
     if (st->failed) return;
     __shared__ float sm[32 * 29];
     __shared__ long long smll[32];
@@ -344,98 +369,93 @@ __global__ void __launch_bounds__(256) k_track_a(TrackLevel L, TrackState* st, f
     const int N = L.W * L.H;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
         const int y = p / L.W, x = p - y * L.W;
-        if (do_icp) {
-            float row[7];
-            if (icp_row(L, cur, last, x, y, row)) add_products(row, acc);
-        }
-        if (do_rgb) {
-            int r = rgb_corresp(L, cur, last, x, y);
-            residual[p] = r;
-            if (r >= 0) {
-                int d = (r & 511) - 255;
-                rc += 1;
-                rsq += d * d;
-            }
+        float row[7];
+        if (icp_row(L, cur, last, x, y, row)) add_products(row, acc);
+        int r = rgb_corresp(L, cur, last, x, y);
+        residual[p] = r;
+        if (r >= 0) {
+            int d = (r & 511) - 255;
+            rc += 1;
+            rsq += d * d;
         }
     }
     block_sum<29>(acc, sm);
     long long bc = block_sum_ll(rc, smll);
     long long bs = block_sum_ll(rsq, smll);
-    float* out = partials + (size_t)blockIdx.x * 32;
     if (threadIdx.x == 0) {
+        float* out = partials + (size_t)blockIdx.x * 32;
 #pragma unroll
         for (int k = 0; k < 29; ++k) out[k] = acc[k];
         st->scratch_cnt[blockIdx.x] = bc;
         st->scratch_sq[blockIdx.x] = bs;
     }
-    if (!last_block(ticket)) return;
-    // final sums in FP64, block order
-    if (threadIdx.x < 29) {
-        double s = 0;
-        for (int b = 0; b < gridDim.x; ++b) s += (double)partials[(size_t)b * 32 + threadIdx.x];
-        st->icp_sums[threadIdx.x] = s;
-    }
-    if (threadIdx.x == 32) {
-        long long c = 0, q = 0;
-        for (int b = 0; b < gridDim.x; ++b) { c += st->scratch_cnt[b]; q += st->scratch_sq[b]; }
-        st->rgb_cnt = c;
-        st->rgb_sq = q;
-        // sigma = sqrt((float) sum / count) on the host in the reference (Reduction.cu:608)
-        st->sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
-        *ticket = 0;
-    }
 }
 
-// pass B + solve
-__global__ void __launch_bounds__(256) k_track_b(TrackLevel L, TrackState* st, float* partials,
-                                                 unsigned int* ticket, const int* residual, int min_count,
-                                                 int do_icp, int do_rgb, int is_final) {
+// pass B: every block derives sigma from pass A's counts (same value in every
+// block), builds the RGB rows, and the last block reduces both passes'
+// partials in FP64 and solves.
+__global__ void __launch_bounds__(256) k_track_b(TrackLevel L, TrackState* st, float* partials, unsigned int* ticket,
+                                                 const int* residual, int min_count, int is_final) {
     if (st->failed) return;
     __shared__ float sm[32 * 29];
+    __shared__ long long smll[32];
+    __shared__ double scratch[8 * 32];
+    __shared__ double sums[64];
     const DevPose cur = st->cur, last = st->last;
-    const float sigma = st->sigma;
+    const int G = gridDim.x;
+    // sigma = sqrt((float) sum / count) (Reduction.cu:606-608), sums in block order
+    long long c = 0, q = 0;
+    for (int b = threadIdx.x; b < G; b += blockDim.x) {
+        c += st->scratch_cnt[b];
+        q += st->scratch_sq[b];
+    }
+    c = block_sum_ll(c, smll);
+    q = block_sum_ll(q, smll);
+    __shared__ float s_sigma;
+    if (threadIdx.x == 0) s_sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
+    __syncthreads();
+    const float sigma = s_sigma;
     float acc[29];
 #pragma unroll
     for (int k = 0; k < 29; ++k) acc[k] = 0.f;
     const int N = L.W * L.H;
-    if (do_rgb) {
-        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
-            int r = residual[p];
-            if (r < 0) continue;
-            const int y = p / L.W, x = p - y * L.W;
-            float row[7];
-            rgb_row(L, cur, last, x, y, r, sigma, row);
-            add_products(row, acc);
-        }
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        int r = residual[p];
+        if (r < 0) continue;
+        const int y = p / L.W, x = p - y * L.W;
+        float row[7];
+        rgb_row(L, cur, last, x, y, r, sigma, row);
+        add_products(row, acc);
     }
     block_sum<29>(acc, sm);
-    float* out = partials + (size_t)blockIdx.x * 32;
+    float* rgbp = partials + (size_t)kTrackMaxBlocks * 32;   // second half of the partials buffer
     if (threadIdx.x == 0)
 #pragma unroll
-        for (int k = 0; k < 29; ++k) out[k] = acc[k];
+        for (int k = 0; k < 29; ++k) rgbp[(size_t)blockIdx.x * 32 + k] = acc[k];
     if (!last_block(ticket)) return;
-    __shared__ double sums[29];
+    reduce_partials(partials, G, 32, 29, sums, scratch);        // ICP
+    reduce_partials(rgbp, G, 32, 29, sums + 32, scratch);       // RGB
     if (threadIdx.x < 29) {
-        double s = 0;
-        for (int b = 0; b < gridDim.x; ++b) s += (double)partials[(size_t)b * 32 + threadIdx.x];
-        sums[threadIdx.x] = s;
-        st->rgb_sums[threadIdx.x] = s;
+        st->icp_sums[threadIdx.x] = sums[threadIdx.x];
+        st->rgb_sums[threadIdx.x] = sums[32 + threadIdx.x];
     }
-    __syncthreads();
     if (threadIdx.x != 0) return;
     *ticket = 0;
+    st->rgb_cnt = c;
+    st->rgb_sq = q;
+    st->sigma = sigma;
     // Tracking.cc:319-394
     bool fail = false;
-    if (do_rgb) {
-        float r0 = (float)sums[27], r1 = (float)sums[28];
+    {
+        float r0 = (float)sums[32 + 27], r1 = (float)sums[32 + 28];
         float err = sqrtf(r0) / r1;
         st->rgb_error = err;
         st->rgb_count = r1;
         if (isnan(err) || (int)r1 < min_count) fail = true;
     }
     float icp_err = st->icp_error;
-    if (!fail && do_icp) {
-        float q0 = (float)st->icp_sums[27], q1 = (float)st->icp_sums[28];
+    if (!fail) {
+        float q0 = (float)sums[27], q1 = (float)sums[28];
         icp_err = sqrtf(q0) / q1;
         st->icp_error = icp_err;
         st->icp_count = q1;
@@ -447,10 +467,8 @@ __global__ void __launch_bounds__(256) k_track_b(TrackLevel L, TrackState* st, f
         return;
     }
     double Ar[36], br[6], Ai[36], bi[6], A[36], b[6], x[6], dT[16], dinv[16];
-    for (int i = 0; i < 36; ++i) Ar[i] = Ai[i] = 0;
-    for (int i = 0; i < 6; ++i) br[i] = bi[i] = 0;
-    if (do_rgb) unpack29(sums, Ar, br);
-    if (do_icp) unpack29(st->icp_sums, Ai, bi);
+    unpack29(sums + 32, Ar, br);
+    unpack29(sums, Ai, bi);
     const float w = 1e-4f;
     for (int i = 0; i < 36; ++i) A[i] = Ar[i] * (double)w + Ai[i];
     for (int i = 0; i < 6; ++i) b[i] = br[i] * (double)w + bi[i];
@@ -492,11 +510,10 @@ __global__ void __launch_bounds__(256) k_step_icp(TrackLevel L, DevPose cur, Dev
 #pragma unroll
         for (int k = 0; k < 29; ++k) partials[(size_t)blockIdx.x * 32 + k] = acc[k];
     if (!last_block(ticket)) return;
-    if (threadIdx.x < 29) {
-        double s = 0;
-        for (int b = 0; b < gridDim.x; ++b) s += (double)partials[(size_t)b * 32 + threadIdx.x];
-        out[threadIdx.x] = s;
-    }
+    __shared__ double scratch[8 * 32];
+    __shared__ double sums[32];
+    reduce_partials(partials, gridDim.x, 32, 29, sums, scratch);
+    if (threadIdx.x < 29) out[threadIdx.x] = sums[threadIdx.x];
     if (threadIdx.x == 0) *ticket = 0;
 }
 
@@ -553,19 +570,28 @@ __global__ void __launch_bounds__(256) k_step_rgb_b(TrackLevel L, DevPose cur, D
 #pragma unroll
         for (int k = 0; k < 29; ++k) partials[(size_t)blockIdx.x * 32 + k] = acc[k];
     if (!last_block(ticket)) return;
-    if (threadIdx.x < 29) {
-        double s = 0;
-        for (int b = 0; b < gridDim.x; ++b) s += (double)partials[(size_t)b * 32 + threadIdx.x];
-        out[threadIdx.x] = s;
-    }
+    __shared__ double scratch[8 * 32];
+    __shared__ double sums[32];
+    reduce_partials(partials, gridDim.x, 32, 29, sums, scratch);
+    if (threadIdx.x < 29) out[threadIdx.x] = sums[threadIdx.x];
     if (threadIdx.x == 0) *ticket = 0;
 }
 
 // ---------------------------------------------------------------- launchers
 
+// Two resident blocks of 256 threads per SM at most (the row kernels use
+// ~110 registers per thread).
 int track_grid(int n) {
+    static int cap = 0;
+    if (!cap) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cap = sms > 0 ? 2 * sms : 296;
+        if (cap > kTrackMaxBlocks) cap = kTrackMaxBlocks;
+    }
     int g = (n + 255) / 256;
-    return g < kTrackMaxBlocks ? g : kTrackMaxBlocks;
+    return g < cap ? g : cap;
 }
 
 int launch_track_begin(TrackState* st, cudaStream_t s) { k_track_begin<<<1, 1, 0, s>>>(st);
@@ -575,8 +601,8 @@ int launch_track_begin(TrackState* st, cudaStream_t s) { k_track_begin<<<1, 1, 0
 int launch_track_iter(const TrackLevel& L, TrackState* st, float* partials, unsigned int* tickets, int* residual,
                        int min_count, bool is_final, cudaStream_t s) {
     const int g = track_grid(L.W * L.H);
-    k_track_a<<<g, 256, 0, s>>>(L, st, partials, tickets + 0, residual, 1, 1);
-    k_track_b<<<g, 256, 0, s>>>(L, st, partials, tickets + 1, residual, min_count, 1, 1, is_final ? 1 : 0);
+    k_track_a<<<g, 256, 0, s>>>(L, st, partials, residual);
+    k_track_b<<<g, 256, 0, s>>>(L, st, partials, tickets + 1, residual, min_count, is_final ? 1 : 0);
     return 2;
 }
 
