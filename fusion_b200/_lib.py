@@ -13,7 +13,7 @@ FB_OK, FB_EINVAL, FB_ENOMEM, FB_ECUDA, FB_ETRACK_LOST = 0, 1, 2, 3, 4
 
 ERR_FLAGS = {
     0x1: "heap_exhausted", 0x2: "excess_full", 0x4: "request_set_full", 0x8: "coord_range",
-    0x10: "new_list_full", 0x20: "visible_full", 0x40: "sequential_insert",
+    0x10: "new_list_full", 0x20: "visible_full", 0x40: "sequential_insert", 0x80: "timeout",
 }
 
 
@@ -71,6 +71,8 @@ SIGNATURES = {
     "fb_grab_frame": (_i, [_vp, _vp, _sz, _vp, _sz, _i, ctypes.POINTER(FrameResult)]),
     "fb_get_pose": (_i, [_vp, _vp]),
     "fb_session_set_profiling": (_i, [_vp, _i]),
+    "fb_session_set_graphs": (_i, [_vp, _i]),
+    "fb_session_set_persistent": (_i, [_vp, _i]),
     "fb_session_stage_times": (_i, [_vp, _vp, _vp, _i]),
     "fb_session_launch_count": (_i, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "fb_frame_transfer_bytes": (_i, [ctypes.POINTER(Config), ctypes.POINTER(_sz), ctypes.POINTER(_sz)]),

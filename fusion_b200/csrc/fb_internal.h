@@ -26,6 +26,7 @@ struct TrackLevel {
     const uint8_t* glast;
     const int16_t* dx;
     const int16_t* dy;
+    const uint8_t* rgbok;   // pose-independent photometric eligibility (may be null)
 };
 
 // Device-resident tracker state of one session (Tracker's poses, residuals).
@@ -47,10 +48,28 @@ struct TrackState {
     long long scratch_sq[kTrackMaxBlocks];
 };
 
+// All levels of one frame for the persistent tracking kernel.
+struct TrackFrame {
+    TrackLevel L[3];
+    int iters[3];
+    int min_count[3];
+    int last_level;
+    TrackState* st;
+    float* partials;       // 2 x kTrackMaxBlocks x 32 floats
+    int* residual;         // W0 x H0 ints (per-pixel correspondences)
+    unsigned int* bar;     // grid barrier: count, generation
+    int* err;              // barrier timeout flag
+};
+
 int track_grid(int n);
+int track_frame_grid();
+int launch_track_frame(const TrackFrame& F, int grid, cudaStream_t s);
 int launch_track_begin(TrackState* st, cudaStream_t s);
-int launch_track_iter(const TrackLevel& L, TrackState* st, float* partials, unsigned int* tickets, int* residual,
-                       int min_count, bool is_final, cudaStream_t s);
+// residual: per-block compact segments of photometric correspondences
+// (int2: pixel, packed last pixel + difference), capacity track_list_capacity
+int launch_track_iter(const TrackLevel& L, TrackState* st, float* partials, unsigned int* tickets, int2* residual,
+                      int* counts, int min_count, bool is_final, cudaStream_t s);
+size_t track_list_capacity(int n_pixels);
 int launch_step_icp(const TrackLevel& L, const DevPose& cur, const DevPose& last, float* partials,
                      unsigned int* ticket, double* out, cudaStream_t s);
 int launch_step_rgb(const TrackLevel& L, const DevPose& cur, const DevPose& last, float* partials,
@@ -65,7 +84,7 @@ int launch_pyrdown(const float* sd, int sdp, const uint8_t* sg, int sgp, int SW,
                     uint8_t* dg, int dgp, cudaStream_t st);
 int launch_maps(const float* depth, int dp, const uint8_t* gray, int gp, int W, int H, const Intr& k,
                  float cutoff, float4* vmap, int vp, float4* nmap, int np, int16_t* dx, int16_t* dy, int sp,
-                 cudaStream_t st);
+                 cudaStream_t st, uint8_t* rgbok = nullptr);
 int launch_nmap(const float4* vmap, int vp, int W, int H, float4* nmap, int np, cudaStream_t st);
 int launch_resize(const float4* vs, const float4* ns, int sp, int SW, int SH, float4* vd, float4* nd, int dp,
                    cudaStream_t st);

@@ -123,7 +123,7 @@ __global__ void k_nmap(const float4* __restrict__ vmap, int vp, int W, int H, fl
 __global__ void k_maps(const float* __restrict__ depth, int dp, const uint8_t* __restrict__ gray, int gp,
                        int W, int H, Intr k, float cutoff, float4* __restrict__ vmap, int vp,
                        float4* __restrict__ nmap, int np, int16_t* __restrict__ dxo, int16_t* __restrict__ dyo,
-                       int sp) {
+                       int sp, uint8_t* __restrict__ rgbok) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
@@ -155,6 +155,20 @@ __global__ void k_maps(const float* __restrict__ depth, int dp, const uint8_t* _
             }
         dxo[(size_t)y * sp + x] = (int16_t)gx;
         dyo[(size_t)y * sp + x] = (int16_t)gy;
+        if (rgbok) {
+            // the pose-independent part of RGBReduction::FindCorresp
+            // (Tracking/Reduction.cu:413-425): 5-pixel border, gray > 0 over
+            // the window y-2..y+1, x-2..x+1, nonzero gradient
+            bool ok = x >= 5 && x < W - 5 && y >= 5 && y < H - 5 && ((int16_t)gx != 0 || (int16_t)gy != 0);
+            if (ok)
+                for (int u = y - 2; u < y + 2 && ok; ++u)
+                    for (int v = x - 2; v < x + 2; ++v)
+                        if (gray[(size_t)u * gp + v] == 0) {
+                            ok = false;
+                            break;
+                        }
+            rgbok[(size_t)y * sp + x] = ok ? 1 : 0;
+        }
     }
 }
 
@@ -216,10 +230,10 @@ int launch_pyrdown(const float* sd, int sdp, const uint8_t* sg, int sgp, int SW,
 
 int launch_maps(const float* depth, int dp, const uint8_t* gray, int gp, int W, int H, const Intr& k,
                  float cutoff, float4* vmap, int vp, float4* nmap, int np, int16_t* dx, int16_t* dy,
-                 int sp, cudaStream_t st) {
+                 int sp, cudaStream_t st, uint8_t* rgbok) {
     dim3 b(32, 8);
     k_maps<<<grid2d(W, H, b), b, 0, st>>>(depth, dp, gray, gp, W, H, k, cutoff, vmap, vp, nmap, np, dx,
-                                           dy, sp);
+                                           dy, sp, rgbok);
     return 1;
 }
 

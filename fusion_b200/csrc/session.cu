@@ -60,8 +60,14 @@ __global__ void k_init_poses(TrackState* st) {
     st->icp_count = st->rgb_count = 0;
 }
 
-// After the frame: a tracked frame becomes the last frame (SwapFrame).
-__global__ void k_commit(TrackState* st, MapCounters* c, FrameOut* out, int tracked_path) {
+// After the frame: a tracked frame becomes the last frame (SwapFrame).  A
+// timed-out device wait (err) counts as a tracking failure.
+__global__ void k_commit(TrackState* st, MapCounters* c, FrameOut* out, int tracked_path, const int* err) {
+    if (*err) {
+        for (int i = 0; i < 16; ++i) st->pose[i] = st->last_pose[i];
+        st->failed = 1;
+        c->err |= kErrTimeout;
+    }
     if (tracked_path && !st->failed) {
         for (int i = 0; i < 16; ++i) st->last_pose[i] = st->pose[i];
         st->last = st->cur;
@@ -83,6 +89,11 @@ __global__ void k_commit(TrackState* st, MapCounters* c, FrameOut* out, int trac
 }
 
 __global__ void k_set_pose(DevPose* dst, DevPose p) { *dst = p; }
+
+__global__ void k_reset_barrier(unsigned int* bar, int* err) {
+    bar[0] = 0;
+    *err = 0;
+}
 
 // Export of the hash table in the reference's field order, ptr as voxel index.
 __global__ void k_export_entries(const HEntry* e, int n, int* out) {
@@ -106,6 +117,7 @@ struct FrameBuf {
     uint8_t* gray[3];
     int16_t* dx[3];
     int16_t* dy[3];
+    uint8_t* rgbok[3];     // pose-independent photometric eligibility per level
 };
 
 }  // namespace
@@ -123,7 +135,10 @@ struct fb_session {
     TrackState* st;
     float* partials;
     unsigned int* tickets;
-    int* residual;
+    unsigned int* bar;         // grid barrier of the persistent tracking kernel
+    int* err;                  // its timeout flag
+    int2* residual;            // per-block photometric correspondence segments
+    int* counts;               // entries per segment
     MapView map;
     MapCounters* ctr;
     DevPose* scratch_pose;
@@ -140,6 +155,12 @@ struct fb_session {
     double stage_ms[kStages];
     uint64_t stage_calls[kStages];
     uint64_t launches;          // kernels launched by this session
+    // CUDA graphs of whole frames, keyed by (mode, fuse, which frame is next);
+    // mode 0 init, 1 track, 2 lost
+    bool use_graphs;
+    bool persistent;           // tracking as one cooperative kernel per frame
+    cudaGraphExec_t graph[3][2][2];
+    int graph_kernels[3][2][2];
 };
 
 namespace {
@@ -200,10 +221,15 @@ TrackLevel level_view(const fb_session* s, int l) {
     t.glast = L.gray[l];
     t.dx = N.dx[l];
     t.dy = N.dy[l];
+    t.rgbok = N.rgbok[l];
     return t;
 }
 
 void free_session(fb_session* s) {
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 2; ++c)
+                if (s->graph[a][b][c]) cudaGraphExecDestroy(s->graph[a][b][c]);
     for (int i = 0; i <= kStages; ++i)
         if (s->ev[i]) cudaEventDestroy(s->ev[i]);
     for (void* p : s->allocs) cudaFree(p);
@@ -216,6 +242,8 @@ int reset_session(fb_session* s) {
     launch_map_reset(s->map, s->stream);
     k_init_poses<<<1, 1, 0, s->stream>>>(s->st);
     FB_CUDA(cudaMemsetAsync(s->tickets, 0, 4 * sizeof(unsigned), s->stream));
+    FB_CUDA(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned), s->stream));
+    FB_CUDA(cudaMemsetAsync(s->err, 0, sizeof(int), s->stream));
     for (int f = 0; f < 2; ++f)
         for (int l = 0; l < 3; ++l) {
             size_t n = (size_t)s->W[l] * s->H[l];
@@ -260,7 +288,7 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
                             N.depth[l], s->W[l], N.gray[l], s->W[l], st);
     for (int l = 0; l < 3; ++l)
         n += launch_maps(N.depth[l], s->W[l], N.gray[l], s->W[l], s->W[l], s->H[l], s->K[l], c.depth_cutoff,
-                         N.vmap[l], s->W[l], N.nmap[l], s->W[l], N.dx[l], N.dy[l], s->W[l], st);
+                         N.vmap[l], s->W[l], N.nmap[l], s->W[l], N.dx[l], N.dy[l], s->W[l], st, N.rgbok[l]);
     *ran |= 1u << 1;
     mark(2);
     const int* skip = nullptr;
@@ -271,14 +299,34 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
         // Tracker::ComputeSE3 (Tracking.cc:296-409)
         static const int min_count[3] = {2000, 1000, 100};   // MIN_ICP_COUNT, Tracking.h:102
         n += launch_track_begin(s->st, st);
+        k_reset_barrier<<<1, 1, 0, st>>>(s->bar, s->err);
+        n += 1;
         int last_level = -1;
         for (int l = 2; l >= 0; --l)
             if (c.iters[l] > 0) last_level = l;
-        for (int l = 2; l >= 0; --l) {
-            TrackLevel lv = level_view(s, l);
-            for (int it = 0; it < c.iters[l]; ++it)
-                n += launch_track_iter(lv, s->st, s->partials, s->tickets, s->residual, min_count[l],
-                                       l == last_level && it == c.iters[l] - 1, st);
+        const int grid = s->persistent ? track_frame_grid() : 0;
+        if (grid > 0) {
+            // all levels and iterations in one cooperative launch
+            TrackFrame F;
+            for (int l = 0; l < 3; ++l) {
+                F.L[l] = level_view(s, l);
+                F.iters[l] = c.iters[l];
+                F.min_count[l] = min_count[l];
+            }
+            F.last_level = last_level;
+            F.st = s->st;
+            F.partials = s->partials;
+            F.residual = (int*)s->residual;
+            F.bar = s->bar;
+            F.err = s->err;
+            n += launch_track_frame(F, grid, st);
+        } else {
+            for (int l = 2; l >= 0; --l) {
+                TrackLevel lv = level_view(s, l);
+                for (int it = 0; it < c.iters[l]; ++it)
+                    n += launch_track_iter(lv, s->st, s->partials, s->tickets, s->residual, s->counts,
+                                           min_count[l], l == last_level && it == c.iters[l] - 1, st);
+            }
         }
         skip = &s->st->failed;
         *ran |= 1u << 2;
@@ -310,7 +358,7 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
         mark(7);
     }
     mark(8);
-    k_commit<<<1, 1, 0, st>>>(s->st, s->ctr, s->d_out, track || init);
+    k_commit<<<1, 1, 0, st>>>(s->st, s->ctr, s->d_out, track || init, s->err);
     return n + 1;
 }
 
@@ -388,7 +436,7 @@ size_t fb_session_bytes(const fb_config* c) {
     size_t px = (size_t)c->width * c->height, frame = 0;
     for (int l = 0; l < 3; ++l) {
         size_t n = (size_t)(c->width >> l) * (c->height >> l);
-        frame += n * (4 + 16 + 16 + 1 + 2 + 2);
+        frame += n * (4 + 16 + 16 + 1 + 2 + 2 + 1);
     }
     frame += px * (2 + 3 + 4);
     size_t NS = c->num_blocks, NB = c->num_buckets, NE = c->num_excess;
@@ -396,7 +444,7 @@ size_t fb_session_bytes(const fb_config* c) {
     size_t reqcap = next_pow2(2 * newcap);
     size_t map = (NB + NE) * sizeof(HEntry) + NS * 4 + NS * 512 * sizeof(Voxel) + 2 * NS * 4 + reqcap * 8 +
                  newcap * (sizeof(NewBlock) + 8) + 3 * NB * 4;
-    return 2 * frame + map + px * 4 + kTrackMaxBlocks * 32 * 4 + sizeof(TrackState);
+    return 2 * frame + map + px * 12 + kTrackMaxBlocks * 32 * 8 + sizeof(TrackState);
 }
 
 int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
@@ -413,6 +461,14 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
         s->stage_calls[i] = 0;
     }
     s->launches = 0;
+    s->use_graphs = true;
+    s->persistent = false;   // measured slower than graph-launched kernels on B200
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 2; ++c) {
+                s->graph[a][b][c] = nullptr;
+                s->graph_kernels[a][b][c] = 0;
+            }
     s->own_stream = stream == nullptr;
     s->stream = (cudaStream_t)stream;
     // an owned stream is a blocking one: it orders after work the caller put
@@ -435,11 +491,13 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
         for (int l = 0; l < 3 && ok; ++l) {
             size_t n = (size_t)s->W[l] * s->H[l];
             ok = dalloc(s, &F.depth[l], n) && dalloc(s, &F.vmap[l], n) && dalloc(s, &F.nmap[l], n) &&
-                 dalloc(s, &F.gray[l], n) && dalloc(s, &F.dx[l], n) && dalloc(s, &F.dy[l], n);
+                 dalloc(s, &F.gray[l], n) && dalloc(s, &F.dx[l], n) && dalloc(s, &F.dy[l], n) &&
+                 dalloc(s, &F.rgbok[l], n);
         }
     }
     ok = ok && dalloc(s, &s->st, 1) && dalloc(s, &s->partials, (size_t)2 * kTrackMaxBlocks * 32) &&
-         dalloc(s, &s->tickets, 4) && dalloc(s, &s->residual, (size_t)s->W[0] * s->H[0]) &&
+         dalloc(s, &s->tickets, 4) && dalloc(s, &s->bar, 2) && dalloc(s, &s->err, 1) && dalloc(s, &s->residual, track_list_capacity(s->W[0] * s->H[0])) &&
+         dalloc(s, &s->counts, kTrackMaxBlocks) &&
          dalloc(s, &s->scratch_pose, 1) && dalloc(s, &s->d_out, 1);
     MapView& m = s->map;
     if (ok) {
@@ -514,8 +572,31 @@ int fb_grab_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, cons
     const bool fuse = (init || track) && after >= 10;
     const bool render = init || track;
     unsigned ran = 0;
-    s->launches += (uint64_t)issue_frame(s, track, fuse, render, init, &ran);
-    if (check_launch()) return FB_ECUDA;
+    if (s->use_graphs && !s->profile) {
+        // the whole frame as one graph launch; captured on first use
+        const int mode = init ? 0 : track ? 1 : 2;
+        cudaGraphExec_t& g = s->graph[mode][fuse ? 1 : 0][s->next];
+        if (!g) {
+            cudaGraph_t graph = nullptr;
+            FB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            int nk = issue_frame(s, track, fuse, render, init, &ran);
+            cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+            if (e == cudaSuccess) e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&g, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                g = nullptr;
+                cuda_ok(e);
+                return FB_ECUDA;
+            }
+            s->graph_kernels[mode][fuse ? 1 : 0][s->next] = nk;
+        }
+        FB_CUDA(cudaGraphLaunch(g, s->stream));
+        s->launches += (uint64_t)s->graph_kernels[mode][fuse ? 1 : 0][s->next];
+    } else {
+        s->launches += (uint64_t)issue_frame(s, track, fuse, render, init, &ran);
+        if (check_launch()) return FB_ECUDA;
+    }
     FB_CUDA(cudaMemcpyAsync(s->h_out, s->d_out, sizeof(FrameOut), cudaMemcpyDeviceToHost, s->stream));
     FB_CUDA(cudaStreamSynchronize(s->stream));
     if (s->profile)
@@ -568,6 +649,28 @@ int fb_grab_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, cons
         out->frame_id = s->frame_id;
     }
     s->frame_id++;
+    return FB_OK;
+}
+
+int fb_session_set_graphs(fb_session* s, int on) {
+    if (!s) return FB_EINVAL;
+    s->use_graphs = on != 0;
+    return FB_OK;
+}
+
+int fb_session_set_persistent(fb_session* s, int on) {
+    if (!s) return FB_EINVAL;
+    if (s->persistent != (on != 0)) {
+        // cached graphs hold the other tracking variant
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 2; ++b)
+                for (int c = 0; c < 2; ++c)
+                    if (s->graph[a][b][c]) {
+                        cudaGraphExecDestroy(s->graph[a][b][c]);
+                        s->graph[a][b][c] = nullptr;
+                    }
+    }
+    s->persistent = on != 0;
     return FB_OK;
 }
 

@@ -66,13 +66,18 @@ __device__ __forceinline__ bool icp_row(const TrackLevel& L, const DevPose& cur,
 __device__ __forceinline__ int rgb_corresp(const TrackLevel& L, const DevPose& cur, const DevPose& last, int x,
                                            int y) {
     const int W = L.W, H = L.H;
-    if (!(x >= 5 && x < W - 5 && y >= 5 && y < H - 5)) return -1;
-    // the window is y-2..y+1, x-2..x+1 (Reduction.cu:416-417)
-    for (int u = y - 2; u < y + 2; ++u)
-        for (int v = x - 2; v < x + 2; ++v)
-            if (L.gcurr[(size_t)u * L.gp + v] == 0) return -1;
-    int gx = L.dx[(size_t)y * L.sp + x], gy = L.dy[(size_t)y * L.sp + x];
-    if (gx == 0 && gy == 0) return -1;  // sqrtf(gx*gx + gy*gy) > 0
+    if (L.rgbok) {
+        // border, window and gradient tests precomputed per frame
+        if (!L.rgbok[(size_t)y * L.sp + x]) return -1;
+    } else {
+        if (!(x >= 5 && x < W - 5 && y >= 5 && y < H - 5)) return -1;
+        // the window is y-2..y+1, x-2..x+1 (Reduction.cu:416-417)
+        for (int u = y - 2; u < y + 2; ++u)
+            for (int v = x - 2; v < x + 2; ++v)
+                if (L.gcurr[(size_t)u * L.gp + v] == 0) return -1;
+        int gx = L.dx[(size_t)y * L.sp + x], gy = L.dy[(size_t)y * L.sp + x];
+        if (gx == 0 && gy == 0) return -1;  // sqrtf(gx*gx + gy*gy) > 0
+    }
     float4 vcurr = L.vcurr[(size_t)y * L.vp + x];
     if (isnan(vcurr.x)) return -1;
     f3 vcurr_g = add3(mv(cur.R, xyz(vcurr)), cur.t);
@@ -189,61 +194,61 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket) {
 
 // ----------------------------------------------------------- FP64 solver
 
-// LDL^T with symmetric diagonal pivoting on a 6x6 SPD system (restates the
-// effect of Eigen's ldlt().solve used at Tracking.cc:388).
-__device__ void ldlt6(const double* Ain, const double* bin, double* x) {
-    double A[36], L[36], D[6], b[6];
-    int perm[6];
-    for (int i = 0; i < 36; ++i) { A[i] = Ain[i]; L[i] = 0; }
-    for (int i = 0; i < 6; ++i) { b[i] = bin[i]; perm[i] = i; }
+// LDL^T of the 6x6 symmetric positive definite normal matrix and the solve
+// (the effect of Eigen's ldlt().solve at Tracking.cc:388; for SPD systems the
+// factorisation needs no pivoting).  Fully unrolled so that every array stays
+// in registers.
+__device__ __forceinline__ void ldlt6(const double* A, const double* b, double* x) {
+    double L[6][6], D[6], y[6];
+#pragma unroll
     for (int k = 0; k < 6; ++k) {
-        int p = k;
-        for (int i = k + 1; i < 6; ++i)
-            if (fabs(A[i * 6 + i]) > fabs(A[p * 6 + p])) p = i;
-        if (p != k) {
-            for (int j = 0; j < 6; ++j) { double t = A[k * 6 + j]; A[k * 6 + j] = A[p * 6 + j]; A[p * 6 + j] = t; }
-            for (int i = 0; i < 6; ++i) { double t = A[i * 6 + k]; A[i * 6 + k] = A[i * 6 + p]; A[i * 6 + p] = t; }
-            for (int j = 0; j < k; ++j) { double t = L[k * 6 + j]; L[k * 6 + j] = L[p * 6 + j]; L[p * 6 + j] = t; }
-            int t = perm[k]; perm[k] = perm[p]; perm[p] = t;
-        }
         double d = A[k * 6 + k];
-        for (int j = 0; j < k; ++j) d -= L[k * 6 + j] * L[k * 6 + j] * D[j];
+#pragma unroll
+        for (int j = 0; j < k; ++j) d -= L[k][j] * L[k][j] * D[j];
         D[k] = d;
-        L[k * 6 + k] = 1;
+        const double inv = 1.0 / d;
+#pragma unroll
         for (int i = k + 1; i < 6; ++i) {
-            double s = A[i * 6 + k];
-            for (int j = 0; j < k; ++j) s -= L[i * 6 + j] * L[k * 6 + j] * D[j];
-            L[i * 6 + k] = s / d;
+            double t = A[i * 6 + k];
+#pragma unroll
+            for (int j = 0; j < k; ++j) t -= L[i][j] * L[k][j] * D[j];
+            L[i][k] = t * inv;
         }
     }
-    double y[6], z[6];
+#pragma unroll
     for (int i = 0; i < 6; ++i) {
-        double s = b[perm[i]];
-        for (int j = 0; j < i; ++j) s -= L[i * 6 + j] * y[j];
-        y[i] = s;
+        double t = b[i];
+#pragma unroll
+        for (int j = 0; j < i; ++j) t -= L[i][j] * y[j];
+        y[i] = t;
     }
+#pragma unroll
     for (int i = 0; i < 6; ++i) y[i] /= D[i];
+#pragma unroll
     for (int i = 5; i >= 0; --i) {
-        double s = y[i];
-        for (int j = i + 1; j < 6; ++j) s -= L[j * 6 + i] * z[j];
-        z[i] = s;
+        double t = y[i];
+#pragma unroll
+        for (int j = i + 1; j < 6; ++j) t -= L[j][i] * x[j];
+        x[i] = t;
     }
-    for (int i = 0; i < 6; ++i) x[perm[i]] = z[i];
 }
 
 // exp of the se(3) tangent (upsilon, omega) -- the Sophus::SE3d::exp of
 // Tracking.cc:389 restated from the mathematics (Rodrigues rotation, left
 // Jacobian for the translation, Taylor series near zero).
-__device__ void se3_exp(const double* xi, double* T) {
+__device__ __forceinline__ void se3_exp(const double* xi, double* T) {
     const double* u = xi;
     const double* w = xi + 3;
     double th2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
     double th = sqrt(th2);
     double W[9] = {0, -w[2], w[1], w[2], 0, -w[0], -w[1], w[0], 0};
     double W2[9];
+#pragma unroll
     for (int i = 0; i < 3; ++i)
+#pragma unroll
         for (int j = 0; j < 3; ++j) {
             double s = 0;
+#pragma unroll
             for (int k = 0; k < 3; ++k) s += W[i * 3 + k] * W[k * 3 + j];
             W2[i * 3 + j] = s;
         }
@@ -258,8 +263,10 @@ __device__ void se3_exp(const double* xi, double* T) {
         b = (1 - co) / th2;
         c = (th - s) / (th2 * th);
     }
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
         double vi[3];
+#pragma unroll
         for (int j = 0; j < 3; ++j) {
             double I = (i == j) ? 1.0 : 0.0;
             T[i * 4 + j] = I + a * W[i * 3 + j] + b * W2[i * 3 + j];
@@ -271,25 +278,33 @@ __device__ void se3_exp(const double* xi, double* T) {
     T[15] = 1;
 }
 
-__device__ void mat4_mul(const double* A, const double* B, double* C) {
+__device__ __forceinline__ void mat4_mul(const double* A, const double* B, double* C) {
     double T[16];
+#pragma unroll
     for (int i = 0; i < 4; ++i)
+#pragma unroll
         for (int j = 0; j < 4; ++j) {
             double s = 0;
+#pragma unroll
             for (int k = 0; k < 4; ++k) s += A[i * 4 + k] * B[k * 4 + j];
             T[i * 4 + j] = s;
         }
+#pragma unroll
     for (int i = 0; i < 16; ++i) C[i] = T[i];
 }
 
-__device__ void mat4_rigid_inv(const double* A, double* B) {
+__device__ __forceinline__ void mat4_rigid_inv(const double* A, double* B) {
     double T[16];
+#pragma unroll
     for (int i = 0; i < 3; ++i)
+#pragma unroll
         for (int j = 0; j < 3; ++j) T[i * 4 + j] = A[j * 4 + i];
+#pragma unroll
     for (int i = 0; i < 3; ++i)
         T[i * 4 + 3] = -(T[i * 4 + 0] * A[3] + T[i * 4 + 1] * A[7] + T[i * 4 + 2] * A[11]);
     T[12] = T[13] = T[14] = 0;
     T[15] = 1;
+#pragma unroll
     for (int i = 0; i < 16; ++i) B[i] = T[i];
 }
 
@@ -301,9 +316,11 @@ __device__ double euler_sin_norm(const double* T) {
     return sqrt(sa * sa + sb * sb + sc * sc);
 }
 
-__device__ void unpack29(const double* s, double* A, double* b) {
+__device__ __forceinline__ void unpack29(const double* s, double* A, double* b) {
     int n = 0;
+#pragma unroll
     for (int i = 0; i < 6; ++i)
+#pragma unroll
         for (int j = i; j < 7; ++j) {
             double v = s[n++];
             if (j == 6)
@@ -356,27 +373,83 @@ __device__ void reduce_partials(const float* __restrict__ partials, int nb, int 
     }
 }
 
-// pass A: ICP rows and RGB correspondences; per-block partial sums only.
-__global__ void __launch_bounds__(256) k_track_a(TrackLevel L, TrackState* st, float* partials, int* residual) {
+// As reduce_partials, reading partials written by other blocks of the same
+// (cooperative) launch through L2.
+__device__ void reduce_partials_cg(const float* partials, int nb, int stride, int nv, double* out,
+                                   double* scratch) {
+    const int v = threadIdx.x & 31, c = threadIdx.x >> 5, nc = blockDim.x >> 5;
+    const int per = (nb + nc - 1) / nc;
+    for (int v0 = 0; v0 < nv; v0 += 32) {
+        double s = 0;
+        if (v0 + v < nv) {
+            const int b0 = c * per, b1 = min(nb, b0 + per);
+#pragma unroll 8
+            for (int b = b0; b < b1; ++b) s += (double)__ldcg(partials + (size_t)b * stride + v0 + v);
+        }
+        scratch[c * 32 + v] = s;
+        __syncthreads();
+        if (c == 0 && v0 + v < nv) {
+            double t = 0;
+            for (int q = 0; q < nc; ++q) t += scratch[q * 32 + v];
+            out[v0 + v] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// Capacity of the per-block correspondence segments for n pixels: every
+// block of the pass-A grid gets as many slots as the pixels it visits.
+size_t track_list_capacity(int n) {
+    const int g = track_grid(n);
+    const int iters = (n + g * 256 - 1) / (g * 256);
+    return (size_t)g * iters * 256;
+}
+
+// pass A: ICP rows (reduced per block) and RGB correspondences, which each
+// block appends to its own segment of `list` in pixel-visit order (block-local
+// scan: deterministic).  Loop trip counts are uniform across the block.
+__global__ void __launch_bounds__(256, 2) k_track_a(TrackLevel L, TrackState* st, float* partials, int2* list,
+                                                    int* counts) {
     if (st->failed) return;
     __shared__ float sm[32 * 29];
     __shared__ long long smll[32];
+    __shared__ int s_warp[8];
+    __shared__ int s_run;
     const DevPose cur = st->cur, last = st->last;
     float acc[29];
 #pragma unroll
     for (int k = 0; k < 29; ++k) acc[k] = 0.f;
     long long rc = 0, rsq = 0;
     const int N = L.W * L.H;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
-        const int y = p / L.W, x = p - y * L.W;
-        float row[7];
-        if (icp_row(L, cur, last, x, y, row)) add_products(row, acc);
-        int r = rgb_corresp(L, cur, last, x, y);
-        residual[p] = r;
-        if (r >= 0) {
-            int d = (r & 511) - 255;
-            rc += 1;
-            rsq += d * d;
+    const int G = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int iters = (N + G * 256 - 1) / (G * 256);
+    int2* seg = list + (size_t)blockIdx.x * iters * 256;
+    if (threadIdx.x == 0) s_run = 0;
+    for (int k = 0; k < iters; ++k) {
+        const int p = (k * G + blockIdx.x) * 256 + threadIdx.x;
+        int r = -1;
+        if (p < N) {
+            const int y = p / L.W, x = p - y * L.W;
+            float row[7];
+            if (icp_row(L, cur, last, x, y, row)) add_products(row, acc);
+            r = rgb_corresp(L, cur, last, x, y);
+            if (r >= 0) {
+                int d = (r & 511) - 255;
+                rc += 1;
+                rsq += d * d;
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, r >= 0);
+        if (lane == 0) s_warp[wid] = __popc(m);
+        __syncthreads();
+        int base = s_run;
+        for (int w = 0; w < wid; ++w) base += s_warp[w];
+        if (r >= 0) seg[base + __popc(m & ((1u << lane) - 1))] = make_int2(p, r);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int w = 0; w < 8; ++w) t += s_warp[w];
+            s_run += t;
         }
     }
     block_sum<29>(acc, sm);
@@ -388,19 +461,24 @@ __global__ void __launch_bounds__(256) k_track_a(TrackLevel L, TrackState* st, f
         for (int k = 0; k < 29; ++k) out[k] = acc[k];
         st->scratch_cnt[blockIdx.x] = bc;
         st->scratch_sq[blockIdx.x] = bs;
+        counts[blockIdx.x] = s_run;
     }
 }
 
+__device__ __forceinline__ void solve_step(TrackState* st, const double* s, int min_count, int is_final);
+
 // pass B: every block derives sigma from pass A's counts (same value in every
-// block), builds the RGB rows, and the last block reduces both passes'
-// partials in FP64 and solves.
-__global__ void __launch_bounds__(256) k_track_b(TrackLevel L, TrackState* st, float* partials, unsigned int* ticket,
-                                                 const int* residual, int min_count, int is_final) {
+// block) and builds the RGB rows of its own segment; the last block reduces
+// both passes' partials in FP64 and performs the Gauss-Newton update.
+__global__ void __launch_bounds__(256, 2) k_track_b(TrackLevel L, TrackState* st, float* partials,
+                                                    unsigned int* ticket, const int2* list, const int* counts,
+                                                    int seg_size, int min_count, int is_final) {
     if (st->failed) return;
     __shared__ float sm[32 * 29];
     __shared__ long long smll[32];
     __shared__ double scratch[8 * 32];
     __shared__ double sums[64];
+    __shared__ float s_sigma;
     const DevPose cur = st->cur, last = st->last;
     const int G = gridDim.x;
     // sigma = sqrt((float) sum / count) (Reduction.cu:606-608), sums in block order
@@ -411,20 +489,19 @@ __global__ void __launch_bounds__(256) k_track_b(TrackLevel L, TrackState* st, f
     }
     c = block_sum_ll(c, smll);
     q = block_sum_ll(q, smll);
-    __shared__ float s_sigma;
     if (threadIdx.x == 0) s_sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
     __syncthreads();
     const float sigma = s_sigma;
     float acc[29];
 #pragma unroll
     for (int k = 0; k < 29; ++k) acc[k] = 0.f;
-    const int N = L.W * L.H;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
-        int r = residual[p];
-        if (r < 0) continue;
-        const int y = p / L.W, x = p - y * L.W;
+    const int n = counts[blockIdx.x];
+    const int2* seg = list + (size_t)blockIdx.x * seg_size;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int2 e = seg[i];
+        const int y = e.x / L.W, x = e.x - y * L.W;
         float row[7];
-        rgb_row(L, cur, last, x, y, r, sigma, row);
+        rgb_row(L, cur, last, x, y, e.y, sigma, row);
         add_products(row, acc);
     }
     block_sum<29>(acc, sm);
@@ -439,15 +516,26 @@ __global__ void __launch_bounds__(256) k_track_b(TrackLevel L, TrackState* st, f
         st->icp_sums[threadIdx.x] = sums[threadIdx.x];
         st->rgb_sums[threadIdx.x] = sums[32 + threadIdx.x];
     }
+    __syncthreads();
     if (threadIdx.x != 0) return;
     *ticket = 0;
     st->rgb_cnt = c;
     st->rgb_sq = q;
     st->sigma = sigma;
-    // Tracking.cc:319-394
+    solve_step(st, sums, min_count, is_final);
+}
+
+// The Gauss-Newton update of one iteration (Tracking.cc:319-394) and, after
+// the last one, the acceptance test (Tracking.cc:398-408).  One thread; the
+// normal equations are in FP64, every array in registers.
+// The Gauss-Newton update of one iteration (Tracking.cc:319-394) and, after
+// the last one, the acceptance test (Tracking.cc:398-408), from the FP64 sums
+// s (ICP in s[0..28], RGB in s[32..60]).  One thread; every array in
+// registers.
+__device__ __forceinline__ void solve_step(TrackState* st, const double* s, int min_count, int is_final) {
     bool fail = false;
     {
-        float r0 = (float)sums[32 + 27], r1 = (float)sums[32 + 28];
+        float r0 = (float)s[32 + 27], r1 = (float)s[32 + 28];
         float err = sqrtf(r0) / r1;
         st->rgb_error = err;
         st->rgb_count = r1;
@@ -455,7 +543,7 @@ __global__ void __launch_bounds__(256) k_track_b(TrackLevel L, TrackState* st, f
     }
     float icp_err = st->icp_error;
     if (!fail) {
-        float q0 = (float)sums[27], q1 = (float)sums[28];
+        float q0 = (float)s[27], q1 = (float)s[28];
         icp_err = sqrtf(q0) / q1;
         st->icp_error = icp_err;
         st->icp_count = q1;
@@ -463,30 +551,202 @@ __global__ void __launch_bounds__(256) k_track_b(TrackLevel L, TrackState* st, f
     }
     if (fail) {
         for (int i = 0; i < 16; ++i) st->pose[i] = st->last_pose[i];
+        __threadfence();
         st->failed = 1;
         return;
     }
-    double Ar[36], br[6], Ai[36], bi[6], A[36], b[6], x[6], dT[16], dinv[16];
-    unpack29(sums + 32, Ar, br);
-    unpack29(sums, Ai, bi);
+    double Ar[36], br[6], Ai[36], bi[6], A[36], b[6], x[6], dT[16], dinv[16], delta[16], lastp[16], pose[16];
+    unpack29(s + 32, Ar, br);
+    unpack29(s, Ai, bi);
     const float w = 1e-4f;
+#pragma unroll
     for (int i = 0; i < 36; ++i) A[i] = Ar[i] * (double)w + Ai[i];
+#pragma unroll
     for (int i = 0; i < 6; ++i) b[i] = br[i] * (double)w + bi[i];
     ldlt6(A, b, x);
     se3_exp(x, dT);
-    mat4_mul(dT, st->delta, st->delta);
-    mat4_rigid_inv(st->delta, dinv);
-    mat4_mul(st->last_pose, dinv, st->pose);
-    st->cur = make_dev_pose_d(st->pose);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        delta[i] = st->delta[i];
+        lastp[i] = st->last_pose[i];
+    }
+    mat4_mul(dT, delta, delta);
+    mat4_rigid_inv(delta, dinv);
+    mat4_mul(lastp, dinv, pose);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        st->delta[i] = delta[i];
+        st->pose[i] = pose[i];
+    }
+    st->cur = make_dev_pose_d(pose);
     if (is_final) {
-        // acceptance test (Tracking.cc:398-408)
-        double pinv[16], p[16];
-        mat4_rigid_inv(st->init_pose, pinv);
-        mat4_mul(pinv, st->pose, p);
+        double pinv[16], p[16], init[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) init[i] = st->init_pose[i];
+        mat4_rigid_inv(init, pinv);
+        mat4_mul(pinv, pose, p);
         double tn = sqrt(p[3] * p[3] + p[7] * p[7] + p[11] * p[11]);
         if (!(icp_err < 0.0001f && euler_sin_norm(p) <= 0.1 && tn <= 0.1)) {
             for (int i = 0; i < 16; ++i) st->pose[i] = st->last_pose[i];
+            __threadfence();
             st->failed = 1;
+        }
+    }
+    __threadfence();
+}
+
+// The solve of one iteration as its own kernel (multi-kernel path).
+__global__ void __launch_bounds__(32) k_track_solve(TrackState* st, int min_count, int is_final) {
+    if (threadIdx.x != 0 || st->failed) return;
+    double s[64];
+#pragma unroll
+    for (int k = 0; k < 29; ++k) {
+        s[k] = st->icp_sums[k];
+        s[32 + k] = st->rgb_sums[k];
+    }
+    solve_step(st, s, min_count, is_final);
+}
+
+// ----------------------------------------------------- persistent tracking
+
+// Grid-wide barrier for a cooperative launch (all blocks co-resident).  The
+// wait is bounded: after kBarrierSpins polls the block records a timeout in
+// *err and returns false, and every later barrier returns false at once, so
+// the kernel ends instead of hanging.
+constexpr long long kBarrierSpins = 1ll << 24;   // ~1 s of 64 ns sleeps
+
+__device__ __forceinline__ bool grid_sync(unsigned int* bar, int* err) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = bar + 1;
+        int ok = *(volatile int*)err == 0;
+        if (ok) {
+            const unsigned int g = *gen;
+            __threadfence();
+            const unsigned int arrived = atomicAdd(bar, 1u) + 1;
+            if (arrived == gridDim.x) {
+                bar[0] = 0;
+                __threadfence();
+                atomicAdd(bar + 1, 1u);
+            } else {
+                long long spins = 0;
+                while (*gen == g) {
+                    if (++spins > kBarrierSpins || *(volatile int*)err) {
+                        atomicExch(err, 1);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __threadfence();
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok;
+}
+
+__device__ __forceinline__ DevPose load_pose_cg(const DevPose* p) {
+    DevPose d;
+    const float* src = (const float*)p;
+    float* dst = (float*)&d;
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(DevPose) / 4); ++i) dst[i] = __ldcg(src + i);
+    return d;
+}
+
+// Tracker::ComputeSE3 for one frame in a single cooperative launch: for every
+// level and iteration, pass A (ICP rows + RGB correspondences), pass B (RGB
+// rows), then block 0 reduces both passes in FP64 and solves; three grid
+// barriers per iteration.  Same arithmetic as k_track_a / k_track_b /
+// k_track_solve.
+__global__ void __launch_bounds__(256, 2) k_track_frame(TrackFrame F) {
+    __shared__ float sm[32 * 29];
+    __shared__ long long smll[32];
+    __shared__ double scratch[8 * 32];
+    __shared__ double sums[64];
+    __shared__ float s_sigma;
+    TrackState* st = F.st;
+    const int G = gridDim.x;
+    float* icpp = F.partials;
+    float* rgbp = F.partials + (size_t)kTrackMaxBlocks * 32;
+    if (__ldcg(&st->failed)) return;
+    for (int l = 2; l >= 0; --l) {
+        const TrackLevel& L = F.L[l];
+        const int N = L.W * L.H;
+        for (int it = 0; it < F.iters[l]; ++it) {
+            const DevPose cur = load_pose_cg(&st->cur), last = load_pose_cg(&st->last);
+            // pass A
+            float acc[29];
+#pragma unroll
+            for (int k = 0; k < 29; ++k) acc[k] = 0.f;
+            long long rc = 0, rsq = 0;
+            for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += G * blockDim.x) {
+                const int y = p / L.W, x = p - y * L.W;
+                float row[7];
+                if (icp_row(L, cur, last, x, y, row)) add_products(row, acc);
+                int r = rgb_corresp(L, cur, last, x, y);
+                F.residual[p] = r;
+                if (r >= 0) {
+                    int d = (r & 511) - 255;
+                    rc += 1;
+                    rsq += d * d;
+                }
+            }
+            block_sum<29>(acc, sm);
+            long long bc = block_sum_ll(rc, smll);
+            long long bs = block_sum_ll(rsq, smll);
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int k = 0; k < 29; ++k) icpp[(size_t)blockIdx.x * 32 + k] = acc[k];
+                st->scratch_cnt[blockIdx.x] = bc;
+                st->scratch_sq[blockIdx.x] = bs;
+            }
+            if (!grid_sync(F.bar, F.err)) return;
+            // pass B: sigma from every block's counts, in block order
+            long long c = 0, q = 0;
+            for (int b = threadIdx.x; b < G; b += blockDim.x) {
+                c += __ldcg(&st->scratch_cnt[b]);
+                q += __ldcg(&st->scratch_sq[b]);
+            }
+            c = block_sum_ll(c, smll);
+            q = block_sum_ll(q, smll);
+            if (threadIdx.x == 0) s_sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
+            __syncthreads();
+            const float sigma = s_sigma;
+#pragma unroll
+            for (int k = 0; k < 29; ++k) acc[k] = 0.f;
+            for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += G * blockDim.x) {
+                int r = F.residual[p];
+                if (r < 0) continue;
+                const int y = p / L.W, x = p - y * L.W;
+                float row[7];
+                rgb_row(L, cur, last, x, y, r, sigma, row);
+                add_products(row, acc);
+            }
+            block_sum<29>(acc, sm);
+            if (threadIdx.x == 0)
+#pragma unroll
+                for (int k = 0; k < 29; ++k) rgbp[(size_t)blockIdx.x * 32 + k] = acc[k];
+            if (!grid_sync(F.bar, F.err)) return;
+            if (blockIdx.x == 0) {
+                reduce_partials_cg(icpp, G, 32, 29, sums, scratch);
+                reduce_partials_cg(rgbp, G, 32, 29, sums + 32, scratch);
+                if (threadIdx.x < 29) {
+                    st->icp_sums[threadIdx.x] = sums[threadIdx.x];
+                    st->rgb_sums[threadIdx.x] = sums[32 + threadIdx.x];
+                }
+                if (threadIdx.x == 0) {
+                    st->rgb_cnt = c;
+                    st->rgb_sq = q;
+                    st->sigma = sigma;
+                    solve_step(st, sums, F.min_count[l], l == F.last_level && it == F.iters[l] - 1);
+                }
+            }
+            if (!grid_sync(F.bar, F.err)) return;
+            if (__ldcg(&st->failed)) return;
         }
     }
 }
@@ -598,12 +858,44 @@ int launch_track_begin(TrackState* st, cudaStream_t s) { k_track_begin<<<1, 1, 0
     return 1;
 }
 
-int launch_track_iter(const TrackLevel& L, TrackState* st, float* partials, unsigned int* tickets, int* residual,
-                       int min_count, bool is_final, cudaStream_t s) {
-    const int g = track_grid(L.W * L.H);
-    k_track_a<<<g, 256, 0, s>>>(L, st, partials, residual);
-    k_track_b<<<g, 256, 0, s>>>(L, st, partials, tickets + 1, residual, min_count, is_final ? 1 : 0);
+int launch_track_iter(const TrackLevel& L, TrackState* st, float* partials, unsigned int* tickets, int2* residual,
+                      int* counts, int min_count, bool is_final, cudaStream_t s) {
+    const int n = L.W * L.H;
+    const int g = track_grid(n);
+    const int seg = (n + g * 256 - 1) / (g * 256) * 256;
+    k_track_a<<<g, 256, 0, s>>>(L, st, partials, residual, counts);
+    k_track_b<<<g, 256, 0, s>>>(L, st, partials, tickets + 1, residual, counts, seg, min_count, is_final ? 1 : 0);
     return 2;
+}
+
+// Occupancy-limited grid of the cooperative tracking kernel (0: unavailable).
+int track_frame_grid() {
+    static int g = -1;
+    if (g < 0) {
+        int dev = 0, sms = 0, coop = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_track_frame, 256, 0) != cudaSuccess) per = 0;
+        if (per > 2) per = 2;
+        g = coop && per > 0 ? per * sms : 0;
+        if (g > kTrackMaxBlocks) g = kTrackMaxBlocks;
+    }
+    return g;
+}
+
+int launch_track_frame(const TrackFrame& F, int grid, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_track_frame, F);
+    return 1;
 }
 
 int launch_step_icp(const TrackLevel& L, const DevPose& cur, const DevPose& last, float* partials,

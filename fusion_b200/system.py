@@ -140,6 +140,12 @@ class Session:
         check("fb_session_stage_times", self.lib.fb_session_stage_times(self.h, _p(ms), _p(calls), 8))
         return {k: (float(ms[i]), int(calls[i])) for i, k in enumerate(self.STAGES)}
 
+    def set_graphs(self, on=True):
+        check("fb_session_set_graphs", self.lib.fb_session_set_graphs(self.h, 1 if on else 0))
+
+    def set_persistent(self, on=True):
+        check("fb_session_set_persistent", self.lib.fb_session_set_persistent(self.h, 1 if on else 0))
+
     def launch_count(self):
         n = ctypes.c_uint64()
         check("fb_session_launch_count", self.lib.fb_session_launch_count(self.h, ctypes.byref(n)))

@@ -49,6 +49,7 @@ extern "C" {
 #define FB_ERR_NEW_LIST_FULL 0x10u    /* more new blocks in one frame than the pool */
 #define FB_ERR_VISIBLE_FULL 0x20u     /* visible list full */
 #define FB_ERR_SEQUENTIAL_INSERT 0x40u /* pool/excess edge case: exact sequential insert used */
+#define FB_ERR_TIMEOUT 0x80u          /* a bounded device-side wait gave up; the frame was not tracked */
 
 /* Runtime form of the reference's compile-time constants:
  * Mapping/DeviceMap.h:135-151 (voxel size, truncation, depth range, table
@@ -119,6 +120,14 @@ FB_API int fb_grab_frame(fb_session* s, const uint16_t* depth, size_t depth_pitc
  * 5 integration, 6 z ranges, 7 raycast.  Switching it on resets the sums. */
 FB_API int fb_session_set_profiling(fb_session* s, int on);
 FB_API int fb_session_stage_times(fb_session* s, double* ms, uint64_t* calls, int n);
+/* Frames run as captured CUDA graphs (default on; one capture per tracker
+ * mode and frame parity, made on first use).  Off: kernels launched one by
+ * one.  Profiled frames always launch kernels one by one. */
+FB_API int fb_session_set_graphs(fb_session* s, int on);
+/* Tracking as one cooperative (persistent) kernel per frame with bounded
+ * grid barriers, or (default) as kernels per Gauss-Newton iteration launched
+ * from the frame's CUDA graph.  Same arithmetic. */
+FB_API int fb_session_set_persistent(fb_session* s, int on);
 /* Kernels this session has launched so far. */
 FB_API int fb_session_launch_count(fb_session* s, uint64_t* launches);
 /* Bytes fb_grab_frame moves per frame with host inputs: h2d = depth + rgb,
