@@ -93,6 +93,8 @@ SIGNATURES = {
     "fb_step_scratch_bytes": (_sz, [_i, _i]),
     "fb_icp_step": (_i, [ctypes.POINTER(Image)] * 4 + [_vp] * 6 + [_vp, _sz, _vp, _vp, _vp, _vp]),
     "fb_rgb_step": (_i, [ctypes.POINTER(Image)] * 6 + [_vp] * 7 + [_vp, _sz, _vp, _vp, _vp, _vp]),
+    "fb_rgb_step_static": (_i, [ctypes.POINTER(Image)] * 6 + [_vp] * 7 + [_vp, _vp, _vp, _vp]),
+    "fb_rgb_step_static_max_pixels": (_sz, []),
     "fb_reset_map": (_i, [_vp]),
     "fb_fuse_map_color": (_i, [_vp] + [ctypes.POINTER(Image)] * 3 + [_vp] * 4 +
                           [ctypes.POINTER(ctypes.c_uint32), _vp]),

@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
-CU_SOURCES = ["preprocess.cu", "track.cu", "map.cu", "raycast.cu", "session.cu"]
+CU_SOURCES = ["preprocess.cu", "track.cu", "map.cu", "raycast.cu", "session.cu", "static_scratch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = os.path.join(HERE, "libfusion_b200.so")
 SYNTH = os.path.join(HERE, "libfbsynth.so")

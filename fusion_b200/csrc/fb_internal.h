@@ -166,4 +166,7 @@ int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, i
 
 }  // namespace fb
 
+// Text returned by fb_last_error() in the calling thread.
+void fb_set_error_text(const char* msg);
+
 #endif

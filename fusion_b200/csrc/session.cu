@@ -122,6 +122,8 @@ struct FrameBuf {
 
 }  // namespace
 
+void fb_set_error_text(const char* msg) { snprintf(g_last_error, sizeof g_last_error, "%s", msg); }
+
 constexpr int kStages = 8;   // resize, pyramid, tracking, allocation, visibility, integration, z ranges, raycast
 
 struct fb_session {

@@ -325,6 +325,24 @@ def rgb_step(gcurr, glast, vcurr, vlast, dx, dy, Rcurr, RcurrInv, Rlast, RlastIn
     return res, A.reshape(6, 6), b
 
 
+def rgb_step_static(gcurr, glast, vcurr, vlast, dx, dy, Rcurr, RcurrInv, Rlast, RlastInv, tcurr, tlast, K,
+                    stream=None):
+    """rgb_step without a scratch argument: for callers that cannot allocate
+    device memory where they track (inside a CUDA graph capture, a frame loop
+    that cannot wait for cudaFree, a host that owns all device memory).  The
+    library's own fixed device buffer limits images to 640 x 480 pixels, and
+    calls that overlap on the GPU share that buffer."""
+    res = np.zeros(2, np.float32)
+    A = np.zeros(36)
+    b = np.zeros(6)
+    args = [_f32(Rcurr), _f32(RcurrInv), _f32(Rlast), _f32(RlastInv), _f32(tcurr), _f32(tlast), _f32(K)]
+    check("fb_rgb_step_static", _lib.load().fb_rgb_step_static(
+        ctypes.byref(_img(gcurr, 1)), ctypes.byref(_img(glast, 1)), ctypes.byref(_img(vcurr, 16)),
+        ctypes.byref(_img(vlast, 16)), ctypes.byref(_img(dx, 2)), ctypes.byref(_img(dy, 2)),
+        *[_p(a) for a in args], _p(res), _p(A), _p(b), _stream(stream)))
+    return res, A.reshape(6, 6), b
+
+
 def step_scratch_bytes(cols, rows):
     return int(_lib.load().fb_step_scratch_bytes(cols, rows))
 

@@ -215,6 +215,24 @@ FB_API int fb_rgb_step(const fb_image* gcurr, const fb_image* glast, const fb_im
                 const float tcurr[3], const float tlast[3], const float K[4], void* scratch,
                 size_t scratch_bytes, float residual[2], double A[36], double b[6], void* stream);
 
+/* No counterpart in the reference.  fb_rgb_step for callers that cannot
+ * allocate device memory when they track a frame -- code recording a CUDA
+ * graph (cudaMalloc is not allowed during stream capture), frame loops that
+ * cannot pay for cudaFree's device-wide wait, hosts whose device memory all
+ * belongs to their own allocator.  Same arguments without the scratch: the
+ * library keeps 1.25 MiB of device memory per GPU for it, so images may have
+ * at most fb_rgb_step_static_max_pixels() (640 x 480) pixels; larger ones are
+ * rejected with FB_EINVAL.  The first call on a device looks up that memory's
+ * address and must not happen during a stream capture.  Every call shares the
+ * memory: calls that overlap on the GPU (other streams, unordered threads)
+ * corrupt each other's results.  Synchronous. */
+FB_API int fb_rgb_step_static(const fb_image* gcurr, const fb_image* glast, const fb_image* vcurr,
+                              const fb_image* vlast, const fb_image* dx, const fb_image* dy,
+                              const float Rcurr[9], const float RcurrInv[9], const float Rlast[9],
+                              const float RlastInv[9], const float tcurr[3], const float tlast[3],
+                              const float K[4], float residual[2], double A[36], double b[6], void* stream);
+FB_API size_t fb_rgb_step_static_max_pixels(void);
+
 /* Replaces: ResetMap (Mapping/FuseMap.cu:352-364) on the session's map. */
 FB_API int fb_reset_map(fb_session* s);
 
