@@ -281,12 +281,15 @@ def main():
     # layout), and one read of the depth, colour and normal of every pixel
     bytes_launch = 2 * 8 * 512 * mean_vis + 32 * mean_vis + 23 * n_px
     achieved = bytes_launch / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
+    # DRAM bytes per launch: ncu's dram__bytes_read.sum + dram__bytes_write.sum
+    # of one full-size k_integrate launch, per visible block of that launch,
+    # scaled here to this run's mean visible-block count
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "integration_traffic.txt")
     if os.path.exists(tpath):
         for ln in open(tpath):
-            if ln.startswith("dram_bytes_per_launch_full_size:"):
-                traffic = float(ln.split(":")[1])
+            if ln.startswith("dram_bytes_per_visible_block:"):
+                traffic = float(ln.split(":")[1]) * mean_vis
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
