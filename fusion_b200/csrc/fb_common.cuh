@@ -127,10 +127,17 @@ __host__ __device__ __forceinline__ uint32_t bucket_of(int x, int y, int z, uint
     uint32_t h = ((uint32_t)x * 73856093u) ^ ((uint32_t)y * 19349669u) ^ ((uint32_t)z * 83492791u);
     return h % nb;
 }
-// voxelPosToBlockPos (DeviceMap.cu:150-161): floor division by 8
-__device__ __forceinline__ int block_of(int v) { return (v < 0 ? v - 7 : v) / 8; }
-// voxelPosToLocalPos (DeviceMap.cu:167-178)
-__device__ __forceinline__ int local_of(int v) { int l = v % 8; return l < 0 ? l + 8 : l; }
+// As bucket_of, with the modulo done as a mask when nb is a power of two
+// (mask = nb - 1; 0 otherwise).  Same result.
+__device__ __forceinline__ uint32_t bucket_of_m(int x, int y, int z, uint32_t nb, uint32_t mask) {
+    uint32_t h = ((uint32_t)x * 73856093u) ^ ((uint32_t)y * 19349669u) ^ ((uint32_t)z * 83492791u);
+    return mask ? (h & mask) : h % nb;
+}
+// voxelPosToBlockPos (DeviceMap.cu:150-161): floor division by 8, i.e. the
+// arithmetic shift
+__device__ __forceinline__ int block_of(int v) { return v >> 3; }
+// voxelPosToLocalPos (DeviceMap.cu:167-178): the non-negative remainder
+__device__ __forceinline__ int local_of(int v) { return v & 7; }
 
 constexpr int kCoordLimit = 32767;
 

@@ -127,6 +127,7 @@ struct MapGeom {
 struct MapView {
     HEntry* entries;
     int NB, NE, NS;
+    uint32_t nb_mask;           // NB - 1 when NB is a power of two, else 0
     int* heap;
     Voxel* voxels;
     MapCounters* ctr;

@@ -34,7 +34,7 @@ namespace fb {
 
 // FindEntry (DeviceMap.cu:122-135): slot of the live entry for a block, or -1.
 __device__ __forceinline__ int find_slot(const MapView& m, int x, int y, int z) {
-    int b = (int)bucket_of(x, y, z, (uint32_t)m.NB);
+    int b = (int)bucket_of_m(x, y, z, (uint32_t)m.NB, m.nb_mask);
     HEntry e = m.entries[b];
     if (e.ptr != -1 && e.x == x && e.y == y && e.z == z) return b;
     for (int guard = 0; e.offset > 0 && e.offset <= m.NE && guard <= m.NE; ++guard) {
@@ -78,7 +78,7 @@ __device__ __forceinline__ void request_block(const MapView& m, int x, int y, in
                 nb.y = (short)y;
                 nb.z = (short)z;
                 nb.pad = 0;
-                nb.bucket = bucket_of(x, y, z, (uint32_t)m.NB);
+                nb.bucket = bucket_of_m(x, y, z, (uint32_t)m.NB, m.nb_mask);
                 nb.setslot = (int)h;
                 nb.j = 0;
                 nb.rank = 0;
@@ -176,26 +176,49 @@ __global__ void __launch_bounds__(256) k_scan_chunks(MapView m) {
     }
 }
 
-// Exclusive scan over the chunk sums; snapshot of the counters and choice of
-// the parallel or sequential insertion path.
-__global__ void k_scan_top(MapView m) {
+// Exclusive scan over the chunk sums (one block of 1024 threads, chunks in
+// order); snapshot of the counters and choice of the parallel or sequential
+// insertion path.
+__global__ void __launch_bounds__(1024) k_scan_top(MapView m) {
     MapCounters* c = m.ctr;
     const int M = min(c->n_req, m.newcap);
-    __shared__ int total_x;
+    __shared__ int s_a[1024], s_e[1024];
+    __shared__ int s_base_a, s_base_e;
     if (threadIdx.x == 0) {
-        int a = 0, e = 0;
-        if (M > 0)
-            for (int i = 0; i < m.nchunks; ++i) {
-                int ca = m.chunk_sums[2 * i], cx = m.chunk_sums[2 * i + 1];
-                m.chunk_sums[2 * i] = a;
-                m.chunk_sums[2 * i + 1] = e;
-                a += ca;
-                e += cx;
-            }
-        total_x = e;
+        s_base_a = 0;
+        s_base_e = 0;
     }
     __syncthreads();
+    if (M > 0) {
+        for (int c0 = 0; c0 < m.nchunks; c0 += 1024) {
+            const int i = c0 + threadIdx.x;
+            const int a = i < m.nchunks ? m.chunk_sums[2 * i] : 0;
+            const int e = i < m.nchunks ? m.chunk_sums[2 * i + 1] : 0;
+            s_a[threadIdx.x] = a;
+            s_e[threadIdx.x] = e;
+            __syncthreads();
+            for (int o = 1; o < 1024; o <<= 1) {   // inclusive Hillis-Steele scan
+                int ta = threadIdx.x >= o ? s_a[threadIdx.x - o] : 0;
+                int te = threadIdx.x >= o ? s_e[threadIdx.x - o] : 0;
+                __syncthreads();
+                s_a[threadIdx.x] += ta;
+                s_e[threadIdx.x] += te;
+                __syncthreads();
+            }
+            if (i < m.nchunks) {
+                m.chunk_sums[2 * i] = s_base_a + s_a[threadIdx.x] - a;
+                m.chunk_sums[2 * i + 1] = s_base_e + s_e[threadIdx.x] - e;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_base_a += s_a[1023];
+                s_base_e += s_e[1023];
+            }
+            __syncthreads();
+        }
+    }
     if (threadIdx.x == 0) {
+        const int total_x = s_base_e;
         c->excess_total = total_x;
         c->snap_M = M;
         c->snap_hc = c->heap_counter;
@@ -286,7 +309,7 @@ __global__ void k_alloc_rank(MapView m) {
 // CreateBlock (DeviceMap.cu:23-62) without lock contention, one block at a
 // time, for the sequential path.  Returns the slot written or -1.
 __device__ int create_block_seq(const MapView& m, int x, int y, int z, int& hc, int& ep, int& holes) {
-    const int b = (int)bucket_of(x, y, z, (uint32_t)m.NB);
+    const int b = (int)bucket_of_m(x, y, z, (uint32_t)m.NB, m.nb_mask);
     HEntry* e = &m.entries[b];
     HEntry* eEmpty = nullptr;
     if (e->x == x && e->y == y && e->z == z && e->ptr != -1) return -1;
@@ -622,7 +645,7 @@ int launch_allocate(const MapView& m, const float* raw, int rp, int W, int H, co
     const int gs = sm_count() * 4;
     k_alloc_count<<<gs, 256, 0, s>>>(m);
     k_scan_chunks<<<m.nchunks, 256, 0, s>>>(m);
-    k_scan_top<<<1, 32, 0, s>>>(m);
+    k_scan_top<<<1, 1024, 0, s>>>(m);
     k_scan_apply<<<m.nchunks, 256, 0, s>>>(m);
     k_alloc_place<<<gs, 256, 0, s>>>(m);
     k_alloc_rank<<<gs, 256, 0, s>>>(m);

@@ -90,7 +90,7 @@ __device__ __forceinline__ const Voxel* find_voxel(const MapView& m, f3 p, Entry
         valid = true;
         return m.voxels + (size_t)c.ptr * 512 + idx;
     }
-    int b = (int)bucket_of(bx, by, bz, (uint32_t)m.NB);
+    int b = (int)bucket_of_m(bx, by, bz, (uint32_t)m.NB, m.nb_mask);
     HEntry e = m.entries[b];
     bool found = e.ptr != -1 && e.x == bx && e.y == by && e.z == bz;
     for (int guard = 0; !found && e.offset > 0 && e.offset <= m.NE && guard <= m.NE; ++guard) {

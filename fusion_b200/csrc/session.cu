@@ -504,6 +504,7 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
     MapView& m = s->map;
     if (ok) {
         m.NB = cfg->num_buckets;
+        m.nb_mask = (m.NB & (m.NB - 1)) == 0 ? (uint32_t)(m.NB - 1) : 0u;
         m.NE = cfg->num_excess;
         m.NS = cfg->num_blocks;
         // new blocks of one frame: at least kMinNewBlocks whatever the pool
