@@ -12,6 +12,12 @@ namespace fb {
 // ------------------------------------------------------------------ tracking
 
 constexpr int kTrackMaxBlocks = 592;   // 4 resident blocks of 256 threads per SM
+// The per-iteration kernels run in thread-block clusters of kTrackCluster
+// blocks; each cluster reduces its blocks' sums through distributed shared
+// memory into one group sum.
+constexpr int kTrackCluster = 4;
+constexpr int kTrackMaxGroups = kTrackMaxBlocks / kTrackCluster;
+constexpr int kTrackWarps = 8;         // warps per block of the per-iteration kernels
 
 // One pyramid level of the current (next) and last frames.  Pitches in
 // elements: vp for float4 maps, gp for u8 images, sp for i16 derivatives.
@@ -46,6 +52,11 @@ struct TrackState {
     double rgb_sums[29];
     long long scratch_cnt[kTrackMaxBlocks];
     long long scratch_sq[kTrackMaxBlocks];
+    // per-cluster group sums of the per-iteration kernels (FP64, fixed order)
+    double grp_icp[kTrackMaxGroups][32];
+    double grp_rgb[kTrackMaxGroups][32];
+    long long grp_cnt[kTrackMaxGroups];
+    long long grp_sq[kTrackMaxGroups];
 };
 
 // All levels of one frame for the persistent tracking kernel.
@@ -62,13 +73,15 @@ struct TrackFrame {
 };
 
 int track_grid(int n);
+int track_cluster_grid(int n);   // track_grid rounded up to whole clusters
 int track_frame_grid();
 int launch_track_frame(const TrackFrame& F, int grid, cudaStream_t s);
 int launch_track_begin(TrackState* st, cudaStream_t s);
-// residual: per-block compact segments of photometric correspondences
-// (int2: pixel, packed last pixel + difference), capacity track_list_capacity
-int launch_track_iter(const TrackLevel& L, TrackState* st, float* partials, unsigned int* tickets, int2* residual,
-                      int* counts, int min_count, bool is_final, cudaStream_t s);
+// residual: per-warp compact segments of photometric correspondences
+// (int2: pixel, packed last pixel + difference), capacity track_list_capacity;
+// counts: entries per segment (kTrackMaxBlocks * kTrackWarps ints)
+int launch_track_iter(const TrackLevel& L, TrackState* st, unsigned int* tickets, int2* residual, int* counts,
+                      int min_count, bool is_final, cudaStream_t s);
 size_t track_list_capacity(int n_pixels);
 int launch_step_icp(const TrackLevel& L, const DevPose& cur, const DevPose& last, float* partials,
                      unsigned int* ticket, double* out, cudaStream_t s);

@@ -326,7 +326,7 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
             for (int l = 2; l >= 0; --l) {
                 TrackLevel lv = level_view(s, l);
                 for (int it = 0; it < c.iters[l]; ++it)
-                    n += launch_track_iter(lv, s->st, s->partials, s->tickets, s->residual, s->counts,
+                    n += launch_track_iter(lv, s->st, s->tickets, s->residual, s->counts,
                                            min_count[l], l == last_level && it == c.iters[l] - 1, st);
             }
         }
@@ -499,7 +499,7 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
     }
     ok = ok && dalloc(s, &s->st, 1) && dalloc(s, &s->partials, (size_t)2 * kTrackMaxBlocks * 32) &&
          dalloc(s, &s->tickets, 4) && dalloc(s, &s->bar, 2) && dalloc(s, &s->err, 1) && dalloc(s, &s->residual, track_list_capacity(s->W[0] * s->H[0])) &&
-         dalloc(s, &s->counts, kTrackMaxBlocks) &&
+         dalloc(s, &s->counts, (size_t)kTrackMaxBlocks * kTrackWarps) &&
          dalloc(s, &s->scratch_pose, 1) && dalloc(s, &s->d_out, 1);
     MapView& m = s->map;
     if (ok) {

@@ -16,7 +16,11 @@
 // Reductions are deterministic: fixed per-thread pixel sets, warp shuffles,
 // block sums in shared memory, then the blocks' partial sums are added in
 // block order in FP64 by the last block (no atomics on values).
+#include <cooperative_groups.h>
+
 #include "fb_internal.h"
+
+namespace cg = cooperative_groups;
 
 namespace fb {
 
@@ -163,6 +167,36 @@ __device__ __forceinline__ void block_sum(float v[NV], float* smem /* [32][NV] *
     }
 }
 
+// Block-wide sum of the 29 per-thread values of the normal equations.  Each
+// warp first reduces its 32 lanes by recursive halving (at every step a lane
+// keeps one half of its values, sends the other half to its partner and adds
+// what it receives: 31 shuffles in all), after which lane l holds the warp
+// sum of value l; warp 0 then adds the warps' sums in warp order.  Result:
+// value l in lane l (< 29) of warp 0.  Deterministic.
+__device__ __forceinline__ float block_sum29(const float (&v)[29], float* smem /* [8][32] */) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    float a[32];
+#pragma unroll
+    for (int k = 0; k < 29; ++k) a[k] = v[k];
+    a[29] = a[30] = a[31] = 0.f;
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        const bool up = (lane & off) != 0;
+#pragma unroll
+        for (int k = 0; k < off; ++k) {
+            const float send = up ? a[k] : a[k + off];
+            const float keep = up ? a[k + off] : a[k];
+            a[k] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+        }
+    }
+    smem[wid * 32 + lane] = a[0];
+    __syncthreads();
+    float r = 0.f;
+    if (wid == 0)
+        for (int w = 0; w < nw; ++w) r += smem[w * 32 + lane];
+    return r;
+}
+
 __device__ __forceinline__ long long block_sum_ll(long long v, long long* smem) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
@@ -199,7 +233,7 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket) {
 // factorisation needs no pivoting).  Fully unrolled so that every array stays
 // in registers.
 __device__ __forceinline__ void ldlt6(const double* A, const double* b, double* x) {
-    double L[6][6], D[6], y[6];
+    double L[6][6], D[6], Dinv[6], y[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
         double d = A[k * 6 + k];
@@ -207,6 +241,7 @@ __device__ __forceinline__ void ldlt6(const double* A, const double* b, double* 
         for (int j = 0; j < k; ++j) d -= L[k][j] * L[k][j] * D[j];
         D[k] = d;
         const double inv = 1.0 / d;
+        Dinv[k] = inv;
 #pragma unroll
         for (int i = k + 1; i < 6; ++i) {
             double t = A[i * 6 + k];
@@ -223,7 +258,7 @@ __device__ __forceinline__ void ldlt6(const double* A, const double* b, double* 
         y[i] = t;
     }
 #pragma unroll
-    for (int i = 0; i < 6; ++i) y[i] /= D[i];
+    for (int i = 0; i < 6; ++i) y[i] *= Dinv[i];
 #pragma unroll
     for (int i = 5; i >= 0; --i) {
         double t = y[i];
@@ -397,24 +432,44 @@ __device__ void reduce_partials_cg(const float* partials, int nb, int stride, in
     }
 }
 
-// Capacity of the per-block correspondence segments for n pixels: every
-// block of the pass-A grid gets as many slots as the pixels it visits.
+// Capacity of the per-warp correspondence segments for n pixels: every warp
+// of the pass-A grid gets as many slots as the pixels it visits.
 size_t track_list_capacity(int n) {
-    const int g = track_grid(n);
+    const int g = track_cluster_grid(n);
     const int iters = (n + g * 256 - 1) / (g * 256);
     return (size_t)g * iters * 256;
 }
 
-// pass A: ICP rows (reduced per block) and RGB correspondences, which each
-// block appends to its own segment of `list` in pixel-visit order (block-local
-// scan: deterministic).  Loop trip counts are uniform across the block.
-__global__ void __launch_bounds__(256, 2) k_track_a(TrackLevel L, TrackState* st, float* partials, int2* list,
-                                                    int* counts) {
-    if (st->failed) return;
-    __shared__ float sm[32 * 29];
+// Sum of a cluster's block sums: rank 0's first `nv` threads add value t of
+// every block of the cluster in rank order (FP64) through distributed shared
+// memory.  Every block of the cluster must call it (it holds two cluster
+// barriers: the block sums are complete before rank 0 reads, and stay alive
+// until it has read them).  Returns the sum in rank 0's threads t < nv.
+template <typename T>
+__device__ __forceinline__ double cluster_sum(cg::cluster_group& cl, T* s_vals, int nv) {
+    double v = 0;
+    cl.sync();
+    if (cl.block_rank() == 0 && (int)threadIdx.x < nv) {
+#pragma unroll
+        for (int r = 0; r < kTrackCluster; ++r) v += (double)cl.map_shared_rank(s_vals, r)[threadIdx.x];
+    }
+    cl.sync();
+    return v;
+}
+
+// pass A (one cluster of kTrackCluster blocks per group): ICP rows reduced per
+// block, then per cluster into the group sums; RGB correspondences appended by
+// each warp to its own segment of `list` in pixel-visit order (ballot +
+// popc: deterministic, no block barrier in the pixel loop), with the
+// correspondence count and sum of squared differences reduced the same way
+// (integers below 2^53, exact as doubles).
+__global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
+    k_track_a(TrackLevel L, TrackState* st, int2* list, int* counts) {
+    if (st->failed) return;   // uniform over the grid: written by the previous kernel
+    cg::cluster_group cl = cg::this_cluster();
+    __shared__ float sm[8 * 32];
     __shared__ long long smll[32];
-    __shared__ int s_warp[8];
-    __shared__ int s_run;
+    __shared__ double s_vals[32];
     const DevPose cur = st->cur, last = st->last;
     float acc[29];
 #pragma unroll
@@ -423,8 +478,10 @@ __global__ void __launch_bounds__(256, 2) k_track_a(TrackLevel L, TrackState* st
     const int N = L.W * L.H;
     const int G = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int iters = (N + G * 256 - 1) / (G * 256);
-    int2* seg = list + (size_t)blockIdx.x * iters * 256;
-    if (threadIdx.x == 0) s_run = 0;
+    const int gw = blockIdx.x * kTrackWarps + wid;
+    int2* seg = list + (size_t)gw * iters * 32;
+    const unsigned lt = (1u << lane) - 1u;
+    int run = 0;
     for (int k = 0; k < iters; ++k) {
         const int p = (k * G + blockIdx.x) * 256 + threadIdx.x;
         int r = -1;
@@ -440,89 +497,221 @@ __global__ void __launch_bounds__(256, 2) k_track_a(TrackLevel L, TrackState* st
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, r >= 0);
-        if (lane == 0) s_warp[wid] = __popc(m);
-        __syncthreads();
-        int base = s_run;
-        for (int w = 0; w < wid; ++w) base += s_warp[w];
-        if (r >= 0) seg[base + __popc(m & ((1u << lane) - 1))] = make_int2(p, r);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int t = 0;
-            for (int w = 0; w < 8; ++w) t += s_warp[w];
-            s_run += t;
-        }
+        if (r >= 0) seg[run + __popc(m & lt)] = make_int2(p, r);
+        run += __popc(m);
     }
-    block_sum<29>(acc, sm);
-    long long bc = block_sum_ll(rc, smll);
-    long long bs = block_sum_ll(rsq, smll);
-    if (threadIdx.x == 0) {
-        float* out = partials + (size_t)blockIdx.x * 32;
-#pragma unroll
-        for (int k = 0; k < 29; ++k) out[k] = acc[k];
-        st->scratch_cnt[blockIdx.x] = bc;
-        st->scratch_sq[blockIdx.x] = bs;
-        counts[blockIdx.x] = s_run;
+    if (lane == 0) counts[gw] = run;
+    const float bsum = block_sum29(acc, sm);
+    // block_sum_ll leaves the total in lane 0 of warp 0
+    const long long bc = __shfl_sync(0xffffffffu, block_sum_ll(rc, smll), 0);
+    const long long bs = __shfl_sync(0xffffffffu, block_sum_ll(rsq, smll), 0);
+    if (wid == 0) s_vals[lane] = lane < 29 ? (double)bsum : lane == 29 ? (double)bc : lane == 30 ? (double)bs : 0.0;
+    const double v = cluster_sum(cl, s_vals, 31);
+    if (cl.block_rank() == 0 && threadIdx.x < 31) {
+        const int g = blockIdx.x / kTrackCluster;
+        if (threadIdx.x < 29)
+            st->grp_icp[g][threadIdx.x] = v;
+        else if (threadIdx.x == 29)
+            st->grp_cnt[g] = (long long)v;
+        else
+            st->grp_sq[g] = (long long)v;
     }
 }
 
-__device__ __forceinline__ void solve_step(TrackState* st, const double* s, int min_count, int is_final);
+// Staging of the tracker state for the solve of one iteration.
+struct SolveIO {
+    double delta[16], last_pose[16], init_pose[16], pose[16];
+    DevPose cur;
+    float icp_error, icp_count, rgb_error, rgb_count;
+    int failed;    // this iteration failed: pose rolled back to last_pose
+    int updated;   // delta, pose and cur hold a Gauss-Newton update
+};
 
-// pass B: every block derives sigma from pass A's counts (same value in every
-// block) and builds the RGB rows of its own segment; the last block reduces
-// both passes' partials in FP64 and performs the Gauss-Newton update.
-__global__ void __launch_bounds__(256, 2) k_track_b(TrackLevel L, TrackState* st, float* partials,
-                                                    unsigned int* ticket, const int2* list, const int* counts,
-                                                    int seg_size, int min_count, int is_final) {
+__device__ void solve_staged(SolveIO& io, const double* s, int min_count, int is_final);
+
+// pass B (clusters as in pass A): every block derives sigma from pass A's
+// group counts (integers: the same value in every block) and builds the RGB
+// rows of its warps' segments; each cluster reduces its rows into a group
+// sum; the last cluster to finish adds the groups of both passes in group
+// order (FP64) and performs the Gauss-Newton update with one warp.
+__global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
+    k_track_b(TrackLevel L, TrackState* st, unsigned int* ticket, const int2* list, const int* counts, int seg_size,
+              int min_count, int is_final) {
     if (st->failed) return;
+    cg::cluster_group cl = cg::this_cluster();
     __shared__ float sm[32 * 29];
     __shared__ long long smll[32];
-    __shared__ double scratch[8 * 32];
+    __shared__ float s_rgb[32];
+    __shared__ double s_part[4][64];
     __shared__ double sums[64];
     __shared__ float s_sigma;
+    __shared__ long long s_cq[2];
+    __shared__ bool s_last;
+    __shared__ SolveIO io;
     const DevPose cur = st->cur, last = st->last;
-    const int G = gridDim.x;
-    // sigma = sqrt((float) sum / count) (Reduction.cu:606-608), sums in block order
+    const int G = gridDim.x, NG = G / kTrackCluster, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    // sigma = sqrt((float) sum / count) (Reduction.cu:606-608)
     long long c = 0, q = 0;
-    for (int b = threadIdx.x; b < G; b += blockDim.x) {
-        c += st->scratch_cnt[b];
-        q += st->scratch_sq[b];
+    for (int g = threadIdx.x; g < NG; g += blockDim.x) {
+        c += st->grp_cnt[g];
+        q += st->grp_sq[g];
     }
     c = block_sum_ll(c, smll);
     q = block_sum_ll(q, smll);
-    if (threadIdx.x == 0) s_sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
+    if (threadIdx.x == 0) {
+        s_sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
+        s_cq[0] = c;
+        s_cq[1] = q;
+    }
     __syncthreads();
     const float sigma = s_sigma;
     float acc[29];
 #pragma unroll
     for (int k = 0; k < 29; ++k) acc[k] = 0.f;
-    const int n = counts[blockIdx.x];
-    const int2* seg = list + (size_t)blockIdx.x * seg_size;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int gw = blockIdx.x * kTrackWarps + wid;
+    const int n = counts[gw];
+    const int2* seg = list + (size_t)gw * seg_size;
+    for (int i = lane; i < n; i += 32) {
         const int2 e = seg[i];
         const int y = e.x / L.W, x = e.x - y * L.W;
         float row[7];
         rgb_row(L, cur, last, x, y, e.y, sigma, row);
         add_products(row, acc);
     }
-    block_sum<29>(acc, sm);
-    float* rgbp = partials + (size_t)kTrackMaxBlocks * 32;   // second half of the partials buffer
-    if (threadIdx.x == 0)
-#pragma unroll
-        for (int k = 0; k < 29; ++k) rgbp[(size_t)blockIdx.x * 32 + k] = acc[k];
-    if (!last_block(ticket)) return;
-    reduce_partials(partials, G, 32, 29, sums, scratch);        // ICP
-    reduce_partials(rgbp, G, 32, 29, sums + 32, scratch);       // RGB
-    if (threadIdx.x < 29) {
-        st->icp_sums[threadIdx.x] = sums[threadIdx.x];
-        st->rgb_sums[threadIdx.x] = sums[32 + threadIdx.x];
+    const float bsum = block_sum29(acc, sm);
+    if (wid == 0) s_rgb[lane] = lane < 29 ? bsum : 0.f;
+    const int grp = blockIdx.x / kTrackCluster;
+    const double v = cluster_sum(cl, s_rgb, 29);
+    if (cl.block_rank() != 0) return;
+    if (threadIdx.x < 29) st->grp_rgb[grp][threadIdx.x] = v;
+    // last cluster (its rank-0 block) to finish
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(ticket, 1u) == (unsigned)(NG - 1);
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // group sums of both passes in group order: value t & 63 (0..28 ICP,
+    // 32..60 RGB) over four fixed ranges of groups, then the ranges in order
+    {
+        const int val = threadIdx.x & 63, part = threadIdx.x >> 6;
+        const int per = (NG + 3) / 4, g0 = part * per, g1 = min(NG, g0 + per);
+        double t = 0;
+        if ((val & 31) < 29) {
+            const double* src = val < 32 ? &st->grp_icp[0][val] : &st->grp_rgb[0][val - 32];
+#pragma unroll 8
+            for (int g = g0; g < g1; ++g) t += __ldcg(src + (size_t)g * 32);
+        }
+        s_part[part][val] = t;
+    }
+    // stage the tracker state while the sums are added
+    if (threadIdx.x >= 64 && threadIdx.x < 80) {
+        const int i = threadIdx.x - 64;
+        io.delta[i] = st->delta[i];
+        io.last_pose[i] = st->last_pose[i];
+        io.init_pose[i] = st->init_pose[i];
+    }
+    if (threadIdx.x == 80) {
+        io.icp_error = st->icp_error;
+        io.icp_count = st->icp_count;
     }
     __syncthreads();
-    if (threadIdx.x != 0) return;
-    *ticket = 0;
-    st->rgb_cnt = c;
-    st->rgb_sq = q;
-    st->sigma = sigma;
-    solve_step(st, sums, min_count, is_final);
+    if (threadIdx.x < 64) sums[threadIdx.x] = ((s_part[0][threadIdx.x] + s_part[1][threadIdx.x]) +
+                                               s_part[2][threadIdx.x]) + s_part[3][threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *ticket = 0;
+        solve_staged(io, sums, min_count, is_final);
+    }
+    __syncthreads();
+    // write back in parallel
+    if (threadIdx.x < 16) {
+        st->pose[threadIdx.x] = io.pose[threadIdx.x];
+        if (io.updated) st->delta[threadIdx.x] = io.delta[threadIdx.x];
+    } else if (threadIdx.x >= 32 && threadIdx.x < 32 + (int)(sizeof(DevPose) / 4)) {
+        if (io.updated) ((float*)&st->cur)[threadIdx.x - 32] = ((const float*)&io.cur)[threadIdx.x - 32];
+    } else if (threadIdx.x >= 64 && threadIdx.x < 93) {
+        st->icp_sums[threadIdx.x - 64] = sums[threadIdx.x - 64];
+        st->rgb_sums[threadIdx.x - 64] = sums[32 + threadIdx.x - 64];
+    } else if (threadIdx.x == 96) {
+        st->icp_error = io.icp_error;
+        st->icp_count = io.icp_count;
+        st->rgb_error = io.rgb_error;
+        st->rgb_count = io.rgb_count;
+        st->rgb_cnt = s_cq[0];
+        st->rgb_sq = s_cq[1];
+        st->sigma = sigma;
+        st->failed = io.failed;
+    }
+}
+
+// The Gauss-Newton update of one iteration (Tracking.cc:319-394) and, after
+// the last one, the acceptance test (Tracking.cc:398-408), on staged state:
+// io.delta / last_pose / init_pose / icp_error in; io.pose, delta, cur,
+// errors, counts, failed and updated out (a failed count or error test
+// leaves delta and cur as they were and sets pose = last_pose; a failed
+// acceptance test does so after the update).  One thread; every array in
+// registers.
+__device__ void solve_staged(SolveIO& io, const double* s, int min_count, int is_final) {
+    bool fail = false;
+    {
+        float r0 = (float)s[32 + 27], r1 = (float)s[32 + 28];
+        float err = sqrtf(r0) / r1;
+        io.rgb_error = err;
+        io.rgb_count = r1;
+        if (isnan(err) || (int)r1 < min_count) fail = true;
+    }
+    if (!fail) {
+        float q0 = (float)s[27], q1 = (float)s[28];
+        float icp_err = sqrtf(q0) / q1;
+        io.icp_error = icp_err;
+        io.icp_count = q1;
+        if (isnan(icp_err) || (int)q1 < min_count) fail = true;
+    }
+    io.failed = 0;
+    io.updated = 0;
+    if (fail) {
+        for (int i = 0; i < 16; ++i) io.pose[i] = io.last_pose[i];
+        io.failed = 1;
+        return;
+    }
+    double Ar[36], br[6], Ai[36], bi[6], A[36], b[6], x[6], dT[16], dinv[16], delta[16], lastp[16], pose[16];
+    unpack29(s + 32, Ar, br);
+    unpack29(s, Ai, bi);
+    const float w = 1e-4f;
+#pragma unroll
+    for (int i = 0; i < 36; ++i) A[i] = Ar[i] * (double)w + Ai[i];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) b[i] = br[i] * (double)w + bi[i];
+    ldlt6(A, b, x);
+    se3_exp(x, dT);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        delta[i] = io.delta[i];
+        lastp[i] = io.last_pose[i];
+    }
+    mat4_mul(dT, delta, delta);
+    mat4_rigid_inv(delta, dinv);
+    mat4_mul(lastp, dinv, pose);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        io.delta[i] = delta[i];
+        io.pose[i] = pose[i];
+    }
+    io.cur = make_dev_pose_d(pose);
+    io.updated = 1;
+    if (is_final) {
+        double pinv[16], p[16], init[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) init[i] = io.init_pose[i];
+        mat4_rigid_inv(init, pinv);
+        mat4_mul(pinv, pose, p);
+        double tn = sqrt(p[3] * p[3] + p[7] * p[7] + p[11] * p[11]);
+        if (!(io.icp_error < 0.0001f && euler_sin_norm(p) <= 0.1 && tn <= 0.1)) {
+            for (int i = 0; i < 16; ++i) io.pose[i] = io.last_pose[i];
+            io.failed = 1;
+        }
+    }
 }
 
 // The Gauss-Newton update of one iteration (Tracking.cc:319-394) and, after
@@ -595,18 +784,6 @@ __device__ __forceinline__ void solve_step(TrackState* st, const double* s, int 
     __threadfence();
 }
 
-// The solve of one iteration as its own kernel (multi-kernel path).
-__global__ void __launch_bounds__(32) k_track_solve(TrackState* st, int min_count, int is_final) {
-    if (threadIdx.x != 0 || st->failed) return;
-    double s[64];
-#pragma unroll
-    for (int k = 0; k < 29; ++k) {
-        s[k] = st->icp_sums[k];
-        s[32 + k] = st->rgb_sums[k];
-    }
-    solve_step(st, s, min_count, is_final);
-}
-
 // ----------------------------------------------------- persistent tracking
 
 // Grid-wide barrier for a cooperative launch (all blocks co-resident).  The
@@ -661,7 +838,7 @@ __device__ __forceinline__ DevPose load_pose_cg(const DevPose* p) {
 // level and iteration, pass A (ICP rows + RGB correspondences), pass B (RGB
 // rows), then block 0 reduces both passes in FP64 and solves; three grid
 // barriers per iteration.  Same arithmetic as k_track_a / k_track_b /
-// k_track_solve.
+// the staged solve of k_track_b.
 __global__ void __launch_bounds__(256, 2) k_track_frame(TrackFrame F) {
     __shared__ float sm[32 * 29];
     __shared__ long long smll[32];
@@ -858,13 +1035,39 @@ int launch_track_begin(TrackState* st, cudaStream_t s) { k_track_begin<<<1, 1, 0
     return 1;
 }
 
-int launch_track_iter(const TrackLevel& L, TrackState* st, float* partials, unsigned int* tickets, int2* residual,
-                      int* counts, int min_count, bool is_final, cudaStream_t s) {
+// Grid of the clustered per-iteration kernels: track_grid rounded up to whole
+// clusters, at most as many clusters as can be resident at once (a cluster
+// needs all its blocks on one GPC, so fewer than 2 x SMs / kTrackCluster may
+// fit), so that every launch runs in a single wave.
+int track_cluster_grid(int n) {
+    static int cap = 0;
+    if (!cap) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int c = sms > 0 ? 2 * sms / kTrackCluster : kTrackMaxGroups;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(c * kTrackCluster);
+        cfg.blockDim = dim3(256);
+        int ca = 0, cb = 0;
+        if (cudaOccupancyMaxActiveClusters(&ca, (void*)k_track_a, &cfg) == cudaSuccess && ca > 0 && ca < c) c = ca;
+        if (cudaOccupancyMaxActiveClusters(&cb, (void*)k_track_b, &cfg) == cudaSuccess && cb > 0 && cb < c) c = cb;
+        cudaGetLastError();
+        if (c > kTrackMaxGroups) c = kTrackMaxGroups;
+        cap = c * kTrackCluster;
+    }
+    const int g = (n + 255) / 256;
+    const int gc = (g + kTrackCluster - 1) / kTrackCluster * kTrackCluster;
+    return gc < cap ? gc : cap;
+}
+
+int launch_track_iter(const TrackLevel& L, TrackState* st, unsigned int* tickets, int2* residual, int* counts,
+                      int min_count, bool is_final, cudaStream_t s) {
     const int n = L.W * L.H;
-    const int g = track_grid(n);
-    const int seg = (n + g * 256 - 1) / (g * 256) * 256;
-    k_track_a<<<g, 256, 0, s>>>(L, st, partials, residual, counts);
-    k_track_b<<<g, 256, 0, s>>>(L, st, partials, tickets + 1, residual, counts, seg, min_count, is_final ? 1 : 0);
+    const int g = track_cluster_grid(n);
+    const int seg = (n + g * 256 - 1) / (g * 256) * 32;
+    k_track_a<<<g, 256, 0, s>>>(L, st, residual, counts);
+    k_track_b<<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, is_final ? 1 : 0);
     return 2;
 }
 
