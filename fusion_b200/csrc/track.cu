@@ -132,6 +132,94 @@ __device__ __forceinline__ void rgb_row(const TrackLevel& L, const DevPose& cur,
     row[6] = -w * (float)diff;
 }
 
+// Pose-independent inputs of one pixel for pass A (loaded one pixel ahead).
+struct PixelIn {
+    float4 vc;      // current vertex
+    float3 nc;      // current normal (xyz)
+    int ok;         // photometric eligibility (border, window, gradient)
+    int gc;         // current gray value
+};
+
+__device__ __forceinline__ PixelIn load_pixel(const TrackLevel& L, int p) {
+    PixelIn in;
+    const int y = p / L.W, x = p - y * L.W;
+    const size_t i = (size_t)y * L.vp + x, k = (size_t)y * L.sp + x;
+    in.vc = L.vcurr[i];
+    const float4 n = L.ncurr[i];
+    in.nc = make_float3(n.x, n.y, n.z);
+    in.ok = L.rgbok[k];
+    in.gc = L.gcurr[(size_t)y * L.gp + x];
+    return in;
+}
+
+// icp_row and rgb_corresp of one pixel together (same arithmetic, same
+// decisions), with the pose-independent loads done by the caller and the four
+// pose-dependent gathers (last vertex and normal at the ICP projection, last
+// vertex and gray value at the photometric projection) issued together.
+// Needs L.rgbok.  Returns whether the ICP row is valid; *rgb = packed
+// correspondence or -1.
+__device__ __forceinline__ bool pixel_pass_a(const TrackLevel& L, const DevPose& cur, const DevPose& last,
+                                             const PixelIn& in, float row[7], int* rgb) {
+    const f3 vcurr_c = xyz(in.vc);
+    const bool vnan = isnan(vcurr_c.x);
+    const f3 vcurr_g = add3(mv(cur.R, vcurr_c), cur.t);
+    // ICP projection (ICPReduce::searchPoint, Reduction.cu:227-250)
+    int ju = -1;
+    if (!vnan && !((double)vcurr_c.z < 1e-3)) {
+        const f3 vcurr_p = mv(last.Rinv, sub3(vcurr_g, last.t));
+        const float invz = (float)(1.0 / (double)vcurr_p.z);
+        const int u = (int)((double)fa(fm(fm(vcurr_p.x, invz), L.k.fx), L.k.cx) + 0.5);
+        const int v = (int)((double)fa(fm(fm(vcurr_p.y, invz), L.k.fy), L.k.cy) + 0.5);
+        if (!(u < 0 || v < 0 || u >= L.W || v >= L.H)) ju = v * L.vp + u;
+    }
+    // photometric projection (RGBReduction::FindCorresp, Reduction.cu:404-451)
+    int jr = -1, ur = 0, vr = 0;
+    if (in.ok && !vnan) {
+        const f3 vcl = mv(last.Rinv, sub3(vcurr_g, last.t));
+        const float pu = fa(fd(fm(L.k.fx, vcl.x), vcl.z), L.k.cx);
+        const float pv = fa(fd(fm(L.k.fy, vcl.y), vcl.z), L.k.cy);
+        ur = (int)floorf((float)((double)pu + 0.5));
+        vr = (int)floorf((float)((double)pv + 0.5));
+        if (ur >= 0 && vr >= 0 && ur < L.W && vr < L.H) jr = vr * L.vp + ur;
+    }
+    const float nanf_ = qnan();
+    const float4 vl4 = ju >= 0 ? L.vlast[ju] : make_float4(nanf_, nanf_, nanf_, nanf_);
+    const float4 nl4 = ju >= 0 ? L.nlast[ju] : make_float4(nanf_, nanf_, nanf_, nanf_);
+    const float4 vr4 = jr >= 0 ? L.vlast[jr] : make_float4(nanf_, nanf_, nanf_, nanf_);
+    const int gl = jr >= 0 ? (int)L.glast[(size_t)vr * L.gp + ur] : 0;
+    // photometric residual
+    *rgb = -1;
+    if (jr >= 0 && !isnan(vr4.x)) {
+        const float ddx = fs(vr4.x, in.vc.x), ddy = fs(vr4.y, in.vc.y), ddz = fs(vr4.z, in.vc.z),
+                    ddw = fs(vr4.w, in.vc.w);
+        const float nd = fsq(fa(fa(fa(fm(ddx, ddx), fm(ddy, ddy)), fm(ddz, ddz)), fm(ddw, ddw)));
+        if ((double)nd < 0.1 && gl != 0) *rgb = ((vr * L.W + ur) << 9) | (in.gc - gl + 255);
+    }
+    // ICP row (ICPReduce::getRow, Reduction.cu:252-286)
+    if (ju < 0) return false;
+    const f3 vlast_c = xyz(vl4);
+    const f3 vlast_g = add3(mv(last.R, vlast_c), last.t);
+    const f3 ncurr_c = mk3(in.nc.x, in.nc.y, in.nc.z);
+    const f3 ncurr_g = mv(cur.R, ncurr_c);
+    const f3 nlast_c = xyz(nl4);
+    const f3 nlast_g = mv(last.R, nlast_c);
+    const float dist = norm3(sub3(vlast_g, vcurr_g));
+    const float sine = norm3(cross3(ncurr_g, nlast_g));
+    if (!(sine < 0.6f && dist <= 0.1f && !isnan(ncurr_c.x) && !isnan(nlast_c.x))) return false;
+    const f3 nl = mv(last.Rinv, nlast_g);
+    const f3 vcl = mv(last.Rinv, sub3(vcurr_g, last.t));
+    const f3 vll = mv(last.Rinv, sub3(vlast_g, last.t));
+    const f3 c = cross3(nl, vll);
+    row[0] = -nl.x;
+    row[1] = -nl.y;
+    row[2] = -nl.z;
+    row[3] = c.x;
+    row[4] = c.y;
+    row[5] = c.z;
+    row[6] = dot3(neg3(nl), sub3(vcl, vll));
+    return true;
+}
+
 __device__ __forceinline__ void add_products(const float row[7], float acc[29]) {
     int n = 0;
 #pragma unroll
@@ -462,7 +550,7 @@ __device__ __forceinline__ double cluster_sum(cg::cluster_group& cl, T* s_vals, 
 // each warp to its own segment of `list` in pixel-visit order (ballot +
 // popc: deterministic, no block barrier in the pixel loop), with the
 // correspondence count and sum of squared differences reduced the same way
-// (integers below 2^53, exact as doubles).
+// (integers below 2^53, exact as doubles).  L.rgbok must be set.
 __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
     k_track_a(TrackLevel L, TrackState* st, int2* list, int* counts) {
     if (st->failed) return;   // uniform over the grid: written by the previous kernel
@@ -482,14 +570,16 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
     int2* seg = list + (size_t)gw * iters * 32;
     const unsigned lt = (1u << lane) - 1u;
     int run = 0;
-    for (int k = 0; k < iters; ++k) {
-        const int p = (k * G + blockIdx.x) * 256 + threadIdx.x;
+    int p = blockIdx.x * 256 + threadIdx.x;
+    PixelIn nxt;
+    if (p < N) nxt = load_pixel(L, p);
+    for (int k = 0; k < iters; ++k, p += G * 256) {
+        const PixelIn in = nxt;
+        if (k + 1 < iters && p + G * 256 < N) nxt = load_pixel(L, p + G * 256);   // one pixel ahead
         int r = -1;
         if (p < N) {
-            const int y = p / L.W, x = p - y * L.W;
             float row[7];
-            if (icp_row(L, cur, last, x, y, row)) add_products(row, acc);
-            r = rgb_corresp(L, cur, last, x, y);
+            if (pixel_pass_a(L, cur, last, in, row, &r)) add_products(row, acc);
             if (r >= 0) {
                 int d = (r & 511) - 255;
                 rc += 1;
