@@ -314,6 +314,15 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket) {
     return is_last;
 }
 
+// Ticket increment with release (this block's prior writes, ordered before it
+// by a block barrier) and acquire (the writes of the blocks that incremented
+// before) semantics at GPU scope.
+__device__ __forceinline__ unsigned int ticket_acq_rel(unsigned int* t) {
+    unsigned int old;
+    asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(old) : "l"(t) : "memory");
+    return old;
+}
+
 // ----------------------------------------------------------- FP64 solver
 
 // LDL^T of the 6x6 symmetric positive definite normal matrix and the solve
@@ -553,7 +562,12 @@ __device__ __forceinline__ double cluster_sum(cg::cluster_group& cl, T* s_vals, 
 // (integers below 2^53, exact as doubles).  L.rgbok must be set.
 __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
     k_track_a(TrackLevel L, TrackState* st, int2* list, int* counts) {
-    if (st->failed) return;   // uniform over the grid: written by the previous kernel
+    const int N = L.W * L.H;
+    const int G = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int p = blockIdx.x * 256 + threadIdx.x;
+    PixelIn nxt;
+    if (p < N) nxt = load_pixel(L, p);
+    if (st->failed) return;   // uniform over the grid: written by an earlier kernel
     cg::cluster_group cl = cg::this_cluster();
     __shared__ float sm[8 * 32];
     __shared__ long long smll[32];
@@ -563,16 +577,11 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
 #pragma unroll
     for (int k = 0; k < 29; ++k) acc[k] = 0.f;
     long long rc = 0, rsq = 0;
-    const int N = L.W * L.H;
-    const int G = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int iters = (N + G * 256 - 1) / (G * 256);
     const int gw = blockIdx.x * kTrackWarps + wid;
     int2* seg = list + (size_t)gw * iters * 32;
     const unsigned lt = (1u << lane) - 1u;
     int run = 0;
-    int p = blockIdx.x * 256 + threadIdx.x;
-    PixelIn nxt;
-    if (p < N) nxt = load_pixel(L, p);
     for (int k = 0; k < iters; ++k, p += G * 256) {
         const PixelIn in = nxt;
         if (k + 1 < iters && p + G * 256 < N) nxt = load_pixel(L, p + G * 256);   // one pixel ahead
@@ -627,34 +636,42 @@ __device__ void solve_staged(SolveIO& io, const double* s, int min_count, int is
 __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
     k_track_b(TrackLevel L, TrackState* st, unsigned int* ticket, const int2* list, const int* counts, int seg_size,
               int min_count, int is_final) {
-    if (st->failed) return;
     cg::cluster_group cl = cg::this_cluster();
     __shared__ float sm[32 * 29];
-    __shared__ long long smll[32];
     __shared__ float s_rgb[32];
     __shared__ double s_part[4][64];
     __shared__ double sums[64];
-    __shared__ float s_sigma;
-    __shared__ long long s_cq[2];
     __shared__ bool s_last;
     __shared__ SolveIO io;
-    const DevPose cur = st->cur, last = st->last;
     const int G = gridDim.x, NG = G / kTrackCluster, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    // sigma = sqrt((float) sum / count) (Reduction.cu:606-608)
+    // stage the solve's inputs early (used by the last cluster's first block)
+    if (cl.block_rank() == 0) {
+        if (threadIdx.x >= 64 && threadIdx.x < 80) {
+            const int i = threadIdx.x - 64;
+            io.delta[i] = st->delta[i];
+            io.last_pose[i] = st->last_pose[i];
+            io.init_pose[i] = st->init_pose[i];
+        }
+        if (threadIdx.x == 80) {
+            io.icp_error = st->icp_error;
+            io.icp_count = st->icp_count;
+        }
+    }
+    if (st->failed) return;
+    const DevPose cur = st->cur, last = st->last;
+    // sigma = sqrt((float) sum / count) (Reduction.cu:606-608); every warp
+    // adds the group counts itself (integers: exact in any order)
     long long c = 0, q = 0;
-    for (int g = threadIdx.x; g < NG; g += blockDim.x) {
-        c += st->grp_cnt[g];
-        q += st->grp_sq[g];
+    for (int g = lane; g < NG; g += 32) {
+        c += __ldcg(&st->grp_cnt[g]);
+        q += __ldcg(&st->grp_sq[g]);
     }
-    c = block_sum_ll(c, smll);
-    q = block_sum_ll(q, smll);
-    if (threadIdx.x == 0) {
-        s_sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
-        s_cq[0] = c;
-        s_cq[1] = q;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+        q += __shfl_xor_sync(0xffffffffu, q, o);
     }
-    __syncthreads();
-    const float sigma = s_sigma;
+    const float sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
     float acc[29];
 #pragma unroll
     for (int k = 0; k < 29; ++k) acc[k] = 0.f;
@@ -675,12 +692,10 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
     if (cl.block_rank() != 0) return;
     if (threadIdx.x < 29) st->grp_rgb[grp][threadIdx.x] = v;
     // last cluster (its rank-0 block) to finish
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(ticket, 1u) == (unsigned)(NG - 1);
+    if (threadIdx.x == 0) s_last = ticket_acq_rel(ticket) == (unsigned)(NG - 1);
     __syncthreads();
     if (!s_last) return;
-    __threadfence();
     // group sums of both passes in group order: value t & 63 (0..28 ICP,
     // 32..60 RGB) over four fixed ranges of groups, then the ranges in order
     {
@@ -693,17 +708,6 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
             for (int g = g0; g < g1; ++g) t += __ldcg(src + (size_t)g * 32);
         }
         s_part[part][val] = t;
-    }
-    // stage the tracker state while the sums are added
-    if (threadIdx.x >= 64 && threadIdx.x < 80) {
-        const int i = threadIdx.x - 64;
-        io.delta[i] = st->delta[i];
-        io.last_pose[i] = st->last_pose[i];
-        io.init_pose[i] = st->init_pose[i];
-    }
-    if (threadIdx.x == 80) {
-        io.icp_error = st->icp_error;
-        io.icp_count = st->icp_count;
     }
     __syncthreads();
     if (threadIdx.x < 64) sums[threadIdx.x] = ((s_part[0][threadIdx.x] + s_part[1][threadIdx.x]) +
@@ -728,8 +732,8 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
         st->icp_count = io.icp_count;
         st->rgb_error = io.rgb_error;
         st->rgb_count = io.rgb_count;
-        st->rgb_cnt = s_cq[0];
-        st->rgb_sq = s_cq[1];
+        st->rgb_cnt = c;
+        st->rgb_sq = q;
         st->sigma = sigma;
         st->failed = io.failed;
     }
