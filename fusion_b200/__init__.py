@@ -6,8 +6,9 @@ cnxyang/Fusion behind a C ABI (include/fusion_b200.h).
     r = s.grab(depth_u16, rgb_u8)      # one System::GrabImage
 """
 from ._lib import FusionError, load  # noqa: F401
+from .batch import Batch, mixed_config, mixed_population  # noqa: F401
 from .system import (Session, System, config_c1, config_c2, config_dict, make_config,  # noqa: F401
                      reference_config)
 
-__all__ = ["Session", "System", "config_c1", "config_c2", "make_config", "reference_config", "config_dict",
-           "FusionError", "load"]
+__all__ = ["Session", "System", "Batch", "mixed_config", "mixed_population", "config_c1", "config_c2",
+           "make_config", "reference_config", "config_dict", "FusionError", "load"]

@@ -55,6 +55,11 @@ class Image(ctypes.Structure):
                 ("rows", ctypes.c_int)]
 
 
+class FrameInput(ctypes.Structure):
+    _fields_ = [("depth", ctypes.c_void_p), ("depth_pitch", ctypes.c_size_t), ("rgb", ctypes.c_void_p),
+                ("rgb_pitch", ctypes.c_size_t), ("on_device", ctypes.c_int)]
+
+
 # name -> (restype, argtypes)
 _vp, _i, _f, _sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_size_t
 _fp = ctypes.POINTER(ctypes.c_float)
@@ -74,6 +79,12 @@ SIGNATURES = {
     "fb_session_set_graphs": (_i, [_vp, _i]),
     "fb_session_set_persistent": (_i, [_vp, _i]),
     "fb_session_stage_times": (_i, [_vp, _vp, _vp, _i]),
+    "fb_session_set_raycast_tile": (_i, [_vp, _i, _i]),
+    "fb_batch_create": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "fb_batch_destroy": (_i, [_vp]),
+    "fb_batch_set_mode": (_i, [_vp, _i]),
+    "fb_batch_step": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "fb_batch_stats": (_i, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "fb_session_launch_count": (_i, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "fb_frame_transfer_bytes": (_i, [ctypes.POINTER(Config), ctypes.POINTER(_sz), ctypes.POINTER(_sz)]),
     "fb_download_level": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),

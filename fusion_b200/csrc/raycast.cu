@@ -238,8 +238,8 @@ int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const in
 }
 
 int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,
-                    const DevPose* pose, const int* skip, cudaStream_t s) {
-    dim3 b(16, 8), g((W + 15) / 16, (H + 7) / 8);
+                    const DevPose* pose, const int* skip, cudaStream_t s, int bx, int by) {
+    dim3 b(bx, by), g((W + bx - 1) / bx, (H + by - 1) / by);
     k_raycast<<<g, b, 0, s>>>(m, vmap, nmap, p, W, H, k, pose, skip);
     return 1;
 }

@@ -12,6 +12,7 @@
 // machine (Tracking/Tracking.cc:58-112) and swaps the frames.
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
 #include <vector>
 
@@ -49,6 +50,14 @@ struct FrameOut {
     int n_alloc, n_visible, n_new, n_tiles;
     unsigned err;
     int heap_counter, entry_ptr, seq_path;
+};
+
+// What one frame does, decided on the host before it is issued.
+struct FramePlan {
+    int state;      // tracker state at this frame: 1 init, 0 tracking, -1 lost
+    bool init, track, fuse, render;
+    int after;      // frames_after_reloc after this frame
+    int mode;       // 0 init, 1 track, 2 lost (graph key)
 };
 
 __global__ void k_init_poses(TrackState* st) {
@@ -163,6 +172,7 @@ struct fb_session {
     bool persistent;           // tracking as one cooperative kernel per frame
     cudaGraphExec_t graph[3][2][2];
     int graph_kernels[3][2][2];
+    int rc_bx, rc_by;          // raycast tile
 };
 
 namespace {
@@ -354,7 +364,8 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
         // Mapping::RayTrace (Mapping.cc:92-109) into the frame's level-0 maps
         n += launch_zrange(s->map, s->K[0], pose, skip, st);
         mark(7);
-        n += launch_raycast(s->map, N.vmap[0], N.nmap[0], s->W[0], s->W[0], s->H[0], s->K[0], pose, skip, st);
+        n += launch_raycast(s->map, N.vmap[0], N.nmap[0], s->W[0], s->W[0], s->H[0], s->K[0], pose, skip, st,
+                            s->rc_bx, s->rc_by);
         *ran |= 3u << 6;
     } else {
         mark(7);
@@ -393,6 +404,139 @@ Intr intr_from(const float K[4]) {
     k.invfx = (float)(1.0 / (double)k.fx);
     k.invfy = (float)(1.0 / (double)k.fy);
     return k;
+}
+
+}  // namespace
+
+namespace {
+
+// Cached frame graphs are released (rebuilt on next use).
+void drop_graphs(fb_session* s) {
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 2; ++c)
+                if (s->graph[a][b][c]) {
+                    cudaGraphExecDestroy(s->graph[a][b][c]);
+                    s->graph[a][b][c] = nullptr;
+                }
+}
+
+// Host input -> the device input buffers of fr[next].
+int copy_frame_in(fb_session* s, const uint16_t* depth, size_t depth_pitch, const uint8_t* rgb, size_t rgb_pitch,
+                  int on_device, cudaStream_t st) {
+    const int W = s->W[0], H = s->H[0];
+    if (depth_pitch < (size_t)W * 2 || rgb_pitch < (size_t)W * 3) return FB_EINVAL;
+    FrameBuf& N = s->fr[s->next];
+    cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    FB_CUDA(cudaMemcpy2DAsync(N.depth_in, (size_t)W * 2, depth, depth_pitch, (size_t)W * 2, H, kind, st));
+    FB_CUDA(cudaMemcpy2DAsync(N.rgb, (size_t)W * 3, rgb, rgb_pitch, (size_t)W * 3, H, kind, st));
+    return FB_OK;
+}
+
+// Tracker::Track (Tracking.cc:58-112): the state is known on the host;
+// whether tracking succeeds is decided on the device.
+FramePlan plan_frame(fb_session* s) {
+    FramePlan p;
+    std::swap(s->state, s->last_state);
+    p.state = s->state;
+    p.init = p.state == 1;
+    p.track = p.state == 0;
+    // System::GrabImage (System.cc:98-115): frames_after_reloc is updated from
+    // the tracker state, which does not depend on this frame's outcome
+    p.after = s->frames_after_reloc;
+    if (p.state == 0) p.after++;
+    if (p.state == -1) p.after = 0;
+    p.fuse = (p.init || p.track) && p.after >= 10;
+    p.render = p.init || p.track;
+    p.mode = p.init ? 0 : p.track ? 1 : 2;
+    return p;
+}
+
+// The frame's kernels on stream `st`: the session's cached graph of this
+// (mode, fuse, next) when graphs are on and profiling is off (captured on
+// first use), else direct launches.
+int enqueue_frame(fb_session* s, const FramePlan& p, cudaStream_t st, unsigned* ran) {
+    *ran = 0;
+    if (s->use_graphs && !s->profile) {
+        cudaGraphExec_t& g = s->graph[p.mode][p.fuse ? 1 : 0][s->next];
+        if (!g) {
+            cudaGraph_t graph = nullptr;
+            cudaStream_t keep = s->stream;
+            s->stream = st;
+            cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            int nk = 0;
+            if (e == cudaSuccess) {
+                nk = issue_frame(s, p.track, p.fuse, p.render, p.init, ran);
+                e = cudaStreamEndCapture(st, &graph);
+            }
+            s->stream = keep;
+            if (e == cudaSuccess) e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&g, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                g = nullptr;
+                cuda_ok(e);
+                return FB_ECUDA;
+            }
+            s->graph_kernels[p.mode][p.fuse ? 1 : 0][s->next] = nk;
+        }
+        FB_CUDA(cudaGraphLaunch(g, st));
+        s->launches += (uint64_t)s->graph_kernels[p.mode][p.fuse ? 1 : 0][s->next];
+        *ran = 0;
+        return FB_OK;
+    }
+    cudaStream_t keep = s->stream;
+    s->stream = st;
+    s->launches += (uint64_t)issue_frame(s, p.track, p.fuse, p.render, p.init, ran);
+    s->stream = keep;
+    return check_launch();
+}
+
+// After the frame's result has reached h_out: the reference's tracking state
+// machine (Tracking.cc:58-112) and SwapFrame, and the caller's result.
+void finish_frame(fb_session* s, const FramePlan& p, fb_frame_result* out) {
+    const FrameOut& o = *s->h_out;
+    bool valid = false;
+    if (p.init) {
+        s->next = 1 - s->next;  // SwapFrame
+        s->last_state = 0;
+        valid = true;
+    } else if (p.track) {
+        if (!o.failed) {
+            s->no_missed = 0;
+            if (s->last_state != -1) {
+                s->last_state = 0;
+                s->next = 1 - s->next;
+                valid = true;
+            } else {
+                s->last_state = 0;
+            }
+        } else {
+            s->last_state = 0;
+            if (++s->no_missed > 9) s->last_state = -1;
+        }
+    } else {
+        s->last_state = -1;
+    }
+    s->frames_after_reloc = p.after;
+    std::memcpy(s->pose, o.pose, sizeof s->pose);
+    if (out) {
+        out->status = valid ? FB_OK : FB_ETRACK_LOST;
+        out->tracked = valid;
+        out->tracker_state = p.state;
+        out->fused = p.fuse && valid;
+        out->no_visible = (p.fuse && valid) ? (uint32_t)o.n_visible : 0;
+        out->no_allocated = (uint32_t)o.n_alloc;
+        out->no_new = (p.fuse && valid) ? (uint32_t)o.n_new : 0;
+        out->error_flags = o.err;
+        out->icp_error = o.icp_error;
+        out->icp_count = o.icp_count;
+        out->rgb_error = o.rgb_error;
+        out->rgb_count = o.rgb_count;
+        std::memcpy(out->pose, o.pose, sizeof out->pose);
+        out->frame_id = s->frame_id;
+    }
+    s->frame_id++;
 }
 
 }  // namespace
@@ -465,6 +609,8 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
     s->launches = 0;
     s->use_graphs = true;
     s->persistent = false;   // measured slower than graph-launched kernels on B200
+    s->rc_bx = 16;
+    s->rc_by = 8;
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 2; ++b)
             for (int c = 0; c < 2; ++c) {
@@ -555,51 +701,12 @@ int fb_session_reset(fb_session* s) {
 int fb_grab_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, const uint8_t* rgb, size_t rgb_pitch,
                   int on_device, fb_frame_result* out) {
     if (!s || !depth || !rgb) return FB_EINVAL;
-    const int W = s->W[0], H = s->H[0];
-    if (depth_pitch < (size_t)W * 2 || rgb_pitch < (size_t)W * 3) return FB_EINVAL;
-    FrameBuf& N = s->fr[s->next];
-    cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    FB_CUDA(cudaMemcpy2DAsync(N.depth_in, (size_t)W * 2, depth, depth_pitch, (size_t)W * 2, H, kind, s->stream));
-    FB_CUDA(cudaMemcpy2DAsync(N.rgb, (size_t)W * 3, rgb, rgb_pitch, (size_t)W * 3, H, kind, s->stream));
-    // Tracker::Track (Tracking.cc:58-112): the state is known on the host;
-    // whether tracking succeeds is decided on the device.
-    std::swap(s->state, s->last_state);
-    const int state = s->state;
-    const bool init = state == 1;
-    const bool track = state == 0;
-    // System::GrabImage (System.cc:98-115): frames_after_reloc is updated from
-    // the tracker state, which does not depend on this frame's outcome
-    int after = s->frames_after_reloc;
-    if (state == 0) after++;
-    if (state == -1) after = 0;
-    const bool fuse = (init || track) && after >= 10;
-    const bool render = init || track;
+    int rc = copy_frame_in(s, depth, depth_pitch, rgb, rgb_pitch, on_device, s->stream);
+    if (rc) return rc;
+    const FramePlan p = plan_frame(s);
     unsigned ran = 0;
-    if (s->use_graphs && !s->profile) {
-        // the whole frame as one graph launch; captured on first use
-        const int mode = init ? 0 : track ? 1 : 2;
-        cudaGraphExec_t& g = s->graph[mode][fuse ? 1 : 0][s->next];
-        if (!g) {
-            cudaGraph_t graph = nullptr;
-            FB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-            int nk = issue_frame(s, track, fuse, render, init, &ran);
-            cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
-            if (e == cudaSuccess) e = cudaGetLastError();
-            if (e == cudaSuccess) e = cudaGraphInstantiate(&g, graph, 0);
-            if (graph) cudaGraphDestroy(graph);
-            if (e != cudaSuccess) {
-                g = nullptr;
-                cuda_ok(e);
-                return FB_ECUDA;
-            }
-            s->graph_kernels[mode][fuse ? 1 : 0][s->next] = nk;
-        }
-        FB_CUDA(cudaGraphLaunch(g, s->stream));
-        s->launches += (uint64_t)s->graph_kernels[mode][fuse ? 1 : 0][s->next];
-    } else {
-        s->launches += (uint64_t)issue_frame(s, track, fuse, render, init, &ran);
-        if (check_launch()) return FB_ECUDA;
-    }
+    rc = enqueue_frame(s, p, s->stream, &ran);
+    if (rc) return rc;
     FB_CUDA(cudaMemcpyAsync(s->h_out, s->d_out, sizeof(FrameOut), cudaMemcpyDeviceToHost, s->stream));
     FB_CUDA(cudaStreamSynchronize(s->stream));
     if (s->profile)
@@ -610,48 +717,16 @@ int fb_grab_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, cons
             s->stage_ms[k] += ms;
             s->stage_calls[k] += 1;
         }
-    const FrameOut& o = *s->h_out;
-    bool valid = false;
-    if (init) {
-        s->next = 1 - s->next;  // SwapFrame
-        s->last_state = 0;
-        valid = true;
-    } else if (track) {
-        if (!o.failed) {
-            s->no_missed = 0;
-            if (s->last_state != -1) {
-                s->last_state = 0;
-                s->next = 1 - s->next;
-                valid = true;
-            } else {
-                s->last_state = 0;
-            }
-        } else {
-            s->last_state = 0;
-            if (++s->no_missed > 9) s->last_state = -1;
-        }
-    } else {
-        s->last_state = -1;
-    }
-    s->frames_after_reloc = after;
-    std::memcpy(s->pose, o.pose, sizeof s->pose);
-    if (out) {
-        out->status = valid ? FB_OK : FB_ETRACK_LOST;
-        out->tracked = valid;
-        out->tracker_state = state;
-        out->fused = fuse && valid;
-        out->no_visible = (fuse && valid) ? (uint32_t)o.n_visible : 0;
-        out->no_allocated = (uint32_t)o.n_alloc;
-        out->no_new = (fuse && valid) ? (uint32_t)o.n_new : 0;
-        out->error_flags = o.err;
-        out->icp_error = o.icp_error;
-        out->icp_count = o.icp_count;
-        out->rgb_error = o.rgb_error;
-        out->rgb_count = o.rgb_count;
-        std::memcpy(out->pose, o.pose, sizeof out->pose);
-        out->frame_id = s->frame_id;
-    }
-    s->frame_id++;
+    finish_frame(s, p, out);
+    return FB_OK;
+}
+
+int fb_session_set_raycast_tile(fb_session* s, int bx, int by) {
+    if (!s || bx < 1 || by < 1 || bx * by > 128 || (bx * by) % 32 != 0) return FB_EINVAL;
+    if (bx == s->rc_bx && by == s->rc_by) return FB_OK;
+    drop_graphs(s);
+    s->rc_bx = bx;
+    s->rc_by = by;
     return FB_OK;
 }
 
@@ -663,16 +738,7 @@ int fb_session_set_graphs(fb_session* s, int on) {
 
 int fb_session_set_persistent(fb_session* s, int on) {
     if (!s) return FB_EINVAL;
-    if (s->persistent != (on != 0)) {
-        // cached graphs hold the other tracking variant
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 2; ++b)
-                for (int c = 0; c < 2; ++c)
-                    if (s->graph[a][b][c]) {
-                        cudaGraphExecDestroy(s->graph[a][b][c]);
-                        s->graph[a][b][c] = nullptr;
-                    }
-    }
+    if (s->persistent != (on != 0)) drop_graphs(s);   // cached graphs hold the other tracking variant
     s->persistent = on != 0;
     return FB_OK;
 }
@@ -1080,6 +1146,187 @@ int fb_raycast(fb_session* s, fb_image* vmap, fb_image* nmap, const float Rview[
         FB_CUDA(cudaMemcpy(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost));
         *rendered = c.n_tiles > 0;
     }
+    return FB_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ batches
+
+struct fb_batch {
+    cudaStream_t origin = nullptr;
+    bool own_origin = false;
+    int mode = 0;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaStream_t> slots;
+    std::vector<cudaEvent_t> done;
+    // mode 1: one graph per composition
+    std::map<std::vector<uint64_t>, std::pair<cudaGraphExec_t, int>> cache;
+    uint64_t steps = 0, captures = 0;
+};
+
+namespace {
+
+constexpr size_t kBatchCacheMax = 32;
+
+void clear_cache(fb_batch* b) {
+    for (auto& kv : b->cache) cudaGraphExecDestroy(kv.second.first);
+    b->cache.clear();
+}
+
+int ensure_slots(fb_batch* b, int n) {
+    while ((int)b->slots.size() < n) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        FB_CUDA(cudaStreamCreate(&st));
+        if (!cuda_ok(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming))) {
+            cudaStreamDestroy(st);
+            return FB_ECUDA;
+        }
+        b->slots.push_back(st);
+        b->done.push_back(ev);
+    }
+    return FB_OK;
+}
+
+// The frames of a step, each on its own slot stream, forked from and joined
+// back into the origin stream.  With capture on, the same calls record one
+// graph.  direct: launch each session's cached frame graph (mode 0), else
+// issue its kernels (captured into the composite graph, mode 1).
+int issue_step(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plans, bool direct, int* kernels) {
+    FB_CUDA(cudaEventRecord(b->fork, b->origin));
+    *kernels = 0;
+    for (int i = 0; i < n; ++i) {
+        fb_session* s = ss[i];
+        cudaStream_t st = b->slots[i];
+        FB_CUDA(cudaStreamWaitEvent(st, b->fork, 0));
+        if (direct) {
+            unsigned ran = 0;
+            int rc = enqueue_frame(s, plans[i], st, &ran);
+            if (rc) return rc;
+        } else {
+            unsigned ran = 0;
+            cudaStream_t keep = s->stream;
+            s->stream = st;
+            *kernels += issue_frame(s, plans[i].track, plans[i].fuse, plans[i].render, plans[i].init, &ran);
+            s->stream = keep;
+        }
+        FB_CUDA(cudaMemcpyAsync(s->h_out, s->d_out, sizeof(FrameOut), cudaMemcpyDeviceToHost, st));
+        FB_CUDA(cudaEventRecord(b->done[i], st));
+        FB_CUDA(cudaStreamWaitEvent(b->origin, b->done[i], 0));
+    }
+    return check_launch();
+}
+
+}  // namespace
+
+extern "C" {
+
+int fb_batch_create(void* stream, fb_batch** out) {
+    if (!out) return FB_EINVAL;
+    fb_batch* b = new (std::nothrow) fb_batch();
+    if (!b) return FB_ENOMEM;
+    b->origin = (cudaStream_t)stream;
+    if (!b->origin) {
+        if (!cuda_ok(cudaStreamCreate(&b->origin))) {
+            delete b;
+            return FB_ECUDA;
+        }
+        b->own_origin = true;
+    }
+    if (!cuda_ok(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming))) {
+        if (b->own_origin) cudaStreamDestroy(b->origin);
+        delete b;
+        return FB_ECUDA;
+    }
+    *out = b;
+    return FB_OK;
+}
+
+int fb_batch_destroy(fb_batch* b) {
+    if (!b) return FB_EINVAL;
+    cudaStreamSynchronize(b->origin);
+    clear_cache(b);
+    for (size_t i = 0; i < b->slots.size(); ++i) {
+        cudaStreamSynchronize(b->slots[i]);
+        cudaStreamDestroy(b->slots[i]);
+        cudaEventDestroy(b->done[i]);
+    }
+    cudaEventDestroy(b->fork);
+    if (b->own_origin) cudaStreamDestroy(b->origin);
+    delete b;
+    return FB_OK;
+}
+
+int fb_batch_set_mode(fb_batch* b, int mode) {
+    if (!b || mode < 0 || mode > 1) return FB_EINVAL;
+    b->mode = mode;
+    return FB_OK;
+}
+
+int fb_batch_stats(fb_batch* b, uint64_t* steps, uint64_t* captures) {
+    if (!b) return FB_EINVAL;
+    if (steps) *steps = b->steps;
+    if (captures) *captures = b->captures;
+    return FB_OK;
+}
+
+int fb_batch_step(fb_batch* b, fb_session* const* ss, int n, const fb_frame_input* in, fb_frame_result* out) {
+    if (!b || !ss || !in || n <= 0) return FB_EINVAL;
+    for (int i = 0; i < n; ++i) {
+        if (!ss[i] || !in[i].depth || !in[i].rgb) return FB_EINVAL;
+        if (in[i].depth_pitch < (size_t)ss[i]->W[0] * 2 || in[i].rgb_pitch < (size_t)ss[i]->W[0] * 3)
+            return FB_EINVAL;
+        for (int j = 0; j < i; ++j)
+            if (ss[j] == ss[i]) return FB_EINVAL;
+    }
+    int rc = ensure_slots(b, n);
+    if (rc) return rc;
+    // inputs first (on the origin stream; the frames fork after them)
+    for (int i = 0; i < n; ++i) {
+        rc = copy_frame_in(ss[i], in[i].depth, in[i].depth_pitch, in[i].rgb, in[i].rgb_pitch, in[i].on_device,
+                           b->origin);
+        if (rc) return rc;
+    }
+    std::vector<FramePlan> plans(n);
+    for (int i = 0; i < n; ++i) plans[i] = plan_frame(ss[i]);
+    if (b->mode == 1) {
+        std::vector<uint64_t> key;
+        key.reserve(2 * n);
+        for (int i = 0; i < n; ++i) {
+            const fb_session* s = ss[i];
+            key.push_back((uint64_t)(uintptr_t)s);
+            key.push_back((uint64_t)plans[i].mode | (uint64_t)plans[i].fuse << 2 | (uint64_t)s->next << 3 |
+                          (uint64_t)s->persistent << 4 | (uint64_t)s->rc_bx << 8 | (uint64_t)s->rc_by << 20);
+        }
+        auto it = b->cache.find(key);
+        if (it == b->cache.end()) {
+            if (b->cache.size() >= kBatchCacheMax) clear_cache(b);
+            cudaGraph_t graph = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            int kernels = 0;
+            FB_CUDA(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
+            rc = issue_step(b, ss, n, plans.data(), false, &kernels);
+            cudaError_t e = cudaStreamEndCapture(b->origin, &graph);
+            if (rc == FB_OK && e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (rc) return rc;
+            FB_CUDA(e);
+            it = b->cache.emplace(key, std::make_pair(exec, kernels)).first;
+            b->captures++;
+        }
+        FB_CUDA(cudaGraphLaunch(it->second.first, b->origin));
+        // kernels per session are not separated in a composite graph: count
+        // them on the first session
+        ss[0]->launches += (uint64_t)it->second.second;
+    } else {
+        int kernels = 0;
+        rc = issue_step(b, ss, n, plans.data(), true, &kernels);
+        if (rc) return rc;
+    }
+    FB_CUDA(cudaStreamSynchronize(b->origin));
+    for (int i = 0; i < n; ++i) finish_frame(ss[i], plans[i], out ? &out[i] : nullptr);
+    b->steps++;
     return FB_OK;
 }
 

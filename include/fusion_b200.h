@@ -134,6 +134,46 @@ FB_API int fb_session_launch_count(fb_session* s, uint64_t* launches);
  * d2h = the frame result read back. */
 FB_API int fb_frame_transfer_bytes(const fb_config* cfg, size_t* h2d, size_t* d2h);
 
+/* Raycast tile (CUDA block shape, bx * by threads, bx * by <= 1024 and a
+ * multiple of 32) of this session's model raycast; default 16 x 8.  Results
+ * do not depend on it (every pixel is traced alone).  Cached frame graphs are
+ * rebuilt on the next frame.  No reference counterpart: a tuning knob for the
+ * batched form's autotuner. */
+FB_API int fb_session_set_raycast_tile(fb_session* s, int bx, int by);
+
+/* ------------------------------------------- batched and served forms
+ * No reference counterpart (the reference runs one System per process).
+ * A batch steps many independent sessions -- any sizes, cameras and voxel
+ * sizes -- by one frame each, with all of their frames in flight on the GPU
+ * together.  Every session's result is the one fb_grab_frame gives for the
+ * same input on that session alone (the same kernels on the same data). */
+typedef struct fb_batch fb_batch;
+
+typedef struct {
+    const uint16_t* depth;   /* u16 depth, depth_pitch bytes per row */
+    size_t depth_pitch;
+    const uint8_t* rgb;      /* packed RGB8, rgb_pitch bytes per row */
+    size_t rgb_pitch;
+    int on_device;           /* 0: host pointers (copied in), 1: device pointers */
+} fb_frame_input;
+
+/* stream: the stream the batch orders its work after (NULL: its own). */
+FB_API int fb_batch_create(void* stream, fb_batch** out);
+FB_API int fb_batch_destroy(fb_batch* b);
+/* How a step reaches the GPU.  0 (default): each session's own frame graph
+ * is launched on one of the batch's streams (no capture when the set of
+ * sessions changes).  1: one graph per step holding every session's frame,
+ * captured once per composition (sessions, their tracker modes and frame
+ * parities) and launched as a single graph; best for a fixed set of sessions
+ * stepped together. */
+FB_API int fb_batch_set_mode(fb_batch* b, int mode);
+/* One frame for each of n distinct sessions; out[i] as fb_grab_frame's.
+ * Synchronous.  A session must not be used elsewhere during the call. */
+FB_API int fb_batch_step(fb_batch* b, fb_session* const* sessions, int n, const fb_frame_input* in,
+                         fb_frame_result* out);
+/* Graph launches and captures so far (mode 1 captures once per composition). */
+FB_API int fb_batch_stats(fb_batch* b, uint64_t* steps, uint64_t* captures);
+
 /* Pose of the last tracked frame (LastFrame->pose). */
 FB_API int fb_get_pose(fb_session* s, double pose[16]);
 

@@ -1,0 +1,126 @@
+"""Batched and served forms (fb_batch_*) through the C ABI.
+
+Each session's result in a batch must be the one the same session gives
+alone: the test runs ragged sessions (three resolutions, three voxel sizes,
+independent seeded sequences) once alone through fb_grab_frame and once
+together through fb_batch_step, in both batch modes, with sessions joining
+and skipping steps the way a server admits them, and compares every frame's
+pose and counts and the final hash table and voxels bit for bit.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from fusion_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+pytest.importorskip("torch")
+
+SPECS = [(160, 120, 0.012, 11), (320, 240, 0.007, 12), (640, 480, 0.005, 13)]
+N_FRAMES = 6
+
+
+def _frames(w, h, seed, n):
+    p = synth.params(w, h, synth.session_seed(4, seed), fx=525.0 * w / 640.0, fy=525.0 * w / 640.0,
+                     cx=w / 2.0, cy=h / 2.0, depth_scale=5000.0)
+    d, c, _ = synth.render(p, 0, n)
+    return d, c
+
+
+def _map_digest(sess):
+    e = sess.entries()
+    occ = e[:, 3] >= 0
+    sdf, w, c = sess.blocks(e[occ][:, 3])
+    h = hashlib.sha1()
+    for a in (e, sdf.view(np.uint32), w, c):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest(), int(occ.sum())
+
+
+def _row(r):
+    return (r.tracked, r.tracker_state, r.fused, r.no_visible, r.no_allocated, r.no_new, r.error_flags,
+            tuple(r.pose[:]), r.icp_count, r.rgb_count)
+
+
+def _alone(frames, schedule):
+    from fusion_b200 import Session, mixed_config
+    out = []
+    for i, (w, h, v, _) in enumerate(SPECS):
+        s = Session(mixed_config(w, h, v))
+        d, c = frames[i]
+        rows = [_row(s.grab(d[k], c[k])) for k in range(len(schedule[i]))]
+        out.append((rows, _map_digest(s)))
+        s.close()
+    return out
+
+
+def _batched(frames, schedule, mode, tiles=None):
+    """schedule[i] = the steps at which session i has a frame."""
+    from fusion_b200 import Batch, Session, mixed_config
+    from fusion_b200.batch import set_raycast_tile
+    sess = [Session(mixed_config(w, h, v)) for (w, h, v, _) in SPECS]
+    if tiles:
+        for s, t in zip(sess, tiles):
+            set_raycast_tile(s, *t)
+    rows = [[] for _ in sess]
+    nxt = [0] * len(sess)
+    with Batch(mode=mode) as b:
+        n_steps = max(max(sch) for sch in schedule) + 1
+        for step in range(n_steps):
+            idx = [i for i in range(len(sess)) if step in schedule[i]]
+            fr = []
+            for i in idx:
+                d, c = frames[i]
+                fr.append((d[nxt[i]], c[nxt[i]]))
+                nxt[i] += 1
+            res = b.step([sess[i] for i in idx], fr)
+            for i, r in zip(idx, res):
+                rows[i].append(_row(r))
+        stats = b.stats()
+    out = [(rows[i], _map_digest(s)) for i, s in enumerate(sess)]
+    for s in sess:
+        s.close()
+    return out, stats
+
+
+@pytest.fixture(scope="module")
+def frames():
+    return [_frames(w, h, seed, N_FRAMES) for (w, h, _, seed) in SPECS]
+
+
+LOCKSTEP = [list(range(N_FRAMES))] * 3
+# session 1 joins at step 2, session 0 skips steps 3 and 4 (no frame arrived)
+STAGGERED = [[0, 1, 2, 5, 6, 7], [2, 3, 4, 5, 6, 7], [0, 1, 2, 3, 4, 5]]
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("schedule", ["lockstep", "staggered"])
+def test_each_session_in_the_batch_equals_it_alone(frames, mode, schedule):
+    sch = LOCKSTEP if schedule == "lockstep" else STAGGERED
+    alone = _alone(frames, sch)
+    batched, (steps, captures) = _batched(frames, sch, mode)
+    for i in range(len(SPECS)):
+        assert batched[i][0] == alone[i][0], f"session {i}: per-frame results differ"
+        assert batched[i][1] == alone[i][1], f"session {i}: final map differs"
+    assert all(any(r[0] for r in rows) for rows, _ in alone)   # the sequences do track
+    if mode == 1 and schedule == "lockstep":
+        # compositions: init, then tracking without fusion for parities 0/1 ...
+        assert captures <= steps
+
+
+def test_raycast_tile_does_not_change_results(frames):
+    base, _ = _batched(frames, LOCKSTEP, 0)
+    tiled, _ = _batched(frames, LOCKSTEP, 0, tiles=[(8, 8), (32, 4), (16, 4)])
+    assert tiled == base
+
+
+def test_batch_rejects_a_session_twice(frames):
+    from fusion_b200 import Batch, FusionError, Session, mixed_config
+    s = Session(mixed_config(160, 120, 0.01))
+    d, c = frames[0]
+    with Batch() as b:
+        with pytest.raises(FusionError):
+            b.step([s, s], [(d[0], c[0]), (d[1], c[1])])
+    s.close()
