@@ -80,8 +80,10 @@ int launch_track_begin(TrackState* st, cudaStream_t s);
 // residual: per-warp compact segments of photometric correspondences
 // (int2: pixel, packed last pixel + difference), capacity track_list_capacity;
 // counts: entries per segment (kTrackMaxBlocks * kTrackWarps ints)
+// shared_gpu: the instance with four resident blocks per SM (other sessions'
+// kernels run beside it); same results as the two-block instance
 int launch_track_iter(const TrackLevel& L, TrackState* st, unsigned int* tickets, int2* residual, int* counts,
-                      int min_count, bool is_final, cudaStream_t s);
+                      int min_count, bool is_final, cudaStream_t s, bool shared_gpu = false);
 size_t track_list_capacity(int n_pixels);
 int launch_step_icp(const TrackLevel& L, const DevPose& cur, const DevPose& last, float* partials,
                      unsigned int* ticket, double* out, cudaStream_t s);

@@ -170,9 +170,11 @@ struct fb_session {
     // mode 0 init, 1 track, 2 lost
     bool use_graphs;
     bool persistent;           // tracking as one cooperative kernel per frame
-    cudaGraphExec_t graph[3][2][2];
-    int graph_kernels[3][2][2];
+    // ... and by whether the GPU is shared with other sessions' frames
+    cudaGraphExec_t graph[3][2][2][2];
+    int graph_kernels[3][2][2][2];
     int rc_bx, rc_by;          // raycast tile
+    bool shared_gpu;           // frames run beside other sessions' (batch steps)
 };
 
 namespace {
@@ -241,7 +243,8 @@ void free_session(fb_session* s) {
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 2; ++b)
             for (int c = 0; c < 2; ++c)
-                if (s->graph[a][b][c]) cudaGraphExecDestroy(s->graph[a][b][c]);
+                for (int d = 0; d < 2; ++d)
+                    if (s->graph[a][b][c][d]) cudaGraphExecDestroy(s->graph[a][b][c][d]);
     for (int i = 0; i <= kStages; ++i)
         if (s->ev[i]) cudaEventDestroy(s->ev[i]);
     for (void* p : s->allocs) cudaFree(p);
@@ -337,7 +340,8 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
                 TrackLevel lv = level_view(s, l);
                 for (int it = 0; it < c.iters[l]; ++it)
                     n += launch_track_iter(lv, s->st, s->tickets, s->residual, s->counts,
-                                           min_count[l], l == last_level && it == c.iters[l] - 1, st);
+                                           min_count[l], l == last_level && it == c.iters[l] - 1, st,
+                                           s->shared_gpu);
             }
         }
         skip = &s->st->failed;
@@ -415,10 +419,11 @@ void drop_graphs(fb_session* s) {
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 2; ++b)
             for (int c = 0; c < 2; ++c)
-                if (s->graph[a][b][c]) {
-                    cudaGraphExecDestroy(s->graph[a][b][c]);
-                    s->graph[a][b][c] = nullptr;
-                }
+                for (int d = 0; d < 2; ++d)
+                    if (s->graph[a][b][c][d]) {
+                        cudaGraphExecDestroy(s->graph[a][b][c][d]);
+                        s->graph[a][b][c][d] = nullptr;
+                    }
 }
 
 // Host input -> the device input buffers of fr[next].
@@ -458,7 +463,8 @@ FramePlan plan_frame(fb_session* s) {
 int enqueue_frame(fb_session* s, const FramePlan& p, cudaStream_t st, unsigned* ran) {
     *ran = 0;
     if (s->use_graphs && !s->profile) {
-        cudaGraphExec_t& g = s->graph[p.mode][p.fuse ? 1 : 0][s->next];
+        const int sh = s->shared_gpu ? 1 : 0;
+        cudaGraphExec_t& g = s->graph[p.mode][p.fuse ? 1 : 0][s->next][sh];
         if (!g) {
             cudaGraph_t graph = nullptr;
             cudaStream_t keep = s->stream;
@@ -478,10 +484,10 @@ int enqueue_frame(fb_session* s, const FramePlan& p, cudaStream_t st, unsigned* 
                 cuda_ok(e);
                 return FB_ECUDA;
             }
-            s->graph_kernels[p.mode][p.fuse ? 1 : 0][s->next] = nk;
+            s->graph_kernels[p.mode][p.fuse ? 1 : 0][s->next][sh] = nk;
         }
         FB_CUDA(cudaGraphLaunch(g, st));
-        s->launches += (uint64_t)s->graph_kernels[p.mode][p.fuse ? 1 : 0][s->next];
+        s->launches += (uint64_t)s->graph_kernels[p.mode][p.fuse ? 1 : 0][s->next][sh];
         *ran = 0;
         return FB_OK;
     }
@@ -611,12 +617,14 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
     s->persistent = false;   // measured slower than graph-launched kernels on B200
     s->rc_bx = 16;
     s->rc_by = 8;
+    s->shared_gpu = false;
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 2; ++b)
-            for (int c = 0; c < 2; ++c) {
-                s->graph[a][b][c] = nullptr;
-                s->graph_kernels[a][b][c] = 0;
-            }
+            for (int c = 0; c < 2; ++c)
+                for (int d = 0; d < 2; ++d) {
+                    s->graph[a][b][c][d] = nullptr;
+                    s->graph_kernels[a][b][c][d] = 0;
+                }
     s->own_stream = stream == nullptr;
     s->stream = (cudaStream_t)stream;
     // an owned stream is a blocking one: it orders after work the caller put
@@ -1288,6 +1296,9 @@ int fb_batch_step(fb_batch* b, fb_session* const* ss, int n, const fb_frame_inpu
                            b->origin);
         if (rc) return rc;
     }
+    // sessions sharing the GPU run the tracking instance that leaves room
+    // for the others (same results)
+    for (int i = 0; i < n; ++i) ss[i]->shared_gpu = n > 1;
     std::vector<FramePlan> plans(n);
     for (int i = 0; i < n; ++i) plans[i] = plan_frame(ss[i]);
     if (b->mode == 1) {
@@ -1297,7 +1308,8 @@ int fb_batch_step(fb_batch* b, fb_session* const* ss, int n, const fb_frame_inpu
             const fb_session* s = ss[i];
             key.push_back((uint64_t)(uintptr_t)s);
             key.push_back((uint64_t)plans[i].mode | (uint64_t)plans[i].fuse << 2 | (uint64_t)s->next << 3 |
-                          (uint64_t)s->persistent << 4 | (uint64_t)s->rc_bx << 8 | (uint64_t)s->rc_by << 20);
+                          (uint64_t)s->persistent << 4 | (uint64_t)s->shared_gpu << 5 | (uint64_t)s->rc_bx << 8 |
+                          (uint64_t)s->rc_by << 20);
         }
         auto it = b->cache.find(key);
         if (it == b->cache.end()) {
@@ -1325,7 +1337,10 @@ int fb_batch_step(fb_batch* b, fb_session* const* ss, int n, const fb_frame_inpu
         if (rc) return rc;
     }
     FB_CUDA(cudaStreamSynchronize(b->origin));
-    for (int i = 0; i < n; ++i) finish_frame(ss[i], plans[i], out ? &out[i] : nullptr);
+    for (int i = 0; i < n; ++i) {
+        finish_frame(ss[i], plans[i], out ? &out[i] : nullptr);
+        ss[i]->shared_gpu = false;
+    }
     b->steps++;
     return FB_OK;
 }

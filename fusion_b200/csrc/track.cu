@@ -16,6 +16,12 @@
 // Reductions are deterministic: fixed per-thread pixel sets, warp shuffles,
 // block sums in shared memory, then the blocks' partial sums are added in
 // block order in FP64 by the last block (no atomics on values).
+//
+// The per-iteration kernels come in two instances of the same code: two
+// resident blocks per SM (registers for latency: a session alone) and four
+// (half the registers, some spilled: sessions sharing the GPU leave room for
+// each other).  This file is compiled without contraction of multiplies and
+// adds into FMAs, so both instances compute the same bits.
 #include <cooperative_groups.h>
 
 #include "fb_internal.h"
@@ -560,7 +566,8 @@ __device__ __forceinline__ double cluster_sum(cg::cluster_group& cl, T* s_vals, 
 // popc: deterministic, no block barrier in the pixel loop), with the
 // correspondence count and sum of squared differences reduced the same way
 // (integers below 2^53, exact as doubles).  L.rgbok must be set.
-__global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
+template <int kMinBlocks>
+__global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMinBlocks)
     k_track_a(TrackLevel L, TrackState* st, int2* list, int* counts) {
     const int N = L.W * L.H;
     const int G = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -633,7 +640,8 @@ __device__ void solve_staged(SolveIO& io, const double* s, int min_count, int is
 // rows of its warps' segments; each cluster reduces its rows into a group
 // sum; the last cluster to finish adds the groups of both passes in group
 // order (FP64) and performs the Gauss-Newton update with one warp.
-__global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, 2)
+template <int kMinBlocks>
+__global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMinBlocks)
     k_track_b(TrackLevel L, TrackState* st, unsigned int* ticket, const int2* list, const int* counts, int seg_size,
               int min_count, int is_final) {
     cg::cluster_group cl = cg::this_cluster();
@@ -1144,8 +1152,9 @@ int track_cluster_grid(int n) {
         cfg.gridDim = dim3(c * kTrackCluster);
         cfg.blockDim = dim3(256);
         int ca = 0, cb = 0;
-        if (cudaOccupancyMaxActiveClusters(&ca, (void*)k_track_a, &cfg) == cudaSuccess && ca > 0 && ca < c) c = ca;
-        if (cudaOccupancyMaxActiveClusters(&cb, (void*)k_track_b, &cfg) == cudaSuccess && cb > 0 && cb < c) c = cb;
+        // the register-rich instances (two blocks per SM) bound the grid of both
+        if (cudaOccupancyMaxActiveClusters(&ca, (void*)k_track_a<2>, &cfg) == cudaSuccess && ca > 0 && ca < c) c = ca;
+        if (cudaOccupancyMaxActiveClusters(&cb, (void*)k_track_b<2>, &cfg) == cudaSuccess && cb > 0 && cb < c) c = cb;
         cudaGetLastError();
         if (c > kTrackMaxGroups) c = kTrackMaxGroups;
         cap = c * kTrackCluster;
@@ -1156,12 +1165,17 @@ int track_cluster_grid(int n) {
 }
 
 int launch_track_iter(const TrackLevel& L, TrackState* st, unsigned int* tickets, int2* residual, int* counts,
-                      int min_count, bool is_final, cudaStream_t s) {
+                      int min_count, bool is_final, cudaStream_t s, bool shared_gpu) {
     const int n = L.W * L.H;
     const int g = track_cluster_grid(n);
     const int seg = (n + g * 256 - 1) / (g * 256) * 32;
-    k_track_a<<<g, 256, 0, s>>>(L, st, residual, counts);
-    k_track_b<<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, is_final ? 1 : 0);
+    if (shared_gpu) {
+        k_track_a<4><<<g, 256, 0, s>>>(L, st, residual, counts);
+        k_track_b<4><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, is_final ? 1 : 0);
+    } else {
+        k_track_a<2><<<g, 256, 0, s>>>(L, st, residual, counts);
+        k_track_b<2><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, is_final ? 1 : 0);
+    }
     return 2;
 }
 

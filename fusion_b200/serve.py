@@ -1,0 +1,234 @@
+"""Served form: a request loop fusing frames of many independent sessions as
+they arrive, on one GPU.
+
+Clients (camera sessions) arrive over time, stream frames as a Poisson
+process (30 Hz by default) for a lognormal lifetime, and leave.  A client is
+admitted when its session's device memory (fb_session_bytes) fits in the HBM
+budget beside the sessions already resident, else it waits in a FIFO queue
+until departures free enough memory.  Each admitted client's hash table,
+voxel blocks, frames and pose stay on the device for its whole life.
+
+The loop is continuous batching: whenever frames are pending, every client
+with a pending frame contributes its oldest one to the next fb_batch_step
+(at most `max_batch` clients, oldest frame first); frames that arrive while a
+step is on the GPU go into the following step.  A frame's latency runs from
+its arrival time to the end of the step that fused it.  Each client's results
+are the ones its session would give alone (fb_batch_step's guarantee), so
+batching changes latency and throughput only.
+
+Frames come from a pool of pre-rendered seeded sequences per resolution
+(pinned host memory; a client plays its sequence forwards then backwards so
+that the camera motion stays continuous), copied to the device inside each
+step.
+"""
+import heapq
+import math
+import time
+
+import numpy as np
+
+from . import _lib, synth
+from .batch import RESOLUTIONS, Batch, mixed_config
+
+
+def sequence_seeds(config_id, count, width=160, height=120, max_median_depth=2.0, limit=1000):
+    """The first `count` session indices of `config_id` whose first frame's
+    median valid depth is at most `max_median_depth` metres.  Beyond ~2 m the
+    generator's depth noise (0.0012 + 0.0019 (z - 0.4)^2 m) approaches the
+    truncation band of the small-voxel sessions and the reference's tracker
+    loses such sequences at their first frame (the FP64 oracle agrees), which
+    would leave them untracked -- doing no fusion or raycast -- for the rest of
+    their life."""
+    out = []
+    for i in range(limit):
+        seed = synth.session_seed(config_id, i)
+        p = synth.params(width, height, seed, fx=525.0 * width / 640.0, fy=525.0 * width / 640.0,
+                         cx=width / 2.0, cy=height / 2.0, depth_scale=5000.0)
+        d, _, _ = synth.render(p, 0, 1)
+        v = d[0][d[0] > 0]
+        if v.size and np.median(v) / 5000.0 <= max_median_depth:
+            out.append(seed)
+            if len(out) == count:
+                break
+    return out
+
+
+class FramePool:
+    """Pre-rendered sequences per resolution, pinned host memory."""
+
+    def __init__(self, seeds, n_frames, resolutions=RESOLUTIONS, pin=True):
+        import torch
+        self.seq = {}
+        for (w, h) in resolutions:
+            for k, seed in enumerate(seeds):
+                p = synth.params(w, h, seed, fx=525.0 * w / 640.0, fy=525.0 * w / 640.0, cx=w / 2.0,
+                                 cy=h / 2.0, depth_scale=5000.0)
+                d, c, _ = synth.render(p, 0, n_frames)
+                if pin:
+                    d = torch.from_numpy(d).pin_memory().numpy()
+                    c = torch.from_numpy(c).pin_memory().numpy()
+                self.seq[(w, h, k)] = (d, c)
+        self.n_seq = len(seeds)
+        self.n_frames = n_frames
+
+    def frame(self, w, h, k, i):
+        """Frame i of sequence k played forwards then backwards."""
+        n = self.n_frames
+        period = 2 * n - 2 if n > 1 else 1
+        j = i % period
+        if j >= n:
+            j = period - j
+        d, c = self.seq[(w, h, k)]
+        return d[j], c[j]
+
+
+class Client:
+    def __init__(self, cid, width, height, voxel, seq, t_arrive, lifetime, rate, rng):
+        self.cid, self.width, self.height, self.voxel, self.seq = cid, width, height, voxel, seq
+        self.t_arrive, self.lifetime, self.rate = t_arrive, lifetime, rate
+        self.rng = rng
+        self.session = None
+        self.t_admit = None
+        self.t_end = None
+        self.pending = []       # arrival times of frames not yet fused
+        self.next_arrival = None
+        self.sent = 0           # frames taken from the sequence so far
+        self.bytes = 0
+
+
+def make_clients(n, seed, rate=30.0, median_life=20.0, life_sigma=0.5, warm_clients=None, horizon=None):
+    """n clients: `warm_clients` (default all) present at t=0 with lifetimes
+    drawn from the lognormal (median `median_life` s), the rest arriving as a
+    Poisson process whose rate keeps the population steady (n / mean life)
+    over `horizon` seconds.  Resolution uniform over RESOLUTIONS, voxel size
+    uniform in [4, 20] mm."""
+    rng = np.random.default_rng(seed)
+    warm = n if warm_clients is None else warm_clients
+    mean_life = median_life * math.exp(life_sigma ** 2 / 2)
+    out = []
+    t = 0.0
+    for i in range(n):
+        if i < warm:
+            ta = 0.0
+        else:
+            t += rng.exponential(mean_life / n)
+            ta = t
+            if horizon is not None and ta > horizon:
+                break
+        w, h = RESOLUTIONS[int(rng.integers(0, len(RESOLUTIONS)))]
+        v = float(np.float32(rng.uniform(0.004, 0.020)))
+        life = float(rng.lognormal(math.log(median_life), life_sigma))
+        out.append(Client(i, w, h, v, 0, ta, life, rate, np.random.default_rng(seed * 1000003 + i)))
+    return out
+
+
+class Server:
+    def __init__(self, pool, budget_bytes=120e9, mode=0, max_batch=256):
+        self.lib = _lib.load()
+        self.pool = pool
+        self.budget = float(budget_bytes)
+        self.batch = Batch(mode=mode)
+        self.max_batch = max_batch
+
+    def close(self):
+        self.batch.close()
+
+    def run(self, clients, duration):
+        """Serve `clients` for `duration` seconds of wall time.  Returns the
+        statistics of the run."""
+        from .system import Session
+        for k, c in enumerate(clients):
+            c.seq = k % self.pool.n_seq
+        events = [(c.t_arrive, 0, c.cid) for c in clients]    # (time, kind 0 arrive / 1 leave, id)
+        heapq.heapify(events)
+        by_id = {c.cid: c for c in clients}
+        queue, active = [], {}
+        used, peak = 0.0, 0.0
+        lat, batch_sizes = [], []
+        admitted = waited = 0
+        wait_times = []
+        t0 = time.perf_counter()
+
+        def now():
+            return time.perf_counter() - t0
+
+        def admit(c, t):
+            nonlocal used, peak, admitted
+            cfg = mixed_config(c.width, c.height, c.voxel)
+            c.bytes = float(self.lib.fb_session_bytes(cfg))
+            c.session = Session(cfg)
+            used += c.bytes
+            peak = max(peak, used)
+            c.t_admit = t
+            c.t_end = t + c.lifetime
+            c.next_arrival = t + c.rng.exponential(1.0 / c.rate)
+            active[c.cid] = c
+            heapq.heappush(events, (c.t_end, 1, c.cid))
+            admitted += 1
+            if c.t_admit > c.t_arrive + 1e-9:
+                wait_times.append(c.t_admit - c.t_arrive)
+
+        def try_admit(t):
+            while queue:
+                c = queue[0]
+                cfg_bytes = float(self.lib.fb_session_bytes(mixed_config(c.width, c.height, c.voxel)))
+                if used + cfg_bytes > self.budget:
+                    break
+                queue.pop(0)
+                admit(c, t)
+
+        while True:
+            t = now()
+            if t >= duration:
+                break
+            # arrivals and departures up to now
+            while events and events[0][0] <= t:
+                _, kind, cid = heapq.heappop(events)
+                c = by_id[cid]
+                if kind == 0:
+                    need = float(self.lib.fb_session_bytes(mixed_config(c.width, c.height, c.voxel)))
+                    if not queue and used + need <= self.budget:
+                        admit(c, t)
+                    else:
+                        queue.append(c)
+                        waited += 1
+                elif cid in active:
+                    del active[cid]
+                    c.session.close()
+                    c.session = None
+                    used -= c.bytes
+                    try_admit(t)
+            # frames that have arrived
+            for c in active.values():
+                while c.next_arrival is not None and c.next_arrival <= t and c.next_arrival < c.t_end:
+                    c.pending.append(c.next_arrival)
+                    c.next_arrival += c.rng.exponential(1.0 / c.rate)
+            ready = sorted((c for c in active.values() if c.pending), key=lambda c: c.pending[0])
+            if not ready:
+                nxt = min([c.next_arrival for c in active.values() if c.next_arrival is not None] +
+                          ([events[0][0]] if events else []) + [duration])
+                time.sleep(max(0.0, min(nxt - now(), 0.002)))
+                continue
+            ready = ready[:self.max_batch]
+            frames = [self.pool.frame(c.width, c.height, c.seq, c.sent) for c in ready]
+            self.batch.step([c.session for c in ready], frames)
+            t_done = now()
+            for c in ready:
+                lat.append(t_done - c.pending.pop(0))
+                c.sent += 1
+            batch_sizes.append(len(ready))
+        wall = now()
+        for c in list(active.values()):
+            c.session.close()
+            c.session = None
+        lat_ms = np.array(lat) * 1e3 if lat else np.zeros(1)
+        backlog = sum(len(c.pending) for c in clients)
+        return {
+            "frames": len(lat), "wall_s": wall, "frames_per_s": len(lat) / wall,
+            "latency_ms": {"p50": float(np.percentile(lat_ms, 50)), "p99": float(np.percentile(lat_ms, 99)),
+                           "max": float(lat_ms.max())},
+            "steps": len(batch_sizes), "mean_batch": float(np.mean(batch_sizes)) if batch_sizes else 0.0,
+            "clients": len(clients), "admitted": admitted, "queued": waited,
+            "still_queued_at_end": len(queue), "mean_wait_s": float(np.mean(wait_times)) if wait_times else 0.0,
+            "backlog_frames_at_end": backlog, "peak_hbm_bytes": peak, "budget_bytes": self.budget,
+        }
