@@ -15,7 +15,14 @@ Our arm prints one JSON line with
   roofline  the integration kernel (the HBM-bound stage) timed with CUDA
           events around its launches in a profiled pass;
   cpu_baseline  the FP64 CPU oracle on the box's host cores (rank 0, N=1),
-          on the first frames of the same sequence.
+          on the first frames of the same sequence;
+  batched the batched form (N=1): many sessions stepped together by
+          fb_batch_step -- sessions of the same full-size configuration (like
+          for like with `value`) and the ragged mix (three resolutions, voxels
+          4-20 mm) with autotuned raycast tiles; aggregate frames/s;
+  served  the served form (N=1): clients arriving and leaving, 30 Hz Poisson
+          frames, HBM admission budget, continuous batching; aggregate
+          frames/s and p50/p99 latency from frame arrival to fusion.
 `--impl reference` times the CPU restatement of the reference's path (the
 reference itself is GPU-only code whose host classes need OpenCV/Eigen/Sophus)
 on all host cores on the same configuration.
@@ -49,6 +56,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-frames", type=int, default=6, help="frames in the CPU-oracle sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurements")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-form measurement")
+    ap.add_argument("--batch-sessions", type=int, default=32)
+    ap.add_argument("--served-clients", type=int, default=64)
+    ap.add_argument("--served-seconds", type=float, default=10.0)
     return ap.parse_args()
 
 
@@ -189,6 +201,97 @@ def run_reference(args):
     return 0
 
 
+def _batched_run(specs, seeds, warmup, steps, tune=False):
+    """Sessions `specs` [(w, h, voxel, config)] stepped together through
+    fb_batch_step, frames resident in HBM (each session plays a pre-rendered
+    seeded sequence forwards and backwards).  Returns aggregate frames/s,
+    ms per step, tracked fraction and the autotuned raycast tiles."""
+    import torch
+    from fusion_b200 import Batch, Session, synth
+    from fusion_b200.batch import autotune_raycast_tiles
+    n_fr = 24
+    seqs = {}
+    for k, (w, h, _, _) in enumerate(specs):
+        key = (w, h, k % len(seeds))
+        if key not in seqs:
+            p = synth.params(w, h, seeds[key[2]], fx=525.0 * w / 640.0, fy=525.0 * w / 640.0, cx=w / 2.0,
+                             cy=h / 2.0, depth_scale=5000.0)
+            d, c, _ = synth.render(p, 0, n_fr)
+            seqs[key] = (torch.from_numpy(d).cuda(), torch.from_numpy(c).cuda())
+    keys = [(w, h, k % len(seeds)) for k, (w, h, _, _) in enumerate(specs)]
+    sess = [Session(cfg) for (_, _, _, cfg) in specs]
+    step_no = [0]
+
+    def frames():
+        i = step_no[0]
+        step_no[0] += 1
+        j = i % (2 * n_fr - 2)
+        j = j if j < n_fr else 2 * n_fr - 2 - j
+        return [(seqs[k][0][j], seqs[k][1][j]) for k in keys]
+
+    b = Batch(mode=0)
+    for _ in range(warmup):
+        b.step(sess, frames(), on_device=True)
+    tiles = None
+    if tune:
+        tiles, _ = autotune_raycast_tiles(b, sess, frames, candidates=((16, 8), (8, 8), (32, 4), (16, 4)),
+                                          steps_per=1, on_device=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tracked = 0
+    for _ in range(steps):
+        tracked += sum(r.tracked for r in b.step(sess, frames(), on_device=True))
+    dt = time.perf_counter() - t0
+    b.close()
+    for s in sess:
+        s.close()
+    n = len(specs)
+    return {"value": n * steps / dt, "unit": "frames/s", "ms_per_step": dt / steps * 1e3, "sessions": n,
+            "steps": steps, "warmup": warmup, "tracked_fraction": tracked / (n * steps),
+            "raycast_tiles": {f"{w}x{h}": list(t) for (w, h), t in tiles.items()} if tiles else None}
+
+
+def batched_forms(args, rank, plain_value):
+    """The batched form on this GPU: (a) sessions of the plain full-size
+    configuration (640x480, 5 mm) stepped together -- the same per-frame work
+    as the plain line, so the ratio is like for like; (b) the ragged mix
+    (resolutions 160x120 / 320x240 / 640x480, voxels 4-20 mm) with the
+    raycast tiles picked by the autotuner.  Wall-clock timed (fb_batch_step
+    is synchronous), frames resident in HBM."""
+    from fusion_b200 import mixed_config, mixed_population
+    from fusion_b200 import system as S
+    from fusion_b200.serve import sequence_seeds
+    n = args.batch_sessions
+    seeds = sequence_seeds(3 + rank, 8)
+    c2 = _batched_run([(640, 480, 0.005, S.config_c2())] * n, seeds, 3, 8)
+    c2["workload"] = f"{n} sessions x plain full-size configuration (640x480, 5 mm, 2^20 buckets, 2^18 blocks)"
+    c2["vs_plain"] = c2["value"] / plain_value
+    mix = _batched_run([(w, h, v, mixed_config(w, h, v)) for (w, h, v) in mixed_population(n, 1234 + rank)],
+                       seeds, 3, 10, tune=True)
+    mix["workload"] = (f"{n} ragged sessions: resolution uniform over 160x120/320x240/640x480, voxel "
+                       "uniform 4-20 mm, truncation 4 voxels, maps sized per voxel size")
+    mix["vs_plain"] = mix["value"] / plain_value
+    return {"same_config": c2, "mixed": mix}
+
+
+def served_form(args, rank, plain_value):
+    """The served form: clients arriving and leaving (lognormal lifetimes,
+    median 20 s), frames arriving as Poisson processes at 30 Hz, admission by
+    a 120 GB HBM budget, continuous batching; latency from frame arrival to
+    the end of its step, frames copied from pinned host memory in the step."""
+    from fusion_b200.serve import FramePool, Server, make_clients, sequence_seeds
+    pool = FramePool(sequence_seeds(7 + rank, 4), 30)
+    srv = Server(pool, budget_bytes=120e9, mode=0, max_batch=256)
+    clients = make_clients(args.served_clients, 99 + rank, horizon=args.served_seconds)
+    st = srv.run(clients, args.served_seconds)
+    srv.close()
+    st["workload"] = (f"{args.served_clients} clients at t=0 plus Poisson arrivals keeping the population steady; "
+                      "30 Hz Poisson frames; lognormal lifetimes (median 20 s); mixed resolutions and voxel "
+                      "sizes; 120 GB HBM admission budget")
+    st["vs_plain"] = st["frames_per_s"] / plain_value
+    return st
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -299,6 +402,11 @@ def main():
 
     value = K * world / (ms / 1000.0)
     lat_ms = np.array(lat) * 1000.0
+
+    # the batched and served forms on one GPU (rank 0 of a single-GPU run)
+    one = world == 1
+    batched = batched_forms(args, rank, value) if one and not args.no_batched else None
+    served = served_form(args, rank, value) if one and not args.no_served else None
     line = {
         "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -316,6 +424,8 @@ def main():
                      "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms},
         "cpu_baseline": cpu,
         "clocks": ck,
+        "batched": batched,
+        "served": served,
     }
     if rank == 0:
         print(json.dumps(line))

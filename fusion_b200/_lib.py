@@ -80,6 +80,7 @@ SIGNATURES = {
     "fb_session_set_persistent": (_i, [_vp, _i]),
     "fb_session_stage_times": (_i, [_vp, _vp, _vp, _i]),
     "fb_session_set_raycast_tile": (_i, [_vp, _i, _i]),
+    "fb_session_prepare": (_i, [_vp, _i]),
     "fb_batch_create": (_i, [_vp, ctypes.POINTER(_vp)]),
     "fb_batch_destroy": (_i, [_vp]),
     "fb_batch_set_mode": (_i, [_vp, _i]),

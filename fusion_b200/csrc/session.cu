@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -155,7 +156,9 @@ struct fb_session {
     DevPose* scratch_pose;
     FrameOut* d_out;
     FrameOut* h_out;           // pinned
-    std::vector<void*> allocs;
+    void* arena;               // one stream-ordered device allocation
+    size_t arena_size, arena_used;
+    bool sizing;               // dalloc only adds up sizes
     // Tracker / System host state (Tracking.cc:19-23, System.cc:72)
     int state, last_state, no_missed, frames_after_reloc;
     uint64_t frame_id;
@@ -179,13 +182,47 @@ struct fb_session {
 
 namespace {
 
+// All device buffers of a session are carved out of one stream-ordered
+// allocation (the arena): a sizing pass adds up the sizes, a second pass
+// hands out 256-byte aligned pieces.  Creating and destroying sessions while
+// other sessions run then costs one cudaMallocAsync / cudaFreeAsync, neither
+// of which waits for the device.
 template <class T>
 bool dalloc(fb_session* s, T** p, size_t n) {
-    void* q = nullptr;
-    if (!cuda_ok(cudaMalloc(&q, sizeof(T) * (n ? n : 1)))) return false;
-    s->allocs.push_back(q);
-    *p = (T*)q;
+    const size_t bytes = (sizeof(T) * (n ? n : 1) + 255) & ~(size_t)255;
+    if (s->sizing) {
+        s->arena_size += bytes;
+        *p = nullptr;
+        return true;
+    }
+    if (s->arena_used + bytes > s->arena_size) return false;
+    *p = (T*)((char*)s->arena + s->arena_used);
+    s->arena_used += bytes;
     return true;
+}
+
+// Pinned host slots for the per-frame results, recycled between sessions
+// (freeing pinned memory may wait for the device).
+std::mutex g_out_lock;
+std::vector<void*> g_out_free;
+
+void* take_out_slot(size_t bytes) {
+    std::lock_guard<std::mutex> guard(g_out_lock);
+    if (g_out_free.empty()) {
+        const size_t stride = (bytes + 255) & ~(size_t)255;
+        char* chunk = nullptr;
+        if (cudaMallocHost((void**)&chunk, 64 * stride) != cudaSuccess) return nullptr;
+        for (int i = 63; i >= 0; --i) g_out_free.push_back(chunk + (size_t)i * stride);
+    }
+    void* p = g_out_free.back();
+    g_out_free.pop_back();
+    return p;
+}
+
+void give_out_slot(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> guard(g_out_lock);
+    g_out_free.push_back(p);
 }
 
 size_t next_pow2(size_t v) {
@@ -247,10 +284,55 @@ void free_session(fb_session* s) {
                     if (s->graph[a][b][c][d]) cudaGraphExecDestroy(s->graph[a][b][c][d]);
     for (int i = 0; i <= kStages; ++i)
         if (s->ev[i]) cudaEventDestroy(s->ev[i]);
-    for (void* p : s->allocs) cudaFree(p);
-    if (s->h_out) cudaFreeHost(s->h_out);
+    if (s->arena) cudaFreeAsync(s->arena, s->stream);
+    give_out_slot(s->h_out);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
+}
+
+// The device buffers of a session (see dalloc): frames, tracker, map.
+bool carve_session(fb_session* s, const fb_config* cfg) {
+    bool ok = true;
+    for (int f = 0; f < 2 && ok; ++f) {
+        FrameBuf& F = s->fr[f];
+        size_t n0 = (size_t)s->W[0] * s->H[0];
+        ok = ok && dalloc(s, &F.depth_in, n0) && dalloc(s, &F.rgb, 3 * n0) && dalloc(s, &F.raw, n0);
+        for (int l = 0; l < 3 && ok; ++l) {
+            size_t n = (size_t)s->W[l] * s->H[l];
+            ok = dalloc(s, &F.depth[l], n) && dalloc(s, &F.vmap[l], n) && dalloc(s, &F.nmap[l], n) &&
+                 dalloc(s, &F.gray[l], n) && dalloc(s, &F.dx[l], n) && dalloc(s, &F.dy[l], n) &&
+                 dalloc(s, &F.rgbok[l], n);
+        }
+    }
+    ok = ok && dalloc(s, &s->st, 1) && dalloc(s, &s->partials, (size_t)2 * kTrackMaxBlocks * 32) &&
+         dalloc(s, &s->tickets, 4) && dalloc(s, &s->bar, 2) && dalloc(s, &s->err, 1) && dalloc(s, &s->residual, track_list_capacity(s->W[0] * s->H[0])) &&
+         dalloc(s, &s->counts, (size_t)kTrackMaxBlocks * kTrackWarps) &&
+         dalloc(s, &s->scratch_pose, 1) && dalloc(s, &s->d_out, 1);
+    MapView& m = s->map;
+    if (ok) {
+        m.NB = cfg->num_buckets;
+        m.nb_mask = (m.NB & (m.NB - 1)) == 0 ? (uint32_t)(m.NB - 1) : 0u;
+        m.NE = cfg->num_excess;
+        m.NS = cfg->num_blocks;
+        // new blocks of one frame: at least kMinNewBlocks whatever the pool
+        // size, so that a frame needing more blocks than the pool still lists
+        // all of them and the exhaustion is handled by the exact sequential path
+        m.newcap = m.NS > kMinNewBlocks ? m.NS : kMinNewBlocks;
+        m.reqcap = (int)next_pow2((size_t)2 * m.newcap);
+        m.nchunks = (m.NB + kScanChunk - 1) / kScanChunk;
+        m.zc = (cfg->width + 7) / 8;
+        m.zr = (cfg->height + 7) / 8;
+        m.g = make_geom(*cfg);
+        ok = dalloc(s, &m.entries, (size_t)m.NB + m.NE) && dalloc(s, &m.heap, m.NS) &&
+             dalloc(s, &m.voxels, (size_t)m.NS * 512) && dalloc(s, &m.ctr, 1) && dalloc(s, &m.alloc_list, m.NS) &&
+             dalloc(s, &m.visible, m.NS) && dalloc(s, &m.reqset, m.reqcap) && dalloc(s, &m.newblk, m.newcap) &&
+             dalloc(s, &m.order, m.newcap) && dalloc(s, &m.arrival, m.newcap) &&
+             dalloc(s, &m.bucket_cnt, m.NB) && dalloc(s, &m.bucket_start, m.NB) && dalloc(s, &m.bucket_x, m.NB) &&
+             dalloc(s, &m.chunk_sums, 2 * (size_t)m.nchunks) && dalloc(s, &m.zmin, (size_t)m.zc * m.zr) &&
+             dalloc(s, &m.zmax, (size_t)m.zc * m.zr);
+        s->ctr = m.ctr;
+    }
+    return ok;
 }
 
 int reset_session(fb_session* s) {
@@ -457,35 +539,46 @@ FramePlan plan_frame(fb_session* s) {
     return p;
 }
 
+// Captures the graph of a frame of plan p for the session's current frame
+// parity and shared-GPU flag, unless it is cached already.  The capture runs
+// on stream st (nothing executes).
+int capture_frame(fb_session* s, const FramePlan& p, cudaStream_t st) {
+    const int sh = s->shared_gpu ? 1 : 0;
+    cudaGraphExec_t& g = s->graph[p.mode][p.fuse ? 1 : 0][s->next][sh];
+    if (g) return FB_OK;
+    cudaGraph_t graph = nullptr;
+    cudaStream_t keep = s->stream;
+    s->stream = st;
+    unsigned ran = 0;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    int nk = 0;
+    if (e == cudaSuccess) {
+        nk = issue_frame(s, p.track, p.fuse, p.render, p.init, &ran);
+        e = cudaStreamEndCapture(st, &graph);
+    }
+    s->stream = keep;
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&g, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        g = nullptr;
+        cuda_ok(e);
+        return FB_ECUDA;
+    }
+    s->graph_kernels[p.mode][p.fuse ? 1 : 0][s->next][sh] = nk;
+    return FB_OK;
+}
+
 // The frame's kernels on stream `st`: the session's cached graph of this
-// (mode, fuse, next) when graphs are on and profiling is off (captured on
-// first use), else direct launches.
+// (mode, fuse, next, shared) when graphs are on and profiling is off
+// (captured on first use), else direct launches.
 int enqueue_frame(fb_session* s, const FramePlan& p, cudaStream_t st, unsigned* ran) {
     *ran = 0;
     if (s->use_graphs && !s->profile) {
         const int sh = s->shared_gpu ? 1 : 0;
-        cudaGraphExec_t& g = s->graph[p.mode][p.fuse ? 1 : 0][s->next][sh];
-        if (!g) {
-            cudaGraph_t graph = nullptr;
-            cudaStream_t keep = s->stream;
-            s->stream = st;
-            cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-            int nk = 0;
-            if (e == cudaSuccess) {
-                nk = issue_frame(s, p.track, p.fuse, p.render, p.init, ran);
-                e = cudaStreamEndCapture(st, &graph);
-            }
-            s->stream = keep;
-            if (e == cudaSuccess) e = cudaGetLastError();
-            if (e == cudaSuccess) e = cudaGraphInstantiate(&g, graph, 0);
-            if (graph) cudaGraphDestroy(graph);
-            if (e != cudaSuccess) {
-                g = nullptr;
-                cuda_ok(e);
-                return FB_ECUDA;
-            }
-            s->graph_kernels[p.mode][p.fuse ? 1 : 0][s->next][sh] = nk;
-        }
+        int rc = capture_frame(s, p, st);
+        if (rc) return rc;
+        cudaGraphExec_t g = s->graph[p.mode][p.fuse ? 1 : 0][s->next][sh];
         FB_CUDA(cudaGraphLaunch(g, st));
         s->launches += (uint64_t)s->graph_kernels[p.mode][p.fuse ? 1 : 0][s->next][sh];
         *ran = 0;
@@ -585,18 +678,18 @@ const char* fb_last_error(void) { return g_last_error; }
 
 size_t fb_session_bytes(const fb_config* c) {
     if (!valid_config(c)) return 0;
-    size_t px = (size_t)c->width * c->height, frame = 0;
+    // the sizing pass of fb_session_create
+    fb_session* s = new (std::nothrow) fb_session();
+    if (!s) return 0;
     for (int l = 0; l < 3; ++l) {
-        size_t n = (size_t)(c->width >> l) * (c->height >> l);
-        frame += n * (4 + 16 + 16 + 1 + 2 + 2 + 1);
+        s->W[l] = c->width >> l;
+        s->H[l] = c->height >> l;
     }
-    frame += px * (2 + 3 + 4);
-    size_t NS = c->num_blocks, NB = c->num_buckets, NE = c->num_excess;
-    size_t newcap = NS > (size_t)kMinNewBlocks ? NS : (size_t)kMinNewBlocks;
-    size_t reqcap = next_pow2(2 * newcap);
-    size_t map = (NB + NE) * sizeof(HEntry) + NS * 4 + NS * 512 * sizeof(Voxel) + 2 * NS * 4 + reqcap * 8 +
-                 newcap * (sizeof(NewBlock) + 8) + 3 * NB * 4;
-    return 2 * frame + map + px * 12 + kTrackMaxBlocks * 32 * 8 + sizeof(TrackState);
+    s->sizing = true;
+    carve_session(s, c);
+    const size_t n = s->arena_size;
+    delete s;
+    return n;
 }
 
 int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
@@ -639,47 +732,19 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
         s->H[l] = cfg->height >> l;
         s->K[l] = make_intr(cfg->fx, cfg->fy, cfg->cx, cfg->cy, l);
     }
-    bool ok = true;
-    for (int f = 0; f < 2 && ok; ++f) {
-        FrameBuf& F = s->fr[f];
-        size_t n0 = (size_t)s->W[0] * s->H[0];
-        ok = ok && dalloc(s, &F.depth_in, n0) && dalloc(s, &F.rgb, 3 * n0) && dalloc(s, &F.raw, n0);
-        for (int l = 0; l < 3 && ok; ++l) {
-            size_t n = (size_t)s->W[l] * s->H[l];
-            ok = dalloc(s, &F.depth[l], n) && dalloc(s, &F.vmap[l], n) && dalloc(s, &F.nmap[l], n) &&
-                 dalloc(s, &F.gray[l], n) && dalloc(s, &F.dx[l], n) && dalloc(s, &F.dy[l], n) &&
-                 dalloc(s, &F.rgbok[l], n);
-        }
-    }
-    ok = ok && dalloc(s, &s->st, 1) && dalloc(s, &s->partials, (size_t)2 * kTrackMaxBlocks * 32) &&
-         dalloc(s, &s->tickets, 4) && dalloc(s, &s->bar, 2) && dalloc(s, &s->err, 1) && dalloc(s, &s->residual, track_list_capacity(s->W[0] * s->H[0])) &&
-         dalloc(s, &s->counts, (size_t)kTrackMaxBlocks * kTrackWarps) &&
-         dalloc(s, &s->scratch_pose, 1) && dalloc(s, &s->d_out, 1);
-    MapView& m = s->map;
+    // sizes first, then one allocation, then the pieces
+    s->arena = nullptr;
+    s->arena_size = s->arena_used = 0;
+    s->sizing = true;
+    carve_session(s, cfg);
+    s->sizing = false;
+    bool ok = cuda_ok(cudaMallocAsync(&s->arena, s->arena_size, s->stream));
+    if (!ok) s->arena = nullptr;
+    ok = ok && carve_session(s, cfg);
     if (ok) {
-        m.NB = cfg->num_buckets;
-        m.nb_mask = (m.NB & (m.NB - 1)) == 0 ? (uint32_t)(m.NB - 1) : 0u;
-        m.NE = cfg->num_excess;
-        m.NS = cfg->num_blocks;
-        // new blocks of one frame: at least kMinNewBlocks whatever the pool
-        // size, so that a frame needing more blocks than the pool still lists
-        // all of them and the exhaustion is handled by the exact sequential path
-        m.newcap = m.NS > kMinNewBlocks ? m.NS : kMinNewBlocks;
-        m.reqcap = (int)next_pow2((size_t)2 * m.newcap);
-        m.nchunks = (m.NB + kScanChunk - 1) / kScanChunk;
-        m.zc = (cfg->width + 7) / 8;
-        m.zr = (cfg->height + 7) / 8;
-        m.g = make_geom(*cfg);
-        ok = dalloc(s, &m.entries, (size_t)m.NB + m.NE) && dalloc(s, &m.heap, m.NS) &&
-             dalloc(s, &m.voxels, (size_t)m.NS * 512) && dalloc(s, &m.ctr, 1) && dalloc(s, &m.alloc_list, m.NS) &&
-             dalloc(s, &m.visible, m.NS) && dalloc(s, &m.reqset, m.reqcap) && dalloc(s, &m.newblk, m.newcap) &&
-             dalloc(s, &m.order, m.newcap) && dalloc(s, &m.arrival, m.newcap) &&
-             dalloc(s, &m.bucket_cnt, m.NB) && dalloc(s, &m.bucket_start, m.NB) && dalloc(s, &m.bucket_x, m.NB) &&
-             dalloc(s, &m.chunk_sums, 2 * (size_t)m.nchunks) && dalloc(s, &m.zmin, (size_t)m.zc * m.zr) &&
-             dalloc(s, &m.zmax, (size_t)m.zc * m.zr);
-        s->ctr = m.ctr;
+        s->h_out = (FrameOut*)take_out_slot(sizeof(FrameOut));
+        ok = s->h_out != nullptr;
     }
-    if (ok) ok = cuda_ok(cudaMallocHost((void**)&s->h_out, sizeof(FrameOut)));
     for (int i = 0; i <= kStages && ok; ++i) ok = cuda_ok(cudaEventCreate(&s->ev[i]));
     if (!ok) {
         free_session(s);
@@ -727,6 +792,32 @@ int fb_grab_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, cons
         }
     finish_frame(s, p, out);
     return FB_OK;
+}
+
+int fb_session_prepare(fb_session* s, int shared) {
+    if (!s) return FB_EINVAL;
+    if (!s->use_graphs) return FB_OK;
+    const bool keep_shared = s->shared_gpu;
+    const int keep_next = s->next;
+    s->shared_gpu = shared != 0;
+    int rc = FB_OK;
+    for (int mode = 0; mode < 3 && rc == FB_OK; ++mode)
+        for (int fuse = 0; fuse < (mode == 2 ? 1 : 2) && rc == FB_OK; ++fuse)
+            for (int next = 0; next < 2 && rc == FB_OK; ++next) {
+                FramePlan p;
+                p.state = mode == 0 ? 1 : mode == 1 ? 0 : -1;
+                p.init = mode == 0;
+                p.track = mode == 1;
+                p.fuse = fuse != 0;
+                p.render = p.init || p.track;
+                p.after = 0;
+                p.mode = mode;
+                s->next = next;
+                rc = capture_frame(s, p, s->stream);
+            }
+    s->next = keep_next;
+    s->shared_gpu = keep_shared;
+    return rc;
 }
 
 int fb_session_set_raycast_tile(fb_session* s, int bx, int by) {
@@ -1247,6 +1338,15 @@ int fb_batch_create(void* stream, fb_batch** out) {
         delete b;
         return FB_ECUDA;
     }
+    // sessions come and go beside running ones: keep the memory of destroyed
+    // sessions in the device's default pool for the next ones
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     *out = b;
     return FB_OK;
 }

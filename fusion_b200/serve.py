@@ -96,25 +96,21 @@ class Client:
         self.bytes = 0
 
 
-def make_clients(n, seed, rate=30.0, median_life=20.0, life_sigma=0.5, warm_clients=None, horizon=None):
-    """n clients: `warm_clients` (default all) present at t=0 with lifetimes
-    drawn from the lognormal (median `median_life` s), the rest arriving as a
-    Poisson process whose rate keeps the population steady (n / mean life)
-    over `horizon` seconds.  Resolution uniform over RESOLUTIONS, voxel size
-    uniform in [4, 20] mm."""
+def make_clients(n, seed, rate=30.0, median_life=20.0, life_sigma=0.5, horizon=0.0):
+    """n clients present at t = 0 (the steady-state population) plus clients
+    arriving as a Poisson process at n / (mean lifetime) per second over
+    `horizon` seconds, which keeps the population steady.  Lifetimes are
+    lognormal (median `median_life` s), frame rate `rate` Hz, resolution
+    uniform over RESOLUTIONS, voxel size uniform in [4, 20] mm."""
     rng = np.random.default_rng(seed)
-    warm = n if warm_clients is None else warm_clients
     mean_life = median_life * math.exp(life_sigma ** 2 / 2)
+    times = [0.0] * n
+    t = rng.exponential(mean_life / n)
+    while t < horizon:
+        times.append(t)
+        t += rng.exponential(mean_life / n)
     out = []
-    t = 0.0
-    for i in range(n):
-        if i < warm:
-            ta = 0.0
-        else:
-            t += rng.exponential(mean_life / n)
-            ta = t
-            if horizon is not None and ta > horizon:
-                break
+    for i, ta in enumerate(times):
         w, h = RESOLUTIONS[int(rng.integers(0, len(RESOLUTIONS)))]
         v = float(np.float32(rng.uniform(0.004, 0.020)))
         life = float(rng.lognormal(math.log(median_life), life_sigma))
@@ -123,6 +119,11 @@ def make_clients(n, seed, rate=30.0, median_life=20.0, life_sigma=0.5, warm_clie
 
 
 class Server:
+    """The request loop.  Session creation (device allocation, map reset and
+    capture of the session's frame graphs) and destruction run on a
+    background admission thread so that the step loop never waits for them;
+    clients present at the start are admitted before the clock starts."""
+
     def __init__(self, pool, budget_bytes=120e9, mode=0, max_batch=256):
         self.lib = _lib.load()
         self.pool = pool
@@ -133,94 +134,144 @@ class Server:
     def close(self):
         self.batch.close()
 
+    def _need(self, c):
+        return float(self.lib.fb_session_bytes(mixed_config(c.width, c.height, c.voxel)))
+
+    @staticmethod
+    def _open(c):
+        from .system import Session
+        s = Session(mixed_config(c.width, c.height, c.voxel))
+        s.prepare(shared=True)
+        return s
+
     def run(self, clients, duration):
         """Serve `clients` for `duration` seconds of wall time.  Returns the
         statistics of the run."""
-        from .system import Session
+        import queue as _q
+        import threading
         for k, c in enumerate(clients):
             c.seq = k % self.pool.n_seq
-        events = [(c.t_arrive, 0, c.cid) for c in clients]    # (time, kind 0 arrive / 1 leave, id)
-        heapq.heapify(events)
         by_id = {c.cid: c for c in clients}
-        queue, active = [], {}
-        used, peak = 0.0, 0.0
-        lat, batch_sizes = [], []
-        admitted = waited = 0
-        wait_times = []
+        requests, opened = _q.Queue(), _q.Queue()
+
+        def admission():
+            while True:
+                kind, obj = requests.get()
+                if kind == "stop":
+                    return
+                if kind == "open":
+                    opened.put((obj, self._open(obj)))
+                else:
+                    obj.close()
+
+        waiting, active = [], {}
+        reserved, peak = 0.0, 0.0
+        lat, batch_sizes, wait_times = [], [], []
+        admitted = queued = 0
+        events = []      # (time, kind 0 arrive / 1 leave, id)
+
+        # clients present at the start: admitted before the clock starts
+        for c in clients:
+            if c.t_arrive > 0:
+                heapq.heappush(events, (c.t_arrive, 0, c.cid))
+                continue
+            need = self._need(c)
+            if not waiting and reserved + need <= self.budget:
+                reserved += need
+                c.bytes = need
+                c.session = self._open(c)
+            else:
+                waiting.append(c)
+                queued += 1
+        peak = reserved
+        worker = threading.Thread(target=admission, daemon=True)
+        worker.start()
         t0 = time.perf_counter()
 
         def now():
             return time.perf_counter() - t0
 
-        def admit(c, t):
-            nonlocal used, peak, admitted
-            cfg = mixed_config(c.width, c.height, c.voxel)
-            c.bytes = float(self.lib.fb_session_bytes(cfg))
-            c.session = Session(cfg)
-            used += c.bytes
-            peak = max(peak, used)
+        def activate(c, t):
+            nonlocal admitted
             c.t_admit = t
             c.t_end = t + c.lifetime
             c.next_arrival = t + c.rng.exponential(1.0 / c.rate)
             active[c.cid] = c
             heapq.heappush(events, (c.t_end, 1, c.cid))
             admitted += 1
-            if c.t_admit > c.t_arrive + 1e-9:
+            if c.t_admit > c.t_arrive + 1e-6:
                 wait_times.append(c.t_admit - c.t_arrive)
 
-        def try_admit(t):
-            while queue:
-                c = queue[0]
-                cfg_bytes = float(self.lib.fb_session_bytes(mixed_config(c.width, c.height, c.voxel)))
-                if used + cfg_bytes > self.budget:
-                    break
-                queue.pop(0)
-                admit(c, t)
+        def request_open(c):
+            nonlocal reserved, peak
+            c.bytes = self._need(c)
+            reserved += c.bytes
+            peak = max(peak, reserved)
+            requests.put(("open", c))
 
-        while True:
-            t = now()
-            if t >= duration:
-                break
-            # arrivals and departures up to now
-            while events and events[0][0] <= t:
-                _, kind, cid = heapq.heappop(events)
-                c = by_id[cid]
-                if kind == 0:
-                    need = float(self.lib.fb_session_bytes(mixed_config(c.width, c.height, c.voxel)))
-                    if not queue and used + need <= self.budget:
-                        admit(c, t)
-                    else:
-                        queue.append(c)
-                        waited += 1
-                elif cid in active:
-                    del active[cid]
+        def admit_waiting():
+            while waiting and reserved + self._need(waiting[0]) <= self.budget:
+                request_open(waiting.pop(0))
+
+        for c in clients:
+            if c.session is not None:
+                activate(c, 0.0)
+        try:
+            while True:
+                t = now()
+                if t >= duration:
+                    break
+                while True:            # sessions the admission thread has opened
+                    try:
+                        c, sess = opened.get_nowait()
+                    except _q.Empty:
+                        break
+                    c.session = sess
+                    activate(c, now())
+                while events and events[0][0] <= t:
+                    _, kind, cid = heapq.heappop(events)
+                    c = by_id[cid]
+                    if kind == 0:
+                        if not waiting and reserved + self._need(c) <= self.budget:
+                            request_open(c)
+                        else:
+                            waiting.append(c)
+                            queued += 1
+                    elif cid in active:
+                        del active[cid]
+                        requests.put(("close", c.session))
+                        c.session = None
+                        reserved -= c.bytes
+                        admit_waiting()
+                for c in active.values():
+                    while c.next_arrival is not None and c.next_arrival <= t and c.next_arrival < c.t_end:
+                        c.pending.append(c.next_arrival)
+                        c.next_arrival += c.rng.exponential(1.0 / c.rate)
+                ready = sorted((c for c in active.values() if c.pending), key=lambda c: c.pending[0])
+                if not ready:
+                    nxt = min([c.next_arrival for c in active.values() if c.next_arrival is not None] +
+                              ([events[0][0]] if events else []) + [duration])
+                    time.sleep(max(0.0, min(nxt - now(), 0.001)))
+                    continue
+                ready = ready[:self.max_batch]
+                frames = [self.pool.frame(c.width, c.height, c.seq, c.sent) for c in ready]
+                self.batch.step([c.session for c in ready], frames)
+                t_done = now()
+                for c in ready:
+                    lat.append(t_done - c.pending.pop(0))
+                    c.sent += 1
+                batch_sizes.append(len(ready))
+            wall = now()
+        finally:
+            requests.put(("stop", None))
+            worker.join()
+            while not opened.empty():
+                _, sess = opened.get_nowait()
+                sess.close()
+            for c in clients:
+                if c.session is not None:
                     c.session.close()
                     c.session = None
-                    used -= c.bytes
-                    try_admit(t)
-            # frames that have arrived
-            for c in active.values():
-                while c.next_arrival is not None and c.next_arrival <= t and c.next_arrival < c.t_end:
-                    c.pending.append(c.next_arrival)
-                    c.next_arrival += c.rng.exponential(1.0 / c.rate)
-            ready = sorted((c for c in active.values() if c.pending), key=lambda c: c.pending[0])
-            if not ready:
-                nxt = min([c.next_arrival for c in active.values() if c.next_arrival is not None] +
-                          ([events[0][0]] if events else []) + [duration])
-                time.sleep(max(0.0, min(nxt - now(), 0.002)))
-                continue
-            ready = ready[:self.max_batch]
-            frames = [self.pool.frame(c.width, c.height, c.seq, c.sent) for c in ready]
-            self.batch.step([c.session for c in ready], frames)
-            t_done = now()
-            for c in ready:
-                lat.append(t_done - c.pending.pop(0))
-                c.sent += 1
-            batch_sizes.append(len(ready))
-        wall = now()
-        for c in list(active.values()):
-            c.session.close()
-            c.session = None
         lat_ms = np.array(lat) * 1e3 if lat else np.zeros(1)
         backlog = sum(len(c.pending) for c in clients)
         return {
@@ -228,7 +279,8 @@ class Server:
             "latency_ms": {"p50": float(np.percentile(lat_ms, 50)), "p99": float(np.percentile(lat_ms, 99)),
                            "max": float(lat_ms.max())},
             "steps": len(batch_sizes), "mean_batch": float(np.mean(batch_sizes)) if batch_sizes else 0.0,
-            "clients": len(clients), "admitted": admitted, "queued": waited,
-            "still_queued_at_end": len(queue), "mean_wait_s": float(np.mean(wait_times)) if wait_times else 0.0,
-            "backlog_frames_at_end": backlog, "peak_hbm_bytes": peak, "budget_bytes": self.budget,
+            "clients": len(clients), "admitted": admitted, "queued": queued,
+            "still_queued_at_end": len(waiting),
+            "mean_wait_s": float(np.mean(wait_times)) if wait_times else 0.0,
+            "backlog_frames_at_end": backlog, "peak_reserved_bytes": peak, "budget_bytes": self.budget,
         }

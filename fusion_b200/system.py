@@ -104,6 +104,11 @@ class Session:
     def reset(self):
         check("fb_session_reset", self.lib.fb_session_reset(self.h))
 
+    def prepare(self, shared=False):
+        """Capture every frame graph now (for frames alone, or in batch steps
+        with shared=True)."""
+        check("fb_session_prepare", self.lib.fb_session_prepare(self.h, 1 if shared else 0))
+
     def grab(self, depth, rgb, on_device=False):
         """One frame.  depth: u16 [H, W]; rgb: u8 [H, W, 3]; numpy arrays
         (host) or, with on_device, objects with data_ptr() (device)."""

@@ -134,6 +134,11 @@ FB_API int fb_session_launch_count(fb_session* s, uint64_t* launches);
  * d2h = the frame result read back. */
 FB_API int fb_frame_transfer_bytes(const fb_config* cfg, size_t* h2d, size_t* d2h);
 
+/* Captures now every frame graph the session can use (tracker modes, fusion
+ * on and off, both frame parities), for frames run alone (shared = 0) or in
+ * batch steps with other sessions (shared = 1), so that later frames launch
+ * without capture work on the host.  No reference counterpart. */
+FB_API int fb_session_prepare(fb_session* s, int shared);
 /* Raycast tile (CUDA block shape, bx * by threads, bx * by <= 1024 and a
  * multiple of 32) of this session's model raycast; default 16 x 8.  Results
  * do not depend on it (every pixel is traced alone).  Cached frame graphs are
@@ -157,7 +162,11 @@ typedef struct {
     int on_device;           /* 0: host pointers (copied in), 1: device pointers */
 } fb_frame_input;
 
-/* stream: the stream the batch orders its work after (NULL: its own). */
+/* stream: the stream the batch orders its work after (NULL: its own).
+ * Session memory is one stream-ordered allocation from the device's default
+ * memory pool; creating a batch sets that pool to keep freed memory for reuse
+ * (release threshold) so that sessions created and destroyed while others
+ * run never wait for the device. */
 FB_API int fb_batch_create(void* stream, fb_batch** out);
 FB_API int fb_batch_destroy(fb_batch* b);
 /* How a step reaches the GPU.  0 (default): each session's own frame graph
