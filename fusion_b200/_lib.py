@@ -81,9 +81,11 @@ SIGNATURES = {
     "fb_session_stage_times": (_i, [_vp, _vp, _vp, _i]),
     "fb_session_set_raycast_tile": (_i, [_vp, _i, _i]),
     "fb_session_prepare": (_i, [_vp, _i]),
+    "fb_session_prepare_some": (_i, [_vp, _i, _i, ctypes.POINTER(ctypes.c_int)]),
     "fb_batch_create": (_i, [_vp, ctypes.POINTER(_vp)]),
     "fb_batch_destroy": (_i, [_vp]),
     "fb_batch_set_mode": (_i, [_vp, _i]),
+    "fb_batch_reserve": (_i, [_vp, _sz]),
     "fb_batch_step": (_i, [_vp, _vp, _i, _vp, _vp]),
     "fb_batch_stats": (_i, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "fb_session_launch_count": (_i, [_vp, ctypes.POINTER(ctypes.c_uint64)]),

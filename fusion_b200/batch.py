@@ -104,6 +104,10 @@ class Batch:
         check("fb_batch_step", self.lib.fb_batch_step(self.h, hs, n, ins, out))
         return list(out)
 
+    def reserve(self, nbytes):
+        """Map `nbytes` of device memory into the pool sessions allocate from."""
+        check("fb_batch_reserve", self.lib.fb_batch_reserve(self.h, int(nbytes)))
+
     def stats(self):
         steps, caps = ctypes.c_uint64(), ctypes.c_uint64()
         check("fb_batch_stats", self.lib.fb_batch_stats(self.h, ctypes.byref(steps), ctypes.byref(caps)))

@@ -209,10 +209,12 @@ std::vector<void*> g_out_free;
 void* take_out_slot(size_t bytes) {
     std::lock_guard<std::mutex> guard(g_out_lock);
     if (g_out_free.empty()) {
+        // 1024 slots at a time: page-locking host memory is slow and may
+        // wait for the device, so it happens rarely (normally once)
         const size_t stride = (bytes + 255) & ~(size_t)255;
         char* chunk = nullptr;
-        if (cudaMallocHost((void**)&chunk, 64 * stride) != cudaSuccess) return nullptr;
-        for (int i = 63; i >= 0; --i) g_out_free.push_back(chunk + (size_t)i * stride);
+        if (cudaMallocHost((void**)&chunk, 1024 * stride) != cudaSuccess) return nullptr;
+        for (int i = 1023; i >= 0; --i) g_out_free.push_back(chunk + (size_t)i * stride);
     }
     void* p = g_out_free.back();
     g_out_free.pop_back();
@@ -794,16 +796,23 @@ int fb_grab_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, cons
     return FB_OK;
 }
 
-int fb_session_prepare(fb_session* s, int shared) {
-    if (!s) return FB_EINVAL;
+int fb_session_prepare_some(fb_session* s, int shared, int max_graphs, int* remaining) {
+    if (!s || max_graphs < 0) return FB_EINVAL;
+    if (remaining) *remaining = 0;
     if (!s->use_graphs) return FB_OK;
     const bool keep_shared = s->shared_gpu;
     const int keep_next = s->next;
     s->shared_gpu = shared != 0;
-    int rc = FB_OK;
+    const int sh = s->shared_gpu ? 1 : 0;
+    int rc = FB_OK, done = 0, left = 0;
     for (int mode = 0; mode < 3 && rc == FB_OK; ++mode)
         for (int fuse = 0; fuse < (mode == 2 ? 1 : 2) && rc == FB_OK; ++fuse)
             for (int next = 0; next < 2 && rc == FB_OK; ++next) {
+                if (s->graph[mode][fuse][next][sh]) continue;
+                if (done == max_graphs) {
+                    ++left;
+                    continue;
+                }
                 FramePlan p;
                 p.state = mode == 0 ? 1 : mode == 1 ? 0 : -1;
                 p.init = mode == 0;
@@ -814,11 +823,15 @@ int fb_session_prepare(fb_session* s, int shared) {
                 p.mode = mode;
                 s->next = next;
                 rc = capture_frame(s, p, s->stream);
+                ++done;
             }
     s->next = keep_next;
     s->shared_gpu = keep_shared;
+    if (remaining) *remaining = left;
     return rc;
 }
+
+int fb_session_prepare(fb_session* s, int shared) { return fb_session_prepare_some(s, shared, 1 << 30, nullptr); }
 
 int fb_session_set_raycast_tile(fb_session* s, int bx, int by) {
     if (!s || bx < 1 || by < 1 || bx * by > 128 || (bx * by) % 32 != 0) return FB_EINVAL;
@@ -1366,6 +1379,16 @@ int fb_batch_destroy(fb_batch* b) {
     return FB_OK;
 }
 
+int fb_batch_reserve(fb_batch* b, size_t bytes) {
+    if (!b) return FB_EINVAL;
+    if (!bytes) return FB_OK;
+    void* p = nullptr;
+    FB_CUDA(cudaMallocAsync(&p, bytes, b->origin));
+    FB_CUDA(cudaFreeAsync(p, b->origin));
+    FB_CUDA(cudaStreamSynchronize(b->origin));
+    return FB_OK;
+}
+
 int fb_batch_set_mode(fb_batch* b, int mode) {
     if (!b || mode < 0 || mode > 1) return FB_EINVAL;
     b->mode = mode;
@@ -1396,9 +1419,10 @@ int fb_batch_step(fb_batch* b, fb_session* const* ss, int n, const fb_frame_inpu
                            b->origin);
         if (rc) return rc;
     }
-    // sessions sharing the GPU run the tracking instance that leaves room
-    // for the others (same results)
-    for (int i = 0; i < n; ++i) ss[i]->shared_gpu = n > 1;
+    // sessions of a batch run the tracking instance that leaves room for
+    // other sessions' frames (same results), also in a step of one session:
+    // its frame graphs are then the ones fb_session_prepare(s, 1) captured
+    for (int i = 0; i < n; ++i) ss[i]->shared_gpu = true;
     std::vector<FramePlan> plans(n);
     for (int i = 0; i < n; ++i) plans[i] = plan_frame(ss[i]);
     if (b->mode == 1) {

@@ -119,10 +119,15 @@ def make_clients(n, seed, rate=30.0, median_life=20.0, life_sigma=0.5, horizon=0
 
 
 class Server:
-    """The request loop.  Session creation (device allocation, map reset and
-    capture of the session's frame graphs) and destruction run on a
-    background admission thread so that the step loop never waits for them;
-    clients present at the start are admitted before the clock starts."""
+    """The request loop.  Admission work -- creating a session (one
+    stream-ordered allocation from memory reserved up front, map reset) and
+    capturing its frame graphs -- is done by the step loop itself in slices
+    between steps: at most one session creation or one graph capture per
+    iteration, so that no step waits for more than one slice (graph
+    instantiation holds driver locks that a second host thread's launches
+    and copies would wait for, which showed as 100+ ms stalls).  A client
+    becomes active, and its frames start arriving, once its session is ready.
+    Clients present at the start are admitted before the clock starts."""
 
     def __init__(self, pool, budget_bytes=120e9, mode=0, max_batch=256):
         self.lib = _lib.load()
@@ -137,40 +142,25 @@ class Server:
     def _need(self, c):
         return float(self.lib.fb_session_bytes(mixed_config(c.width, c.height, c.voxel)))
 
-    @staticmethod
-    def _open(c):
-        from .system import Session
-        s = Session(mixed_config(c.width, c.height, c.voxel))
-        s.prepare(shared=True)
-        return s
-
     def run(self, clients, duration):
         """Serve `clients` for `duration` seconds of wall time.  Returns the
         statistics of the run."""
-        import queue as _q
-        import threading
+        from .system import Session
         for k, c in enumerate(clients):
             c.seq = k % self.pool.n_seq
         by_id = {c.cid: c for c in clients}
-        requests, opened = _q.Queue(), _q.Queue()
-
-        def admission():
-            while True:
-                kind, obj = requests.get()
-                if kind == "stop":
-                    return
-                if kind == "open":
-                    opened.put((obj, self._open(obj)))
-                else:
-                    obj.close()
-
-        waiting, active = [], {}
+        waiting, active, preparing, to_open = [], {}, [], []
         reserved, peak = 0.0, 0.0
         lat, batch_sizes, wait_times = [], [], []
         admitted = queued = 0
         events = []      # (time, kind 0 arrive / 1 leave, id)
 
-        # clients present at the start: admitted before the clock starts
+        # device memory for the sessions expected at once (those present at the
+        # start and as many again for arrivals, within the budget), mapped
+        # before the clock starts
+        warm_bytes = sum(self._need(c) for c in clients if c.t_arrive <= 0)
+        self.batch.reserve(min(self.budget, 2.0 * warm_bytes))
+        warm = []
         for c in clients:
             if c.t_arrive > 0:
                 heapq.heappush(events, (c.t_arrive, 0, c.cid))
@@ -179,13 +169,13 @@ class Server:
             if not waiting and reserved + need <= self.budget:
                 reserved += need
                 c.bytes = need
-                c.session = self._open(c)
+                c.session = Session(mixed_config(c.width, c.height, c.voxel))
+                c.session.prepare(shared=True)
+                warm.append(c)
             else:
                 waiting.append(c)
                 queued += 1
         peak = reserved
-        worker = threading.Thread(target=admission, daemon=True)
-        worker.start()
         t0 = time.perf_counter()
 
         def now():
@@ -202,56 +192,63 @@ class Server:
             if c.t_admit > c.t_arrive + 1e-6:
                 wait_times.append(c.t_admit - c.t_arrive)
 
-        def request_open(c):
+        def reserve_for(c):
             nonlocal reserved, peak
             c.bytes = self._need(c)
             reserved += c.bytes
             peak = max(peak, reserved)
-            requests.put(("open", c))
+            to_open.append(c)
 
         def admit_waiting():
             while waiting and reserved + self._need(waiting[0]) <= self.budget:
-                request_open(waiting.pop(0))
+                reserve_for(waiting.pop(0))
 
-        for c in clients:
-            if c.session is not None:
-                activate(c, 0.0)
+        def admission_slice():
+            """One session creation or one graph capture."""
+            if preparing:
+                c = preparing[0]
+                if c.session.prepare_some(1, shared=True) == 0:
+                    preparing.pop(0)
+                    activate(c, now())
+            elif to_open:
+                c = to_open.pop(0)
+                c.session = Session(mixed_config(c.width, c.height, c.voxel))
+                preparing.append(c)
+
+        for c in warm:
+            activate(c, 0.0)
         try:
             while True:
                 t = now()
                 if t >= duration:
                     break
-                while True:            # sessions the admission thread has opened
-                    try:
-                        c, sess = opened.get_nowait()
-                    except _q.Empty:
-                        break
-                    c.session = sess
-                    activate(c, now())
                 while events and events[0][0] <= t:
                     _, kind, cid = heapq.heappop(events)
                     c = by_id[cid]
                     if kind == 0:
                         if not waiting and reserved + self._need(c) <= self.budget:
-                            request_open(c)
+                            reserve_for(c)
                         else:
                             waiting.append(c)
                             queued += 1
                     elif cid in active:
                         del active[cid]
-                        requests.put(("close", c.session))
+                        c.session.close()
                         c.session = None
                         reserved -= c.bytes
                         admit_waiting()
+                if preparing or to_open:
+                    admission_slice()
                 for c in active.values():
                     while c.next_arrival is not None and c.next_arrival <= t and c.next_arrival < c.t_end:
                         c.pending.append(c.next_arrival)
                         c.next_arrival += c.rng.exponential(1.0 / c.rate)
                 ready = sorted((c for c in active.values() if c.pending), key=lambda c: c.pending[0])
                 if not ready:
-                    nxt = min([c.next_arrival for c in active.values() if c.next_arrival is not None] +
-                              ([events[0][0]] if events else []) + [duration])
-                    time.sleep(max(0.0, min(nxt - now(), 0.001)))
+                    if not (preparing or to_open):
+                        nxt = min([c.next_arrival for c in active.values() if c.next_arrival is not None] +
+                                  ([events[0][0]] if events else []) + [duration])
+                        time.sleep(max(0.0, min(nxt - now(), 0.001)))
                     continue
                 ready = ready[:self.max_batch]
                 frames = [self.pool.frame(c.width, c.height, c.seq, c.sent) for c in ready]
@@ -263,11 +260,6 @@ class Server:
                 batch_sizes.append(len(ready))
             wall = now()
         finally:
-            requests.put(("stop", None))
-            worker.join()
-            while not opened.empty():
-                _, sess = opened.get_nowait()
-                sess.close()
             for c in clients:
                 if c.session is not None:
                     c.session.close()

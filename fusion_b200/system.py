@@ -109,6 +109,14 @@ class Session:
         with shared=True)."""
         check("fb_session_prepare", self.lib.fb_session_prepare(self.h, 1 if shared else 0))
 
+    def prepare_some(self, max_graphs=1, shared=False):
+        """Capture at most max_graphs of the missing frame graphs; returns how
+        many are still missing."""
+        left = ctypes.c_int()
+        check("fb_session_prepare_some", self.lib.fb_session_prepare_some(
+            self.h, 1 if shared else 0, int(max_graphs), ctypes.byref(left)))
+        return left.value
+
     def grab(self, depth, rgb, on_device=False):
         """One frame.  depth: u16 [H, W]; rgb: u8 [H, W, 3]; numpy arrays
         (host) or, with on_device, objects with data_ptr() (device)."""

@@ -139,6 +139,12 @@ FB_API int fb_frame_transfer_bytes(const fb_config* cfg, size_t* h2d, size_t* d2
  * batch steps with other sessions (shared = 1), so that later frames launch
  * without capture work on the host.  No reference counterpart. */
 FB_API int fb_session_prepare(fb_session* s, int shared);
+/* As fb_session_prepare, capturing at most max_graphs graphs now;
+ * *remaining = how many are still missing.  Lets a request loop spread the
+ * capture work of a newly admitted session over several steps (graph
+ * instantiation takes driver locks that other threads' launches and copies
+ * wait for). */
+FB_API int fb_session_prepare_some(fb_session* s, int shared, int max_graphs, int* remaining);
 /* Raycast tile (CUDA block shape, bx * by threads, bx * by <= 1024 and a
  * multiple of 32) of this session's model raycast; default 16 x 8.  Results
  * do not depend on it (every pixel is traced alone).  Cached frame graphs are
@@ -169,6 +175,11 @@ typedef struct {
  * run never wait for the device. */
 FB_API int fb_batch_create(void* stream, fb_batch** out);
 FB_API int fb_batch_destroy(fb_batch* b);
+/* Maps `bytes` of device memory into the default pool now (allocated and
+ * freed at once; the pool keeps it), so that sessions created later while
+ * others run do not map new memory, which the driver serialises with kernel
+ * launches. */
+FB_API int fb_batch_reserve(fb_batch* b, size_t bytes);
 /* How a step reaches the GPU.  0 (default): each session's own frame graph
  * is launched on one of the batch's streams (no capture when the set of
  * sessions changes).  1: one graph per step holding every session's frame,
