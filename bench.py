@@ -196,9 +196,76 @@ def run_reference(args):
         "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
                          "sample": f"first {done} frames of the sequence (frame 0 initialises the map)"},
         "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cuda": reference_cuda(args),
     }
     print(json.dumps(line))
     return 0
+
+
+REF_CONSTANTS = ("the reference's compile-time map constants (6 mm voxels, truncation 48 mm, fusion depth "
+                 "0.1-3.0 m, 1e6 buckets, 5e5 excess, 7e5 blocks), 640x480 camera fx = fy = 525, depth cutoff "
+                 "3.0 m, ICP 10/5/3")
+
+
+def reference_cuda(args, frames=80, warmup=5):
+    """The reference's own CUDA kernels (built unmodified from its sources for
+    sm_100a into oracle/_ref by `make -C oracle ref`) driven by the
+    restatement of its host loop (System::GrabImage), on the full-size
+    sequence's first frames with host frames in, as the reference takes
+    them.  Its map sizes are compile-time constants, so this runs at the
+    reference's constants; the our-arm line reports this build at the same
+    constants ("reference_constants").  None when the library or a GPU is
+    missing."""
+    try:
+        import torch
+        from oracle import refharness
+        if not (refharness.available() and torch.cuda.is_available()):
+            return None
+    except Exception:
+        return None
+    from fusion_b200 import synth
+    from fusion_b200 import system as S
+    cfg = S.config_c2()
+    depth, rgb = frames_for(cfg, synth.session_seed(2, 0), warmup + frames)
+    h = refharness.RefHarness(640, 480, 525.0, 525.0, 320.0, 240.0, 5000.0, 3.0)
+    for i in range(warmup):
+        h.grab(depth[i], rgb[i])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tracked = 0
+    for i in range(warmup, warmup + frames):
+        tracked += int(h.grab(depth[i], rgb[i])[0])
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    h.close()
+    return {"value": frames / dt, "unit": "frames/s", "frames": frames, "warmup": warmup,
+            "tracked_frames": tracked, "config": REF_CONSTANTS,
+            "timing": "wall clock around each synchronous GrabImage, host frames in"}
+
+
+def ours_at_reference_constants(depth, rgb, frames=80, warmup=5):
+    """This build at the reference's constants on the same frames, host
+    frames in through fb_grab_frame (like reference_cuda)."""
+    import torch
+    from fusion_b200 import Session
+    from fusion_b200 import system as S
+    cfg = S.reference_config(640, 480, fx=525.0, fy=525.0, depth_scale=5000.0, depth_cutoff=3.0)
+    frames = max(1, min(frames, len(depth) - warmup))
+    p_depth = torch.from_numpy(depth[:warmup + frames]).pin_memory().numpy()
+    p_rgb = torch.from_numpy(rgb[:warmup + frames]).pin_memory().numpy()
+    sess = Session(cfg)
+    for i in range(warmup):
+        sess.grab(p_depth[i], p_rgb[i])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tracked = 0
+    for i in range(warmup, warmup + frames):
+        tracked += sess.grab(p_depth[i], p_rgb[i]).tracked
+    dt = time.perf_counter() - t0
+    sess.close()
+    return {"value": frames / dt, "unit": "frames/s", "frames": frames, "warmup": warmup,
+            "tracked_frames": int(tracked), "config": REF_CONSTANTS,
+            "timing": "wall clock around each synchronous fb_grab_frame, pinned host frames in"}
 
 
 def _batched_run(specs, seeds, warmup, steps, tune=False):
@@ -405,6 +472,7 @@ def main():
 
     # the batched and served forms on one GPU (rank 0 of a single-GPU run)
     one = world == 1
+    at_ref = ours_at_reference_constants(depth, rgb) if one else None
     batched = batched_forms(args, rank, value) if one and not args.no_batched else None
     served = served_form(args, rank, value) if one and not args.no_served else None
     line = {
@@ -424,6 +492,7 @@ def main():
                      "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms},
         "cpu_baseline": cpu,
         "clocks": ck,
+        "reference_constants": at_ref,
         "batched": batched,
         "served": served,
     }
