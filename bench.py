@@ -318,6 +318,71 @@ def _batched_run(specs, seeds, warmup, steps, tune=False):
             "raycast_tiles": {f"{w}x{h}": list(t) for (w, h), t in tiles.items()} if tiles else None}
 
 
+def precision_form(depth, rgb, W, K, plain_value, peak, peak_kind):
+    """The precision form (fb_config.form = FB_FORM_PRECISION) on the same
+    full-size frames, resident in HBM: 6-byte voxels (FP16 TSDF), contracted
+    FP32 integration, compensated FP32 normal equations.  Frames/s, the
+    integration roofline with the 6-byte algorithmic bytes, and the pose and
+    TSDF differences from the reference-form run on the same frames (the
+    errors against the FP64 oracle are stated by tests/test_gpu_precision.py)."""
+    import torch
+    from fusion_b200 import Session
+    from fusion_b200 import system as S
+    from fusion_b200._lib import FB_FORM_PRECISION
+    d_depth = torch.from_numpy(depth).cuda()
+    d_rgb = torch.from_numpy(rgb).cuda()
+    out = {}
+    poses = {}
+    for form in (0, FB_FORM_PRECISION):
+        cfg = S.config_c2()
+        cfg.form = form
+        stream = torch.cuda.Stream()
+        sess = Session(cfg, stream=stream.cuda_stream)
+        for i in range(W):
+            sess.grab(d_depth[i], d_rgb[i], on_device=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ps = []
+        for i in range(W, W + K):
+            ps.append(np.array(sess.grab(d_depth[i], d_rgb[i], on_device=True).pose[:]).reshape(4, 4))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        poses[form] = ps
+        if form == FB_FORM_PRECISION:
+            out["value"] = K / (e0.elapsed_time(e1) / 1000.0)
+            # per-stage times on a fresh session over the same frames
+            sess.close()
+            sess = Session(cfg, stream=stream.cuda_stream)
+            for i in range(W):
+                sess.grab(d_depth[i], d_rgb[i], on_device=True)
+            sess.set_profiling(True)
+            nvis = []
+            for i in range(W, min(W + K, W + 60)):
+                r = sess.grab(d_depth[i], d_rgb[i], on_device=True)
+                if r.fused:
+                    nvis.append(r.no_visible)
+            st = sess.stage_times()
+            ms, calls = st["integration"]
+            avg = ms / max(calls, 1)
+            mv = float(np.mean(nvis)) if nvis else 0.0
+            b = 2 * 6 * 512 * mv + 32 * mv + 23 * cfg.width * cfg.height
+            ach = b / (avg * 1e-3) / 1e9 if avg > 0 else 0.0
+            out["stage_ms_per_frame"] = {k: (v[0] / v[1] if v[1] else 0.0) for k, v in st.items()}
+            out["roofline"] = {"kernel": "k_integrate_compact", "bound": "hbm", "achieved": ach, "peak": peak,
+                               "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak,
+                               "bytes_per_launch": b, "avg_launch_ms": avg, "mean_visible_blocks": mv}
+        sess.close()
+    rot = [float(np.arccos(np.clip((np.trace(a[:3, :3].T @ b[:3, :3]) - 1) / 2, -1, 1)))
+           for a, b in zip(poses[0], poses[FB_FORM_PRECISION])]
+    tra = [float(np.abs(a[:3, 3] - b[:3, 3]).max()) for a, b in zip(poses[0], poses[FB_FORM_PRECISION])]
+    out.update({"unit": "frames/s", "vs_plain": out["value"] / plain_value, "bytes_per_voxel": 6,
+                "bytes_per_voxel_reference_form": 8,
+                "pose_vs_reference_form": {"max_rot_rad": max(rot), "max_t_m": max(tra), "frames": K},
+                "workload": "plain full-size configuration (640x480, 5 mm) in the precision form"})
+    return out
+
+
 def batched_forms(args, rank, plain_value):
     """The batched form on this GPU: (a) sessions of the plain full-size
     configuration (640x480, 5 mm) stepped together -- the same per-frame work
@@ -473,6 +538,7 @@ def main():
     # the batched and served forms on one GPU (rank 0 of a single-GPU run)
     one = world == 1
     at_ref = ours_at_reference_constants(depth, rgb) if one else None
+    precision = precision_form(depth, rgb, W, min(K, 200), value, peak, peak_kind) if one else None
     batched = batched_forms(args, rank, value) if one and not args.no_batched else None
     served = served_form(args, rank, value) if one and not args.no_served else None
     line = {
@@ -493,6 +559,7 @@ def main():
         "cpu_baseline": cpu,
         "clocks": ck,
         "reference_constants": at_ref,
+        "precision": precision,
         "batched": batched,
         "served": served,
     }

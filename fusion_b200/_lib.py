@@ -10,6 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfusion_b200.so")
 
 FB_OK, FB_EINVAL, FB_ENOMEM, FB_ECUDA, FB_ETRACK_LOST = 0, 1, 2, 3, 4
+FB_FORM_REFERENCE, FB_FORM_PRECISION = 0, 1
 
 ERR_FLAGS = {
     0x1: "heap_exhausted", 0x2: "excess_full", 0x4: "request_set_full", 0x8: "coord_range",
@@ -26,6 +27,7 @@ class Config(ctypes.Structure):
         ("depth_min", ctypes.c_float), ("depth_max", ctypes.c_float),
         ("num_buckets", ctypes.c_int), ("num_excess", ctypes.c_int), ("num_blocks", ctypes.c_int),
         ("iters", ctypes.c_int * 3),
+        ("form", ctypes.c_int),
     ]
 
 

@@ -121,6 +121,12 @@ struct __align__(8) Voxel {
     unsigned char r, g, b;
 };
 
+// Precision form: a voxel block is 3072 bytes, structure of arrays --
+// TSDF as FP16 [512] (bytes 0-1023), weight u8 [512] (1024-1535), red,
+// green, blue u8 [512] each (1536-3071).  6 bytes per voxel.
+constexpr int kCBlockBytes = 3072;
+constexpr int kCWeight = 1024, kCRed = 1536, kCGreen = 2048, kCBlue = 2560;
+
 // Bucket of a block (Mapping/DeviceMap.cu:3-10): products wrap in 32 bits and
 // the modulo is unsigned because NumBuckets is an unsigned constant.
 __host__ __device__ __forceinline__ uint32_t bucket_of(int x, int y, int z, uint32_t nb) {

@@ -57,6 +57,9 @@ struct TrackState {
     double grp_rgb[kTrackMaxGroups][32];
     long long grp_cnt[kTrackMaxGroups];
     long long grp_sq[kTrackMaxGroups];
+    // precision form: the group sums as compensated FP32 pairs (hi, lo)
+    float2 grp_icp2[kTrackMaxGroups][32];
+    float2 grp_rgb2[kTrackMaxGroups][32];
 };
 
 // All levels of one frame for the persistent tracking kernel.
@@ -83,7 +86,8 @@ int launch_track_begin(TrackState* st, cudaStream_t s);
 // shared_gpu: the instance with four resident blocks per SM (other sessions'
 // kernels run beside it); same results as the two-block instance
 int launch_track_iter(const TrackLevel& L, TrackState* st, unsigned int* tickets, int2* residual, int* counts,
-                      int min_count, bool is_final, cudaStream_t s, bool shared_gpu = false);
+                      int min_count, bool is_final, cudaStream_t s, bool shared_gpu = false,
+                      bool compensated = false);
 size_t track_list_capacity(int n_pixels);
 int launch_step_icp(const TrackLevel& L, const DevPose& cur, const DevPose& last, float* partials,
                      unsigned int* ticket, double* out, cudaStream_t s);
@@ -144,10 +148,12 @@ struct MapView {
     int NB, NE, NS;
     uint32_t nb_mask;           // NB - 1 when NB is a power of two, else 0
     int* heap;
-    Voxel* voxels;
+    Voxel* voxels;              // reference form: NS x 512 voxels of 8 B
+    uint8_t* cvox;              // precision form: NS blocks of kCBlockBytes (voxels then null)
     MapCounters* ctr;
     int* alloc_list;            // slots of allocated entries, allocation order (NS)
     int* visible;               // slots of visible entries (NS)
+    HEntry* vis_blocks;         // the visible entries themselves (NS), same order
     unsigned long long* reqset; // request set, open addressing (reqcap, power of 2)
     int reqcap;
     NewBlock* newblk;           // this frame's new blocks (newcap)

@@ -28,6 +28,8 @@
 // the table (CheckVisibleBlockKernel, FuseMap.cu:113-138, scans all of them).
 // Integration processes one visible block per CTA iteration: 256 threads, two
 // voxels each, one 16-byte load and at most one 16-byte store per thread.
+#include <cuda_fp16.h>
+
 #include "fb_internal.h"
 
 namespace fb {
@@ -489,9 +491,10 @@ __global__ void __launch_bounds__(256) k_visibility(MapView m, int W, int H, Int
         const int i = (it * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
         bool vis = false;
         int slot = -1;
+        HEntry e;
         if (i < n) {
             slot = m.alloc_list[i];
-            HEntry e = m.entries[slot];
+            e = m.entries[slot];
             vis = block_visible(e.x, e.y, e.z, P, k, W, H, m.g);
         }
         // warp-aggregated append
@@ -502,8 +505,12 @@ __global__ void __launch_bounds__(256) k_visibility(MapView m, int W, int H, Int
             base = __shfl_sync(0xffffffffu, base, 0);
             if (vis) {
                 int o = base + __popc(mask & ((1u << lane) - 1));
-                if (o < m.NS) m.visible[o] = slot;
-                else atomicOr(&m.ctr->err, kErrVisibleFull);
+                if (o < m.NS) {
+                    m.visible[o] = slot;
+                    m.vis_blocks[o] = e;   // read by integration and z ranges without a second gather
+                } else {
+                    atomicOr(&m.ctr->err, kErrVisibleFull);
+                }
             }
         }
     }
@@ -567,7 +574,7 @@ __global__ void __launch_bounds__(256) k_integrate(MapView m, const float* __res
     const int t = threadIdx.x;
     const int lx = (2 * t) & 7, ly = (t >> 2) & 7, lz = t >> 5;
     for (int b = blockIdx.x; b < n; b += gridDim.x) {
-        const HEntry e = m.entries[m.visible[b]];
+        const HEntry e = m.vis_blocks[b];
         const int vx = e.x * 8 + lx, vy = e.y * 8 + ly, vz = e.z * 8 + lz;
         uint4* base = (uint4*)(m.voxels + (size_t)e.ptr * 512) + t;
         uint4 raw2 = *base;
@@ -579,6 +586,132 @@ __global__ void __launch_bounds__(256) k_integrate(MapView m, const float* __res
             *(Voxel*)&o.x = v0;
             *(Voxel*)&o.z = v1;
             *base = o;
+        }
+    }
+}
+
+// Precision form of k_integrate: 6-byte voxels (FP16 TSDF), contracted FP32.
+// One CTA of 128 threads per visible block per iteration; thread t owns the
+// four x-consecutive voxels (4 (t & 1) .. +3, (t >> 1) & 7, t >> 4), so its
+// TSDF (8 B), weights (4 B) and colours (3 x 4 B) are aligned vector loads
+// of the block's arrays, and the block's 3 KB is read by one coalesced pass.
+// Camera-space positions come from a per-block origin and the columns of
+// Rinv scaled by the voxel size (basis), one FMA chain per coordinate.  The
+// update rule is integrateColor's (FuseMap.cu:140-191): project (truncated
+// pixel), depth in range, sdf >= -T, sdf = min(1, sdf / T), skip a NaN
+// normal, w = n . normalised(p, 1) over four lanes, first observation or
+// weighted running average, weight + 1 capped at 255, colour blend 0.2 w.
+__global__ void __launch_bounds__(128, 8) k_integrate_compact(MapView m, const float* __restrict__ raw, int rp,
+                                                           const uint8_t* __restrict__ rgb, int cp,
+                                                           const float4* __restrict__ nmap, int np, int W, int H,
+                                                           Intr k, const DevPose* __restrict__ posep,
+                                                           const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const DevPose P = *posep;
+    const int n = min(m.ctr->n_visible, m.NS);
+    const int t = threadIdx.x;
+    const int lx = 4 * (t & 1), ly = (t >> 1) & 7, lz = t >> 4;
+    const int idx = lz * 64 + ly * 8 + lx;
+    const float vs = m.g.voxel_size, T = m.g.trunc_dist, invT = 1.0f / T;
+    // camera = Rinv (world - t): basis columns Rinv e_i * vs and offset -Rinv t
+    const f3 bx = mk3(P.Rinv.r0.x * vs, P.Rinv.r1.x * vs, P.Rinv.r2.x * vs);
+    const f3 by = mk3(P.Rinv.r0.y * vs, P.Rinv.r1.y * vs, P.Rinv.r2.y * vs);
+    const f3 bz = mk3(P.Rinv.r0.z * vs, P.Rinv.r1.z * vs, P.Rinv.r2.z * vs);
+    const f3 c0 = mk3(-(P.Rinv.r0.x * P.t.x + P.Rinv.r0.y * P.t.y + P.Rinv.r0.z * P.t.z),
+                      -(P.Rinv.r1.x * P.t.x + P.Rinv.r1.y * P.t.y + P.Rinv.r1.z * P.t.z),
+                      -(P.Rinv.r2.x * P.t.x + P.Rinv.r2.y * P.t.y + P.Rinv.r2.z * P.t.z));
+    for (int b = blockIdx.x; b < n; b += gridDim.x) {
+        const HEntry e = m.vis_blocks[b];
+        const float ox = (float)(e.x * 8 + lx), oy = (float)(e.y * 8 + ly), oz = (float)(e.z * 8 + lz);
+        // position of the thread's first voxel
+        f3 p;
+        p.x = fmaf(bx.x, ox, fmaf(by.x, oy, fmaf(bz.x, oz, c0.x)));
+        p.y = fmaf(bx.y, ox, fmaf(by.y, oy, fmaf(bz.y, oz, c0.y)));
+        p.z = fmaf(bx.z, ox, fmaf(by.z, oy, fmaf(bz.z, oz, c0.z)));
+        uint8_t* blk = m.cvox + (size_t)e.ptr * kCBlockBytes;
+        uint2 sd = *(const uint2*)(blk + 2 * idx);
+        uint32_t wq = *(const uint32_t*)(blk + kCWeight + idx);
+        uint32_t rq = *(const uint32_t*)(blk + kCRed + idx);
+        uint32_t gq = *(const uint32_t*)(blk + kCGreen + idx);
+        uint32_t bq = *(const uint32_t*)(blk + kCBlue + idx);
+        __half2 s01 = *(__half2*)&sd.x, s23 = *(__half2*)&sd.y;
+        float sdf[4] = {__low2float(s01), __high2float(s01), __low2float(s23), __high2float(s23)};
+        bool changed = false;
+        // phase 1: the four projections; phase 2: their depth gathers issued
+        // together; phase 3: normal and colour gathers of the voxels that
+        // update, issued together; phase 4: the updates
+        int pix[4], uv[4];
+        f3 pq[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            pq[q] = mk3(fmaf(bx.x, (float)q, p.x), fmaf(bx.y, (float)q, p.y), fmaf(bx.z, (float)q, p.z));
+            const float iz = __fdividef(1.0f, pq[q].z);
+            const int u = __float2int_rz(fmaf(k.fx * pq[q].x, iz, k.cx));
+            const int v = __float2int_rz(fmaf(k.fy * pq[q].y, iz, k.cy));
+            const bool in = !(u < 0 || v < 0 || u >= W || v >= H);
+            pix[q] = in ? v * rp + u : -1;
+            uv[q] = u | v << 16;
+        }
+        float dp[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dp[q] = pix[q] >= 0 ? __ldg(raw + pix[q]) : qnan();
+        float so[4];
+        bool upd[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            so[q] = dp[q] - pq[q].z;
+            upd[q] = !(isnan(dp[q]) || dp[q] > m.g.depth_max || dp[q] < m.g.depth_min) && so[q] >= -T;
+            so[q] = fminf(1.0f, so[q] * invT);
+        }
+        float4 nl[4];
+        uint32_t px[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (upd[q]) {
+                const int u = uv[q] & 0xffff, v = uv[q] >> 16;
+                nl[q] = __ldg(nmap + (size_t)v * np + u);
+                const uint8_t* c3 = rgb + (size_t)v * cp + 3 * u;
+                px[q] = (uint32_t)__ldg(c3) | (uint32_t)__ldg(c3 + 1) << 8 | (uint32_t)__ldg(c3 + 2) << 16;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (!upd[q] || isnan(nl[q].x)) continue;
+            const float w = (nl[q].x * pq[q].x + nl[q].y * pq[q].y + nl[q].z * pq[q].z + nl[q].w) *
+                            rsqrtf(pq[q].x * pq[q].x + pq[q].y * pq[q].y + pq[q].z * pq[q].z + 1.0f);
+            const uint32_t sh = 8 * q, keep = ~(255u << sh);
+            const uint32_t W0 = (wq >> sh) & 255u;
+            const uint32_t cr = px[q] & 255u, cg = (px[q] >> 8) & 255u, cb = px[q] >> 16;
+            uint32_t nr, ng, nb;
+            if (W0 == 0) {
+                sdf[q] = so[q];
+                wq = (wq & keep) | (1u << sh);
+                nr = cr;
+                ng = cg;
+                nb = cb;
+            } else {
+                const float a = 0.2f * w, oa = 1.0f - a, Wf = (float)W0;
+                sdf[q] = __fdividef(sdf[q] * Wf + w * so[q], Wf + w);
+                wq = (wq & keep) | ((W0 < 255u ? W0 + 1u : 255u) << sh);
+                nr = (uint32_t)__float2int_rz(fmaf(a, (float)cr, oa * (float)((rq >> sh) & 255u))) & 255u;
+                ng = (uint32_t)__float2int_rz(fmaf(a, (float)cg, oa * (float)((gq >> sh) & 255u))) & 255u;
+                nb = (uint32_t)__float2int_rz(fmaf(a, (float)cb, oa * (float)((bq >> sh) & 255u))) & 255u;
+            }
+            rq = (rq & keep) | (nr << sh);
+            gq = (gq & keep) | (ng << sh);
+            bq = (bq & keep) | (nb << sh);
+            changed = true;
+        }
+        if (changed) {
+            s01 = __floats2half2_rn(sdf[0], sdf[1]);
+            s23 = __floats2half2_rn(sdf[2], sdf[3]);
+            sd.x = *(uint32_t*)&s01;
+            sd.y = *(uint32_t*)&s23;
+            *(uint2*)(blk + 2 * idx) = sd;
+            *(uint32_t*)(blk + kCWeight + idx) = wq;
+            *(uint32_t*)(blk + kCRed + idx) = rq;
+            *(uint32_t*)(blk + kCGreen + idx) = gq;
+            *(uint32_t*)(blk + kCBlue + idx) = bq;
         }
     }
 }
@@ -599,9 +732,18 @@ __global__ void k_map_reset(MapView m) {
         m.entries[i] = e;
     }
     for (size_t i = tid; i < (size_t)m.NS; i += stride) m.heap[i] = m.NS - (int)i - 1;
-    const uint4 released = make_uint4(0x7fffffffu, 0u, 0x7fffffffu, 0u);  // {NaN, w 0, rgb 0} x 2
-    uint4* vv = (uint4*)m.voxels;
-    for (size_t i = tid; i < (size_t)m.NS * 256; i += stride) vv[i] = released;
+    if (m.cvox) {
+        // precision form: FP16 NaN TSDF, weight 0, colour 0 (64 + 128 uint4 per block)
+        const uint4 nan8 = make_uint4(0x7e007e00u, 0x7e007e00u, 0x7e007e00u, 0x7e007e00u);
+        const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+        uint4* vv = (uint4*)m.cvox;
+        for (size_t i = tid; i < (size_t)m.NS * (kCBlockBytes / 16); i += stride)
+            vv[i] = (i % (kCBlockBytes / 16)) < 64 ? nan8 : zero;
+    } else {
+        const uint4 released = make_uint4(0x7fffffffu, 0u, 0x7fffffffu, 0u);  // {NaN, w 0, rgb 0} x 2
+        uint4* vv = (uint4*)m.voxels;
+        for (size_t i = tid; i < (size_t)m.NS * 256; i += stride) vv[i] = released;
+    }
     for (size_t i = tid; i < (size_t)m.NB; i += stride) m.bucket_cnt[i] = 0;
     for (size_t i = tid; i < (size_t)m.reqcap; i += stride) m.reqset[i] = 0ull;
     if (tid == 0) {
@@ -663,7 +805,10 @@ int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPo
 
 int launch_integrate(const MapView& m, const float* raw, int rp, const uint8_t* rgb, int cp, const float4* nmap,
                       int np, int W, int H, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s) {
-    k_integrate<<<sm_count() * 8, 256, 0, s>>>(m, raw, rp, rgb, cp, nmap, np, W, H, k, pose, skip);
+    if (m.cvox)
+        k_integrate_compact<<<sm_count() * 16, 128, 0, s>>>(m, raw, rp, rgb, cp, nmap, np, W, H, k, pose, skip);
+    else
+        k_integrate<<<sm_count() * 8, 256, 0, s>>>(m, raw, rp, rgb, cp, nmap, np, W, H, k, pose, skip);
     return 1;
 }
 

@@ -12,6 +12,8 @@
 // lower-right corner is taken from the block's upper-left corner
 // (RenderScene.cu:115-116), only the first tile of a block ever covers
 // pixels: [ul, min(ul + 15, lr)].  That is the rectangle filled here.
+#include <cuda_fp16.h>
+
 #include "fb_internal.h"
 
 namespace fb {
@@ -34,7 +36,7 @@ __global__ void __launch_bounds__(256) k_zrange(MapView m, Intr k, const DevPose
     const int n = min(m.ctr->n_visible, m.NS);
     const int zc = m.zc, zr = m.zr;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const HEntry e = m.entries[m.visible[i]];
+        const HEntry e = m.vis_blocks[i];
         int ulx = zc, uly = zr, lrx = -1, lry = -1;
         float zx = m.g.depth_max, zy = m.g.depth_min;
         for (int c = 0; c < 8; ++c) {
@@ -78,17 +80,47 @@ struct EntryCache {
     bool set;
 };
 
+// Voxel access of the two forms.  Reference form: 8-byte voxels.
+struct ExactVox {
+    using ref = const Voxel*;
+    static __device__ __forceinline__ ref at(const MapView& m, int ptr, int idx) {
+        return m.voxels + (size_t)ptr * 512 + idx;
+    }
+    static __device__ __forceinline__ ref none() { return nullptr; }
+    static __device__ __forceinline__ bool null(ref v) { return v == nullptr; }
+    static __device__ __forceinline__ float sdf(ref v) { return v->sdf; }
+    static __device__ __forceinline__ int weight(ref v) { return v->weight; }
+};
+
+// Precision form: block arrays, FP16 TSDF.
+struct CompactVox {
+    struct ref {
+        const uint8_t* blk;
+        int idx;
+    };
+    static __device__ __forceinline__ ref at(const MapView& m, int ptr, int idx) {
+        return ref{m.cvox + (size_t)ptr * kCBlockBytes, idx};
+    }
+    static __device__ __forceinline__ ref none() { return ref{nullptr, 0}; }
+    static __device__ __forceinline__ bool null(ref v) { return v.blk == nullptr; }
+    static __device__ __forceinline__ float sdf(ref v) {
+        return __half2float(*(const __half*)(v.blk + 2 * v.idx));
+    }
+    static __device__ __forceinline__ int weight(ref v) { return v.blk[kCWeight + v.idx]; }
+};
+
 // FindVoxel(float3, cache, valid) (DeviceMap.cu:97-114).  The reference's
 // cache starts as HashEntry() -- position (0,0,0), ptr -1 -- and a first probe
 // inside block (0,0,0) then reads voxel index -1 + local index; here the cache
 // starts empty.  Returns nullptr for a missing block.
-__device__ __forceinline__ const Voxel* find_voxel(const MapView& m, f3 p, EntryCache& c, bool& valid) {
+template <class VR>
+__device__ __forceinline__ typename VR::ref find_voxel(const MapView& m, f3 p, EntryCache& c, bool& valid) {
     const int vx = __float2int_rz(p.x), vy = __float2int_rz(p.y), vz = __float2int_rz(p.z);
     const int bx = block_of(vx), by = block_of(vy), bz = block_of(vz);
     const int idx = local_of(vz) * 64 + local_of(vy) * 8 + local_of(vx);
     if (c.set && bx == c.x && by == c.y && bz == c.z) {
         valid = true;
-        return m.voxels + (size_t)c.ptr * 512 + idx;
+        return VR::at(m, c.ptr, idx);
     }
     int b = (int)bucket_of_m(bx, by, bz, (uint32_t)m.NB, m.nb_mask);
     HEntry e = m.entries[b];
@@ -99,7 +131,7 @@ __device__ __forceinline__ const Voxel* find_voxel(const MapView& m, f3 p, Entry
     }
     if (!found) {
         valid = false;
-        return nullptr;
+        return VR::none();
     }
     valid = true;
     c.x = bx;
@@ -107,48 +139,51 @@ __device__ __forceinline__ const Voxel* find_voxel(const MapView& m, f3 p, Entry
     c.z = bz;
     c.ptr = e.ptr;
     c.set = true;
-    return m.voxels + (size_t)e.ptr * 512 + idx;
+    return VR::at(m, e.ptr, idx);
 }
 
-__device__ __forceinline__ float vsdf(const Voxel* v) { return v ? v->sdf : qnan(); }
+template <class VR>
+__device__ __forceinline__ float vsdf(typename VR::ref v) { return VR::null(v) ? qnan() : VR::sdf(v); }
 
 // Rendering::readSdf (RenderScene.cu:290-295)
+template <class VR>
 __device__ __forceinline__ float read_sdf(const MapView& m, f3 p, EntryCache& c, bool& valid) {
-    const Voxel* v = find_voxel(m, p, c, valid);
-    if (!v) return qnan();
-    Voxel vv = *v;
-    if (vv.weight == 0) valid = false;
-    return vv.sdf;
+    const typename VR::ref v = find_voxel<VR>(m, p, c, valid);
+    if (VR::null(v)) return qnan();
+    if (VR::weight(v) == 0) valid = false;
+    return VR::sdf(v);
 }
 
 // Rendering::readSdfInterped (RenderScene.cu:297-319)
+template <class VR>
 __device__ float read_sdf_interp(const MapView& m, f3 pt, EntryCache& c, bool& valid) {
     const f3 f = mk3(fs(pt.x, floorf(pt.x)), fs(pt.y, floorf(pt.y)), fs(pt.z, floorf(pt.z)));
     auto lerp = [](float a, float b, float t) { return fa(fm(fs(1.0f, t), a), fm(t, b)); };
-    float s0 = vsdf(find_voxel(m, pt, c, valid));
-    float s1 = vsdf(find_voxel(m, mk3(fa(pt.x, 1.f), pt.y, pt.z), c, valid));
+    float s0 = vsdf<VR>(find_voxel<VR>(m, pt, c, valid));
+    float s1 = vsdf<VR>(find_voxel<VR>(m, mk3(fa(pt.x, 1.f), pt.y, pt.z), c, valid));
     float r0 = lerp(s0, s1, f.x);
-    s0 = vsdf(find_voxel(m, mk3(pt.x, fa(pt.y, 1.f), pt.z), c, valid));
-    s1 = vsdf(find_voxel(m, mk3(fa(pt.x, 1.f), fa(pt.y, 1.f), pt.z), c, valid));
+    s0 = vsdf<VR>(find_voxel<VR>(m, mk3(pt.x, fa(pt.y, 1.f), pt.z), c, valid));
+    s1 = vsdf<VR>(find_voxel<VR>(m, mk3(fa(pt.x, 1.f), fa(pt.y, 1.f), pt.z), c, valid));
     float r1 = lerp(s0, s1, f.x);
     float r2 = lerp(r0, r1, f.y);
-    s0 = vsdf(find_voxel(m, mk3(pt.x, pt.y, fa(pt.z, 1.f)), c, valid));
-    s1 = vsdf(find_voxel(m, mk3(fa(pt.x, 1.f), pt.y, fa(pt.z, 1.f)), c, valid));
+    s0 = vsdf<VR>(find_voxel<VR>(m, mk3(pt.x, pt.y, fa(pt.z, 1.f)), c, valid));
+    s1 = vsdf<VR>(find_voxel<VR>(m, mk3(fa(pt.x, 1.f), pt.y, fa(pt.z, 1.f)), c, valid));
     r0 = lerp(s0, s1, f.x);
-    s0 = vsdf(find_voxel(m, mk3(pt.x, fa(pt.y, 1.f), fa(pt.z, 1.f)), c, valid));
-    s1 = vsdf(find_voxel(m, mk3(fa(pt.x, 1.f), fa(pt.y, 1.f), fa(pt.z, 1.f)), c, valid));
+    s0 = vsdf<VR>(find_voxel<VR>(m, mk3(pt.x, fa(pt.y, 1.f), fa(pt.z, 1.f)), c, valid));
+    s1 = vsdf<VR>(find_voxel<VR>(m, mk3(fa(pt.x, 1.f), fa(pt.y, 1.f), fa(pt.z, 1.f)), c, valid));
     r1 = lerp(s0, s1, f.x);
     float r3 = lerp(r0, r1, f.y);
     return lerp(r2, r3, f.z);
 }
 
 // Rendering::readNormal (RenderScene.cu:321-352)
+template <class VR>
 __device__ bool read_normal(const MapView& m, f3 pt, EntryCache& c, const M3& Rinv, f3& n) {
     bool valid;
     float s[6];
     const float off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
     for (int q = 0; q < 6; ++q) {
-        s[q] = read_sdf_interp(m, mk3(fa(pt.x, off[q][0]), fa(pt.y, off[q][1]), fa(pt.z, off[q][2])), c, valid);
+        s[q] = read_sdf_interp<VR>(m, mk3(fa(pt.x, off[q][0]), fa(pt.y, off[q][1]), fa(pt.z, off[q][2])), c, valid);
         if (isnan(s[q]) || s[q] == 1.0f || !valid) return false;
     }
     n = normalised3(mv(Rinv, mk3(fs(s[0], s[1]), fs(s[2], s[3]), fs(s[4], s[5]))));
@@ -156,6 +191,7 @@ __device__ bool read_normal(const MapView& m, f3 pt, EntryCache& c, const M3& Ri
 }
 
 // Rendering::operator() (RenderScene.cu:354-440)
+template <class VR>
 __global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__ vmap, float4* __restrict__ nmap,
                                                  int vp, int W, int H, Intr k, const DevPose* __restrict__ posep,
                                                  const int* __restrict__ skip) {
@@ -190,11 +226,11 @@ __global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__
         EntryCache c;
         c.set = false;
         while (dist_s < dist_e) {
-            sdf = read_sdf(m, result, c, valid);
+            sdf = read_sdf<VR>(m, result, c, valid);
             if (!valid) {
                 step = 8.0f;
             } else {
-                if (sdf <= 0.1f && sdf >= -0.5f) sdf = read_sdf_interp(m, result, c, valid);
+                if (sdf <= 0.1f && sdf >= -0.5f) sdf = read_sdf_interp<VR>(m, result, c, valid);
                 if (sdf <= 0.0f) break;
                 step = !isnan(sdf) ? fmaxf(fm(sdf, stepScale), 1.0f) : 8.0f;
             }
@@ -204,13 +240,13 @@ __global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__
         if (sdf <= 0.0f) {
             step = fm(sdf, stepScale);
             result = add3(result, smul3(step, dir));
-            sdf = read_sdf_interp(m, result, c, valid);
+            sdf = read_sdf_interp<VR>(m, result, c, valid);
             step = fm(sdf, stepScale);
             result = add3(result, smul3(step, dir));
             found = true;
         }
         f3 n;
-        if (found && read_normal(m, result, c, P.Rinv, n)) {
+        if (found && read_normal<VR>(m, result, c, P.Rinv, n)) {
             const f3 r = mv(P.Rinv, sub3(mul3(result, m.g.voxel_size), P.t));
             vout = make_float4(r.x, r.y, r.z, 1.0f);
             nout = make_float4(n.x, n.y, n.z, 1.0f);
@@ -240,7 +276,10 @@ int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const in
 int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,
                     const DevPose* pose, const int* skip, cudaStream_t s, int bx, int by) {
     dim3 b(bx, by), g((W + bx - 1) / bx, (H + by - 1) / by);
-    k_raycast<<<g, b, 0, s>>>(m, vmap, nmap, p, W, H, k, pose, skip);
+    if (m.cvox)
+        k_raycast<CompactVox><<<g, b, 0, s>>>(m, vmap, nmap, p, W, H, k, pose, skip);
+    else
+        k_raycast<ExactVox><<<g, b, 0, s>>>(m, vmap, nmap, p, W, H, k, pose, skip);
     return 1;
 }
 

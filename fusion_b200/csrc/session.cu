@@ -233,12 +233,41 @@ size_t next_pow2(size_t v) {
     return p;
 }
 
+// IEEE binary16 bits -> float (host; exact for every value incl. NaN, inf,
+// subnormals).
+float half_bits_to_float(uint16_t h) {
+    const uint32_t sign = (uint32_t)(h >> 15) << 31;
+    const int exp = (h >> 10) & 31;
+    uint32_t mant = h & 1023;
+    uint32_t bits;
+    if (exp == 31) {
+        bits = sign | 0x7f800000u | (mant << 13);
+    } else if (exp == 0) {
+        if (!mant) {
+            bits = sign;
+        } else {   // subnormal: normalise
+            int e = -1;
+            do {
+                ++e;
+                mant <<= 1;
+            } while (!(mant & 1024));
+            bits = sign | (uint32_t)(127 - 15 - e) << 23 | ((mant & 1023) << 13);
+        }
+    } else {
+        bits = sign | (uint32_t)(exp - 15 + 127) << 23 | (mant << 13);
+    }
+    float f;
+    std::memcpy(&f, &bits, 4);
+    return f;
+}
+
 bool valid_config(const fb_config* c) {
     if (!c || c->width < 16 || c->height < 16 || c->width > 4096 || c->height > 2048) return false;
     if ((size_t)c->width * c->height >= (1u << 22)) return false;  // packed RGB correspondences
     if (!(c->fx > 0) || !(c->fy > 0) || !(c->depth_scale > 0) || !(c->voxel_size > 0) || !(c->trunc_dist > 0))
         return false;
     if (c->num_buckets <= 0 || c->num_excess < 0 || c->num_blocks <= 0) return false;
+    if (c->form != FB_FORM_REFERENCE && c->form != FB_FORM_PRECISION) return false;
     if ((size_t)c->num_blocks * 512 >= ((size_t)1 << 40)) return false;
     for (int i = 0; i < 3; ++i)
         if (c->iters[i] < 0 || c->iters[i] > 1000) return false;
@@ -326,8 +355,11 @@ bool carve_session(fb_session* s, const fb_config* cfg) {
         m.zr = (cfg->height + 7) / 8;
         m.g = make_geom(*cfg);
         ok = dalloc(s, &m.entries, (size_t)m.NB + m.NE) && dalloc(s, &m.heap, m.NS) &&
-             dalloc(s, &m.voxels, (size_t)m.NS * 512) && dalloc(s, &m.ctr, 1) && dalloc(s, &m.alloc_list, m.NS) &&
-             dalloc(s, &m.visible, m.NS) && dalloc(s, &m.reqset, m.reqcap) && dalloc(s, &m.newblk, m.newcap) &&
+             (cfg->form == FB_FORM_PRECISION ? dalloc(s, &m.cvox, (size_t)m.NS * kCBlockBytes)
+                                             : dalloc(s, &m.voxels, (size_t)m.NS * 512)) &&
+             dalloc(s, &m.ctr, 1) && dalloc(s, &m.alloc_list, m.NS) &&
+             dalloc(s, &m.visible, m.NS) && dalloc(s, &m.vis_blocks, m.NS) && dalloc(s, &m.reqset, m.reqcap) &&
+             dalloc(s, &m.newblk, m.newcap) &&
              dalloc(s, &m.order, m.newcap) && dalloc(s, &m.arrival, m.newcap) &&
              dalloc(s, &m.bucket_cnt, m.NB) && dalloc(s, &m.bucket_start, m.NB) && dalloc(s, &m.bucket_x, m.NB) &&
              dalloc(s, &m.chunk_sums, 2 * (size_t)m.nchunks) && dalloc(s, &m.zmin, (size_t)m.zc * m.zr) &&
@@ -425,7 +457,7 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
                 for (int it = 0; it < c.iters[l]; ++it)
                     n += launch_track_iter(lv, s->st, s->tickets, s->residual, s->counts,
                                            min_count[l], l == last_level && it == c.iters[l] - 1, st,
-                                           s->shared_gpu);
+                                           s->shared_gpu, c.form == FB_FORM_PRECISION);
             }
         }
         skip = &s->st->failed;
@@ -949,11 +981,28 @@ int fb_map_download_entries(fb_session* s, int32_t* entries) {
 int fb_map_download_blocks(fb_session* s, const int32_t* ptrs, int n, float* sdf, uint8_t* weight, uint8_t* rgb) {
     if (!s || (n > 0 && !ptrs) || n < 0) return FB_EINVAL;
     std::vector<Voxel> tmp(512);
+    std::vector<uint8_t> cb(kCBlockBytes);
     for (int i = 0; i < n; ++i) {
         if (ptrs[i] < 0 || ptrs[i] % 512 || ptrs[i] / 512 >= s->map.NS) return FB_EINVAL;
-        FB_CUDA(cudaMemcpyAsync(tmp.data(), s->map.voxels + ptrs[i], 512 * sizeof(Voxel), cudaMemcpyDeviceToHost,
-                                s->stream));
-        FB_CUDA(cudaStreamSynchronize(s->stream));
+        if (s->map.cvox) {
+            // precision form: FP16 TSDF widened to float, weight and colour as stored
+            FB_CUDA(cudaMemcpyAsync(cb.data(), s->map.cvox + (size_t)(ptrs[i] / 512) * kCBlockBytes, kCBlockBytes,
+                                    cudaMemcpyDeviceToHost, s->stream));
+            FB_CUDA(cudaStreamSynchronize(s->stream));
+            for (int v = 0; v < 512; ++v) {
+                uint16_t h;
+                std::memcpy(&h, cb.data() + 2 * v, 2);
+                tmp[v].sdf = half_bits_to_float(h);
+                tmp[v].weight = cb[kCWeight + v];
+                tmp[v].r = cb[kCRed + v];
+                tmp[v].g = cb[kCGreen + v];
+                tmp[v].b = cb[kCBlue + v];
+            }
+        } else {
+            FB_CUDA(cudaMemcpyAsync(tmp.data(), s->map.voxels + ptrs[i], 512 * sizeof(Voxel), cudaMemcpyDeviceToHost,
+                                    s->stream));
+            FB_CUDA(cudaStreamSynchronize(s->stream));
+        }
         for (int v = 0; v < 512; ++v) {
             size_t o = (size_t)i * 512 + v;
             if (sdf) sdf[o] = tmp[v].sdf;

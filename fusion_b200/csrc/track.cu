@@ -560,13 +560,32 @@ __device__ __forceinline__ double cluster_sum(cg::cluster_group& cl, T* s_vals, 
     return v;
 }
 
+// Compensated FP32 (the precision form's reduction).  two_sum is Knuth's
+// error-free sum (s + e == a + b exactly); pair_add adds two (hi, lo) pairs
+// with the rounding error of the high parts carried into the low part and
+// the result renormalised (Dekker's fast two-sum), so a sum of many block
+// sums keeps about twice the float precision.
+__device__ __forceinline__ float2 two_sum(float a, float b) {
+    const float s = __fadd_rn(a, b);
+    const float bb = __fsub_rn(s, a);
+    const float e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+    return make_float2(s, e);
+}
+
+__device__ __forceinline__ float2 pair_add(float2 x, float2 y) {
+    const float2 s = two_sum(x.x, y.x);
+    const float lo = __fadd_rn(__fadd_rn(x.y, y.y), s.y);
+    const float hi = __fadd_rn(s.x, lo);
+    return make_float2(hi, __fsub_rn(lo, __fsub_rn(hi, s.x)));
+}
+
 // pass A (one cluster of kTrackCluster blocks per group): ICP rows reduced per
 // block, then per cluster into the group sums; RGB correspondences appended by
 // each warp to its own segment of `list` in pixel-visit order (ballot +
 // popc: deterministic, no block barrier in the pixel loop), with the
 // correspondence count and sum of squared differences reduced the same way
 // (integers below 2^53, exact as doubles).  L.rgbok must be set.
-template <int kMinBlocks>
+template <int kMinBlocks, bool kComp>
 __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMinBlocks)
     k_track_a(TrackLevel L, TrackState* st, int2* list, int* counts) {
     const int N = L.W * L.H;
@@ -611,6 +630,37 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     // block_sum_ll leaves the total in lane 0 of warp 0
     const long long bc = __shfl_sync(0xffffffffu, block_sum_ll(rc, smll), 0);
     const long long bs = __shfl_sync(0xffffffffu, block_sum_ll(rsq, smll), 0);
+    if constexpr (kComp) {
+        // precision form: block sums as compensated FP32 pairs, counts as integers
+        __shared__ float s_f[32];
+        __shared__ long long s_c[2];
+        if (wid == 0) s_f[lane] = lane < 29 ? bsum : 0.f;
+        if (threadIdx.x == 0) {
+            s_c[0] = bc;
+            s_c[1] = bs;
+        }
+        cl.sync();
+        if (cl.block_rank() == 0 && threadIdx.x < 31) {
+            const int g = blockIdx.x / kTrackCluster;
+            if (threadIdx.x < 29) {
+                float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int r = 0; r < kTrackCluster; ++r)
+                    acc = pair_add(acc, make_float2(cl.map_shared_rank(s_f, r)[threadIdx.x], 0.f));
+                st->grp_icp2[g][threadIdx.x] = acc;
+            } else {
+                long long t = 0;
+#pragma unroll
+                for (int r = 0; r < kTrackCluster; ++r) t += cl.map_shared_rank(s_c, r)[threadIdx.x - 29];
+                if (threadIdx.x == 29)
+                    st->grp_cnt[g] = t;
+                else
+                    st->grp_sq[g] = t;
+            }
+        }
+        cl.sync();
+        return;
+    }
     if (wid == 0) s_vals[lane] = lane < 29 ? (double)bsum : lane == 29 ? (double)bc : lane == 30 ? (double)bs : 0.0;
     const double v = cluster_sum(cl, s_vals, 31);
     if (cl.block_rank() == 0 && threadIdx.x < 31) {
@@ -640,7 +690,7 @@ __device__ void solve_staged(SolveIO& io, const double* s, int min_count, int is
 // rows of its warps' segments; each cluster reduces its rows into a group
 // sum; the last cluster to finish adds the groups of both passes in group
 // order (FP64) and performs the Gauss-Newton update with one warp.
-template <int kMinBlocks>
+template <int kMinBlocks, bool kComp>
 __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMinBlocks)
     k_track_b(TrackLevel L, TrackState* st, unsigned int* ticket, const int2* list, const int* counts, int seg_size,
               int min_count, int is_final) {
@@ -648,6 +698,7 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     __shared__ float sm[32 * 29];
     __shared__ float s_rgb[32];
     __shared__ double s_part[4][64];
+    __shared__ float2 s_partc[4][64];
     __shared__ double sums[64];
     __shared__ bool s_last;
     __shared__ SolveIO io;
@@ -696,9 +747,22 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     const float bsum = block_sum29(acc, sm);
     if (wid == 0) s_rgb[lane] = lane < 29 ? bsum : 0.f;
     const int grp = blockIdx.x / kTrackCluster;
-    const double v = cluster_sum(cl, s_rgb, 29);
-    if (cl.block_rank() != 0) return;
-    if (threadIdx.x < 29) st->grp_rgb[grp][threadIdx.x] = v;
+    if constexpr (kComp) {
+        cl.sync();
+        if (cl.block_rank() == 0 && threadIdx.x < 29) {
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int r = 0; r < kTrackCluster; ++r)
+                acc = pair_add(acc, make_float2(cl.map_shared_rank(s_rgb, r)[threadIdx.x], 0.f));
+            st->grp_rgb2[grp][threadIdx.x] = acc;
+        }
+        cl.sync();
+        if (cl.block_rank() != 0) return;
+    } else {
+        const double v = cluster_sum(cl, s_rgb, 29);
+        if (cl.block_rank() != 0) return;
+        if (threadIdx.x < 29) st->grp_rgb[grp][threadIdx.x] = v;
+    }
     // last cluster (its rank-0 block) to finish
     __syncthreads();
     if (threadIdx.x == 0) s_last = ticket_acq_rel(ticket) == (unsigned)(NG - 1);
@@ -709,17 +773,37 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     {
         const int val = threadIdx.x & 63, part = threadIdx.x >> 6;
         const int per = (NG + 3) / 4, g0 = part * per, g1 = min(NG, g0 + per);
-        double t = 0;
-        if ((val & 31) < 29) {
-            const double* src = val < 32 ? &st->grp_icp[0][val] : &st->grp_rgb[0][val - 32];
+        if constexpr (kComp) {
+            // compensated FP32 over the groups; to FP64 only for the solve
+            float2 t = make_float2(0.f, 0.f);
+            if ((val & 31) < 29) {
+                const float2* src = val < 32 ? &st->grp_icp2[0][val] : &st->grp_rgb2[0][val - 32];
 #pragma unroll 8
-            for (int g = g0; g < g1; ++g) t += __ldcg(src + (size_t)g * 32);
+                for (int g = g0; g < g1; ++g) t = pair_add(t, __ldcg(src + (size_t)g * 32));
+            }
+            s_partc[part][val] = t;
+        } else {
+            double t = 0;
+            if ((val & 31) < 29) {
+                const double* src = val < 32 ? &st->grp_icp[0][val] : &st->grp_rgb[0][val - 32];
+#pragma unroll 8
+                for (int g = g0; g < g1; ++g) t += __ldcg(src + (size_t)g * 32);
+            }
+            s_part[part][val] = t;
         }
-        s_part[part][val] = t;
     }
     __syncthreads();
-    if (threadIdx.x < 64) sums[threadIdx.x] = ((s_part[0][threadIdx.x] + s_part[1][threadIdx.x]) +
-                                               s_part[2][threadIdx.x]) + s_part[3][threadIdx.x];
+    if (threadIdx.x < 64) {
+        if constexpr (kComp) {
+            const float2 t = pair_add(pair_add(pair_add(s_partc[0][threadIdx.x], s_partc[1][threadIdx.x]),
+                                               s_partc[2][threadIdx.x]),
+                                      s_partc[3][threadIdx.x]);
+            sums[threadIdx.x] = (double)t.x + (double)t.y;
+        } else {
+            sums[threadIdx.x] = ((s_part[0][threadIdx.x] + s_part[1][threadIdx.x]) + s_part[2][threadIdx.x]) +
+                                s_part[3][threadIdx.x];
+        }
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         *ticket = 0;
@@ -1153,8 +1237,10 @@ int track_cluster_grid(int n) {
         cfg.blockDim = dim3(256);
         int ca = 0, cb = 0;
         // the register-rich instances (two blocks per SM) bound the grid of both
-        if (cudaOccupancyMaxActiveClusters(&ca, (void*)k_track_a<2>, &cfg) == cudaSuccess && ca > 0 && ca < c) c = ca;
-        if (cudaOccupancyMaxActiveClusters(&cb, (void*)k_track_b<2>, &cfg) == cudaSuccess && cb > 0 && cb < c) c = cb;
+        if (cudaOccupancyMaxActiveClusters(&ca, (void*)k_track_a<2, false>, &cfg) == cudaSuccess && ca > 0 && ca < c)
+            c = ca;
+        if (cudaOccupancyMaxActiveClusters(&cb, (void*)k_track_b<2, false>, &cfg) == cudaSuccess && cb > 0 && cb < c)
+            c = cb;
         cudaGetLastError();
         if (c > kTrackMaxGroups) c = kTrackMaxGroups;
         cap = c * kTrackCluster;
@@ -1165,16 +1251,25 @@ int track_cluster_grid(int n) {
 }
 
 int launch_track_iter(const TrackLevel& L, TrackState* st, unsigned int* tickets, int2* residual, int* counts,
-                      int min_count, bool is_final, cudaStream_t s, bool shared_gpu) {
+                      int min_count, bool is_final, cudaStream_t s, bool shared_gpu, bool compensated) {
     const int n = L.W * L.H;
     const int g = track_cluster_grid(n);
     const int seg = (n + g * 256 - 1) / (g * 256) * 32;
-    if (shared_gpu) {
-        k_track_a<4><<<g, 256, 0, s>>>(L, st, residual, counts);
-        k_track_b<4><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, is_final ? 1 : 0);
+    const int fin = is_final ? 1 : 0;
+    if (compensated) {
+        if (shared_gpu) {
+            k_track_a<4, true><<<g, 256, 0, s>>>(L, st, residual, counts);
+            k_track_b<4, true><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, fin);
+        } else {
+            k_track_a<2, true><<<g, 256, 0, s>>>(L, st, residual, counts);
+            k_track_b<2, true><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, fin);
+        }
+    } else if (shared_gpu) {
+        k_track_a<4, false><<<g, 256, 0, s>>>(L, st, residual, counts);
+        k_track_b<4, false><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, fin);
     } else {
-        k_track_a<2><<<g, 256, 0, s>>>(L, st, residual, counts);
-        k_track_b<2><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, is_final ? 1 : 0);
+        k_track_a<2, false><<<g, 256, 0, s>>>(L, st, residual, counts);
+        k_track_b<2, false><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, fin);
     }
     return 2;
 }

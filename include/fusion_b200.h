@@ -67,7 +67,19 @@ typedef struct fb_config {
     int num_excess;             /* excess-list entries (DeviceMap::NumExcess) */
     int num_blocks;             /* voxel blocks of 8^3 in the pool (DeviceMap::NumSdfBlocks) */
     int iters[3];               /* Gauss-Newton iterations at levels 0, 1, 2 */
+    int form;                   /* FB_FORM_REFERENCE (0) or FB_FORM_PRECISION (1); no reference counterpart */
 } fb_config;
+
+/* fb_config.form.  FB_FORM_REFERENCE: the reference's arithmetic, operation
+ * by operation, 8-byte voxels {f32 sdf, u8 weight, u8 r, g, b}.
+ * FB_FORM_PRECISION: 6-byte voxels (FP16 TSDF, u8 weight, RGB8, stored per
+ * block as separate arrays), integration in contracted FP32 with the
+ * per-block camera-space basis, tracking rows in FP32 with the normal
+ * equations reduced in compensated (two-float) FP32 and only the 6x6
+ * solve and pose update in FP64.  Block allocation, visibility and the
+ * raycast's stepping rule are the same in both forms. */
+#define FB_FORM_REFERENCE 0
+#define FB_FORM_PRECISION 1
 
 /* Result of one frame (System::GrabImage). */
 typedef struct fb_frame_result {
