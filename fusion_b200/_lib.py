@@ -84,6 +84,9 @@ SIGNATURES = {
     "fb_session_set_raycast_tile": (_i, [_vp, _i, _i]),
     "fb_session_prepare": (_i, [_vp, _i]),
     "fb_session_prepare_some": (_i, [_vp, _i, _i, ctypes.POINTER(ctypes.c_int)]),
+    "fb_snapshot_bytes": (_i, [_vp, ctypes.POINTER(_sz)]),
+    "fb_snapshot": (_i, [_vp, _vp, _sz, ctypes.POINTER(_sz)]),
+    "fb_restore": (_i, [_vp, _vp, _sz]),
     "fb_batch_create": (_i, [_vp, ctypes.POINTER(_vp)]),
     "fb_batch_destroy": (_i, [_vp]),
     "fb_batch_set_mode": (_i, [_vp, _i]),

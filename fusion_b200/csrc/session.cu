@@ -1312,6 +1312,166 @@ int fb_raycast(fb_session* s, fb_image* vmap, fb_image* nmap, const float Rview[
 
 }  // extern "C"
 
+// ---------------------------------------------------------------- snapshots
+//
+// A snapshot holds everything a session needs to continue exactly where it
+// was: the tracker's host state, the device tracker state, both frames, and
+// the map -- counters, the whole hash table, the free-block stack, the
+// allocated and visible lists and the used prefix of the voxel pool.  Blocks
+// are taken from the free stack in order and never given back, so the used
+// blocks are exactly the pool prefix [0, NumBlocks - 1 - heap_counter); the
+// rest of the pool is in its reset state and is not stored.  The reference
+// dumps its whole device map (System::WriteMapToDisk, Core/System.cc:195-236);
+// this is the same idea with the unused pool left out and the tracker added.
+
+namespace {
+
+constexpr char kSnapMagic[8] = {'F', 'B', 'S', 'N', 'A', 'P', '0', '1'};
+
+struct SnapHeader {
+    char magic[8];
+    fb_config cfg;
+    int next, state, last_state, no_missed, frames_after_reloc, used_blocks;
+    uint64_t frame_id;
+    double pose[16];
+    MapCounters ctr;
+    uint64_t total_bytes;
+};
+
+int clamp_count(int v, int hi) { return v < 0 ? 0 : v > hi ? hi : v; }
+
+// The byte ranges of a session's state in snapshot order (device pointer,
+// size), after the header.
+std::vector<std::pair<void*, size_t>> snapshot_ranges(fb_session* s, const MapCounters& c) {
+    std::vector<std::pair<void*, size_t>> r;
+    const MapView& m = s->map;
+    const int used = clamp_count(m.NS - 1 - c.heap_counter, m.NS);
+    const int na = clamp_count(c.n_alloc, m.NS);
+    const int nv = clamp_count(c.n_visible, m.NS);
+    r.push_back({m.entries, ((size_t)m.NB + m.NE) * sizeof(HEntry)});
+    r.push_back({m.heap, (size_t)m.NS * sizeof(int)});
+    r.push_back({m.alloc_list, (size_t)na * sizeof(int)});
+    r.push_back({m.visible, (size_t)nv * sizeof(int)});
+    r.push_back({m.vis_blocks, (size_t)nv * sizeof(HEntry)});
+    if (m.cvox)
+        r.push_back({m.cvox, (size_t)used * kCBlockBytes});
+    else
+        r.push_back({m.voxels, (size_t)used * 512 * sizeof(Voxel)});
+    r.push_back({s->st, sizeof(TrackState)});
+    for (int f = 0; f < 2; ++f) {
+        FrameBuf& F = s->fr[f];
+        const size_t n0 = (size_t)s->W[0] * s->H[0];
+        r.push_back({F.depth_in, n0 * 2});
+        r.push_back({F.rgb, n0 * 3});
+        r.push_back({F.raw, n0 * 4});
+        for (int l = 0; l < 3; ++l) {
+            const size_t n = (size_t)s->W[l] * s->H[l];
+            r.push_back({F.depth[l], n * 4});
+            r.push_back({F.vmap[l], n * 16});
+            r.push_back({F.nmap[l], n * 16});
+            r.push_back({F.gray[l], n});
+            r.push_back({F.dx[l], n * 2});
+            r.push_back({F.dy[l], n * 2});
+            r.push_back({F.rgbok[l], n});
+        }
+    }
+    return r;
+}
+
+int read_counters(fb_session* s, MapCounters* c) {
+    FB_CUDA(cudaMemcpyAsync(c, s->ctr, sizeof *c, cudaMemcpyDeviceToHost, s->stream));
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    return FB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fb_snapshot_bytes(fb_session* s, size_t* bytes) {
+    if (!s || !bytes) return FB_EINVAL;
+    MapCounters c;
+    int rc = read_counters(s, &c);
+    if (rc) return rc;
+    size_t n = sizeof(SnapHeader);
+    for (auto& r : snapshot_ranges(s, c)) n += r.second;
+    *bytes = n;
+    return FB_OK;
+}
+
+int fb_snapshot(fb_session* s, void* buf, size_t capacity, size_t* written) {
+    if (!s || !buf) return FB_EINVAL;
+    SnapHeader h;
+    std::memset(&h, 0, sizeof h);
+    int rc = read_counters(s, &h.ctr);
+    if (rc) return rc;
+    const auto ranges = snapshot_ranges(s, h.ctr);
+    size_t total = sizeof h;
+    for (auto& r : ranges) total += r.second;
+    if (capacity < total) {
+        fb_set_error_text("fb_snapshot: buffer smaller than fb_snapshot_bytes");
+        return FB_EINVAL;
+    }
+    std::memcpy(h.magic, kSnapMagic, 8);
+    h.cfg = s->cfg;
+    h.next = s->next;
+    h.state = s->state;
+    h.last_state = s->last_state;
+    h.no_missed = s->no_missed;
+    h.frames_after_reloc = s->frames_after_reloc;
+    h.frame_id = s->frame_id;
+    std::memcpy(h.pose, s->pose, sizeof h.pose);
+    h.used_blocks = clamp_count(s->map.NS - 1 - h.ctr.heap_counter, s->map.NS);
+    h.total_bytes = total;
+    char* out = (char*)buf;
+    std::memcpy(out, &h, sizeof h);
+    size_t o = sizeof h;
+    for (auto& r : ranges) {
+        if (r.second) FB_CUDA(cudaMemcpyAsync(out + o, r.first, r.second, cudaMemcpyDeviceToHost, s->stream));
+        o += r.second;
+    }
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    if (written) *written = total;
+    return FB_OK;
+}
+
+int fb_restore(fb_session* s, const void* buf, size_t size) {
+    if (!s || !buf || size < sizeof(SnapHeader)) return FB_EINVAL;
+    SnapHeader h;
+    std::memcpy(&h, buf, sizeof h);
+    if (std::memcmp(h.magic, kSnapMagic, 8) != 0 || h.total_bytes != size) {
+        fb_set_error_text("fb_restore: not a snapshot of this format");
+        return FB_EINVAL;
+    }
+    if (std::memcmp(&h.cfg, &s->cfg, sizeof h.cfg) != 0) {
+        fb_set_error_text("fb_restore: the snapshot was taken with another configuration");
+        return FB_EINVAL;
+    }
+    // the unused pool and the per-frame scratch in their reset state first
+    launch_map_reset(s->map, s->stream);
+    if (check_launch()) return FB_ECUDA;
+    const auto ranges = snapshot_ranges(s, h.ctr);
+    size_t o = sizeof h;
+    for (auto& r : ranges) {
+        if (o + r.second > size) return FB_EINVAL;
+        if (r.second)
+            FB_CUDA(cudaMemcpyAsync(r.first, (const char*)buf + o, r.second, cudaMemcpyHostToDevice, s->stream));
+        o += r.second;
+    }
+    FB_CUDA(cudaMemcpyAsync(s->ctr, &h.ctr, sizeof h.ctr, cudaMemcpyHostToDevice, s->stream));
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    s->next = h.next;
+    s->state = h.state;
+    s->last_state = h.last_state;
+    s->no_missed = h.no_missed;
+    s->frames_after_reloc = h.frames_after_reloc;
+    s->frame_id = h.frame_id;
+    std::memcpy(s->pose, h.pose, sizeof s->pose);
+    return FB_OK;
+}
+
+}  // extern "C"
+
 // ------------------------------------------------------------------ batches
 
 struct fb_batch {

@@ -104,6 +104,20 @@ class Session:
     def reset(self):
         check("fb_session_reset", self.lib.fb_session_reset(self.h))
 
+    def snapshot(self):
+        """The session's whole state as bytes (fb_snapshot)."""
+        n = ctypes.c_size_t()
+        check("fb_snapshot_bytes", self.lib.fb_snapshot_bytes(self.h, ctypes.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        w = ctypes.c_size_t()
+        check("fb_snapshot", self.lib.fb_snapshot(self.h, _p(buf), buf.nbytes, ctypes.byref(w)))
+        return buf[:w.value]
+
+    def restore(self, snap):
+        """Continue from a snapshot of a session with the same configuration."""
+        snap = np.ascontiguousarray(snap, np.uint8)
+        check("fb_restore", self.lib.fb_restore(self.h, _p(snap), snap.nbytes))
+
     def prepare(self, shared=False):
         """Capture every frame graph now (for frames alone, or in batch steps
         with shared=True)."""

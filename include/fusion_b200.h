@@ -164,6 +164,19 @@ FB_API int fb_session_prepare_some(fb_session* s, int shared, int max_graphs, in
  * batched form's autotuner. */
 FB_API int fb_session_set_raycast_tile(fb_session* s, int bx, int by);
 
+/* Snapshots (System::WriteMapToDisk / ReadMapFromDisk, Core/System.cc:195-271,
+ * in memory and with the tracker included): everything a session needs to
+ * continue exactly where it was -- tracker state, both frames, counters, the
+ * whole hash table, the free-block stack, the allocated and visible lists
+ * and the used prefix of the voxel pool (the reference writes its whole
+ * pool).  A session of the same configuration restored from a snapshot gives
+ * the same results, bit for bit, as the original would have.  Uses:
+ * persistence, and evicting a session from HBM to bring it back later.  The
+ * buffer's layout is this library's own. */
+FB_API int fb_snapshot_bytes(fb_session* s, size_t* bytes);
+FB_API int fb_snapshot(fb_session* s, void* host_buf, size_t capacity, size_t* written);
+FB_API int fb_restore(fb_session* s, const void* host_buf, size_t size);
+
 /* ------------------------------------------- batched and served forms
  * No reference counterpart (the reference runs one System per process).
  * A batch steps many independent sessions -- any sizes, cameras and voxel
