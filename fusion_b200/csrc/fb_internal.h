@@ -119,6 +119,10 @@ struct MapCounters {
     int n_new;             // blocks inserted by the last allocation
     int n_visible;         // visible blocks of the last fusion / visibility pass
     int n_tiles;           // rendering rectangles of the last z-range pass
+    // dense block index of the last z-range pass: the box of the visible
+    // blocks (+1 block each side) when it fits the grid's capacity
+    int bmin[3], bmax[3];
+    int g_o[3], g_n[3], g_on;
     int excess_total;      // new blocks going to the excess list this frame
     unsigned int err;      // ErrFlag bits, sticky
     int seq_path;          // last allocation used the sequential path
@@ -154,6 +158,8 @@ struct MapView {
     int* alloc_list;            // slots of allocated entries, allocation order (NS)
     int* visible;               // slots of visible entries (NS)
     HEntry* vis_blocks;         // the visible entries themselves (NS), same order
+    int* grid;                  // dense block index for the raycast (grid_cap cells, -1: none)
+    int grid_cap;
     unsigned long long* reqset; // request set, open addressing (reqcap, power of 2)
     int reqcap;
     NewBlock* newblk;           // this frame's new blocks (newcap)

@@ -20,6 +20,10 @@ namespace fb {
 
 __global__ void k_zrange_init(MapView m, const int* __restrict__ skip) {
     if (skip && *skip) return;
+    if (blockIdx.x == 0 && threadIdx.x < 3) {
+        m.ctr->bmin[threadIdx.x] = 0x7fffffff;
+        m.ctr->bmax[threadIdx.x] = -0x7fffffff;
+    }
     const int n = m.zc * m.zr;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         m.zmin[i] = 100.f;   // CreateRenderingBlocks uploads 100 (RenderScene.cu:245-251)
@@ -35,6 +39,31 @@ __global__ void __launch_bounds__(256) k_zrange(MapView m, Intr k, const DevPose
     const DevPose P = *posep;
     const int n = min(m.ctr->n_visible, m.NS);
     const int zc = m.zc, zr = m.zr;
+    // box of the visible blocks (warp-reduced, then one atomic per warp)
+    {
+        int lo[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, hi[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+            const HEntry e = m.vis_blocks[i];
+            lo[0] = min(lo[0], (int)e.x);
+            lo[1] = min(lo[1], (int)e.y);
+            lo[2] = min(lo[2], (int)e.z);
+            hi[0] = max(hi[0], (int)e.x);
+            hi[1] = max(hi[1], (int)e.y);
+            hi[2] = max(hi[2], (int)e.z);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = __reduce_min_sync(0xffffffffu, lo[a]);
+            hi[a] = __reduce_max_sync(0xffffffffu, hi[a]);
+        }
+        if ((threadIdx.x & 31) == 0 && lo[0] <= hi[0]) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                atomicMin(&m.ctr->bmin[a], lo[a]);
+                atomicMax(&m.ctr->bmax[a], hi[a]);
+            }
+        }
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const HEntry e = m.vis_blocks[i];
         int ulx = zc, uly = zr, lrx = -1, lry = -1;
@@ -72,6 +101,62 @@ __global__ void __launch_bounds__(256) k_zrange(MapView m, Intr k, const DevPose
             }
     }
 }
+
+// Dense block index for the raycast: every allocated block inside the box of
+// this frame's visible blocks (one block of margin) gets its pool index in
+// grid[], -1 elsewhere; outside the box, or when the box exceeds the grid,
+// lookups walk the hash table as before.  The index holds exactly what the
+// hash table holds for those coordinates (one entry per block), so every
+// lookup returns the same block: a ray's samples turn one indexed load instead
+// of a bucket probe and chain walk, which also keeps a warp's lanes together.
+__global__ void k_grid_prepare(MapView m, const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    MapCounters* c = m.ctr;
+    long long vol = 1;
+    int n[3], o[3];
+    for (int a = 0; a < 3; ++a) {
+        o[a] = c->bmin[a] - 1;
+        n[a] = c->bmax[a] - c->bmin[a] + 3;
+        if (n[a] < 1) n[a] = 0;
+        vol *= n[a];
+    }
+    const bool on = c->bmin[0] <= c->bmax[0] && vol > 0 && vol <= m.grid_cap;
+    for (int a = 0; a < 3; ++a) {
+        c->g_o[a] = o[a];
+        c->g_n[a] = on ? n[a] : 0;
+    }
+    c->g_on = on ? 1 : 0;
+}
+
+__global__ void k_grid_clear(MapView m, const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const MapCounters* c = m.ctr;
+    if (!c->g_on) return;
+    const int vol = c->g_n[0] * c->g_n[1] * c->g_n[2];
+    int4* g4 = (int4*)m.grid;
+    const int4 none = make_int4(-1, -1, -1, -1);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (vol + 3) / 4; i += gridDim.x * blockDim.x) g4[i] = none;
+}
+
+__global__ void k_grid_fill(MapView m, const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const MapCounters* c = m.ctr;
+    if (!c->g_on) return;
+    const int ox = c->g_o[0], oy = c->g_o[1], oz = c->g_o[2];
+    const int nx = c->g_n[0], ny = c->g_n[1], nz = c->g_n[2];
+    const int n = min(c->n_alloc, m.NS);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const HEntry e = m.entries[m.alloc_list[i]];
+        const int gx = e.x - ox, gy = e.y - oy, gz = e.z - oz;
+        if ((unsigned)gx < (unsigned)nx && (unsigned)gy < (unsigned)ny && (unsigned)gz < (unsigned)nz)
+            m.grid[(gz * ny + gy) * nx + gx] = e.ptr;
+    }
+}
+
+// The raycast's view of the dense index (registers).
+struct GridView {
+    int ox, oy, oz, nx, ny, nz;
+};
 
 // ----------------------------------------------------------------- raycast
 
@@ -114,13 +199,29 @@ struct CompactVox {
 // inside block (0,0,0) then reads voxel index -1 + local index; here the cache
 // starts empty.  Returns nullptr for a missing block.
 template <class VR>
-__device__ __forceinline__ typename VR::ref find_voxel(const MapView& m, f3 p, EntryCache& c, bool& valid) {
+__device__ __forceinline__ typename VR::ref find_voxel(const MapView& m, const GridView& gv, f3 p, EntryCache& c,
+                                                       bool& valid) {
     const int vx = __float2int_rz(p.x), vy = __float2int_rz(p.y), vz = __float2int_rz(p.z);
     const int bx = block_of(vx), by = block_of(vy), bz = block_of(vz);
     const int idx = local_of(vz) * 64 + local_of(vy) * 8 + local_of(vx);
     if (c.set && bx == c.x && by == c.y && bz == c.z) {
         valid = true;
         return VR::at(m, c.ptr, idx);
+    }
+    const int gx = bx - gv.ox, gy = by - gv.oy, gz = bz - gv.oz;
+    if ((unsigned)gx < (unsigned)gv.nx && (unsigned)gy < (unsigned)gv.ny && (unsigned)gz < (unsigned)gv.nz) {
+        const int ptr = __ldg(m.grid + (gz * gv.ny + gy) * gv.nx + gx);
+        if (ptr < 0) {
+            valid = false;
+            return VR::none();
+        }
+        valid = true;
+        c.x = bx;
+        c.y = by;
+        c.z = bz;
+        c.ptr = ptr;
+        c.set = true;
+        return VR::at(m, ptr, idx);
     }
     int b = (int)bucket_of_m(bx, by, bz, (uint32_t)m.NB, m.nb_mask);
     HEntry e = m.entries[b];
@@ -147,8 +248,8 @@ __device__ __forceinline__ float vsdf(typename VR::ref v) { return VR::null(v) ?
 
 // Rendering::readSdf (RenderScene.cu:290-295)
 template <class VR>
-__device__ __forceinline__ float read_sdf(const MapView& m, f3 p, EntryCache& c, bool& valid) {
-    const typename VR::ref v = find_voxel<VR>(m, p, c, valid);
+__device__ __forceinline__ float read_sdf(const MapView& m, const GridView& gv, f3 p, EntryCache& c, bool& valid) {
+    const typename VR::ref v = find_voxel<VR>(m, gv, p, c, valid);
     if (VR::null(v)) return qnan();
     if (VR::weight(v) == 0) valid = false;
     return VR::sdf(v);
@@ -156,21 +257,21 @@ __device__ __forceinline__ float read_sdf(const MapView& m, f3 p, EntryCache& c,
 
 // Rendering::readSdfInterped (RenderScene.cu:297-319)
 template <class VR>
-__device__ float read_sdf_interp(const MapView& m, f3 pt, EntryCache& c, bool& valid) {
+__device__ float read_sdf_interp(const MapView& m, const GridView& gv, f3 pt, EntryCache& c, bool& valid) {
     const f3 f = mk3(fs(pt.x, floorf(pt.x)), fs(pt.y, floorf(pt.y)), fs(pt.z, floorf(pt.z)));
     auto lerp = [](float a, float b, float t) { return fa(fm(fs(1.0f, t), a), fm(t, b)); };
-    float s0 = vsdf<VR>(find_voxel<VR>(m, pt, c, valid));
-    float s1 = vsdf<VR>(find_voxel<VR>(m, mk3(fa(pt.x, 1.f), pt.y, pt.z), c, valid));
+    float s0 = vsdf<VR>(find_voxel<VR>(m, gv, pt, c, valid));
+    float s1 = vsdf<VR>(find_voxel<VR>(m, gv, mk3(fa(pt.x, 1.f), pt.y, pt.z), c, valid));
     float r0 = lerp(s0, s1, f.x);
-    s0 = vsdf<VR>(find_voxel<VR>(m, mk3(pt.x, fa(pt.y, 1.f), pt.z), c, valid));
-    s1 = vsdf<VR>(find_voxel<VR>(m, mk3(fa(pt.x, 1.f), fa(pt.y, 1.f), pt.z), c, valid));
+    s0 = vsdf<VR>(find_voxel<VR>(m, gv, mk3(pt.x, fa(pt.y, 1.f), pt.z), c, valid));
+    s1 = vsdf<VR>(find_voxel<VR>(m, gv, mk3(fa(pt.x, 1.f), fa(pt.y, 1.f), pt.z), c, valid));
     float r1 = lerp(s0, s1, f.x);
     float r2 = lerp(r0, r1, f.y);
-    s0 = vsdf<VR>(find_voxel<VR>(m, mk3(pt.x, pt.y, fa(pt.z, 1.f)), c, valid));
-    s1 = vsdf<VR>(find_voxel<VR>(m, mk3(fa(pt.x, 1.f), pt.y, fa(pt.z, 1.f)), c, valid));
+    s0 = vsdf<VR>(find_voxel<VR>(m, gv, mk3(pt.x, pt.y, fa(pt.z, 1.f)), c, valid));
+    s1 = vsdf<VR>(find_voxel<VR>(m, gv, mk3(fa(pt.x, 1.f), pt.y, fa(pt.z, 1.f)), c, valid));
     r0 = lerp(s0, s1, f.x);
-    s0 = vsdf<VR>(find_voxel<VR>(m, mk3(pt.x, fa(pt.y, 1.f), fa(pt.z, 1.f)), c, valid));
-    s1 = vsdf<VR>(find_voxel<VR>(m, mk3(fa(pt.x, 1.f), fa(pt.y, 1.f), fa(pt.z, 1.f)), c, valid));
+    s0 = vsdf<VR>(find_voxel<VR>(m, gv, mk3(pt.x, fa(pt.y, 1.f), fa(pt.z, 1.f)), c, valid));
+    s1 = vsdf<VR>(find_voxel<VR>(m, gv, mk3(fa(pt.x, 1.f), fa(pt.y, 1.f), fa(pt.z, 1.f)), c, valid));
     r1 = lerp(s0, s1, f.x);
     float r3 = lerp(r0, r1, f.y);
     return lerp(r2, r3, f.z);
@@ -178,12 +279,12 @@ __device__ float read_sdf_interp(const MapView& m, f3 pt, EntryCache& c, bool& v
 
 // Rendering::readNormal (RenderScene.cu:321-352)
 template <class VR>
-__device__ bool read_normal(const MapView& m, f3 pt, EntryCache& c, const M3& Rinv, f3& n) {
+__device__ bool read_normal(const MapView& m, const GridView& gv, f3 pt, EntryCache& c, const M3& Rinv, f3& n) {
     bool valid;
     float s[6];
     const float off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
     for (int q = 0; q < 6; ++q) {
-        s[q] = read_sdf_interp<VR>(m, mk3(fa(pt.x, off[q][0]), fa(pt.y, off[q][1]), fa(pt.z, off[q][2])), c, valid);
+        s[q] = read_sdf_interp<VR>(m, gv, mk3(fa(pt.x, off[q][0]), fa(pt.y, off[q][1]), fa(pt.z, off[q][2])), c, valid);
         if (isnan(s[q]) || s[q] == 1.0f || !valid) return false;
     }
     n = normalised3(mv(Rinv, mk3(fs(s[0], s[1]), fs(s[2], s[3]), fs(s[4], s[5]))));
@@ -201,6 +302,13 @@ __global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
     const DevPose P = *posep;
+    GridView gv;
+    gv.ox = m.ctr->g_o[0];
+    gv.oy = m.ctr->g_o[1];
+    gv.oz = m.ctr->g_o[2];
+    gv.nx = m.ctr->g_n[0];   // 0 when the index is off: every lookup walks the table
+    gv.ny = m.ctr->g_n[1];
+    gv.nz = m.ctr->g_n[2];
     const size_t o = (size_t)y * vp + x;
     const float4 nan4 = make_float4(qnan(), qnan(), qnan(), qnan());
     float4 vout = nan4, nout = nan4;
@@ -226,11 +334,11 @@ __global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__
         EntryCache c;
         c.set = false;
         while (dist_s < dist_e) {
-            sdf = read_sdf<VR>(m, result, c, valid);
+            sdf = read_sdf<VR>(m, gv, result, c, valid);
             if (!valid) {
                 step = 8.0f;
             } else {
-                if (sdf <= 0.1f && sdf >= -0.5f) sdf = read_sdf_interp<VR>(m, result, c, valid);
+                if (sdf <= 0.1f && sdf >= -0.5f) sdf = read_sdf_interp<VR>(m, gv, result, c, valid);
                 if (sdf <= 0.0f) break;
                 step = !isnan(sdf) ? fmaxf(fm(sdf, stepScale), 1.0f) : 8.0f;
             }
@@ -240,13 +348,13 @@ __global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__
         if (sdf <= 0.0f) {
             step = fm(sdf, stepScale);
             result = add3(result, smul3(step, dir));
-            sdf = read_sdf_interp<VR>(m, result, c, valid);
+            sdf = read_sdf_interp<VR>(m, gv, result, c, valid);
             step = fm(sdf, stepScale);
             result = add3(result, smul3(step, dir));
             found = true;
         }
         f3 n;
-        if (found && read_normal<VR>(m, result, c, P.Rinv, n)) {
+        if (found && read_normal<VR>(m, gv, result, c, P.Rinv, n)) {
             const f3 r = mv(P.Rinv, sub3(mul3(result, m.g.voxel_size), P.t));
             vout = make_float4(r.x, r.y, r.z, 1.0f);
             nout = make_float4(n.x, n.y, n.z, 1.0f);
@@ -270,7 +378,10 @@ static int sm_count_rc() {
 int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s) {
     k_zrange_init<<<(m.zc * m.zr + 255) / 256, 256, 0, s>>>(m, skip);
     k_zrange<<<sm_count_rc() * 2, 256, 0, s>>>(m, k, pose, skip);
-    return 2;
+    k_grid_prepare<<<1, 1, 0, s>>>(m, skip);
+    k_grid_clear<<<sm_count_rc() * 4, 256, 0, s>>>(m, skip);
+    k_grid_fill<<<sm_count_rc() * 4, 256, 0, s>>>(m, skip);
+    return 5;
 }
 
 int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,

@@ -351,6 +351,11 @@ bool carve_session(fb_session* s, const fb_config* cfg) {
         m.newcap = m.NS > kMinNewBlocks ? m.NS : kMinNewBlocks;
         m.reqcap = (int)next_pow2((size_t)2 * m.newcap);
         m.nchunks = (m.NB + kScanChunk - 1) / kScanChunk;
+        // dense raycast index: 16 cells per pool block, 64 K to 4 M cells
+        {
+            const size_t cap = (size_t)16 * m.NS;
+            m.grid_cap = (int)(cap < ((size_t)1 << 16) ? ((size_t)1 << 16) : cap > ((size_t)1 << 22) ? ((size_t)1 << 22) : cap);
+        }
         m.zc = (cfg->width + 7) / 8;
         m.zr = (cfg->height + 7) / 8;
         m.g = make_geom(*cfg);
@@ -363,6 +368,7 @@ bool carve_session(fb_session* s, const fb_config* cfg) {
              dalloc(s, &m.order, m.newcap) && dalloc(s, &m.arrival, m.newcap) &&
              dalloc(s, &m.bucket_cnt, m.NB) && dalloc(s, &m.bucket_start, m.NB) && dalloc(s, &m.bucket_x, m.NB) &&
              dalloc(s, &m.chunk_sums, 2 * (size_t)m.nchunks) && dalloc(s, &m.zmin, (size_t)m.zc * m.zr) &&
+             dalloc(s, &m.grid, (size_t)m.grid_cap) &&
              dalloc(s, &m.zmax, (size_t)m.zc * m.zr);
         s->ctr = m.ctr;
     }
