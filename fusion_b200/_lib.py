@@ -84,6 +84,9 @@ SIGNATURES = {
     "fb_session_set_raycast_tile": (_i, [_vp, _i, _i]),
     "fb_session_prepare": (_i, [_vp, _i]),
     "fb_session_prepare_some": (_i, [_vp, _i, _i, ctypes.POINTER(ctypes.c_int)]),
+    "fb_render_image": (_i, [ctypes.POINTER(Image), ctypes.POINTER(Image), _vp, ctypes.POINTER(Image), _vp]),
+    "fb_depth_to_image": (_i, [ctypes.POINTER(Image), ctypes.POINTER(Image), _vp]),
+    "fb_rgb_to_rgba": (_i, [ctypes.POINTER(Image), ctypes.POINTER(Image), _vp]),
     "fb_snapshot_bytes": (_i, [_vp, ctypes.POINTER(_sz)]),
     "fb_snapshot": (_i, [_vp, _vp, _sz, ctypes.POINTER(_sz)]),
     "fb_restore": (_i, [_vp, _vp, _sz]),

@@ -398,3 +398,21 @@ def raycast(session, vmap, nmap, T, K, stream=None):
         session.h, ctypes.byref(_img(vmap, 16)), ctypes.byref(_img(nmap, 16)), _p(np.ascontiguousarray(R)),
         _p(np.ascontiguousarray(Ri)), _p(t), _p(_f32(K)), ctypes.byref(rendered), _stream(stream)))
     return bool(rendered.value)
+
+
+def render_image(vmap, nmap, light, rgba, stream=None):
+    """RenderImage: Phong shading of a vertex/normal map into rgba (uchar4
+    per pixel, device tensors)."""
+    check("fb_render_image", _lib.load().fb_render_image(
+        ctypes.byref(_img(vmap, 16)), ctypes.byref(_img(nmap, 16)), _p(_f32(light)), ctypes.byref(_img(rgba, 4)),
+        _stream(stream)))
+
+
+def depth_to_image(depth, rgba, stream=None):
+    check("fb_depth_to_image", _lib.load().fb_depth_to_image(ctypes.byref(_img(depth, 4)),
+                                                              ctypes.byref(_img(rgba, 4)), _stream(stream)))
+
+
+def rgb_to_rgba(rgb, rgba, stream=None):
+    check("fb_rgb_to_rgba", _lib.load().fb_rgb_to_rgba(ctypes.byref(_img(rgb, 3)), ctypes.byref(_img(rgba, 4)),
+                                                        _stream(stream)))

@@ -345,6 +345,19 @@ FB_API int fb_raycast(fb_session* s, fb_image* vmap, fb_image* nmap, const float
                const float RviewInv[9], const float tview[3], const float K[4], int* rendered,
                void* stream);
 
+/* Headless rendering (no graphics API; the image is device memory).
+ * fb_render_image replaces RenderImage (Tracking/Reduction.h:44-46,
+ * Tracking/Pyrdown.cu:322-380): Phong shading of a raycast vertex/normal map
+ * (camera frame) lit from `light`, RGBA8, a gradient where there is no
+ * vertex.  fb_depth_to_image replaces DepthToImage (Reduction.h:48-49,
+ * Pyrdown.cu:382-405), fb_rgb_to_rgba RgbImageToRgba (Reduction.h:51-52,
+ * Pyrdown.cu:407-428).  rgba: uchar4 per pixel. */
+FB_API int fb_render_image(const fb_image* vmap, const fb_image* nmap, const float light[3], fb_image* rgba,
+                           void* stream);
+FB_API int fb_depth_to_image(const fb_image* depth, fb_image* rgba, void* stream);
+FB_API int fb_rgb_to_rgba(const fb_image* rgb, fb_image* rgba, void* stream);
+
+
 #ifdef __cplusplus
 }
 #endif

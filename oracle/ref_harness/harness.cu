@@ -442,6 +442,35 @@ int ref_download_range(void* h, int which, float* range) {
     return 0;
 }
 
+// The reference's display kernels on host arrays (Tracking/Pyrdown.cu:322-428).
+int ref_render_image(int cols, int rows, const float* vmap, const float* nmap, const float* light, uint8_t* out) {
+    DeviceArray2D<float4> v(cols, rows), n(cols, rows);
+    DeviceArray2D<uchar4> img(cols, rows);
+    v.upload(vmap, sizeof(float4) * cols);
+    n.upload(nmap, sizeof(float4) * cols);
+    RenderImage(v, n, make_float3(light[0], light[1], light[2]), img);
+    img.download(out, sizeof(uchar4) * cols);
+    return 0;
+}
+
+int ref_depth_to_image(int cols, int rows, const float* depth, uint8_t* out) {
+    DeviceArray2D<float> d(cols, rows);
+    DeviceArray2D<uchar4> img(cols, rows);
+    d.upload(depth, sizeof(float) * cols);
+    DepthToImage(d, img);
+    img.download(out, sizeof(uchar4) * cols);
+    return 0;
+}
+
+int ref_rgb_to_rgba(int cols, int rows, const uint8_t* rgb, uint8_t* out) {
+    DeviceArray2D<uchar3> c(cols, rows);
+    DeviceArray2D<uchar4> img(cols, rows);
+    c.upload(rgb, 3 * cols);
+    RgbImageToRgba(c, img);
+    img.download(out, sizeof(uchar4) * cols);
+    return 0;
+}
+
 int ref_upload_maps(void* h, int which, int level, const float* vmap, const float* nmap) {
     RFrame* f = pick((RefCtx*)h, which);
     if (vmap) f->vmap[level].upload(vmap, sizeof(float4) * f->vmap[level].cols);

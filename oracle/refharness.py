@@ -148,3 +148,29 @@ class RefHarness:
         zmax = np.zeros((60, 80), np.float32)
         self._call("ref_download_zrange", _p(zmin), _p(zmax))
         return zmin, zmax
+
+
+def render_image(vmap, nmap, light):
+    """The reference's RenderImage on host float4 maps; uint8 [H, W, 4]."""
+    lib = ctypes.CDLL(LIB_PATH)
+    H, W, _ = vmap.shape
+    out = np.zeros((H, W, 4), np.uint8)
+    lib.ref_render_image(W, H, _p(np.ascontiguousarray(vmap, np.float32)), _p(np.ascontiguousarray(nmap, np.float32)),
+                         _p(np.ascontiguousarray(light, np.float32)), _p(out))
+    return out
+
+
+def depth_to_image(depth):
+    lib = ctypes.CDLL(LIB_PATH)
+    H, W = depth.shape
+    out = np.zeros((H, W, 4), np.uint8)
+    lib.ref_depth_to_image(W, H, _p(np.ascontiguousarray(depth, np.float32)), _p(out))
+    return out
+
+
+def rgb_to_rgba(rgb):
+    lib = ctypes.CDLL(LIB_PATH)
+    H, W, _ = rgb.shape
+    out = np.zeros((H, W, 4), np.uint8)
+    lib.ref_rgb_to_rgba(W, H, _p(np.ascontiguousarray(rgb, np.uint8)), _p(out))
+    return out
