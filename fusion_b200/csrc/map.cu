@@ -523,7 +523,8 @@ __global__ void __launch_bounds__(256) k_visibility(MapView m, int W, int H, Int
 __device__ __forceinline__ bool integrate_voxel(Voxel& vox, int vx, int vy, int vz, const float* __restrict__ raw,
                                                 int rp, const uint8_t* __restrict__ rgb, int cp,
                                                 const float4* __restrict__ nmap, int np, int W, int H,
-                                                const Intr& k, const DevPose& P, const MapGeom& g) {
+                                                const Intr& k, const DevPose& P, const MapGeom& g,
+                                                const float* __restrict__ div255) {
     f3 pos = mk3(fm((float)vx, g.voxel_size), fm((float)vy, g.voxel_size), fm((float)vz, g.voxel_size));
     pos = mv(P.Rinv, sub3(pos, P.t));
     const float pu = fa(fd(fm(k.fx, pos.x), pos.z), k.cx), pv = fa(fd(fm(k.fy, pos.y), pos.z), k.cy);
@@ -552,9 +553,10 @@ __device__ __forceinline__ bool integrate_voxel(Voxel& vox, int vx, int vy, int 
     }
     const float a = fm(w, 0.2f), oa = fs(1.0f, a);
     const float W0 = (float)vox.weight;
-    float rr = fm(fa(fm(a, fd((float)px[0], 255.f)), fm(oa, fd((float)vox.r, 255.f))), 255.f);
-    float gg = fm(fa(fm(a, fd((float)px[1], 255.f)), fm(oa, fd((float)vox.g, 255.f))), 255.f);
-    float bb = fm(fa(fm(a, fd((float)px[2], 255.f)), fm(oa, fd((float)vox.b, 255.f))), 255.f);
+    // (float)c / 255 of a byte c: the table holds those 256 IEEE quotients
+    float rr = fm(fa(fm(a, div255[px[0]]), fm(oa, div255[vox.r])), 255.f);
+    float gg = fm(fa(fm(a, div255[px[1]]), fm(oa, div255[vox.g])), 255.f);
+    float bb = fm(fa(fm(a, div255[px[2]]), fm(oa, div255[vox.b])), 255.f);
     vox.sdf = fd(fa(fm(vox.sdf, W0), fm(w, sdf)), fa(W0, w));
     vox.weight = (unsigned char)min(255, (int)vox.weight + 1);
     // make_uchar3(float3): truncate to int, then to the low byte
@@ -569,6 +571,9 @@ __global__ void __launch_bounds__(256) k_integrate(MapView m, const float* __res
                                                    const float4* __restrict__ nmap, int np, int W, int H, Intr k,
                                                    const DevPose* __restrict__ posep, const int* __restrict__ skip) {
     if (skip && *skip) return;
+    __shared__ float s_div255[256];
+    s_div255[threadIdx.x] = fd((float)threadIdx.x, 255.f);   // blockDim.x == 256
+    __syncthreads();
     const DevPose P = *posep;
     const int n = min(m.ctr->n_visible, m.NS);
     const int t = threadIdx.x;
@@ -579,8 +584,8 @@ __global__ void __launch_bounds__(256) k_integrate(MapView m, const float* __res
         uint4* base = (uint4*)(m.voxels + (size_t)e.ptr * 512) + t;
         uint4 raw2 = *base;
         Voxel v0 = *(Voxel*)&raw2.x, v1 = *(Voxel*)&raw2.z;
-        bool c0 = integrate_voxel(v0, vx, vy, vz, raw, rp, rgb, cp, nmap, np, W, H, k, P, m.g);
-        bool c1 = integrate_voxel(v1, vx + 1, vy, vz, raw, rp, rgb, cp, nmap, np, W, H, k, P, m.g);
+        bool c0 = integrate_voxel(v0, vx, vy, vz, raw, rp, rgb, cp, nmap, np, W, H, k, P, m.g, s_div255);
+        bool c1 = integrate_voxel(v1, vx + 1, vy, vz, raw, rp, rgb, cp, nmap, np, W, H, k, P, m.g, s_div255);
         if (c0 || c1) {
             uint4 o;
             *(Voxel*)&o.x = v0;
