@@ -193,6 +193,12 @@ int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const in
 int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,
                     const DevPose* pose, const int* skip, cudaStream_t s, int bx = 16, int by = 8);
 
+// Marching-cubes mesh of the map over its n_blocks allocated blocks: *total =
+// triangles found; the first min(total, cap) written to V / N (float3 per
+// vertex) and C (uchar3) when all three are given.  Synchronous on st.
+int launch_mesh(const MapView& m, int n_blocks, float* V, float* N, uint8_t* C, unsigned long long cap,
+                unsigned long long* total, cudaStream_t st);
+
 }  // namespace fb
 
 // Text returned by fb_last_error() in the calling thread.

@@ -1316,6 +1316,56 @@ int fb_raycast(fb_session* s, fb_image* vmap, fb_image* nmap, const float Rview[
     return FB_OK;
 }
 
+int fb_mesh_scene(fb_session* s, float* vertex, float* normal, uint8_t* color, uint64_t max_triangles,
+                  uint64_t* no_triangles, void* stream) {
+    if (!s || !no_triangles) return FB_EINVAL;
+    const bool any = vertex || normal || color;
+    if (any && !(vertex && normal && color)) return FB_EINVAL;
+    cudaStream_t st = stream ? as_stream(stream) : s->stream;
+    MapCounters c;
+    FB_CUDA(cudaMemcpyAsync(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    unsigned long long total = 0;
+    const int rc = launch_mesh(s->map, c.n_alloc, vertex, normal, color, any ? max_triangles : 0, &total, st);
+    if (rc != FB_OK) return rc;
+    s->launches += any ? 3 : 2;
+    *no_triangles = total;
+    return FB_OK;
+}
+
+int fb_save_mesh(fb_session* s, const char* path, uint64_t* no_triangles) {
+    if (!s || !path) return FB_EINVAL;
+    uint64_t n = 0;
+    int rc = fb_mesh_scene(s, nullptr, nullptr, nullptr, 0, &n, nullptr);
+    if (rc != FB_OK) return rc;
+    std::vector<float> V(n * 9), N(n * 9);
+    std::vector<uint8_t> C(n * 9);
+    if (n) {
+        float* dv = nullptr;
+        FB_CUDA(cudaMallocAsync((void**)&dv, n * 9 * (2 * sizeof(float) + 1), s->stream));
+        float* dn = dv + n * 9;
+        uint8_t* dc = (uint8_t*)(dn + n * 9);
+        uint64_t m = 0;
+        rc = fb_mesh_scene(s, dv, dn, dc, n, &m, nullptr);
+        cudaError_t e = cudaSuccess;
+        if (rc == FB_OK) {
+            e = cudaMemcpyAsync(V.data(), dv, n * 9 * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(N.data(), dn, n * 9 * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(C.data(), dc, n * 9, cudaMemcpyDeviceToHost, s->stream);
+        }
+        cudaFreeAsync(dv, s->stream);
+        const cudaError_t se = cudaStreamSynchronize(s->stream);
+        if (rc != FB_OK) return rc;
+        if (e != cudaSuccess || se != cudaSuccess) {
+            fb_set_error_text(cudaGetErrorString(e != cudaSuccess ? e : se));
+            return FB_ECUDA;
+        }
+    }
+    if (no_triangles) *no_triangles = n;
+    return fb_write_ply(path, V.data(), N.data(), C.data(), n);
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------- snapshots

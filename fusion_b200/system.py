@@ -7,6 +7,7 @@ reference's kernel free functions (Tracking/Reduction.h, Mapping/RenderScene.h)
 on torch CUDA tensors, which serve only as device memory here.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -117,6 +118,33 @@ class Session:
         """Continue from a snapshot of a session with the same configuration."""
         snap = np.ascontiguousarray(snap, np.uint8)
         check("fb_restore", self.lib.fb_restore(self.h, _p(snap), snap.nbytes))
+
+    def mesh(self, max_triangles=None, device=False):
+        """MeshScene (fb_mesh_scene): the map's marching-cubes triangle soup as
+        (vertex, normal, color), three rows per triangle -- float32 [3T, 3]
+        metres and unit normals, uint8 [3T, 3] colours -- as numpy arrays, or
+        as CUDA tensors with device=True.  At most max_triangles triangles."""
+        import torch
+        n = ctypes.c_uint64()
+        check("fb_mesh_scene", self.lib.fb_mesh_scene(self.h, None, None, None, 0, ctypes.byref(n), None))
+        cap = n.value if max_triangles is None else min(n.value, int(max_triangles))
+        V = torch.empty((3 * cap, 3), dtype=torch.float32, device="cuda")
+        N = torch.empty((3 * cap, 3), dtype=torch.float32, device="cuda")
+        C = torch.empty((3 * cap, 3), dtype=torch.uint8, device="cuda")
+        if cap:
+            torch.cuda.current_stream().synchronize()
+            check("fb_mesh_scene", self.lib.fb_mesh_scene(self.h, V.data_ptr(), N.data_ptr(), C.data_ptr(), cap,
+                                                          ctypes.byref(n), None))
+        if device:
+            return V, N, C
+        return V.cpu().numpy(), N.cpu().numpy(), C.cpu().numpy()
+
+    def save_mesh(self, path):
+        """System::WriteMeshToDisk: mesh the map and write it to `path` as
+        ASCII PLY (fb_save_mesh).  Returns the triangle count."""
+        n = ctypes.c_uint64()
+        check("fb_save_mesh", self.lib.fb_save_mesh(self.h, os.fsencode(path), ctypes.byref(n)))
+        return n.value
 
     def prepare(self, shared=False):
         """Capture every frame graph now (for frames alone, or in batch steps
@@ -398,6 +426,26 @@ def raycast(session, vmap, nmap, T, K, stream=None):
         session.h, ctypes.byref(_img(vmap, 16)), ctypes.byref(_img(nmap, 16)), _p(np.ascontiguousarray(R)),
         _p(np.ascontiguousarray(Ri)), _p(t), _p(_f32(K)), ctypes.byref(rendered), _stream(stream)))
     return bool(rendered.value)
+
+
+def mesh_case_table():
+    """The marching-cubes case table of fb_mesh_scene: (tri int8 [256, 16]
+    edge triples, -1 filled; counts int32 [256])."""
+    tri = np.zeros((256, 16), np.int8)
+    cnt = np.zeros(256, np.int32)
+    check("fb_mesh_case_table", _lib.load().fb_mesh_case_table(_p(tri), _p(cnt)))
+    return tri, cnt
+
+
+def write_ply(path, vertex, normal, color):
+    """The file writing of System::WriteMeshToDisk (fb_write_ply): ASCII PLY
+    of a triangle soup (host arrays, three rows per triangle)."""
+    V = np.ascontiguousarray(vertex, np.float32)
+    N = np.ascontiguousarray(normal, np.float32)
+    C = np.ascontiguousarray(color, np.uint8)
+    if not (V.shape == N.shape == C.shape and V.ndim == 2 and V.shape[1] == 3 and V.shape[0] % 3 == 0):
+        raise ValueError("vertex, normal and color must be [3T, 3] arrays of one shape")
+    check("fb_write_ply", _lib.load().fb_write_ply(os.fsencode(path), _p(V), _p(N), _p(C), V.shape[0] // 3))
 
 
 def render_image(vmap, nmap, light, rgba, stream=None):

@@ -357,6 +357,34 @@ FB_API int fb_render_image(const fb_image* vmap, const fb_image* nmap, const flo
 FB_API int fb_depth_to_image(const fb_image* depth, fb_image* rgba, void* stream);
 FB_API int fb_rgb_to_rgba(const fb_image* rgb, fb_image* rgba, void* stream);
 
+/* Replaces: MeshScene (Mapping/MeshScene.cu:306-355) as called by
+ * Mapping::CreateModel (Mapping/Mapping.cc:131-140): marching cubes over every
+ * voxel of every allocated block.  Triangle soup, three vertices per
+ * triangle: vertex and normal float3 (metres, unit gradient normals), color
+ * uchar3, device pointers.  *no_triangles = all triangles the map holds; the
+ * first min(that, max_triangles) are written, in a deterministic order
+ * (blocks in allocation order, voxels in index order).  vertex = normal =
+ * color = NULL counts only.  The vertices are the reference's, bit for bit;
+ * the triangles over them come from this library's case table
+ * (fb_mesh_case_table), which keeps ambiguous faces consistent between
+ * neighbouring cubes.  Synchronous. */
+FB_API int fb_mesh_scene(fb_session* s, float* vertex, float* normal, uint8_t* color, uint64_t max_triangles,
+                         uint64_t* no_triangles, void* stream);
+/* The marching-cubes case table fb_mesh_scene uses (the role of the
+ * reference's triangleTableHost / vertexTableHost, Mapping/Constant.h): for
+ * each of the 256 cases (bit i set: corner i has sdf < 0, corners in
+ * MeshScene.cu's order) up to 5 triangles as edge triples, -1 filled;
+ * counts[case] = triangles.  tri: 256 x 16.  Host only. */
+FB_API int fb_mesh_case_table(int8_t* tri, int32_t* counts);
+/* Replaces the file writing of System::WriteMeshToDisk (Core/System.cc:
+ * 140-193): ASCII PLY with the reference's header and number formatting,
+ * one PLY vertex per triangle corner.  Host pointers.  Synchronous. */
+FB_API int fb_write_ply(const char* path, const float* vertex, const float* normal, const uint8_t* color,
+                        uint64_t no_triangles);
+/* System::WriteMeshToDisk as one call: fb_mesh_scene into temporary device
+ * memory, download, fb_write_ply to `path`.  *no_triangles may be NULL. */
+FB_API int fb_save_mesh(fb_session* s, const char* path, uint64_t* no_triangles);
+
 
 #ifdef __cplusplus
 }

@@ -1054,6 +1054,114 @@ template <class R> int grab(System& s, const uint16_t* depth, const uint8_t* rgb
     return 0;
 }
 
+// ------------------------------------------------------------------ mesh --
+//
+// MeshScene (Mapping/MeshScene.cu:20-295) restated on the CPU, driven by a
+// case table given as an argument (the reference's Constant.h table or the
+// library's own), over every entry with ptr >= 0 in slot order.  `fused`
+// selects how the normal is rounded: 0 as written (n_a + val * (n_b - n_a),
+// n . n left to right, each operation rounded), 1 with the multiply-adds
+// fused (fma(val, n_b - n_a, n_a); fma(z, z, fma(y, y, x x))), the form a
+// CUDA build contracts these expressions to.
+
+struct MeshVox { float sdf; const uint8_t* rgb; };
+
+// FindVoxel(int3) (DeviceMap.cu:78-84): Voxel() -- NaN, colour 0 -- where the
+// block is missing
+inline MeshVox mesh_voxel(const Map& m, int x, int y, int z) {
+    static const uint8_t kBlack[3] = {0, 0, 0};
+    const int slot = m.find(block_of(x), block_of(y), block_of(z));
+    if (slot < 0) return {kNaN, kBlack};
+    const Voxel& v = m.voxels[(size_t)m.entries[slot].ptr + local_of(z) * 64 + local_of(y) * 8 + local_of(x)];
+    return {v.sdf, v.rgb};
+}
+
+// interp (MeshScene.cu:142-150): float operands, double thresholds
+inline float mesh_interp(float v1, float v2) {
+    if (std::fabs(0.f - v1) < 1e-6) return 0.f;
+    if (std::fabs(0.f - v2) < 1e-6) return 1.f;
+    if (std::fabs(v1 - v2) < 1e-6) return 0.f;
+    return (0.f - v1) / (v2 - v1);
+}
+
+const int kMC[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+const int kME[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+
+uint64_t mesh_scene(const Map& m, const int8_t* tri, const int32_t* ntri, int fused, float* V, float* N,
+                    uint8_t* C, uint64_t cap) {
+    uint64_t count = 0;
+    for (size_t slot = 0; slot < m.entries.size(); ++slot) {
+        const Entry& e = m.entries[slot];
+        if (e.ptr < 0) continue;
+        for (int lz = 0; lz < 8; ++lz)
+            for (int ly = 0; ly < 8; ++ly)
+                for (int lx = 0; lx < 8; ++lx) {
+                    const int px = e.x * 8 + lx, py = e.y * 8 + ly, pz = e.z * 8 + lz;
+                    // readVertexAndColor (MeshScene.cu:105-140)
+                    float sdf[8];
+                    const uint8_t* col[8];
+                    bool ok = true;
+                    for (int i = 0; i < 8 && ok; ++i) {
+                        MeshVox v = mesh_voxel(m, px + kMC[i][0], py + kMC[i][1], pz + kMC[i][2]);
+                        sdf[i] = v.sdf;
+                        col[i] = v.rgb;
+                        ok = !(sdf[i] == 1.0 || std::isnan(sdf[i]));
+                    }
+                    if (!ok) continue;
+                    // readNormal (MeshScene.cu:43-103): central differences
+                    float nrm[8][3];
+                    for (int i = 0; i < 8 && ok; ++i)
+                        for (int a = 0; a < 3 && ok; ++a) {
+                            int hi[3] = {px + kMC[i][0], py + kMC[i][1], pz + kMC[i][2]};
+                            int lo[3] = {hi[0], hi[1], hi[2]};
+                            hi[a] += 1;
+                            lo[a] -= 1;
+                            const float h = mesh_voxel(m, hi[0], hi[1], hi[2]).sdf;
+                            const float l = mesh_voxel(m, lo[0], lo[1], lo[2]).sdf;
+                            ok = !(std::isnan(h) || std::isnan(l));
+                            nrm[i][a] = h - l;
+                        }
+                    if (!ok) continue;
+                    int ci = 0;
+                    for (int i = 0; i < 8; ++i)
+                        if (sdf[i] < 0) ci |= 1 << i;
+                    if (ci == 0 || ci == 255) continue;
+                    // buildVertexList (MeshScene.cu:152-259) and MarchingCube's
+                    // output (MeshScene.cu:277-293)
+                    for (int t = 0; t < ntri[ci]; ++t, ++count) {
+                        if (count >= cap) continue;
+                        for (int k = 0; k < 3; ++k) {
+                            const int ed = tri[ci * 16 + 3 * t + k];
+                            const int a = kME[ed][0], b = kME[ed][1];
+                            const float val = mesh_interp(sdf[a], sdf[b]);
+                            float p[3];
+                            for (int c = 0; c < 3; ++c) {
+                                const int d = kMC[b][c] - kMC[a][c];
+                                const float off = d > 0 ? val : (d < 0 ? 1.f - val : (float)kMC[a][c]);
+                                const int base = c == 0 ? px : (c == 1 ? py : pz);
+                                p[c] = ((float)base + off) * m.cfg.voxel_size;
+                            }
+                            float n[3];
+                            for (int c = 0; c < 3; ++c)
+                                n[c] = fused ? std::fmaf(val, nrm[b][c] - nrm[a][c], nrm[a][c])
+                                             : nrm[a][c] + val * (nrm[b][c] - nrm[a][c]);
+                            const float nn = fused ? std::fmaf(n[2], n[2], std::fmaf(n[1], n[1], n[0] * n[0]))
+                                                   : n[0] * n[0] + n[1] * n[1] + n[2] * n[2];
+                            const float len = std::sqrt(nn);
+                            const uint64_t o = (count * 3 + k) * 3;
+                            const int iv = (int)val;
+                            for (int c = 0; c < 3; ++c) {
+                                V[o + c] = p[c];
+                                N[o + c] = n[c] / len;
+                                C[o + c] = (uint8_t)(col[a][c] + (uint8_t)((uint8_t)(col[b][c] - col[a][c]) * iv));
+                            }
+                        }
+                    }
+                }
+    }
+    return count;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ C API --
@@ -1178,6 +1286,12 @@ int fbo_map_load_blocks(void* mp, const int32_t* ptrs, int n, const double* sdf,
             x.weight = w[o];
             for (int k = 0; k < 3; ++k) x.rgb[k] = rgb[3 * o + k];
         }
+    return 0;
+}
+
+int fbo_map_mesh(void* mp, const int8_t* tri, const int32_t* ntri, int fused, float* V, float* N, uint8_t* C,
+                 uint64_t cap, uint64_t* count) {
+    *count = mesh_scene(*(Map*)mp, tri, ntri, fused, V, N, C, (V && N && C) ? cap : 0);
     return 0;
 }
 

@@ -93,6 +93,12 @@ int fbo_map_set_entries(void* m, const int32_t* slots, const int32_t* entries, i
 int fbo_map_set_visible(void* m, const int32_t* slots, int n);
 int fbo_map_load_blocks(void* m, const int32_t* ptrs, int n, const double* sdf,
                         const uint8_t* weight, const uint8_t* rgb);
+// MeshScene (Mapping/MeshScene.cu:20-295) with a given case table (tri:
+// 256 x 16 edge triples, ntri: triangles per case): *count = triangles; the
+// first min(count, cap) written (3 vertices each: V, N float3, C uchar3).
+// fused: 1 rounds the normal's multiply-adds fused, 0 as written.
+int fbo_map_mesh(void* m, const int8_t* tri, const int32_t* ntri, int fused, float* V, float* N, uint8_t* C,
+                 uint64_t cap, uint64_t* count);
 
 // ---- whole per-frame loop (System::GrabImage) ----
 void* fbo_system_create(const fbo_config* cfg);

@@ -265,6 +265,22 @@ class Map:
         lib().fbo_map_voxels(ctypes.c_void_p(self.h), _p(ptrs), n, _p(sdf), _p(w), _p(rgb))
         return sdf, w, rgb
 
+    def mesh(self, tri, ntri, fused=1):
+        """MeshScene on this map with case table (tri [256, 16] edge triples,
+        ntri [256]): (vertex, normal, color), three rows per triangle."""
+        tri = np.ascontiguousarray(tri, np.int8)
+        ntri = np.ascontiguousarray(ntri, np.int32)
+        n = ctypes.c_uint64()
+        L = lib()
+        L.fbo_map_mesh.argtypes = [ctypes.c_void_p] * 7 + [ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
+        L.fbo_map_mesh(ctypes.c_void_p(self.h), _p(tri), _p(ntri), fused, None, None, None, 0, ctypes.byref(n))
+        V = np.zeros((3 * n.value, 3), np.float32)
+        N = np.zeros((3 * n.value, 3), np.float32)
+        C = np.zeros((3 * n.value, 3), np.uint8)
+        L.fbo_map_mesh(ctypes.c_void_p(self.h), _p(tri), _p(ntri), fused, _p(V), _p(N), _p(C), n.value,
+                       ctypes.byref(n))
+        return V, N, C
+
 
 class System:
     def __init__(self, cfg):

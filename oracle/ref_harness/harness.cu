@@ -2,8 +2,8 @@
 //
 // Drives the reference's own CUDA kernels (Tracking/Pyrdown.cu,
 // Tracking/Reduction.cu, Mapping/DeviceMap.cu, Mapping/FuseMap.cu,
-// Mapping/RenderScene.cu, compiled unmodified from the reference tree by
-// oracle/Makefile) through their public free functions (Tracking/Reduction.h,
+// Mapping/RenderScene.cu, Mapping/MeshScene.cu, compiled unmodified from the
+// reference tree by oracle/Makefile) through their public free functions (Tracking/Reduction.h,
 // Mapping/RenderScene.h), in the order the reference's host classes call
 // them.  The host classes themselves (Core/Frame.cc, Tracking/Tracking.cc,
 // Mapping/Mapping.cc, Core/System.cc) need OpenCV, Eigen and Sophus, none of
@@ -29,6 +29,7 @@
 //     view starts one block into the allocation so that index stays owned.
 // The hash table is zero-filled before ResetMap because ResetHashKernel only
 // clears ptr (Mapping/FuseMap.cu:321-332, DeviceMap.h:36-38).
+#include "Constant.h"
 #include "Reduction.h"
 #include "RenderScene.h"
 #include "../se3.hpp"
@@ -566,6 +567,43 @@ int ref_download_zrange(void* h, float* zmin, float* zmax) {
     RefCtx* c = (RefCtx*)h;
     download2d(c->zRangeMin, zmin);
     download2d(c->zRangeMax, zmax);
+    return 0;
+}
+
+// The reference's marching-cubes tables (Mapping/Constant.h, included from
+// the reference tree): tri 256 x 16 edge indices (-1 filled), ntri =
+// vertexTableHost / 3.
+int ref_mesh_tables(int8_t* tri, int32_t* ntri) {
+    for (int i = 0; i < 256; ++i) {
+        for (int k = 0; k < 16; ++k) tri[i * 16 + k] = (int8_t)triangleTableHost[i][k];
+        ntri[i] = vertexTableHost[i] / 3;
+    }
+    return 0;
+}
+
+// Mapping::CreateModel (Mapping/Mapping.cc:131-140) with the buffers and
+// tables of Mapping's constructor (Mapping.cc:22-34): MeshScene on the
+// current map.  *count = the triangle counter (MeshScene's return value);
+// the first min(count, cap) triangles are downloaded (3 vertices each).
+int ref_mesh_scene(void* h, float* vertex, float* normal, uint8_t* color, uint32_t cap, uint32_t* count) {
+    RefCtx* c = (RefCtx*)h;
+    DeviceArray<uint> nBlocks(1), noTriangles(1);
+    DeviceArray<int> edgeTable(256), vertexTable(256);
+    DeviceArray2D<int> triangleTable;
+    triangleTable.create(16, 256);
+    edgeTable.upload(edgeTableHost);
+    vertexTable.upload(vertexTableHost);
+    triangleTable.upload(triangleTableHost);
+    DeviceArray<float3> modelVertex(DeviceMap::MaxVertices), modelNormal(DeviceMap::MaxVertices);
+    DeviceArray<uchar3> modelColor(DeviceMap::MaxVertices);
+    DeviceArray<int3> blockPoses(DeviceMap::NumEntries);
+    const uint n = MeshScene(nBlocks, noTriangles, c->devmap(), edgeTable, vertexTable, triangleTable,
+                             modelNormal, modelVertex, modelColor, blockPoses);
+    *count = n;
+    const size_t m = (size_t)(n < cap ? n : cap) * 3;
+    if (m && vertex) modelVertex.download(vertex, m);
+    if (m && normal) modelNormal.download(normal, m);
+    if (m && color) modelColor.download(color, m);
     return 0;
 }
 

@@ -143,6 +143,20 @@ class RefHarness:
         self._call("ref_download_blocks", _p(ptrs), ctypes.c_int(n), _p(sdf), _p(w), _p(rgb))
         return sdf, w, rgb
 
+    def mesh(self):
+        """Mapping::CreateModel with the reference's MeshScene and tables:
+        (vertex, normal, color), three rows per triangle."""
+        n = ctypes.c_uint32(0)
+        fn = self.lib.ref_mesh_scene
+        fn.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_uint32, ctypes.c_void_p]
+        fn(ctypes.c_void_p(self.h), None, None, None, ctypes.c_uint32(0), ctypes.byref(n))
+        # the count is only known after a run; run again to download
+        V = np.zeros((3 * n.value, 3), np.float32)
+        N = np.zeros((3 * n.value, 3), np.float32)
+        C = np.zeros((3 * n.value, 3), np.uint8)
+        fn(ctypes.c_void_p(self.h), _p(V), _p(N), _p(C), ctypes.c_uint32(n.value), ctypes.byref(n))
+        return V, N, C
+
     def zrange(self):
         zmin = np.zeros((60, 80), np.float32)
         zmax = np.zeros((60, 80), np.float32)
@@ -174,3 +188,13 @@ def rgb_to_rgba(rgb):
     out = np.zeros((H, W, 4), np.uint8)
     lib.ref_rgb_to_rgba(W, H, _p(np.ascontiguousarray(rgb, np.uint8)), _p(out))
     return out
+
+
+def mesh_tables():
+    """The reference's marching-cubes tables (Mapping/Constant.h): (tri int8
+    [256, 16], triangles per case int32 [256])."""
+    lib = ctypes.CDLL(LIB_PATH)
+    tri = np.zeros((256, 16), np.int8)
+    ntri = np.zeros(256, np.int32)
+    lib.ref_mesh_tables(_p(tri), _p(ntri))
+    return tri, ntri
