@@ -16,6 +16,7 @@
 #include <mutex>
 #include <new>
 #include <vector>
+#include <cmath>
 
 #include "../../include/fusion_b200.h"
 #include "fb_internal.h"
@@ -1313,6 +1314,47 @@ int fb_raycast(fb_session* s, fb_image* vmap, fb_image* nmap, const float Rview[
         FB_CUDA(cudaMemcpy(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost));
         *rendered = c.n_tiles > 0;
     }
+    return FB_OK;
+}
+
+int fb_render_top_down(fb_session* s, float dist, fb_image* vmap, fb_image* nmap, fb_image* rgba, int* rendered,
+                       void* stream) {
+    if (!s || !image_ok(vmap, 16) || !image_ok(nmap, 16) || !image_ok(rgba, 4) || vmap->pitch != nmap->pitch ||
+        !(dist >= 0.f))
+        return FB_EINVAL;
+    const int W = vmap->cols, H = vmap->rows;
+    if (nmap->cols != W || nmap->rows != H || rgba->cols != W || rgba->rows != H || (W + 7) / 8 > s->map.zc ||
+        (H + 7) / 8 > s->map.zr)
+        return FB_EINVAL;
+    cudaStream_t st = stream ? as_stream(stream) : s->stream;
+    // Eigen::AngleAxisd(M_PI / 2, -UnitX).toRotationMatrix() rounded to float
+    // (System.cc:77-81): c I + s [a]x + (1 - c) a a^T with a = -x, s = 1 and
+    // c = cos(pi / 2) = 6.1e-17, which float keeps
+    const float c = (float)std::cos(M_PI / 2);
+    const float R[9] = {1.f, 0.f, 0.f, 0.f, c, 1.f, 0.f, -1.f, c};
+    const float Rinv[9] = {1.f, 0.f, 0.f, 0.f, c, -1.f, 0.f, 1.f, c};
+    const float t[3] = {0.f, -dist, 0.f};
+    // Frame::fx(0), Frame::fy(0) and the image centre in whole pixels
+    const float K[4] = {s->K[0].fx, s->K[0].fy, (float)(W / 2), (float)(H / 2)};
+    MapView m = s->map;
+    m.g.depth_min = dist + s->map.g.depth_min;
+    m.g.depth_max = dist + s->map.g.depth_max;
+    k_set_pose<<<1, 1, 0, st>>>(s->scratch_pose, pose_from(R, Rinv, t));
+    const Intr k = intr_from(K);
+    // Mapping::UpdateVisibility (Mapping.cc:68-74) scans for a 640 x 480
+    // camera whatever the image size
+    launch_visibility(m, 640, 480, k, s->scratch_pose, nullptr, st);
+    launch_zrange(m, k, s->scratch_pose, nullptr, st);
+    launch_raycast(m, (float4*)vmap->data, (float4*)nmap->data, (int)(vmap->pitch / 16), W, H, k, s->scratch_pose,
+                   nullptr, st);
+    if (check_launch()) return FB_ECUDA;
+    MapCounters ctr;
+    FB_CUDA(cudaMemcpyAsync(&ctr, s->ctr, sizeof ctr, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    const float light[3] = {0.f, 0.f, 0.f};
+    const int rc = fb_render_image(vmap, nmap, light, rgba, st);
+    if (rc != FB_OK) return rc;
+    if (rendered) *rendered = ctr.n_tiles > 0;
     return FB_OK;
 }
 

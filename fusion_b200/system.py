@@ -428,6 +428,24 @@ def raycast(session, vmap, nmap, T, K, stream=None):
     return bool(rendered.value)
 
 
+def render_top_down(session, dist, vmap, nmap, rgba, stream=None):
+    """System::RenderTopDown (fb_render_top_down): the model from `dist`
+    metres above, raycast into vmap/nmap (float4 device tensors) and shaded
+    into rgba (uchar4).  Returns whether any block was in view."""
+    rendered = ctypes.c_int()
+    check("fb_render_top_down", _lib.load().fb_render_top_down(
+        session.h, float(dist), ctypes.byref(_img(vmap, 16)), ctypes.byref(_img(nmap, 16)),
+        ctypes.byref(_img(rgba, 4)), ctypes.byref(rendered), _stream(stream)))
+    return bool(rendered.value)
+
+
+def top_down_pose(dist):
+    """The pose System::RenderTopDown renders from (4x4, double): rotation
+    by pi/2 about -x (cos(pi/2) kept as computed), camera at (0, -dist, 0)."""
+    c = np.cos(np.pi / 2)
+    return np.array([[1, 0, 0, 0], [0, c, 1, -float(np.float32(dist))], [0, -1, c, 0], [0, 0, 0, 1]], np.float64)
+
+
 def mesh_case_table():
     """The marching-cubes case table of fb_mesh_scene: (tri int8 [256, 16]
     edge triples, -1 filled; counts int32 [256])."""

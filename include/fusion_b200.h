@@ -357,6 +357,19 @@ FB_API int fb_render_image(const fb_image* vmap, const fb_image* nmap, const flo
 FB_API int fb_depth_to_image(const fb_image* depth, fb_image* rgba, void* stream);
 FB_API int fb_rgb_to_rgba(const fb_image* rgb, fb_image* rgba, void* stream);
 
+/* Replaces: System::RenderTopDown (Core/System.cc:75-90): the model seen
+ * from `dist` metres above the origin looking down (+y), the depth range
+ * shifted by `dist`: visibility for a 640 x 480 camera (as the reference's
+ * Mapping::UpdateVisibility), z ranges, raycast into vmap/nmap (float4,
+ * camera frame, the frame's fx, fy and the image centre), then Phong shading
+ * into rgba (uchar4, light at the camera).  All images one size, at most the
+ * session's.  Replaces the session's visible-block list, as the reference
+ * does.  *rendered = 0 when no block was in view: vmap/nmap are then left
+ * as they were and rgba is shaded from them, as in the reference.
+ * Synchronous. */
+FB_API int fb_render_top_down(fb_session* s, float dist, fb_image* vmap, fb_image* nmap, fb_image* rgba,
+                              int* rendered, void* stream);
+
 /* Replaces: MeshScene (Mapping/MeshScene.cu:306-355) as called by
  * Mapping::CreateModel (Mapping/Mapping.cc:131-140): marching cubes over every
  * voxel of every allocated block.  Triangle soup, three vertices per

@@ -1228,6 +1228,15 @@ int fbo_map_raycast(void* mp, const double* T, float* vm, float* nm, float* zmin
     return m.cfg.precision == 32 ? raytrace<float>(m, T, vm, nm, zmin, zmax)
                                  : raytrace<double>(m, T, vm, nm, zmin, zmax);
 }
+int fbo_map_visibility(void* mp, const double* T, uint32_t* nv) {
+    Map& m = *(Map*)mp;
+    if (m.cfg.precision == 32)
+        visibility<float>(m, T);
+    else
+        visibility<double>(m, T);
+    if (nv) *nv = (uint32_t)m.visible.size();
+    return 0;
+}
 int fbo_map_counters(void* mp, int32_t* hc, int32_t* ep, uint32_t* nv) {
     Map& m = *(Map*)mp;
     if (hc) *hc = m.heapCounter;

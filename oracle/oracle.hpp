@@ -93,6 +93,9 @@ int fbo_map_set_entries(void* m, const int32_t* slots, const int32_t* entries, i
 int fbo_map_set_visible(void* m, const int32_t* slots, int n);
 int fbo_map_load_blocks(void* m, const int32_t* ptrs, int n, const double* sdf,
                         const uint8_t* weight, const uint8_t* rgb);
+// CheckBlockVisibility (Mapping/FuseMap.cu:206-249) at pose T for the
+// configured camera and depth range; *nv = visible blocks.
+int fbo_map_visibility(void* m, const double* T, uint32_t* nv);
 // MeshScene (Mapping/MeshScene.cu:20-295) with a given case table (tri:
 // 256 x 16 edge triples, ntri: triangles per case): *count = triangles; the
 // first min(count, cap) written (3 vertices each: V, N float3, C uchar3).

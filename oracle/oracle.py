@@ -265,6 +265,14 @@ class Map:
         lib().fbo_map_voxels(ctypes.c_void_p(self.h), _p(ptrs), n, _p(sdf), _p(w), _p(rgb))
         return sdf, w, rgb
 
+    def visibility(self, pose):
+        """CheckBlockVisibility at `pose` (4x4) for the configured camera and
+        depth range; returns the visible block count."""
+        n = ctypes.c_uint32()
+        lib().fbo_map_visibility(ctypes.c_void_p(self.h), _p(np.ascontiguousarray(pose, np.float64)),
+                                 ctypes.byref(n))
+        return n.value
+
     def mesh(self, tri, ntri, fused=1):
         """MeshScene on this map with case table (tri [256, 16] edge triples,
         ntri [256]): (vertex, normal, color), three rows per triangle."""
