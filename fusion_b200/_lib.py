@@ -87,6 +87,9 @@ SIGNATURES = {
     "fb_render_image": (_i, [ctypes.POINTER(Image), ctypes.POINTER(Image), _vp, ctypes.POINTER(Image), _vp]),
     "fb_depth_to_image": (_i, [ctypes.POINTER(Image), ctypes.POINTER(Image), _vp]),
     "fb_rgb_to_rgba": (_i, [ctypes.POINTER(Image), ctypes.POINTER(Image), _vp]),
+    "fb_write_map_file": (_i, [_vp, ctypes.c_char_p]),
+    "fb_read_map_file": (_i, [_vp, ctypes.c_char_p]),
+    "fb_session_set_mapping": (_i, [_vp, _i]),
     "fb_render_top_down": (_i, [_vp, _f, ctypes.POINTER(Image), ctypes.POINTER(Image), ctypes.POINTER(Image),
                                 ctypes.POINTER(ctypes.c_int), _vp]),
     "fb_mesh_scene": (_i, [_vp, _vp, _vp, _vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), _vp]),

@@ -218,7 +218,10 @@ __device__ void stage_block(const MapView& m, const HEntry& self, MeshSmem& s) {
     const int t = threadIdx.x;
     if (t < 27) {
         const int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
-        s.ptr[t] = (t == 13) ? self.ptr : find_block(m, self.x + dx, self.y + dy, self.z + dz);
+        // the block itself is looked up too: a map with duplicate entries
+        // for one block (the reference's racy allocator makes them) reads the
+        // first one, as FindVoxel does
+        s.ptr[t] = find_block(m, self.x + dx, self.y + dy, self.z + dz);
     }
     __syncthreads();
     for (int r = t; r < kRegion; r += kMeshThreads) {

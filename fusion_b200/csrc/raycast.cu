@@ -138,6 +138,18 @@ __global__ void k_grid_clear(MapView m, const int* __restrict__ skip) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (vol + 3) / 4; i += gridDim.x * blockDim.x) g4[i] = none;
 }
 
+// FindEntry's block (DeviceMap.cu:122-135): the first entry of the chain
+// holding block (x, y, z), or -1.
+__device__ __forceinline__ int first_ptr(const MapView& m, int x, int y, int z) {
+    HEntry e = m.entries[bucket_of_m(x, y, z, (uint32_t)m.NB, m.nb_mask)];
+    if (e.ptr != -1 && e.x == x && e.y == y && e.z == z) return e.ptr;
+    for (int guard = 0; e.offset > 0 && e.offset <= m.NE && guard <= m.NE; ++guard) {
+        e = m.entries[m.NB + e.offset - 1];
+        if (e.x == x && e.y == y && e.z == z && e.ptr != -1) return e.ptr;
+    }
+    return -1;
+}
+
 __global__ void k_grid_fill(MapView m, const int* __restrict__ skip) {
     if (skip && *skip) return;
     const MapCounters* c = m.ctr;
@@ -148,8 +160,10 @@ __global__ void k_grid_fill(MapView m, const int* __restrict__ skip) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const HEntry e = m.entries[m.alloc_list[i]];
         const int gx = e.x - ox, gy = e.y - oy, gz = e.z - oz;
+        // a map with two entries for one block (the reference's racy
+        // allocator makes them) gets the block the hash lookup finds
         if ((unsigned)gx < (unsigned)nx && (unsigned)gy < (unsigned)ny && (unsigned)gz < (unsigned)nz)
-            m.grid[(gz * ny + gy) * nx + gx] = e.ptr;
+            m.grid[(gz * ny + gy) * nx + gx] = first_ptr(m, e.x, e.y, e.z);
     }
 }
 

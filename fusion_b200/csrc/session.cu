@@ -10,6 +10,7 @@
 // frame was not tracked.  One small device-to-host copy at the end returns the
 // frame result, and the host then advances the reference's tracking state
 // machine (Tracking/Tracking.cc:58-112) and swaps the frames.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -17,6 +18,8 @@
 #include <new>
 #include <vector>
 #include <cmath>
+
+#include <cuda_fp16.h>
 
 #include "../../include/fusion_b200.h"
 #include "fb_internal.h"
@@ -179,6 +182,9 @@ struct fb_session {
     int graph_kernels[3][2][2][2];
     int rc_bx, rc_by;          // raycast tile
     bool shared_gpu;           // frames run beside other sessions' (batch steps)
+    // Tracker::mappingDisabled (set by System::ReadMapFromDisk): frames track
+    // and render against the map without fusing into it
+    bool mapping_disabled;
 };
 
 namespace {
@@ -488,6 +494,9 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
     }
     mark(6);
     if (render) {
+        // with mapping disabled, System::GrabImage refreshes the visible
+        // blocks first (Mapping::UpdateVisibility, System.cc:116-118)
+        if (!fuse && s->mapping_disabled) n += launch_visibility(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st);
         // Mapping::RayTrace (Mapping.cc:92-109) into the frame's level-0 maps
         n += launch_zrange(s->map, s->K[0], pose, skip, st);
         mark(7);
@@ -574,7 +583,7 @@ FramePlan plan_frame(fb_session* s) {
     p.after = s->frames_after_reloc;
     if (p.state == 0) p.after++;
     if (p.state == -1) p.after = 0;
-    p.fuse = (p.init || p.track) && p.after >= 10;
+    p.fuse = !s->mapping_disabled && (p.init || p.track) && p.after >= 10;
     p.render = p.init || p.track;
     p.mode = p.init ? 0 : p.track ? 1 : 2;
     return p;
@@ -878,6 +887,13 @@ int fb_session_set_raycast_tile(fb_session* s, int bx, int by) {
     drop_graphs(s);
     s->rc_bx = bx;
     s->rc_by = by;
+    return FB_OK;
+}
+
+int fb_session_set_mapping(fb_session* s, int on) {
+    if (!s) return FB_EINVAL;
+    if (s->mapping_disabled == (on != 0)) drop_graphs(s);   // cached graphs hold the other variant
+    s->mapping_disabled = on == 0;
     return FB_OK;
 }
 
@@ -1570,6 +1586,278 @@ int fb_restore(fb_session* s, const void* buf, size_t size) {
 
 }  // extern "C"
 
+// ---------------------------------------------------------------- map files
+//
+// System::WriteMapToDisk / ReadMapFromDisk (Core/System.cc:195-271, through
+// Mapping::DownloadToRAM / UploadFromRAM, Mapping/Mapping.cc:153-213): the
+// reference's dump of its device map, in its byte layout -- four int sizes
+// (NumSdfBlocks, NumBuckets, NumVoxels, NumEntries), the heap counter, the
+// excess-list counter and the visible count, the free-block stack, the
+// bucket locks, every voxel (8 bytes: sdf, weight, rgb), every hash entry,
+// the visible-entry list (32-byte HashEntry: int3 pos, ptr as a voxel index,
+// offset, padding), then the key-point map (an int lock per key and a
+// 288-byte SURF per entry).  This library keeps no key points: it writes
+// them unlocked (-1) and zero, and skips them when reading.  A file loads
+// into a session whose sizes match the file's.
+
+namespace {
+
+struct RefEntry {
+    int32_t x, y, z, ptr, offset, pad[3];
+};
+static_assert(sizeof(RefEntry) == 32, "the reference's __align__(16) HashEntry");
+static_assert(sizeof(Voxel) == 8, "the reference's Voxel");
+constexpr size_t kKeyLocks = 100000;    // KeyMap::MaxKeys (Mapping/DeviceMap.h)
+constexpr size_t kKeyEntries = 500000;  // KeyMap::maxEntries = MaxKeys * nBuckets
+constexpr size_t kSurfBytes = 288;      // sizeof(SURF): bool, float3, float4 (16-aligned), float[64]
+constexpr int kFileChunkBlocks = 4096;  // voxel blocks per host staging chunk
+
+struct FileCloser {
+    FILE* f;
+    ~FileCloser() {
+        if (f) std::fclose(f);
+    }
+};
+
+bool put(FILE* f, const void* p, size_t n) { return std::fwrite(p, 1, n, f) == n; }
+bool get(FILE* f, void* p, size_t n) { return std::fread(p, 1, n, f) == n; }
+
+bool put_fill(FILE* f, int32_t value, size_t count) {
+    std::vector<int32_t> buf(std::min(count, (size_t)1 << 18), value);
+    for (size_t done = 0; done < count;) {
+        const size_t k = std::min(buf.size(), count - done);
+        if (!put(f, buf.data(), k * 4)) return false;
+        done += k;
+    }
+    return true;
+}
+
+bool skip(FILE* f, size_t bytes) {
+    std::vector<char> buf(std::min(bytes, (size_t)1 << 22));
+    for (size_t done = 0; done < bytes;) {
+        const size_t k = std::min(buf.size(), bytes - done);
+        if (!get(f, buf.data(), k)) return false;
+        done += k;
+    }
+    return true;
+}
+
+RefEntry to_ref(const HEntry& e) {
+    RefEntry r{};
+    r.x = e.x;
+    r.y = e.y;
+    r.z = e.z;
+    r.ptr = e.ptr >= 0 ? e.ptr * 512 : -1;
+    r.offset = e.offset;
+    return r;
+}
+
+int file_error(const char* what) {
+    fb_set_error_text(what);
+    return FB_EINVAL;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fb_write_map_file(fb_session* s, const char* path) {
+    if (!s || !path) return FB_EINVAL;
+    const MapView& m = s->map;
+    const size_t NE_all = (size_t)m.NB + m.NE;
+    if ((size_t)m.NS * 512 > (size_t)INT32_MAX || NE_all > (size_t)INT32_MAX)
+        return file_error("fb_write_map_file: the map is too large for the file's int sizes");
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    MapCounters c;
+    FB_CUDA(cudaMemcpy(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost));
+    FileCloser fc{std::fopen(path, "wb")};
+    if (!fc.f) return file_error("fb_write_map_file: cannot open the file");
+    FILE* f = fc.f;
+    const int32_t head[4] = {m.NS, m.NB, m.NS * 512, (int32_t)NE_all};
+    const uint32_t nvis = (uint32_t)std::max(c.n_visible, 0);
+    bool ok = put(f, head, sizeof head) && put(f, &c.heap_counter, 4) && put(f, &c.entry_ptr, 4) && put(f, &nvis, 4);
+    std::vector<int32_t> heap(m.NS);
+    FB_CUDA(cudaMemcpy(heap.data(), m.heap, 4 * heap.size(), cudaMemcpyDeviceToHost));
+    ok = ok && put(f, heap.data(), 4 * heap.size()) && put_fill(f, -1, m.NB);   // locks: EntryAvailable
+    std::vector<Voxel> vox((size_t)kFileChunkBlocks * 512);
+    std::vector<uint8_t> cb(m.cvox ? (size_t)kFileChunkBlocks * kCBlockBytes : 0);
+    for (int b0 = 0; ok && b0 < m.NS; b0 += kFileChunkBlocks) {
+        const int nb = std::min(kFileChunkBlocks, m.NS - b0);
+        if (m.cvox) {
+            FB_CUDA(cudaMemcpy(cb.data(), m.cvox + (size_t)b0 * kCBlockBytes, (size_t)nb * kCBlockBytes,
+                               cudaMemcpyDeviceToHost));
+            for (int b = 0; b < nb; ++b) {
+                const uint8_t* blk = cb.data() + (size_t)b * kCBlockBytes;
+                for (int v = 0; v < 512; ++v) {
+                    uint16_t h;
+                    std::memcpy(&h, blk + 2 * v, 2);
+                    Voxel& o = vox[(size_t)b * 512 + v];
+                    o.sdf = half_bits_to_float(h);
+                    o.weight = blk[kCWeight + v];
+                    o.r = blk[kCRed + v];
+                    o.g = blk[kCGreen + v];
+                    o.b = blk[kCBlue + v];
+                }
+            }
+        } else {
+            FB_CUDA(cudaMemcpy(vox.data(), m.voxels + (size_t)b0 * 512, (size_t)nb * 512 * sizeof(Voxel),
+                               cudaMemcpyDeviceToHost));
+        }
+        ok = put(f, vox.data(), (size_t)nb * 512 * sizeof(Voxel));
+    }
+    std::vector<HEntry> ent(NE_all);
+    FB_CUDA(cudaMemcpy(ent.data(), m.entries, sizeof(HEntry) * NE_all, cudaMemcpyDeviceToHost));
+    std::vector<RefEntry> ref(NE_all);
+    for (size_t i = 0; i < NE_all; ++i) ref[i] = to_ref(ent[i]);
+    ok = ok && put(f, ref.data(), sizeof(RefEntry) * NE_all);
+    // the visible-entry list, the rest of its array zero
+    const size_t nv = std::min<size_t>(nvis, (size_t)m.NS);
+    std::vector<HEntry> vis(nv);
+    if (nv) FB_CUDA(cudaMemcpy(vis.data(), m.vis_blocks, sizeof(HEntry) * nv, cudaMemcpyDeviceToHost));
+    std::fill(ref.begin(), ref.end(), RefEntry{});
+    for (size_t i = 0; i < nv; ++i) ref[i] = to_ref(vis[i]);
+    ok = ok && put(f, ref.data(), sizeof(RefEntry) * NE_all);
+    ok = ok && put_fill(f, -1, kKeyLocks) && put_fill(f, 0, kKeyEntries * kSurfBytes / 4);
+    if (!ok || std::fflush(f) != 0) return file_error("fb_write_map_file: write failed");
+    return FB_OK;
+}
+
+int fb_read_map_file(fb_session* s, const char* path) {
+    if (!s || !path) return FB_EINVAL;
+    const MapView& m = s->map;
+    const size_t NE_all = (size_t)m.NB + m.NE;
+    FileCloser fc{std::fopen(path, "rb")};
+    if (!fc.f) return file_error("fb_read_map_file: cannot open the file");
+    FILE* f = fc.f;
+    int32_t head[4], hc, ep;
+    uint32_t nvis;
+    if (!get(f, head, sizeof head) || !get(f, &hc, 4) || !get(f, &ep, 4) || !get(f, &nvis, 4))
+        return file_error("fb_read_map_file: truncated header");
+    if (head[0] != m.NS || head[1] != m.NB || (int64_t)head[2] != (int64_t)m.NS * 512 || (size_t)head[3] != NE_all)
+        return file_error("fb_read_map_file: the file's map sizes differ from the session's");
+    std::vector<int32_t> heap(m.NS);
+    if (!get(f, heap.data(), 4 * heap.size()) || !skip(f, 4 * (size_t)m.NB))
+        return file_error("fb_read_map_file: truncated file");
+    for (int32_t v : heap)
+        if (v < -1 || v >= m.NS) return file_error("fb_read_map_file: free-block stack out of range");
+    // reset first: the per-frame scratch and anything not in the file
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    launch_map_reset(s->map, s->stream);
+    if (check_launch()) return FB_ECUDA;
+    FB_CUDA(cudaStreamSynchronize(s->stream));
+    FB_CUDA(cudaMemcpy(m.heap, heap.data(), 4 * heap.size(), cudaMemcpyHostToDevice));
+    std::vector<Voxel> vox((size_t)kFileChunkBlocks * 512);
+    std::vector<uint8_t> cb(m.cvox ? (size_t)kFileChunkBlocks * kCBlockBytes : 0);
+    for (int b0 = 0; b0 < m.NS; b0 += kFileChunkBlocks) {
+        const int nb = std::min(kFileChunkBlocks, m.NS - b0);
+        if (!get(f, vox.data(), (size_t)nb * 512 * sizeof(Voxel))) return file_error("fb_read_map_file: truncated voxels");
+        if (m.cvox) {
+            // precision form: TSDF rounded to FP16, weight and colour as stored
+            for (int b = 0; b < nb; ++b) {
+                uint8_t* blk = cb.data() + (size_t)b * kCBlockBytes;
+                for (int v = 0; v < 512; ++v) {
+                    const Voxel& x = vox[(size_t)b * 512 + v];
+                    const __half h = __float2half_rn(x.sdf);
+                    std::memcpy(blk + 2 * v, &h, 2);
+                    blk[kCWeight + v] = x.weight;
+                    blk[kCRed + v] = x.r;
+                    blk[kCGreen + v] = x.g;
+                    blk[kCBlue + v] = x.b;
+                }
+            }
+            FB_CUDA(cudaMemcpy(m.cvox + (size_t)b0 * kCBlockBytes, cb.data(), (size_t)nb * kCBlockBytes,
+                               cudaMemcpyHostToDevice));
+        } else {
+            FB_CUDA(cudaMemcpy(m.voxels + (size_t)b0 * 512, vox.data(), (size_t)nb * 512 * sizeof(Voxel),
+                               cudaMemcpyHostToDevice));
+        }
+    }
+    std::vector<RefEntry> ref(NE_all);
+    if (!get(f, ref.data(), sizeof(RefEntry) * NE_all)) return file_error("fb_read_map_file: truncated hash table");
+    std::vector<HEntry> ent(NE_all);
+    std::vector<std::pair<int, int>> alloc;   // (block, slot)
+    int holes = 0;
+    for (size_t i = 0; i < NE_all; ++i) {
+        const RefEntry& r = ref[i];
+        if (r.ptr != -1 && (r.ptr < 0 || r.ptr % 512 || r.ptr / 512 >= m.NS))
+            return file_error("fb_read_map_file: hash entry with a bad voxel pointer");
+        if (r.offset > m.NE) return file_error("fb_read_map_file: hash entry with a bad link");
+        HEntry& e = ent[i];
+        if (r.ptr >= 0) {
+            if (r.x < -32767 || r.x > 32767 || r.y < -32767 || r.y > 32767 || r.z < -32767 || r.z > 32767)
+                return file_error("fb_read_map_file: block coordinates beyond +-32767");
+            e.x = (short)r.x;
+            e.y = (short)r.y;
+            e.z = (short)r.z;
+            alloc.push_back({r.ptr / 512, (int)i});
+        } else {
+            const bool fits = r.x >= -32767 && r.x <= 32767 && r.y >= -32767 && r.y <= 32767 && r.z >= -32767 &&
+                              r.z <= 32767;
+            e.x = fits ? (short)r.x : 0;
+            e.y = fits ? (short)r.y : 0;
+            e.z = fits ? (short)r.z : 0;
+            // an empty slot a chain passes through -- a bucket head with a
+            // link or a used excess slot -- means the pool ran out once
+            const bool linked_head = i < (size_t)m.NB && r.offset > 0;
+            const bool used_excess = i >= (size_t)m.NB && i < (size_t)m.NB + (size_t)std::max(0, ep - 1);
+            if (linked_head || used_excess) holes = 1;
+        }
+        e.pad = 0;
+        e.ptr = r.ptr >= 0 ? r.ptr / 512 : -1;
+        e.offset = std::max(r.offset, 0);   // the reference ends a chain at any offset <= 0
+    }
+    if (alloc.size() > (size_t)m.NS) return file_error("fb_read_map_file: more allocated entries than blocks");
+    FB_CUDA(cudaMemcpy(m.entries, ent.data(), sizeof(HEntry) * NE_all, cudaMemcpyHostToDevice));
+    // the allocated list in block order (this library allocates blocks in
+    // list order, so its own maps come back in their original order)
+    std::sort(alloc.begin(), alloc.end());
+    std::vector<int> alloc_slots(alloc.size());
+    for (size_t i = 0; i < alloc.size(); ++i) alloc_slots[i] = alloc[i].second;
+    if (!alloc_slots.empty())
+        FB_CUDA(cudaMemcpy(m.alloc_list, alloc_slots.data(), 4 * alloc_slots.size(), cudaMemcpyHostToDevice));
+    // the visible list: the entries' slots found through the hash chains
+    if (nvis > NE_all) return file_error("fb_read_map_file: visible count out of range");
+    if (!get(f, ref.data(), sizeof(RefEntry) * NE_all)) return file_error("fb_read_map_file: truncated visible list");
+    std::vector<int> vis_slots;
+    std::vector<HEntry> vis_entries;
+    for (uint32_t i = 0; i < nvis && vis_slots.size() < (size_t)m.NS; ++i) {
+        const RefEntry& r = ref[i];
+        size_t b = bucket_of(r.x, r.y, r.z, (uint32_t)m.NB);
+        for (int guard = 0; guard <= m.NE; ++guard) {
+            const HEntry& e = ent[b];
+            if (e.ptr >= 0 && e.x == r.x && e.y == r.y && e.z == r.z) {
+                vis_slots.push_back((int)b);
+                vis_entries.push_back(e);
+                break;
+            }
+            if (e.offset <= 0) break;
+            b = (size_t)m.NB + e.offset - 1;
+        }
+    }
+    if (!vis_slots.empty()) {
+        FB_CUDA(cudaMemcpy(m.visible, vis_slots.data(), 4 * vis_slots.size(), cudaMemcpyHostToDevice));
+        FB_CUDA(cudaMemcpy(m.vis_blocks, vis_entries.data(), sizeof(HEntry) * vis_entries.size(),
+                           cudaMemcpyHostToDevice));
+    }
+    if (!skip(f, 4 * kKeyLocks + kKeyEntries * kSurfBytes)) return file_error("fb_read_map_file: truncated key map");
+    MapCounters c;
+    FB_CUDA(cudaMemcpy(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost));
+    c.heap_counter = hc;
+    c.entry_ptr = ep;
+    c.holes = holes;
+    c.n_alloc = (int)alloc_slots.size();
+    c.n_visible = (int)vis_slots.size();
+    c.err = 0;
+    FB_CUDA(cudaMemcpy(s->ctr, &c, sizeof c, cudaMemcpyHostToDevice));
+    // System::ReadMapFromDisk: the tracker restarts and the map is no longer fused
+    s->state = s->last_state = 1;
+    if (!s->mapping_disabled) drop_graphs(s);
+    s->mapping_disabled = true;
+    return FB_OK;
+}
+
+}  // extern "C"
+
 // ------------------------------------------------------------------ batches
 
 struct fb_batch {
@@ -1739,7 +2027,8 @@ int fb_batch_step(fb_batch* b, fb_session* const* ss, int n, const fb_frame_inpu
             const fb_session* s = ss[i];
             key.push_back((uint64_t)(uintptr_t)s);
             key.push_back((uint64_t)plans[i].mode | (uint64_t)plans[i].fuse << 2 | (uint64_t)s->next << 3 |
-                          (uint64_t)s->persistent << 4 | (uint64_t)s->shared_gpu << 5 | (uint64_t)s->rc_bx << 8 |
+                          (uint64_t)s->persistent << 4 | (uint64_t)s->shared_gpu << 5 |
+                          (uint64_t)s->mapping_disabled << 6 | (uint64_t)s->rc_bx << 8 |
                           (uint64_t)s->rc_by << 20);
         }
         auto it = b->cache.find(key);

@@ -146,6 +146,19 @@ class Session:
         check("fb_save_mesh", self.lib.fb_save_mesh(self.h, os.fsencode(path), ctypes.byref(n)))
         return n.value
 
+    def write_map_file(self, path):
+        """System::WriteMapToDisk: the map in the reference's dump layout."""
+        check("fb_write_map_file", self.lib.fb_write_map_file(self.h, os.fsencode(path)))
+
+    def read_map_file(self, path):
+        """System::ReadMapFromDisk: load a map in the reference's dump layout;
+        the tracker restarts and mapping is disabled (set_mapping)."""
+        check("fb_read_map_file", self.lib.fb_read_map_file(self.h, os.fsencode(path)))
+
+    def set_mapping(self, on):
+        """Fuse frames into the map (True) or only track against it."""
+        check("fb_session_set_mapping", self.lib.fb_session_set_mapping(self.h, 1 if on else 0))
+
     def prepare(self, shared=False):
         """Capture every frame graph now (for frames alone, or in batch steps
         with shared=True)."""

@@ -357,6 +357,28 @@ FB_API int fb_render_image(const fb_image* vmap, const fb_image* nmap, const flo
 FB_API int fb_depth_to_image(const fb_image* depth, fb_image* rgba, void* stream);
 FB_API int fb_rgb_to_rgba(const fb_image* rgb, fb_image* rgba, void* stream);
 
+/* Replaces: System::WriteMapToDisk (Core/System.cc:195-236, with
+ * Mapping::DownloadToRAM, Mapping/Mapping.cc:170-184): the map in the
+ * reference's dump layout -- int sizes {NumSdfBlocks, NumBuckets, NumVoxels,
+ * NumEntries}, heap counter, excess counter, visible count, free-block
+ * stack, bucket locks, voxels (8 B), hash entries and visible entries
+ * (32-byte HashEntry, ptr a voxel index), key-point locks and SURF entries
+ * (none kept here: unlocked and zero).  Either form (the precision form's
+ * TSDF is widened to float).  The reference reads a file whose sizes match
+ * its compile-time constants (fb_default_config's). */
+FB_API int fb_write_map_file(fb_session* s, const char* path);
+/* Replaces: System::ReadMapFromDisk (Core/System.cc:238-271, with
+ * Mapping::UploadFromRAM, Mapping.cc:186-200) for the map: loads a file in
+ * that layout whose sizes equal the session's, rebuilds this library's
+ * allocated list (in block order) and visible list, and, as the reference,
+ * restarts the tracker and disables mapping (fb_session_set_mapping).  The
+ * reference's CreateModel after loading is fb_mesh_scene, on demand. */
+FB_API int fb_read_map_file(fb_session* s, const char* path);
+/* Tracker::mappingDisabled (Tracking/Tracking.h) off (on = 1, the default)
+ * or on (on = 0): frames then track and raycast against the map, refreshing
+ * the visible blocks first, without fusing (System.cc:109-118). */
+FB_API int fb_session_set_mapping(fb_session* s, int on);
+
 /* Replaces: System::RenderTopDown (Core/System.cc:75-90): the model seen
  * from `dist` metres above the origin looking down (+y), the depth range
  * shifted by `dist`: visibility for a 640 x 480 camera (as the reference's

@@ -34,7 +34,9 @@
 #include "RenderScene.h"
 #include "../se3.hpp"
 
+#include <algorithm>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -569,6 +571,88 @@ int ref_download_zrange(void* h, float* zmin, float* zmax) {
     download2d(c->zRangeMax, zmax);
     return 0;
 }
+
+// System::WriteMapToDisk (Core/System.cc:195-236) with Mapping::DownloadToRAM
+// (Mapping.cc:170-184) over the harness's arrays.  The harness has no
+// key-point map: its section is written at the reference's sizes in the
+// reset state (locks -1, entries zero).
+int ref_write_map(void* h, const char* path) {
+    RefCtx* c = (RefCtx*)h;
+    const int NumSdfBlocks = DeviceMap::NumSdfBlocks, NumBuckets = DeviceMap::NumBuckets;
+    const int NumVoxels = DeviceMap::NumVoxels, NumEntries = DeviceMap::NumEntries;
+    int hc = 0, ep = 0;
+    uint nv = 0;
+    c->heapCounter.download(&hc, 1);
+    c->hashCounter.download(&ep, 1);
+    c->noVisibleEntries.download(&nv, 1);
+    std::vector<int> heap(NumSdfBlocks), mutex(NumBuckets);
+    c->heap.download(heap.data(), NumSdfBlocks);
+    c->bucketMutex.download(mutex.data(), NumBuckets);
+    std::vector<Voxel> vox(NumVoxels);
+    SafeCall(cudaMemcpy(vox.data(), (const Voxel*)c->sdfBlock.data + DeviceMap::BlockSize3,
+                        sizeof(Voxel) * (size_t)NumVoxels, cudaMemcpyDeviceToHost));
+    std::vector<HashEntry> ent(NumEntries), vis(NumEntries);
+    c->hashEntries.download(ent.data(), NumEntries);
+    c->visibleEntries.download(vis.data(), NumEntries);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return 1;
+    bool ok = std::fwrite(&NumSdfBlocks, 4, 1, f) == 1 && std::fwrite(&NumBuckets, 4, 1, f) == 1 &&
+              std::fwrite(&NumVoxels, 4, 1, f) == 1 && std::fwrite(&NumEntries, 4, 1, f) == 1;
+    ok = ok && std::fwrite(&hc, 4, 1, f) == 1 && std::fwrite(&ep, 4, 1, f) == 1 && std::fwrite(&nv, 4, 1, f) == 1;
+    ok = ok && std::fwrite(heap.data(), 4, heap.size(), f) == heap.size();
+    ok = ok && std::fwrite(mutex.data(), 4, mutex.size(), f) == mutex.size();
+    ok = ok && std::fwrite(vox.data(), sizeof(Voxel), vox.size(), f) == vox.size();
+    ok = ok && std::fwrite(ent.data(), sizeof(HashEntry), ent.size(), f) == ent.size();
+    ok = ok && std::fwrite(vis.data(), sizeof(HashEntry), vis.size(), f) == vis.size();
+    std::vector<int> keyMutex(KeyMap::MaxKeys, -1);
+    ok = ok && std::fwrite(keyMutex.data(), 4, keyMutex.size(), f) == keyMutex.size();
+    std::vector<SURF> keys(1024);
+    std::memset((void*)keys.data(), 0, sizeof(SURF) * keys.size());
+    for (int i = 0; ok && i < KeyMap::maxEntries; i += 1024) {
+        const size_t k = std::min(1024, KeyMap::maxEntries - i);
+        ok = std::fwrite(keys.data(), sizeof(SURF), k, f) == k;
+    }
+    ok = std::fclose(f) == 0 && ok;
+    return ok ? 0 : 1;
+}
+
+// System::ReadMapFromDisk (Core/System.cc:238-271) with Mapping::UploadFromRAM
+// (Mapping.cc:186-200): the dense map only (the key-point section is read
+// past); the reference then builds the mesh and disables mapping, which the
+// tests do themselves.
+int ref_read_map(void* h, const char* path) {
+    RefCtx* c = (RefCtx*)h;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return 1;
+    int head[4], hc = 0, ep = 0;
+    uint nv = 0;
+    bool ok = std::fread(head, 4, 4, f) == 4 && head[0] == (int)DeviceMap::NumSdfBlocks &&
+              head[1] == (int)DeviceMap::NumBuckets && head[2] == (int)DeviceMap::NumVoxels &&
+              head[3] == (int)DeviceMap::NumEntries;
+    ok = ok && std::fread(&hc, 4, 1, f) == 1 && std::fread(&ep, 4, 1, f) == 1 && std::fread(&nv, 4, 1, f) == 1;
+    std::vector<int> heap(DeviceMap::NumSdfBlocks), mutex(DeviceMap::NumBuckets);
+    std::vector<Voxel> vox(DeviceMap::NumVoxels);
+    std::vector<HashEntry> ent(DeviceMap::NumEntries), vis(DeviceMap::NumEntries);
+    ok = ok && std::fread(heap.data(), 4, heap.size(), f) == heap.size();
+    ok = ok && std::fread(mutex.data(), 4, mutex.size(), f) == mutex.size();
+    ok = ok && std::fread(vox.data(), sizeof(Voxel), vox.size(), f) == vox.size();
+    ok = ok && std::fread(ent.data(), sizeof(HashEntry), ent.size(), f) == ent.size();
+    ok = ok && std::fread(vis.data(), sizeof(HashEntry), vis.size(), f) == vis.size();
+    std::fclose(f);
+    if (!ok) return 1;
+    c->heapCounter.upload(&hc, 1);
+    c->hashCounter.upload(&ep, 1);
+    c->noVisibleEntries.upload(&nv, 1);
+    c->heap.upload(heap.data(), heap.size());
+    c->bucketMutex.upload(mutex.data(), mutex.size());
+    SafeCall(cudaMemcpy((Voxel*)c->sdfBlock.data + DeviceMap::BlockSize3, vox.data(),
+                        sizeof(Voxel) * vox.size(), cudaMemcpyHostToDevice));
+    c->hashEntries.upload(ent.data(), ent.size());
+    c->visibleEntries.upload(vis.data(), vis.size());
+    return 0;
+}
+
+int ref_sizeof_surf(void) { return (int)sizeof(SURF); }
 
 // The reference's marching-cubes tables (Mapping/Constant.h, included from
 // the reference tree): tri 256 x 16 edge indices (-1 filled), ntri =

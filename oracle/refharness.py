@@ -157,6 +157,20 @@ class RefHarness:
         fn(ctypes.c_void_p(self.h), _p(V), _p(N), _p(C), ctypes.c_uint32(n.value), ctypes.byref(n))
         return V, N, C
 
+    def write_map(self, path):
+        """System::WriteMapToDisk of the harness's map to `path`."""
+        fn = self.lib.ref_write_map
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        if fn(ctypes.c_void_p(self.h), os.fsencode(path)) != 0:
+            raise RuntimeError("ref_write_map failed")
+
+    def read_map(self, path):
+        """The map part of System::ReadMapFromDisk from `path`."""
+        fn = self.lib.ref_read_map
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        if fn(ctypes.c_void_p(self.h), os.fsencode(path)) != 0:
+            raise RuntimeError("ref_read_map failed")
+
     def zrange(self):
         zmin = np.zeros((60, 80), np.float32)
         zmax = np.zeros((60, 80), np.float32)
@@ -198,3 +212,7 @@ def mesh_tables():
     ntri = np.zeros(256, np.int32)
     lib.ref_mesh_tables(_p(tri), _p(ntri))
     return tri, ntri
+
+
+def sizeof_surf():
+    return int(ctypes.CDLL(LIB_PATH).ref_sizeof_surf())
