@@ -246,10 +246,46 @@ def reference_cuda(args, frames=80, warmup=5):
         tracked += int(h.grab(depth[i], rgb[i])[0])
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
+    mesh_ms, mesh_tris = h.mesh_time()
     h.close()
     return {"value": frames / dt, "unit": "frames/s", "frames": frames, "warmup": warmup,
             "tracked_frames": tracked, "config": REF_CONSTANTS,
-            "timing": "wall clock around each synchronous GrabImage, host frames in"}
+            "timing": "wall clock around each synchronous GrabImage, host frames in",
+            "mesh": {"what": "Mapping::CreateModel (MeshScene) on the map of these frames, buffers allocated once",
+                     "wall_ms": mesh_ms, "triangles": mesh_tris}}
+
+
+def mesh_timing(sess, reps=5):
+    """fb_mesh_scene on a session's current map: device time (CUDA events
+    on the stream the call is given) and wall time of the synchronous call,
+    output buffers allocated once."""
+    import ctypes
+    import torch
+    lib = sess.lib
+    n = ctypes.c_uint64()
+    lib.fb_mesh_scene(sess.h, None, None, None, 0, ctypes.byref(n), None)
+    T = n.value
+    V = torch.empty((max(3 * T, 1), 3), dtype=torch.float32, device="cuda")
+    N = torch.empty_like(V)
+    C = torch.empty((max(3 * T, 1), 3), dtype=torch.uint8, device="cuda")
+    st = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    dev, wall = [], []
+    for i in range(reps + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t = time.perf_counter()
+        e0.record(st)
+        lib.fb_mesh_scene(sess.h, V.data_ptr(), N.data_ptr(), C.data_ptr(), T, ctypes.byref(n), st.cuda_stream)
+        e1.record(st)
+        st.synchronize()
+        if i:
+            wall.append((time.perf_counter() - t) * 1e3)
+            dev.append(e0.elapsed_time(e1))
+    blocks = sess.stats()["no_allocated"]
+    d = float(np.median(dev))
+    return {"triangles": T, "allocated_blocks": int(blocks), "device_ms": d, "wall_ms": float(np.median(wall)),
+            "Mtriangles_per_s": T / (d * 1e-3) / 1e6 if d > 0 else 0.0,
+            "timing": "CUDA events around fb_mesh_scene (count, scan, emit) on its stream; median of 5"}
 
 
 def ours_at_reference_constants(depth, rgb, frames=80, warmup=5):
@@ -271,10 +307,12 @@ def ours_at_reference_constants(depth, rgb, frames=80, warmup=5):
     for i in range(warmup, warmup + frames):
         tracked += sess.grab(p_depth[i], p_rgb[i]).tracked
     dt = time.perf_counter() - t0
+    mesh = mesh_timing(sess)
     sess.close()
     return {"value": frames / dt, "unit": "frames/s", "frames": frames, "warmup": warmup,
             "tracked_frames": int(tracked), "config": REF_CONSTANTS,
-            "timing": "wall clock around each synchronous fb_grab_frame, pinned host frames in"}
+            "timing": "wall clock around each synchronous fb_grab_frame, pinned host frames in",
+            "mesh": mesh}
 
 
 def _batched_run(specs, seeds, warmup, steps, tune=False):
@@ -512,6 +550,7 @@ def main():
         if r.fused:
             nvis.append(r.no_visible)
     stages = sess.stage_times()
+    mesh = mesh_timing(sess) if world == 1 else None
     sess.close()
     del d_depth, d_rgb
 
@@ -567,6 +606,7 @@ def main():
                      "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms},
         "cpu_baseline": cpu,
         "clocks": ck,
+        "mesh": mesh,
         "reference_constants": at_ref,
         "precision": precision,
         "batched": batched,

@@ -35,6 +35,7 @@
 #include "../se3.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -653,6 +654,33 @@ int ref_read_map(void* h, const char* path) {
 }
 
 int ref_sizeof_surf(void) { return (int)sizeof(SURF); }
+
+// Mapping::CreateModel timed: Mapping's buffers allocated once (as its
+// constructor does), then `iters` MeshScene calls (each synchronises the
+// device itself); *ms = mean wall milliseconds per call.
+int ref_mesh_time(void* h, int iters, double* ms, uint32_t* count) {
+    RefCtx* c = (RefCtx*)h;
+    DeviceArray<uint> nBlocks(1), noTriangles(1);
+    DeviceArray<int> edgeTable(256), vertexTable(256);
+    DeviceArray2D<int> triangleTable;
+    triangleTable.create(16, 256);
+    edgeTable.upload(edgeTableHost);
+    vertexTable.upload(vertexTableHost);
+    triangleTable.upload(triangleTableHost);
+    DeviceArray<float3> modelVertex(DeviceMap::MaxVertices), modelNormal(DeviceMap::MaxVertices);
+    DeviceArray<uchar3> modelColor(DeviceMap::MaxVertices);
+    DeviceArray<int3> blockPoses(DeviceMap::NumEntries);
+    uint n = MeshScene(nBlocks, noTriangles, c->devmap(), edgeTable, vertexTable, triangleTable, modelNormal,
+                       modelVertex, modelColor, blockPoses);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int i = 0; i < iters; ++i)
+        n = MeshScene(nBlocks, noTriangles, c->devmap(), edgeTable, vertexTable, triangleTable, modelNormal,
+                      modelVertex, modelColor, blockPoses);
+    const auto t1 = std::chrono::steady_clock::now();
+    *ms = std::chrono::duration<double, std::milli>(t1 - t0).count() / (iters > 0 ? iters : 1);
+    *count = n;
+    return 0;
+}
 
 // The reference's marching-cubes tables (Mapping/Constant.h, included from
 // the reference tree): tri 256 x 16 edge indices (-1 filled), ntri =

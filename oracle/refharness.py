@@ -171,6 +171,16 @@ class RefHarness:
         if fn(ctypes.c_void_p(self.h), os.fsencode(path)) != 0:
             raise RuntimeError("ref_read_map failed")
 
+    def mesh_time(self, iters=5):
+        """Mean wall ms of the reference's MeshScene on the current map (its
+        buffers allocated once) and its triangle count."""
+        ms = ctypes.c_double()
+        n = ctypes.c_uint32()
+        fn = self.lib.ref_mesh_time
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        fn(ctypes.c_void_p(self.h), iters, ctypes.byref(ms), ctypes.byref(n))
+        return ms.value, n.value
+
     def zrange(self):
         zmin = np.zeros((60, 80), np.float32)
         zmax = np.zeros((60, 80), np.float32)
