@@ -52,6 +52,11 @@ class MapStats(ctypes.Structure):
     ]
 
 
+class KeypointStats(ctypes.Structure):
+    _fields_ = [("keys", ctypes.c_uint32), ("matches", ctypes.c_uint32), ("bootstrap", ctypes.c_int32),
+                ("relocalised", ctypes.c_int32), ("keyframes", ctypes.c_uint32), ("map_keys", ctypes.c_uint32)]
+
+
 class Image(ctypes.Structure):
     _fields_ = [("data", ctypes.c_void_p), ("pitch", ctypes.c_size_t), ("cols", ctypes.c_int),
                 ("rows", ctypes.c_int)]
@@ -87,6 +92,12 @@ SIGNATURES = {
     "fb_render_image": (_i, [ctypes.POINTER(Image), ctypes.POINTER(Image), _vp, ctypes.POINTER(Image), _vp]),
     "fb_depth_to_image": (_i, [ctypes.POINTER(Image), ctypes.POINTER(Image), _vp]),
     "fb_rgb_to_rgba": (_i, [ctypes.POINTER(Image), ctypes.POINTER(Image), _vp]),
+    "fb_session_set_keypoints": (_i, [_vp, _i]),
+    "fb_session_keypoint_stats": (_i, [_vp, ctypes.POINTER(KeypointStats)]),
+    "fb_download_keypoints": (_i, [_vp, _i, _vp, _vp, _vp, _vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
+    "fb_match_descriptors": (_i, [_vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp, _vp, _vp]),
+    "fb_pose_estimate": (_i, [_vp, _vp, ctypes.c_uint32, _i, _i, ctypes.c_uint64, _vp, _vp,
+                              ctypes.POINTER(ctypes.c_int)]),
     "fb_write_map_file": (_i, [_vp, ctypes.c_char_p]),
     "fb_read_map_file": (_i, [_vp, ctypes.c_char_p]),
     "fb_session_set_mapping": (_i, [_vp, _i]),

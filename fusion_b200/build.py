@@ -20,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
-CU_SOURCES = ["preprocess.cu", "track.cu", "map.cu", "raycast.cu", "session.cu", "shade.cu", "static_scratch.cu", "mesh.cu"]
+CU_SOURCES = ["preprocess.cu", "track.cu", "map.cu", "raycast.cu", "session.cu", "shade.cu", "static_scratch.cu", "mesh.cu", "keypoints.cu"]
 EXTRA_FLAGS = {"track.cu": ["-fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = os.path.join(HERE, "libfusion_b200.so")

@@ -193,6 +193,51 @@ int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const in
 int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,
                     const DevPose* pose, const int* skip, cudaStream_t s, int bx = 16, int by = 8);
 
+// ----------------------------------------------------------------- key points
+
+constexpr int kSurfOctaves = 4;      // SURF_CUDA defaults: 4 octaves ...
+constexpr int kSurfLayers = 4;       // ... of nOctaveLayers + 2 = 4 filter sizes
+constexpr int kSurfMaxCand = 16384;  // candidates ranked per detection
+constexpr int kKeyDesc = 64;         // descriptor values
+
+// Device scratch of one detection on a W x H image.
+struct KeyScratch {
+    int W, H, max_keys;              // max_keys: 1 % of the pixels (SURF_CUDA keypointsRatio)
+    uint32_t* integral;              // (W + 1) x (H + 1)
+    float* det[kSurfOctaves];        // [layer][H >> o][W >> o]
+    int ow[kSurfOctaves], oh[kSurfOctaves];
+    float4* cand;                    // kSurfMaxCand: x, y, scale, response
+    unsigned long long* keys;        // kSurfMaxCand sort keys
+    int* slotmap;                    // sample index -> candidate slot
+    int* counter;
+    float4* kp;                      // max_keys selected: x, y, scale, angle
+    float* desc;                     // max_keys x kKeyDesc
+};
+
+// The key points of a frame that have a 3-D point (Frame::ExtractKeyPoints).
+struct KeySet {
+    float4* kp;     // x, y, scale, angle
+    float4* pt;     // camera-space point, w = 1
+    float4* nrm;    // normal (level-0 normal map, interpolated)
+    float* desc;    // kKeyDesc per key
+    int cap;
+};
+
+size_t key_scratch_bytes(int W, int H);
+int key_scratch_carve(void* base, size_t bytes, int W, int H, KeyScratch& ks);
+// detection and description on the level-0 gray image; *n_keys = key points
+// described into ks.kp / ks.desc (synchronises st)
+int launch_surf(const uint8_t* gray, int gp, float threshold, const KeyScratch& ks, int* n_keys, cudaStream_t st);
+// the key points with a depth and a normal -> out (count in *d_n, device)
+int launch_backproject(const KeyScratch& ks, int n, const float* depth, int dp, const float4* nmap, int np,
+                       const Intr& k, float cutoff, const KeySet& out, int* d_n, cudaStream_t st);
+// two nearest train descriptors per query: idx {best, second}, dist {d1, d2}
+int launch_match2(const float* q, int nq, const float* t, int nt, int2* idx, float2* dist, cudaStream_t st);
+// Solver::PoseEstimate: T (4x4, row-major) maps ref points onto src points;
+// outlier[i] = 0 for the final inliers.  Host.
+bool pose_estimate(const double* src, const double* ref, int n, int iterations, bool check_angle, uint64_t seed,
+                   double T[16], uint8_t* outlier);
+
 // Marching-cubes mesh of the map over its n_blocks allocated blocks: *total =
 // triangles found; the first min(total, cap) written to V / N (float3 per
 // vertex) and C (uchar3) when all three are given.  Synchronous on st.

@@ -146,6 +146,29 @@ class Session:
         check("fb_save_mesh", self.lib.fb_save_mesh(self.h, os.fsencode(path), ctypes.byref(n)))
         return n.value
 
+    def set_keypoints(self, on):
+        """Key points on every frame, the bootstrap from the last frame's key
+        points, keyframes, the key map and relocalisation (fb_session_set_keypoints)."""
+        check("fb_session_set_keypoints", self.lib.fb_session_set_keypoints(self.h, 1 if on else 0))
+
+    def keypoint_stats(self):
+        st = _lib.KeypointStats()
+        check("fb_session_keypoint_stats", self.lib.fb_session_keypoint_stats(self.h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in _lib.KeypointStats._fields_}
+
+    def keypoints(self, which=0):
+        """The key points of the last (0) or next (1) frame: kp [n, 4] (x, y,
+        scale, angle), pts [n, 4], nrm [n, 4], desc [n, 64]."""
+        n = ctypes.c_uint32()
+        check("fb_download_keypoints", self.lib.fb_download_keypoints(self.h, which, None, None, None, None, 0,
+                                                                      ctypes.byref(n)))
+        k = n.value
+        kp, pts, nrm = (np.zeros((k, 4), np.float32) for _ in range(3))
+        desc = np.zeros((k, 64), np.float32)
+        check("fb_download_keypoints", self.lib.fb_download_keypoints(self.h, which, _p(kp), _p(pts), _p(nrm),
+                                                                      _p(desc), k, ctypes.byref(n)))
+        return {"kp": kp, "pts": pts, "nrm": nrm, "desc": desc}
+
     def write_map_file(self, path):
         """System::WriteMapToDisk: the map in the reference's dump layout."""
         check("fb_write_map_file", self.lib.fb_write_map_file(self.h, os.fsencode(path)))
@@ -457,6 +480,34 @@ def top_down_pose(dist):
     by pi/2 about -x (cos(pi/2) kept as computed), camera at (0, -dist, 0)."""
     c = np.cos(np.pi / 2)
     return np.array([[1, 0, 0, 0], [0, c, 1, -float(np.float32(dist))], [0, -1, c, 0], [0, 0, 0, 1]], np.float64)
+
+
+def match_descriptors(query, train, stream=None):
+    """Two nearest train descriptors of every query (fb_match_descriptors);
+    CUDA float32 tensors [n, 64].  Returns (best int32 [nq, 2], dist [nq, 2])
+    as tensors on the device."""
+    import torch
+    nq, nt = int(query.shape[0]), int(train.shape[0])
+    best = torch.empty((nq, 2), dtype=torch.int32, device=query.device)
+    dist = torch.empty((nq, 2), dtype=torch.float32, device=query.device)
+    check("fb_match_descriptors", _lib.load().fb_match_descriptors(
+        query.data_ptr() if nq else None, nq, train.data_ptr() if nt else None, nt,
+        best.data_ptr() if nq else None, dist.data_ptr() if nq else None, _stream(stream)))
+    return best, dist
+
+
+def pose_estimate(src, ref, iterations=35, check_angle=True, seed=1):
+    """Solver::PoseEstimate (fb_pose_estimate) on host arrays [n, 3]:
+    (ok, T 4x4 mapping ref onto src, inlier mask)."""
+    src = np.ascontiguousarray(src, np.float64)
+    ref = np.ascontiguousarray(ref, np.float64)
+    n = len(src)
+    T = np.zeros((4, 4), np.float64)
+    inl = np.zeros(max(n, 1), np.uint8)
+    ok = ctypes.c_int()
+    check("fb_pose_estimate", _lib.load().fb_pose_estimate(_p(src), _p(ref), n, int(iterations), 1 if check_angle else 0,
+                                                           int(seed), _p(T), _p(inl), ctypes.byref(ok)))
+    return bool(ok.value), T, inl[:n].astype(bool)
 
 
 def mesh_case_table():

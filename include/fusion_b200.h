@@ -379,6 +379,50 @@ FB_API int fb_read_map_file(fb_session* s, const char* path);
  * the visible blocks first, without fusing (System.cc:109-118). */
 FB_API int fb_session_set_mapping(fb_session* s, int on);
 
+/* ------------------------------------------------------------ key points
+ * The reference's SURF path (OpenCV CUDA SURF, absent here; this library's
+ * own detector and descriptor follow the published SURF method): key points
+ * of every frame with a 3-D point (Frame::ExtractKeyPoints, Core/Frame.cc:
+ * 165-212), the bootstrap pose from matches with the last frame before ICP
+ * (Tracker::TrackLastFrame, Tracking/Tracking.cc:169-204), keyframes with
+ * observation counts (Tracking.cc:75-85, 113-148, 208-234), the key map they
+ * are fused into (Mapping::FuseKeyFrame, Mapping/Mapping.cc:220-275) and
+ * relocalisation against it when the camera is lost (Tracker::Relocalise,
+ * Tracking.cc:411-470).  Off by default (the rest of this library runs the
+ * reference's loop as it runs without key points); sessions with key points
+ * on are stepped by fb_grab_frame only (not in batches).  The RANSAC solver
+ * (Solver::PoseEstimate) draws its samples from a seeded sequence instead of
+ * the clock. */
+typedef struct fb_keypoint_stats {
+    uint32_t keys;          /* key points with a 3-D point in the last frame */
+    uint32_t matches;       /* ratio-test matches of its bootstrap or relocalisation */
+    int32_t bootstrap;      /* TrackLastFrame: 1 pose found, 0 not, -1 not run */
+    int32_t relocalised;    /* Relocalise: 1 pose found, 0 not, -1 not run */
+    uint32_t keyframes;     /* keyframes created */
+    uint32_t map_keys;      /* keys in the key map */
+} fb_keypoint_stats;
+FB_API int fb_session_set_keypoints(fb_session* s, int on);
+FB_API int fb_session_keypoint_stats(fb_session* s, fb_keypoint_stats* out);
+/* The key points of the last (which = 0) or next (1) frame, host arrays:
+ * kp {x, y, scale, angle}, pts {x, y, z, 1} camera space, nrm (float4),
+ * desc 64 floats each; any may be NULL.  *n = keys (at most capacity
+ * written). */
+FB_API int fb_download_keypoints(fb_session* s, int which, float* kp, float* pts, float* nrm, float* desc,
+                                 uint32_t capacity, uint32_t* n);
+/* Brute-force two-nearest-neighbour matching (cv::cuda BFMatcher knnMatch,
+ * L2, k = 2) of nq query descriptors against nt train descriptors (64
+ * floats each, device pointers): best (nq x 2 int: nearest, second nearest,
+ * -1 when missing) and dist (nq x 2 float, L2 distances), device pointers.
+ * Synchronous. */
+FB_API int fb_match_descriptors(const float* query, uint32_t nq, const float* train, uint32_t nt, int32_t* best,
+                                float* dist, void* stream);
+/* Replaces: Solver::PoseEstimate (Optimization/Solver.cc:6-186), host
+ * arrays: n matched points src / ref (3 doubles each); T (4x4 row-major)
+ * maps ref onto src; inlier[i] = 1 for the final inliers (may be NULL).
+ * Returns FB_OK with *ok = 1 when a pose was accepted.  Host only. */
+FB_API int fb_pose_estimate(const double* src, const double* ref, uint32_t n, int iterations, int check_angle,
+                            uint64_t seed, double T[16], uint8_t* inlier, int* ok);
+
 /* Replaces: System::RenderTopDown (Core/System.cc:75-90): the model seen
  * from `dist` metres above the origin looking down (+y), the depth range
  * shifted by `dist`: visibility for a 640 x 480 camera (as the reference's
