@@ -445,8 +445,6 @@ int reset_session(fb_session* s) {
     return FB_OK;
 }
 
-// The frame's kernels after the input has reached fr[next].  Returns the
-// number of kernels launched and which stages ran (bit k = stage k).
 // The tracker's starting pose of a frame (the key-point bootstrap's).
 struct Pose16 {
     double m[16];
@@ -464,6 +462,8 @@ __global__ void k_track_reloc(TrackState* st, Pose16 T) {
     st->failed = 0;
 }
 
+// The frame's kernels after the input has reached fr[next].  Returns the
+// number of kernels launched and which stages ran (bit k = stage k).
 // part 0: the whole frame; 1: ResizeImages + FillImages only; 2: the rest.
 // start: the tracker's starting pose when not the last pose.
 int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, unsigned* ran, int part = 0,
@@ -678,6 +678,8 @@ int capture_frame(fb_session* s, const FramePlan& p, cudaStream_t st) {
     s->stream = keep;
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaGraphInstantiate(&g, graph, 0);
+    // upload now, so that the frame that first launches it does not wait
+    if (e == cudaSuccess) e = cudaGraphUpload(g, st);
     if (graph) cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
         g = nullptr;
@@ -2399,6 +2401,13 @@ void clear_cache(fb_batch* b) {
     b->cache.clear();
 }
 
+// Slot streams of a batch: a fixed set, created with the batch.  Creating a
+// stream while frames run can take tens of milliseconds (the driver
+// serialises it with the device's work), so a step never creates one; beyond
+// kBatchSlots sessions, sessions share slots round-robin (their frames then
+// run one after the other on that slot, with the same results).
+constexpr int kBatchSlots = 32;
+
 int ensure_slots(fb_batch* b, int n) {
     while ((int)b->slots.size() < n) {
         cudaStream_t st = nullptr;
@@ -2414,17 +2423,19 @@ int ensure_slots(fb_batch* b, int n) {
     return FB_OK;
 }
 
-// The frames of a step, each on its own slot stream, forked from and joined
-// back into the origin stream.  With capture on, the same calls record one
-// graph.  direct: launch each session's cached frame graph (mode 0), else
-// issue its kernels (captured into the composite graph, mode 1).
+// The frames of a step on the slot streams (session i on slot i mod
+// kBatchSlots), forked from and joined back into the origin stream.  With
+// capture on, the same calls record one graph.  direct: launch each session's
+// cached frame graph (mode 0), else issue its kernels (captured into the
+// composite graph, mode 1).
 int issue_step(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plans, bool direct, int* kernels) {
     FB_CUDA(cudaEventRecord(b->fork, b->origin));
     *kernels = 0;
+    const int used = std::min(n, kBatchSlots);
+    for (int k = 0; k < used; ++k) FB_CUDA(cudaStreamWaitEvent(b->slots[k], b->fork, 0));
     for (int i = 0; i < n; ++i) {
         fb_session* s = ss[i];
-        cudaStream_t st = b->slots[i];
-        FB_CUDA(cudaStreamWaitEvent(st, b->fork, 0));
+        cudaStream_t st = b->slots[i % kBatchSlots];
         if (direct) {
             unsigned ran = 0;
             int rc = enqueue_frame(s, plans[i], st, &ran);
@@ -2437,8 +2448,10 @@ int issue_step(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plans
             s->stream = keep;
         }
         FB_CUDA(cudaMemcpyAsync(s->h_out, s->d_out, sizeof(FrameOut), cudaMemcpyDeviceToHost, st));
-        FB_CUDA(cudaEventRecord(b->done[i], st));
-        FB_CUDA(cudaStreamWaitEvent(b->origin, b->done[i], 0));
+    }
+    for (int k = 0; k < used; ++k) {
+        FB_CUDA(cudaEventRecord(b->done[k], b->slots[k]));
+        FB_CUDA(cudaStreamWaitEvent(b->origin, b->done[k], 0));
     }
     return check_launch();
 }
@@ -2462,6 +2475,10 @@ int fb_batch_create(void* stream, fb_batch** out) {
     if (!cuda_ok(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming))) {
         if (b->own_origin) cudaStreamDestroy(b->origin);
         delete b;
+        return FB_ECUDA;
+    }
+    if (ensure_slots(b, kBatchSlots) != FB_OK) {
+        fb_batch_destroy(b);
         return FB_ECUDA;
     }
     // sessions come and go beside running ones: keep the memory of destroyed
@@ -2524,8 +2541,7 @@ int fb_batch_step(fb_batch* b, fb_session* const* ss, int n, const fb_frame_inpu
         for (int j = 0; j < i; ++j)
             if (ss[j] == ss[i]) return FB_EINVAL;
     }
-    int rc = ensure_slots(b, n);
-    if (rc) return rc;
+    int rc = FB_OK;
     // inputs first (on the origin stream; the frames fork after them)
     for (int i = 0; i < n; ++i) {
         rc = copy_frame_in(ss[i], in[i].depth, in[i].depth_pitch, in[i].rgb, in[i].rgb_pitch, in[i].on_device,

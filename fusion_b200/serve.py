@@ -130,11 +130,17 @@ class Server:
     Clients present at the start are admitted before the clock starts."""
 
     def __init__(self, pool, budget_bytes=120e9, mode=0, max_batch=256):
+        import torch
         self.lib = _lib.load()
         self.pool = pool
         self.budget = float(budget_bytes)
         self.batch = Batch(mode=mode)
         self.max_batch = max_batch
+        # one stream for every session's own work (creation, graph capture):
+        # creating a stream per session while frames run can stall the loop
+        # for tens of milliseconds
+        self._stream = torch.cuda.Stream()
+        self.stream = self._stream.cuda_stream
 
     def close(self):
         self.batch.close()
@@ -152,6 +158,8 @@ class Server:
         waiting, active, preparing, to_open = [], {}, [], []
         reserved, peak = 0.0, 0.0
         lat, batch_sizes, wait_times = [], [], []
+        worst = {"step_ms": 0.0, "step_with_new_session_ms": 0.0, "create_ms": 0.0, "capture_ms": 0.0,
+                 "close_ms": 0.0}
         admitted = queued = 0
         events = []      # (time, kind 0 arrive / 1 leave, id)
 
@@ -169,7 +177,7 @@ class Server:
             if not waiting and reserved + need <= self.budget:
                 reserved += need
                 c.bytes = need
-                c.session = Session(mixed_config(c.width, c.height, c.voxel))
+                c.session = Session(mixed_config(c.width, c.height, c.voxel), stream=self.stream)
                 c.session.prepare(shared=True)
                 warm.append(c)
             else:
@@ -205,15 +213,21 @@ class Server:
 
         def admission_slice():
             """One session creation or one graph capture."""
+            t_s = time.perf_counter()
             if preparing:
                 c = preparing[0]
                 if c.session.prepare_some(1, shared=True) == 0:
                     preparing.pop(0)
                     activate(c, now())
+                key = "capture_ms"
             elif to_open:
                 c = to_open.pop(0)
-                c.session = Session(mixed_config(c.width, c.height, c.voxel))
+                c.session = Session(mixed_config(c.width, c.height, c.voxel), stream=self.stream)
                 preparing.append(c)
+                key = "create_ms"
+            else:
+                return
+            worst[key] = max(worst[key], (time.perf_counter() - t_s) * 1e3)
 
         for c in warm:
             activate(c, 0.0)
@@ -233,7 +247,9 @@ class Server:
                             queued += 1
                     elif cid in active:
                         del active[cid]
+                        t_c = time.perf_counter()
                         c.session.close()
+                        worst["close_ms"] = max(worst["close_ms"], (time.perf_counter() - t_c) * 1e3)
                         c.session = None
                         reserved -= c.bytes
                         admit_waiting()
@@ -252,8 +268,11 @@ class Server:
                     continue
                 ready = ready[:self.max_batch]
                 frames = [self.pool.frame(c.width, c.height, c.seq, c.sent) for c in ready]
+                t_s = now()
                 self.batch.step([c.session for c in ready], frames)
                 t_done = now()
+                key = "step_with_new_session_ms" if any(c.sent < 2 for c in ready) else "step_ms"
+                worst[key] = max(worst[key], (t_done - t_s) * 1e3)
                 for c in ready:
                     lat.append(t_done - c.pending.pop(0))
                     c.sent += 1
@@ -275,4 +294,5 @@ class Server:
             "still_queued_at_end": len(waiting),
             "mean_wait_s": float(np.mean(wait_times)) if wait_times else 0.0,
             "backlog_frames_at_end": backlog, "peak_reserved_bytes": peak, "budget_bytes": self.budget,
+            "worst_host_ms": worst,
         }
