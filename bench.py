@@ -255,6 +255,40 @@ def reference_cuda(args, frames=80, warmup=5):
                      "wall_ms": mesh_ms, "triangles": mesh_tris}}
 
 
+def keypoint_form(depth, rgb, frames=60, warmup=5):
+    """The plain configuration with key points on (detection, description and
+    matching on every frame, the bootstrap pose, keyframes): frames/s through
+    fb_grab_frame from pinned host frames, and how often the bootstrap found a
+    pose."""
+    import torch
+    from fusion_b200 import Session
+    from fusion_b200 import system as S
+    cfg = S.config_c2()
+    frames = max(1, min(frames, len(depth) - warmup))
+    p_depth = torch.from_numpy(depth[:warmup + frames]).pin_memory().numpy()
+    p_rgb = torch.from_numpy(rgb[:warmup + frames]).pin_memory().numpy()
+    sess = Session(cfg)
+    sess.set_keypoints(True)
+    for i in range(warmup):
+        sess.grab(p_depth[i], p_rgb[i])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    boot, keys = [], []
+    for i in range(warmup, warmup + frames):
+        sess.grab(p_depth[i], p_rgb[i])
+        st = sess.keypoint_stats()
+        boot.append(st["bootstrap"])
+        keys.append(st["keys"])
+    dt = time.perf_counter() - t0
+    st = sess.keypoint_stats()
+    sess.close()
+    return {"value": frames / dt, "unit": "frames/s", "frames": frames,
+            "bootstrap_found_fraction": float(np.mean([b == 1 for b in boot])),
+            "mean_keys_with_3d_point": float(np.mean(keys)), "keyframes": st["keyframes"], "map_keys": st["map_keys"],
+            "timing": "wall clock around each synchronous fb_grab_frame with key points on, pinned host frames in",
+            "workload": "plain full-size configuration (640x480, 5 mm) with key points"}
+
+
 def mesh_timing(sess, reps=5):
     """fb_mesh_scene on a session's current map: device time (CUDA events
     on the stream the call is given) and wall time of the synchronous call,
@@ -586,6 +620,7 @@ def main():
     # the batched and served forms on one GPU (rank 0 of a single-GPU run)
     one = world == 1
     at_ref = ours_at_reference_constants(depth, rgb) if one else None
+    keypoints = keypoint_form(depth, rgb) if one else None
     precision = precision_form(depth, rgb, W, min(K, 200), value, peak, peak_kind) if one else None
     batched = batched_forms(args, rank, value) if one and not args.no_batched else None
     served = served_form(args, rank, value) if one and not args.no_served else None
@@ -607,6 +642,7 @@ def main():
         "cpu_baseline": cpu,
         "clocks": ck,
         "mesh": mesh,
+        "keypoints": keypoints,
         "reference_constants": at_ref,
         "precision": precision,
         "batched": batched,
