@@ -289,6 +289,60 @@ def keypoint_form(depth, rgb, frames=60, warmup=5):
             "workload": "plain full-size configuration (640x480, 5 mm) with key points"}
 
 
+def widened_timing(sess, reps=5):
+    """The rows beside the per-frame path on a session's current map: the
+    top-down view (visibility, z ranges, raycast and shading from the
+    overhead pose), Phong shading of a 640x480 raycast alone, a snapshot and a
+    restore (device <-> host), and the reference's map file written and read
+    back (host file in a temporary directory).  Median milliseconds."""
+    import tempfile
+    import torch
+    from fusion_b200 import Session
+    from fusion_b200 import system as S
+    cfg = sess.cfg
+    W, H = cfg.width, cfg.height
+    vm = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+    nm = torch.empty_like(vm)
+    img = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
+    out = {}
+
+    def med(fn, n=reps):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(n):
+            t = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append((time.perf_counter() - t) * 1e3)
+        return float(np.median(ts))
+
+    out["top_down_ms"] = med(lambda: S.render_top_down(sess, 8.0, vm, nm, img))
+    light = np.zeros(3, np.float32)
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    S.render_image(vm, nm, light, img, st)
+    e0.record(st)
+    for _ in range(reps):
+        S.render_image(vm, nm, light, img, st)
+    e1.record(st)
+    torch.cuda.synchronize()
+    out["render_image_device_ms"] = e0.elapsed_time(e1) / reps
+    snap = sess.snapshot()
+    out["snapshot_bytes"] = int(snap.nbytes)
+    out["snapshot_ms"] = med(lambda: sess.snapshot())
+    other = Session(cfg)
+    out["restore_ms"] = med(lambda: other.restore(snap))
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "map.bin")
+        out["map_file_write_ms"] = med(lambda: sess.write_map_file(path), 2)
+        out["map_file_bytes"] = os.path.getsize(path)
+        out["map_file_read_ms"] = med(lambda: other.read_map_file(path), 2)
+    other.close()
+    out["timing"] = "wall clock around each synchronous call, median of %d (map files: of 2)" % reps
+    return out
+
+
 def mesh_timing(sess, reps=5):
     """fb_mesh_scene on a session's current map: device time (CUDA events
     on the stream the call is given) and wall time of the synchronous call,
@@ -382,7 +436,7 @@ def _batched_run(specs, seeds, warmup, steps, tune=False):
         b.step(sess, frames(), on_device=True)
     tiles = None
     if tune:
-        tiles, _ = autotune_raycast_tiles(b, sess, frames, candidates=((16, 8), (8, 8), (32, 4), (16, 4)),
+        tiles, _ = autotune_raycast_tiles(b, sess, frames, candidates=((0, 0), (16, 8), (8, 8), (32, 4), (16, 4)),
                                           steps_per=1, on_device=True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -585,6 +639,7 @@ def main():
             nvis.append(r.no_visible)
     stages = sess.stage_times()
     mesh = mesh_timing(sess) if world == 1 else None
+    widened = widened_timing(sess) if world == 1 else None
     sess.close()
     del d_depth, d_rgb
 
@@ -643,6 +698,7 @@ def main():
         "clocks": ck,
         "mesh": mesh,
         "keypoints": keypoints,
+        "widened": widened,
         "reference_constants": at_ref,
         "precision": precision,
         "batched": batched,

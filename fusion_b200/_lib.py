@@ -77,6 +77,7 @@ SIGNATURES = {
     "fb_status_string": (ctypes.c_char_p, [_i]),
     "fb_last_error": (ctypes.c_char_p, []),
     "fb_session_bytes": (_sz, [ctypes.POINTER(Config)]),
+    "fb_graph_exec_stats": (None, [ctypes.POINTER(ctypes.c_longlong)] * 3),
     "fb_session_create": (_i, [ctypes.POINTER(Config), _vp, ctypes.POINTER(_vp)]),
     "fb_session_destroy": (_i, [_vp]),
     "fb_session_reset": (_i, [_vp]),

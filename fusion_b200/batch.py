@@ -24,7 +24,7 @@ from ._lib import FrameInput, FrameResult, check
 from .system import make_config
 
 RESOLUTIONS = ((160, 120), (320, 240), (640, 480))
-TILE_CANDIDATES = ((16, 8), (8, 8), (32, 4), (8, 16), (16, 4), (32, 2))
+TILE_CANDIDATES = ((0, 0), (16, 8), (8, 8), (32, 4), (8, 16), (16, 4), (32, 2))
 
 
 def _next_pow2(v):

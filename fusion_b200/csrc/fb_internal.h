@@ -129,7 +129,7 @@ struct MapCounters {
     // snapshot taken before insertion (read by the insert kernel only)
     int snap_M, snap_hc, snap_ep, snap_na;
     int fast;              // the parallel insertion path applies
-    int pad;
+    unsigned int ray_next; // work counter of the pooled raycast (zeroed with the z ranges)
 };
 
 struct NewBlock {
@@ -189,7 +189,8 @@ int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPo
 int launch_integrate(const MapView& m, const float* raw, int rp, const uint8_t* rgb, int cp, const float4* nmap,
                       int np, int W, int H, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s);
 int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s);
-// tile bx x by threads: bx * by <= 128 (the kernel's launch bound), a multiple of 32
+// tile bx x by threads: bx * by <= 128 (the kernel's launch bound), a multiple
+// of 32; bx = by = 0: the pooled raycast (lane refill)
 int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,
                     const DevPose* pose, const int* skip, cudaStream_t s, int bx = 16, int by = 8);
 

@@ -11,6 +11,7 @@
 // frame result, and the host then advances the reference's tracking state
 // machine (Tracking/Tracking.cc:58-112) and swaps the frames.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -353,13 +354,11 @@ void free_keys(fb_session* s) {
     s->keys = nullptr;
 }
 
+void drop_graphs(fb_session* s);
+
 void free_session(fb_session* s) {
     free_keys(s);
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 2; ++b)
-            for (int c = 0; c < 2; ++c)
-                for (int d = 0; d < 2; ++d)
-                    if (s->graph[a][b][c][d]) cudaGraphExecDestroy(s->graph[a][b][c][d]);
+    drop_graphs(s);
     for (int i = 0; i <= kStages; ++i)
         if (s->ev[i]) cudaEventDestroy(s->ev[i]);
     if (s->arena) cudaFreeAsync(s->arena, s->stream);
@@ -615,6 +614,43 @@ Intr intr_from(const float K[4]) {
 
 namespace {
 
+// Frame-graph executables of closed sessions (and of dropped graphs) are
+// kept for reuse: a later graph of the same shape is written into one with
+// cudaGraphExecUpdate instead of being instantiated.  Instantiating while
+// other sessions' frames run stalled the calling thread for up to 80 ms on
+// B200 once a thousand executables had been made; an update only rewrites
+// node parameters.  An update that the driver refuses falls back to
+// instantiation.
+using ExecKey = std::tuple<int, int, int, int, int, int, int, int, int, int, int>;
+std::mutex g_exec_lock;
+std::multimap<ExecKey, cudaGraphExec_t> g_exec_pool;
+constexpr size_t kExecPoolMax = 4096;
+std::atomic<long long> g_exec_updated{0}, g_exec_instantiated{0};
+
+ExecKey exec_key(const fb_session* s, int mode, int fuse, int shared) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return ExecKey(dev, s->W[0], s->H[0], s->cfg.form, mode, fuse, shared, s->persistent ? 1 : 0, s->rc_bx, s->rc_by,
+                   s->mapping_disabled ? 1 : 0);
+}
+
+void release_exec(const fb_session* s, int mode, int fuse, int shared, cudaGraphExec_t g) {
+    std::lock_guard<std::mutex> guard(g_exec_lock);
+    if (g_exec_pool.size() < kExecPoolMax)
+        g_exec_pool.emplace(exec_key(s, mode, fuse, shared), g);
+    else
+        cudaGraphExecDestroy(g);
+}
+
+cudaGraphExec_t take_exec(const ExecKey& key) {
+    std::lock_guard<std::mutex> guard(g_exec_lock);
+    auto it = g_exec_pool.find(key);
+    if (it == g_exec_pool.end()) return nullptr;
+    cudaGraphExec_t g = it->second;
+    g_exec_pool.erase(it);
+    return g;
+}
+
 // Cached frame graphs are released (rebuilt on next use).
 void drop_graphs(fb_session* s) {
     for (int a = 0; a < 3; ++a)
@@ -622,7 +658,7 @@ void drop_graphs(fb_session* s) {
             for (int c = 0; c < 2; ++c)
                 for (int d = 0; d < 2; ++d)
                     if (s->graph[a][b][c][d]) {
-                        cudaGraphExecDestroy(s->graph[a][b][c][d]);
+                        release_exec(s, a, b, d, s->graph[a][b][c][d]);
                         s->graph[a][b][c][d] = nullptr;
                     }
 }
@@ -677,7 +713,23 @@ int capture_frame(fb_session* s, const FramePlan& p, cudaStream_t st) {
     }
     s->stream = keep;
     if (e == cudaSuccess) e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&g, graph, 0);
+    if (e == cudaSuccess) {
+        cudaGraphExec_t r = take_exec(exec_key(s, p.mode, p.fuse ? 1 : 0, sh));
+        if (r) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(r, graph, &info) == cudaSuccess) {
+                g = r;
+                g_exec_updated.fetch_add(1);
+            } else {
+                cudaGetLastError();
+                cudaGraphExecDestroy(r);
+            }
+        }
+        if (!g) {
+            e = cudaGraphInstantiate(&g, graph, 0);
+            g_exec_instantiated.fetch_add(1);
+        }
+    }
     // upload now, so that the frame that first launches it does not wait
     if (e == cudaSuccess) e = cudaGraphUpload(g, st);
     if (graph) cudaGraphDestroy(graph);
@@ -1177,6 +1229,15 @@ const char* fb_status_string(int st) {
 
 const char* fb_last_error(void) { return g_last_error; }
 
+void fb_graph_exec_stats(long long* pooled, long long* updated, long long* instantiated) {
+    {
+        std::lock_guard<std::mutex> guard(g_exec_lock);
+        if (pooled) *pooled = (long long)g_exec_pool.size();
+    }
+    if (updated) *updated = g_exec_updated.load();
+    if (instantiated) *instantiated = g_exec_instantiated.load();
+}
+
 size_t fb_session_bytes(const fb_config* c) {
     if (!valid_config(c)) return 0;
     // the sizing pass of fb_session_create
@@ -1334,7 +1395,8 @@ int fb_session_prepare_some(fb_session* s, int shared, int max_graphs, int* rema
 int fb_session_prepare(fb_session* s, int shared) { return fb_session_prepare_some(s, shared, 1 << 30, nullptr); }
 
 int fb_session_set_raycast_tile(fb_session* s, int bx, int by) {
-    if (!s || bx < 1 || by < 1 || bx * by > 128 || (bx * by) % 32 != 0) return FB_EINVAL;
+    const bool pooled = bx == 0 && by == 0;
+    if (!s || (!pooled && (bx < 1 || by < 1 || bx * by > 128 || (bx * by) % 32 != 0))) return FB_EINVAL;
     if (bx == s->rc_bx && by == s->rc_by) return FB_OK;
     drop_graphs(s);
     s->rc_bx = bx;

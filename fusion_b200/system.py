@@ -482,6 +482,14 @@ def top_down_pose(dist):
     return np.array([[1, 0, 0, 0], [0, c, 1, -float(np.float32(dist))], [0, -1, c, 0], [0, 0, 0, 1]], np.float64)
 
 
+def graph_exec_stats():
+    """Frame-graph executables kept for reuse, and the captures served by an
+    update of a kept one and by a new instantiation (fb_graph_exec_stats)."""
+    v = [ctypes.c_longlong() for _ in range(3)]
+    _lib.load().fb_graph_exec_stats(*[ctypes.byref(x) for x in v])
+    return {"pooled": v[0].value, "updated": v[1].value, "instantiated": v[2].value}
+
+
 def match_descriptors(query, train, stream=None):
     """Two nearest train descriptors of every query (fb_match_descriptors);
     CUDA float32 tensors [n, 64].  Returns (best int32 [nq, 2], dist [nq, 2])

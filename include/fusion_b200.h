@@ -109,6 +109,12 @@ FB_API const char* fb_status_string(int status);
 FB_API const char* fb_last_error(void);
 /* Device bytes a session with this configuration allocates. */
 FB_API size_t fb_session_bytes(const fb_config* cfg);
+/* Frame-graph executables: those kept for reuse by later sessions (the
+ * executables of closed sessions, rewritten with cudaGraphExecUpdate when a
+ * session of the same image size, form and options captures its frame
+ * graphs), and the counts of captures served by an update and by a new
+ * instantiation since the library was loaded.  Any pointer may be NULL. */
+FB_API void fb_graph_exec_stats(long long* pooled, long long* updated, long long* instantiated);
 
 /* Replaces: System::System (Core/System.cc:16-73) -- Mapping::Create,
  * Tracker::Tracker, Frame::Create. stream: cudaStream_t or NULL (a stream is
@@ -157,11 +163,14 @@ FB_API int fb_session_prepare(fb_session* s, int shared);
  * instantiation takes driver locks that other threads' launches and copies
  * wait for). */
 FB_API int fb_session_prepare_some(fb_session* s, int shared, int max_graphs, int* remaining);
-/* Raycast tile (CUDA block shape, bx * by threads, bx * by <= 1024 and a
- * multiple of 32) of this session's model raycast; default 16 x 8.  Results
- * do not depend on it (every pixel is traced alone).  Cached frame graphs are
- * rebuilt on the next frame.  No reference counterpart: a tuning knob for the
- * batched form's autotuner. */
+/* The model raycast's launch shape for this session: one thread per pixel
+ * in CUDA blocks of bx x by threads (bx * by <= 128 and a multiple of 32;
+ * default 16 x 8), or with bx = by = 0 the pooled raycast, whose warps take
+ * 8 x 4 pixel tiles from a work counter and refill every lane whose ray has
+ * ended (it pays off on small images only).  Results do not depend on it
+ * (every pixel is traced alone, by the same operations).  Cached frame
+ * graphs are rebuilt on the next frame.  No reference counterpart: a tuning
+ * knob for the batched form's autotuner. */
 FB_API int fb_session_set_raycast_tile(fb_session* s, int bx, int by);
 
 /* Snapshots (System::WriteMapToDisk / ReadMapFromDisk, Core/System.cc:195-271,

@@ -112,7 +112,7 @@ def test_each_session_in_the_batch_equals_it_alone(frames, mode, schedule):
 
 def test_raycast_tile_does_not_change_results(frames):
     base, _ = _batched(frames, LOCKSTEP, 0)
-    tiled, _ = _batched(frames, LOCKSTEP, 0, tiles=[(8, 8), (32, 4), (16, 4)])
+    tiled, _ = _batched(frames, LOCKSTEP, 0, tiles=[(0, 0), (32, 4), (8, 8)])
     assert tiled == base
 
 
@@ -124,3 +124,40 @@ def test_batch_rejects_a_session_twice(frames):
         with pytest.raises(FusionError):
             b.step([s, s], [(d[0], c[0]), (d[1], c[1])])
     s.close()
+
+
+def test_recycled_frame_graphs_give_the_same_results():
+    """A session whose frame graphs are rewritten from a closed session's
+    executables (cudaGraphExecUpdate) gives the results of one whose graphs
+    were instantiated.  A raycast tile no other test uses keeps these
+    sessions' executables apart from the rest of the pool."""
+    from fusion_b200 import Session, mixed_config
+    from fusion_b200.batch import set_raycast_tile
+    from fusion_b200.system import graph_exec_stats
+    w, h, v, seed = SPECS[1]
+    d, c = _frames(w, h, seed, N_FRAMES)
+    d2, c2 = _frames(w, h, seed + 100, N_FRAMES)
+
+    def run(voxel, dd, cc, close):
+        s = Session(mixed_config(w, h, voxel))
+        set_raycast_tile(s, 32, 2)
+        rows = [_row(s.grab(dd[k], cc[k])) for k in range(N_FRAMES)]
+        dig = _map_digest(s)
+        if close:
+            s.close()
+        return s, rows, dig
+
+    st0 = graph_exec_stats()
+    a, rows_a, dig_a = run(v, d, c, close=False)
+    st1 = graph_exec_stats()
+    assert st1["instantiated"] > st0["instantiated"] and st1["updated"] == st0["updated"]
+    run(0.011, d2, c2, close=True)      # its executables go back to the pool
+    st2 = graph_exec_stats()
+    _, rows_c, dig_c = run(v, d, c, close=True)
+    st3 = graph_exec_stats()
+    a.close()
+    print("graph executables:", st0, st1, st2, st3)
+    assert st3["updated"] > st2["updated"]
+    assert st3["instantiated"] == st2["instantiated"]
+    assert rows_c == rows_a
+    assert dig_c == dig_a
