@@ -94,6 +94,7 @@ class Client:
         self.next_arrival = None
         self.sent = 0           # frames taken from the sequence so far
         self.bytes = 0
+        self.load = 0.0         # GPU milliseconds per second while admitted
 
 
 def make_clients(n, seed, rate=30.0, median_life=20.0, life_sigma=0.5, horizon=0.0):
@@ -118,6 +119,48 @@ def make_clients(n, seed, rate=30.0, median_life=20.0, life_sigma=0.5, horizon=0
     return out
 
 
+class Admission:
+    """Admission control.  A client is admitted when its session's device
+    memory (`need(c)` bytes) fits in the HBM budget beside the resident
+    sessions and -- when per-frame GPU costs are known -- when its expected
+    GPU time per second of wall time (frame rate x the per-frame cost of its
+    resolution) fits beside theirs under `load_max` of the GPU.  The compute
+    test keeps the admitted load below saturation, so that admitted clients
+    keep their latency when more clients arrive than one GPU can serve; the
+    rest wait in FIFO order (head-of-line: a later, smaller client does not
+    pass the head)."""
+
+    def __init__(self, budget_bytes, need, frame_cost_ms=None, load_max=0.85):
+        self.budget = float(budget_bytes)
+        self.need = need
+        self.cost = dict(frame_cost_ms) if frame_cost_ms else None
+        self.load_max = float(load_max)
+        self.reserved = 0.0
+        self.load = 0.0          # admitted GPU milliseconds per second
+        self.peak = 0.0
+        self.peak_load = 0.0
+
+    def gpu_ms_per_s(self, c):
+        return c.rate * self.cost[(c.width, c.height)] if self.cost else 0.0
+
+    def fits(self, c):
+        if self.reserved + self.need(c) > self.budget:
+            return False
+        return self.cost is None or self.load + self.gpu_ms_per_s(c) <= self.load_max * 1000.0
+
+    def take(self, c):
+        c.bytes = self.need(c)
+        c.load = self.gpu_ms_per_s(c)
+        self.reserved += c.bytes
+        self.load += c.load
+        self.peak = max(self.peak, self.reserved)
+        self.peak_load = max(self.peak_load, self.load)
+
+    def release(self, c):
+        self.reserved -= c.bytes
+        self.load -= c.load
+
+
 class Server:
     """The request loop.  Admission work -- creating a session (one
     stream-ordered allocation from memory reserved up front, map reset) and
@@ -129,13 +172,15 @@ class Server:
     becomes active, and its frames start arriving, once its session is ready.
     Clients present at the start are admitted before the clock starts."""
 
-    def __init__(self, pool, budget_bytes=120e9, mode=0, max_batch=256):
+    def __init__(self, pool, budget_bytes=120e9, mode=0, max_batch=256, frame_cost_ms=None, load_max=0.85):
         import torch
         self.lib = _lib.load()
         self.pool = pool
         self.budget = float(budget_bytes)
         self.batch = Batch(mode=mode)
         self.max_batch = max_batch
+        self.frame_cost_ms = dict(frame_cost_ms) if frame_cost_ms else None
+        self.load_max = float(load_max)
         # one stream for every session's own work (creation, graph capture):
         # creating a stream per session while frames run can stall the loop
         # for tens of milliseconds
@@ -148,6 +193,28 @@ class Server:
     def _need(self, c):
         return float(self.lib.fb_session_bytes(mixed_config(c.width, c.height, c.voxel)))
 
+    def calibrate(self, resolutions=RESOLUTIONS, sessions=8, voxel=0.012, steps=6, warmup=3):
+        """Per-frame GPU cost of each resolution, for compute admission: the
+        wall time of batch steps of `sessions` sessions of that resolution
+        (frames copied from the pool's pinned host memory, as in serving)
+        divided by the frames fused.  Sets and returns {(w, h): ms}."""
+        from .system import Session
+        cost = {}
+        for (w, h) in resolutions:
+            group = [Session(mixed_config(w, h, voxel), stream=self.stream) for _ in range(sessions)]
+            for g in group:
+                g.prepare(shared=True)
+            for i in range(warmup + steps):
+                if i == warmup:
+                    t = time.perf_counter()
+                frames = [self.pool.frame(w, h, k % self.pool.n_seq, i) for k in range(sessions)]
+                self.batch.step(group, frames)
+            cost[(w, h)] = (time.perf_counter() - t) * 1e3 / (steps * sessions)
+            for g in group:
+                g.close()
+        self.frame_cost_ms = cost
+        return cost
+
     def run(self, clients, duration):
         """Serve `clients` for `duration` seconds of wall time.  Returns the
         statistics of the run."""
@@ -156,7 +223,7 @@ class Server:
             c.seq = k % self.pool.n_seq
         by_id = {c.cid: c for c in clients}
         waiting, active, preparing, to_open = [], {}, [], []
-        reserved, peak = 0.0, 0.0
+        adm = Admission(self.budget, self._need, self.frame_cost_ms, self.load_max)
         lat, batch_sizes, wait_times = [], [], []
         worst = {"step_ms": 0.0, "step_with_new_session_ms": 0.0, "create_ms": 0.0, "capture_ms": 0.0,
                  "close_ms": 0.0}
@@ -173,17 +240,14 @@ class Server:
             if c.t_arrive > 0:
                 heapq.heappush(events, (c.t_arrive, 0, c.cid))
                 continue
-            need = self._need(c)
-            if not waiting and reserved + need <= self.budget:
-                reserved += need
-                c.bytes = need
+            if not waiting and adm.fits(c):
+                adm.take(c)
                 c.session = Session(mixed_config(c.width, c.height, c.voxel), stream=self.stream)
                 c.session.prepare(shared=True)
                 warm.append(c)
             else:
                 waiting.append(c)
                 queued += 1
-        peak = reserved
         # frame-graph executables for the sessions expected to arrive, made
         # before the clock and released into the library's executable pool:
         # an arriving session's capture then rewrites one of them
@@ -191,15 +255,15 @@ class Server:
         # sessions' frames run, which stalled the loop for up to 80 ms
         # (held open together, as far as the budget allows, so that each
         # arrival finds its own set of executables)
-        group, held = [], reserved
+        group, held = [], adm.reserved
         for c in clients:
-            if c.t_arrive <= 0:
+            if c.t_arrive <= 0 and c.session is not None:
                 continue
             need = self._need(c)
             if group and held + need > self.budget:
                 for g in group:
                     g.close()
-                group, held = [], reserved
+                group, held = [], adm.reserved
             g = Session(mixed_config(c.width, c.height, c.voxel), stream=self.stream)
             g.prepare(shared=True)
             group.append(g)
@@ -224,14 +288,11 @@ class Server:
                 wait_times.append(c.t_admit - c.t_arrive)
 
         def reserve_for(c):
-            nonlocal reserved, peak
-            c.bytes = self._need(c)
-            reserved += c.bytes
-            peak = max(peak, reserved)
+            adm.take(c)
             to_open.append(c)
 
         def admit_waiting():
-            while waiting and reserved + self._need(waiting[0]) <= self.budget:
+            while waiting and adm.fits(waiting[0]):
                 reserve_for(waiting.pop(0))
 
         def admission_slice():
@@ -263,7 +324,7 @@ class Server:
                     _, kind, cid = heapq.heappop(events)
                     c = by_id[cid]
                     if kind == 0:
-                        if not waiting and reserved + self._need(c) <= self.budget:
+                        if not waiting and adm.fits(c):
                             reserve_for(c)
                         else:
                             waiting.append(c)
@@ -274,7 +335,7 @@ class Server:
                         c.session.close()
                         worst["close_ms"] = max(worst["close_ms"], (time.perf_counter() - t_c) * 1e3)
                         c.session = None
-                        reserved -= c.bytes
+                        adm.release(c)
                         admit_waiting()
                 if preparing or to_open:
                     admission_slice()
@@ -317,7 +378,10 @@ class Server:
             "clients": len(clients), "admitted": admitted, "queued": queued,
             "still_queued_at_end": len(waiting),
             "mean_wait_s": float(np.mean(wait_times)) if wait_times else 0.0,
-            "backlog_frames_at_end": backlog, "peak_reserved_bytes": peak, "budget_bytes": self.budget,
+            "backlog_frames_at_end": backlog, "peak_reserved_bytes": adm.peak, "budget_bytes": self.budget,
+            "admission": ({"frame_cost_ms": {f"{w}x{h}": v for (w, h), v in adm.cost.items()},
+                           "load_max": adm.load_max, "peak_admitted_load": adm.peak_load / 1000.0}
+                          if adm.cost else "memory only"),
             "worst_host_ms": worst,
             "graph_captures": {"updated": ex1["updated"] - ex0["updated"],
                                "instantiated": ex1["instantiated"] - ex0["instantiated"]},
