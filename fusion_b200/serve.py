@@ -130,7 +130,7 @@ class Admission:
     rest wait in FIFO order (head-of-line: a later, smaller client does not
     pass the head)."""
 
-    def __init__(self, budget_bytes, need, frame_cost_ms=None, load_max=0.85):
+    def __init__(self, budget_bytes, need, frame_cost_ms=None, load_max=0.95):
         self.budget = float(budget_bytes)
         self.need = need
         self.cost = dict(frame_cost_ms) if frame_cost_ms else None
@@ -172,7 +172,7 @@ class Server:
     becomes active, and its frames start arriving, once its session is ready.
     Clients present at the start are admitted before the clock starts."""
 
-    def __init__(self, pool, budget_bytes=120e9, mode=0, max_batch=256, frame_cost_ms=None, load_max=0.85):
+    def __init__(self, pool, budget_bytes=120e9, mode=0, max_batch=256, frame_cost_ms=None, load_max=0.95):
         import torch
         self.lib = _lib.load()
         self.pool = pool
