@@ -95,6 +95,9 @@ CASES = {
     "ref_320x240": ("ref", 0x5EEDF00D, 8),
     # the full-size plain configuration, 640x480, 5 mm voxels
     "c2_640x480": ("c2", None, 5),
+    # a ragged camera: levels 322x242, 161x121, 80x60 (odd sizes, rows and
+    # columns that are not multiples of 8)
+    "ragged_322x242": ("ragged", 0x0DDC0FFE, 6),
 }
 
 
@@ -104,6 +107,9 @@ def test_teacher_forced_tracking(name):
     kind, seed, n = CASES[name]
     if kind == "ref":
         cfg = S.reference_config(320, 240, fx=525.0, fy=525.0, depth_scale=5000.0, depth_cutoff=3.0)
+    elif kind == "ragged":
+        f = 525.0 * 322 / 640
+        cfg = S.reference_config(322, 242, fx=f, fy=f, depth_scale=5000.0, depth_cutoff=3.0)
     else:
         cfg = S.config_c2()
         seed = synth.session_seed(2, 0)
