@@ -579,9 +579,13 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
     return n + 1;
 }
 
+// A pitch must hold a row; for the word-sized element types the kernels index
+// rows in elements, so it must also be a multiple of the element.  RGB8
+// (3-byte) rows are indexed in bytes: cudaMallocPitch's pitch of a uchar3
+// image (a multiple of 512 bytes, not of 3) is valid.
 int image_ok(const fb_image* im, size_t elem) {
     return im && im->data && im->cols > 0 && im->rows > 0 && im->pitch >= elem * (size_t)im->cols &&
-           im->pitch % elem == 0;
+           (elem == 3 || im->pitch % elem == 0);
 }
 
 cudaStream_t as_stream(void* s) { return (cudaStream_t)s; }

@@ -107,3 +107,18 @@ def test_stages_at_ragged_sizes(size, empty):
         _same(host(dd), od)
         assert np.array_equal(host(dg), og)
         d_l, g_l = od, og
+
+
+def test_pitched_rgb_rows():
+    """RGB8 images whose rows are padded the way cudaMallocPitch pads them (a
+    pitch that is a multiple of 512 bytes, not of 3): the reference's own
+    DeviceArray2D<uchar3> buffers."""
+    from fusion_b200 import system as S
+    W, H = 320, 240
+    _, rgb = _frame(W, H, False)
+    padded = torch.zeros((H, 1024), dtype=torch.uint8, device="cuda")
+    view = padded.as_strided((H, W, 3), (1024, 3, 1))
+    view.copy_(torch.from_numpy(rgb).cuda())
+    gray = torch.empty((H, W), dtype=torch.uint8, device="cuda")
+    S.image_to_intensity(view, gray)
+    assert np.array_equal(host(gray), O.intensity(rgb))
