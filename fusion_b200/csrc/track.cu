@@ -685,6 +685,77 @@ struct SolveIO {
 
 __device__ void solve_staged(SolveIO& io, const double* s, int min_count, int is_final);
 
+// The end of an iteration, in the block that finished last: the group sums
+// of both passes in group order (FP64, or compensated FP32 in the precision
+// form) -- value t & 63 (0..28 ICP, 32..60 RGB) over four fixed ranges of
+// groups, then the ranges in order -- the Gauss-Newton update with one
+// thread, and the new state written back in parallel.
+template <bool kComp>
+__device__ __forceinline__ void finish_iteration(TrackState* st, unsigned int* ticket, int NG, long long c,
+                                                 long long q, float sigma, int min_count, int is_final,
+                                                 SolveIO& io, double (&s_part)[4][64], float2 (&s_partc)[4][64],
+                                                 double (&sums)[64]) {
+    {
+        const int val = threadIdx.x & 63, part = threadIdx.x >> 6;
+        const int per = (NG + 3) / 4, g0 = part * per, g1 = min(NG, g0 + per);
+        if constexpr (kComp) {
+            // compensated FP32 over the groups; to FP64 only for the solve
+            float2 t = make_float2(0.f, 0.f);
+            if ((val & 31) < 29) {
+                const float2* src = val < 32 ? &st->grp_icp2[0][val] : &st->grp_rgb2[0][val - 32];
+#pragma unroll 8
+                for (int g = g0; g < g1; ++g) t = pair_add(t, __ldcg(src + (size_t)g * 32));
+            }
+            s_partc[part][val] = t;
+        } else {
+            double t = 0;
+            if ((val & 31) < 29) {
+                const double* src = val < 32 ? &st->grp_icp[0][val] : &st->grp_rgb[0][val - 32];
+#pragma unroll 8
+                for (int g = g0; g < g1; ++g) t += __ldcg(src + (size_t)g * 32);
+            }
+            s_part[part][val] = t;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        if constexpr (kComp) {
+            const float2 t = pair_add(pair_add(pair_add(s_partc[0][threadIdx.x], s_partc[1][threadIdx.x]),
+                                               s_partc[2][threadIdx.x]),
+                                      s_partc[3][threadIdx.x]);
+            sums[threadIdx.x] = (double)t.x + (double)t.y;
+        } else {
+            sums[threadIdx.x] = ((s_part[0][threadIdx.x] + s_part[1][threadIdx.x]) + s_part[2][threadIdx.x]) +
+                                s_part[3][threadIdx.x];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *ticket = 0;
+        solve_staged(io, sums, min_count, is_final);
+    }
+    __syncthreads();
+    // write back in parallel
+    if (threadIdx.x < 16) {
+        st->pose[threadIdx.x] = io.pose[threadIdx.x];
+        if (io.updated) st->delta[threadIdx.x] = io.delta[threadIdx.x];
+    } else if (threadIdx.x >= 32 && threadIdx.x < 32 + (int)(sizeof(DevPose) / 4)) {
+        if (io.updated) ((float*)&st->cur)[threadIdx.x - 32] = ((const float*)&io.cur)[threadIdx.x - 32];
+    } else if (threadIdx.x >= 64 && threadIdx.x < 93) {
+        st->icp_sums[threadIdx.x - 64] = sums[threadIdx.x - 64];
+        st->rgb_sums[threadIdx.x - 64] = sums[32 + threadIdx.x - 64];
+    } else if (threadIdx.x == 96) {
+        st->icp_error = io.icp_error;
+        st->icp_count = io.icp_count;
+        st->rgb_error = io.rgb_error;
+        st->rgb_count = io.rgb_count;
+        st->rgb_cnt = c;
+        st->rgb_sq = q;
+        st->sigma = sigma;
+        st->failed = io.failed;
+    }
+}
+
 // pass B (clusters as in pass A): every block derives sigma from pass A's
 // group counts (integers: the same value in every block) and builds the RGB
 // rows of its warps' segments; each cluster reduces its rows into a group
@@ -768,67 +839,199 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     if (threadIdx.x == 0) s_last = ticket_acq_rel(ticket) == (unsigned)(NG - 1);
     __syncthreads();
     if (!s_last) return;
-    // group sums of both passes in group order: value t & 63 (0..28 ICP,
-    // 32..60 RGB) over four fixed ranges of groups, then the ranges in order
-    {
-        const int val = threadIdx.x & 63, part = threadIdx.x >> 6;
-        const int per = (NG + 3) / 4, g0 = part * per, g1 = min(NG, g0 + per);
+    finish_iteration<kComp>(st, ticket, NG, c, q, sigma, min_count, is_final, io, s_part, s_partc, sums);
+}
+
+// Shape of the group forms below: groups per block and resident blocks per
+// SM (4: half the registers, some spilled; 2: none spilled).
+constexpr int kGroupsPerBlock = 1;
+constexpr int kGrpMinBlocks = 4;
+
+// Group forms of k_track_a / k_track_b for sessions sharing the GPU: one
+// block per group does the work of the group's kTrackCluster clustered
+// blocks -- logical blocks b = kTrackCluster * group + r, r in rank order,
+// each with the pixels, warp segments and block sums the clustered block b
+// has in a grid of G blocks -- and adds their sums in rank order as the
+// cluster reduction does.  The results are therefore the clustered kernels'
+// bit for bit, on a grid of G / kTrackCluster blocks: a session's pass holds
+// a quarter of the block slots for longer, and other sessions' passes run
+// beside it.
+template <int kMinBlocks, bool kComp>
+__global__ void __launch_bounds__(256, kMinBlocks)
+    k_track_a_grp(TrackLevel L, TrackState* st, int2* list, int* counts, int G, int gpc) {
+    const int N = L.W * L.H, NG = G / kTrackCluster;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (st->failed) return;   // uniform over the grid: written by an earlier kernel
+    __shared__ float sm[8 * 32];
+    __shared__ long long smll[32];
+    __shared__ double s_vals[kTrackCluster][32];
+    __shared__ float s_f[kTrackCluster][32];
+    __shared__ long long s_c[kTrackCluster][2];
+    const DevPose cur = st->cur, last = st->last;
+    const int iters = (N + G * 256 - 1) / (G * 256);
+    const unsigned lt = (1u << lane) - 1u;
+    for (int j = 0; j < gpc; ++j) {
+    const int g = blockIdx.x * gpc + j;
+    if (g >= NG) break;
+    for (int r = 0; r < kTrackCluster; ++r) {
+        const int b = g * kTrackCluster + r;
+        int p = b * 256 + threadIdx.x;
+        PixelIn nxt;
+        if (p < N) nxt = load_pixel(L, p);
+        float acc[29];
+#pragma unroll
+        for (int k = 0; k < 29; ++k) acc[k] = 0.f;
+        long long rc = 0, rsq = 0;
+        const int gw = b * kTrackWarps + wid;
+        int2* seg = list + (size_t)gw * iters * 32;
+        int run = 0;
+        for (int k = 0; k < iters; ++k, p += G * 256) {
+            const PixelIn in = nxt;
+            if (k + 1 < iters && p + G * 256 < N) nxt = load_pixel(L, p + G * 256);   // one pixel ahead
+            int rr = -1;
+            if (p < N) {
+                float row[7];
+                if (pixel_pass_a(L, cur, last, in, row, &rr)) add_products(row, acc);
+                if (rr >= 0) {
+                    int d = (rr & 511) - 255;
+                    rc += 1;
+                    rsq += d * d;
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, rr >= 0);
+            if (rr >= 0) seg[run + __popc(m & lt)] = make_int2(p, rr);
+            run += __popc(m);
+        }
+        if (lane == 0) counts[gw] = run;
+        const float bsum = block_sum29(acc, sm);
+        const long long bc = __shfl_sync(0xffffffffu, block_sum_ll(rc, smll), 0);
+        const long long bs = __shfl_sync(0xffffffffu, block_sum_ll(rsq, smll), 0);
         if constexpr (kComp) {
-            // compensated FP32 over the groups; to FP64 only for the solve
-            float2 t = make_float2(0.f, 0.f);
-            if ((val & 31) < 29) {
-                const float2* src = val < 32 ? &st->grp_icp2[0][val] : &st->grp_rgb2[0][val - 32];
-#pragma unroll 8
-                for (int g = g0; g < g1; ++g) t = pair_add(t, __ldcg(src + (size_t)g * 32));
+            if (wid == 0) s_f[r][lane] = lane < 29 ? bsum : 0.f;
+            if (threadIdx.x == 0) {
+                s_c[r][0] = bc;
+                s_c[r][1] = bs;
             }
-            s_partc[part][val] = t;
         } else {
-            double t = 0;
-            if ((val & 31) < 29) {
-                const double* src = val < 32 ? &st->grp_icp[0][val] : &st->grp_rgb[0][val - 32];
-#pragma unroll 8
-                for (int g = g0; g < g1; ++g) t += __ldcg(src + (size_t)g * 32);
+            if (wid == 0)
+                s_vals[r][lane] = lane < 29 ? (double)bsum : lane == 29 ? (double)bc : lane == 30 ? (double)bs : 0.0;
+        }
+        __syncthreads();   // sm / smll are reused by the next logical block
+    }
+    if (threadIdx.x < 31) {
+        if constexpr (kComp) {
+            if (threadIdx.x < 29) {
+                float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int r = 0; r < kTrackCluster; ++r) acc = pair_add(acc, make_float2(s_f[r][threadIdx.x], 0.f));
+                st->grp_icp2[g][threadIdx.x] = acc;
+            } else {
+                long long t = 0;
+#pragma unroll
+                for (int r = 0; r < kTrackCluster; ++r) t += s_c[r][threadIdx.x - 29];
+                if (threadIdx.x == 29)
+                    st->grp_cnt[g] = t;
+                else
+                    st->grp_sq[g] = t;
             }
-            s_part[part][val] = t;
+        } else {
+            double v = 0;
+#pragma unroll
+            for (int r = 0; r < kTrackCluster; ++r) v += s_vals[r][threadIdx.x];
+            if (threadIdx.x < 29)
+                st->grp_icp[g][threadIdx.x] = v;
+            else if (threadIdx.x == 29)
+                st->grp_cnt[g] = (long long)v;
+            else
+                st->grp_sq[g] = (long long)v;
         }
     }
-    __syncthreads();
-    if (threadIdx.x < 64) {
-        if constexpr (kComp) {
-            const float2 t = pair_add(pair_add(pair_add(s_partc[0][threadIdx.x], s_partc[1][threadIdx.x]),
-                                               s_partc[2][threadIdx.x]),
-                                      s_partc[3][threadIdx.x]);
-            sums[threadIdx.x] = (double)t.x + (double)t.y;
-        } else {
-            sums[threadIdx.x] = ((s_part[0][threadIdx.x] + s_part[1][threadIdx.x]) + s_part[2][threadIdx.x]) +
-                                s_part[3][threadIdx.x];
+    __syncthreads();   // s_vals / s_f / s_c are reused by the next group
+    }
+}
+
+template <int kMinBlocks, bool kComp>
+__global__ void __launch_bounds__(256, kMinBlocks)
+    k_track_b_grp(TrackLevel L, TrackState* st, unsigned int* ticket, const int2* list, const int* counts,
+                  int seg_size, int min_count, int is_final, int NG, int gpc) {
+    __shared__ float sm[32 * 29];
+    __shared__ float s_rgb[kTrackCluster][32];
+    __shared__ double s_part[4][64];
+    __shared__ float2 s_partc[4][64];
+    __shared__ double sums[64];
+    __shared__ bool s_last;
+    __shared__ SolveIO io;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    // stage the solve's inputs early (used by the last block)
+    if (threadIdx.x >= 64 && threadIdx.x < 80) {
+        const int i = threadIdx.x - 64;
+        io.delta[i] = st->delta[i];
+        io.last_pose[i] = st->last_pose[i];
+        io.init_pose[i] = st->init_pose[i];
+    }
+    if (threadIdx.x == 80) {
+        io.icp_error = st->icp_error;
+        io.icp_count = st->icp_count;
+    }
+    if (st->failed) return;
+    const DevPose cur = st->cur, last = st->last;
+    // sigma as in k_track_b
+    long long c = 0, q = 0;
+    for (int g = lane; g < NG; g += 32) {
+        c += __ldcg(&st->grp_cnt[g]);
+        q += __ldcg(&st->grp_sq[g]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+        q += __shfl_xor_sync(0xffffffffu, q, o);
+    }
+    const float sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
+    for (int j = 0; j < gpc; ++j) {
+    const int grp = blockIdx.x * gpc + j;
+    if (grp >= NG) break;
+    for (int r = 0; r < kTrackCluster; ++r) {
+        const int b = grp * kTrackCluster + r;
+        float acc[29];
+#pragma unroll
+        for (int k = 0; k < 29; ++k) acc[k] = 0.f;
+        const int gw = b * kTrackWarps + wid;
+        const int n = counts[gw];
+        const int2* seg = list + (size_t)gw * seg_size;
+        for (int i = lane; i < n; i += 32) {
+            const int2 e = seg[i];
+            const int y = e.x / L.W, x = e.x - y * L.W;
+            float row[7];
+            rgb_row(L, cur, last, x, y, e.y, sigma, row);
+            add_products(row, acc);
+        }
+        const float bsum = block_sum29(acc, sm);
+        if (wid == 0) s_rgb[r][lane] = lane < 29 ? bsum : 0.f;
+        __syncthreads();   // sm is reused by the next logical block
+    }
+    if constexpr (kComp) {
+        if (threadIdx.x < 29) {
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int r = 0; r < kTrackCluster; ++r) acc = pair_add(acc, make_float2(s_rgb[r][threadIdx.x], 0.f));
+            st->grp_rgb2[grp][threadIdx.x] = acc;
+        }
+    } else {
+        if (threadIdx.x < 29) {
+            double v = 0;
+#pragma unroll
+            for (int r = 0; r < kTrackCluster; ++r) v += (double)s_rgb[r][threadIdx.x];
+            st->grp_rgb[grp][threadIdx.x] = v;
         }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        *ticket = 0;
-        solve_staged(io, sums, min_count, is_final);
+    __syncthreads();   // s_rgb is reused by the next group
     }
+    // last block to finish
     __syncthreads();
-    // write back in parallel
-    if (threadIdx.x < 16) {
-        st->pose[threadIdx.x] = io.pose[threadIdx.x];
-        if (io.updated) st->delta[threadIdx.x] = io.delta[threadIdx.x];
-    } else if (threadIdx.x >= 32 && threadIdx.x < 32 + (int)(sizeof(DevPose) / 4)) {
-        if (io.updated) ((float*)&st->cur)[threadIdx.x - 32] = ((const float*)&io.cur)[threadIdx.x - 32];
-    } else if (threadIdx.x >= 64 && threadIdx.x < 93) {
-        st->icp_sums[threadIdx.x - 64] = sums[threadIdx.x - 64];
-        st->rgb_sums[threadIdx.x - 64] = sums[32 + threadIdx.x - 64];
-    } else if (threadIdx.x == 96) {
-        st->icp_error = io.icp_error;
-        st->icp_count = io.icp_count;
-        st->rgb_error = io.rgb_error;
-        st->rgb_count = io.rgb_count;
-        st->rgb_cnt = c;
-        st->rgb_sq = q;
-        st->sigma = sigma;
-        st->failed = io.failed;
-    }
+    if (threadIdx.x == 0) s_last = ticket_acq_rel(ticket) == gridDim.x - 1u;
+    __syncthreads();
+    if (!s_last) return;
+    finish_iteration<kComp>(st, ticket, NG, c, q, sigma, min_count, is_final, io, s_part, s_partc, sums);
 }
 
 // The Gauss-Newton update of one iteration (Tracking.cc:319-394) and, after
@@ -1256,17 +1459,22 @@ int launch_track_iter(const TrackLevel& L, TrackState* st, unsigned int* tickets
     const int g = track_cluster_grid(n);
     const int seg = (n + g * 256 - 1) / (g * 256) * 32;
     const int fin = is_final ? 1 : 0;
+    // sessions sharing the GPU: the group forms, kGroupsPerBlock groups per
+    // block, the same results
+    const int ng = g / kTrackCluster, gpc = kGroupsPerBlock, gb = (ng + gpc - 1) / gpc;
     if (compensated) {
         if (shared_gpu) {
-            k_track_a<4, true><<<g, 256, 0, s>>>(L, st, residual, counts);
-            k_track_b<4, true><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, fin);
+            k_track_a_grp<kGrpMinBlocks, true><<<gb, 256, 0, s>>>(L, st, residual, counts, g, gpc);
+            k_track_b_grp<kGrpMinBlocks, true><<<gb, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg,
+                                                                  min_count, fin, ng, gpc);
         } else {
             k_track_a<2, true><<<g, 256, 0, s>>>(L, st, residual, counts);
             k_track_b<2, true><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, fin);
         }
     } else if (shared_gpu) {
-        k_track_a<4, false><<<g, 256, 0, s>>>(L, st, residual, counts);
-        k_track_b<4, false><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, fin);
+        k_track_a_grp<kGrpMinBlocks, false><<<gb, 256, 0, s>>>(L, st, residual, counts, g, gpc);
+        k_track_b_grp<kGrpMinBlocks, false><<<gb, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count,
+                                                               fin, ng, gpc);
     } else {
         k_track_a<2, false><<<g, 256, 0, s>>>(L, st, residual, counts);
         k_track_b<2, false><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, fin);
