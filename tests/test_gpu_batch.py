@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 from fusion_b200 import synth
+from fusion_b200.invariants import check_session
 
 pytestmark = pytest.mark.gpu
 
@@ -52,6 +53,7 @@ def _alone(frames, schedule):
         d, c = frames[i]
         rows = [_row(s.grab(d[k], c[k])) for k in range(len(schedule[i]))]
         out.append((rows, _map_digest(s)))
+        assert check_session(s) == []
         s.close()
     return out
 

@@ -11,6 +11,7 @@ pixels with the FP64 oracle.
 import numpy as np
 import pytest
 
+from fusion_b200.invariants import check_session
 from oracle import oracle as O
 from tests import golden_util as G
 
@@ -121,6 +122,7 @@ def test_allocation_is_deterministic_and_duplicate_free():
         tables.append(e)
         occ = e[e[:, 3] >= 0]
         assert len({tuple(r) for r in occ[:, :3].tolist()}) == len(occ)
+        assert check_session(s) == []
         s.close()
     assert np.array_equal(tables[0], tables[1])
 
@@ -143,5 +145,6 @@ def test_exhausted_pool_takes_exact_sequential_path():
     st = _compare_maps(sess, M)
     assert st["sequential"] == 1
     assert st["error_flags"] & 0x1         # heap exhausted reported
+    assert check_session(sess) == []       # what stays checkable after exhaustion
     M.close()
     sess.close()
