@@ -82,6 +82,7 @@ SIGNATURES = {
     "fb_session_destroy": (_i, [_vp]),
     "fb_session_reset": (_i, [_vp]),
     "fb_grab_frame": (_i, [_vp, _vp, _sz, _vp, _sz, _i, ctypes.POINTER(FrameResult)]),
+    "fb_stage_frame": (_i, [_vp, _vp, _sz, _vp, _sz]),
     "fb_get_pose": (_i, [_vp, _vp]),
     "fb_session_set_profiling": (_i, [_vp, _i]),
     "fb_session_set_graphs": (_i, [_vp, _i]),

@@ -172,10 +172,23 @@ struct KeyState {
     fb_keypoint_stats stats{};
 };
 
+// Frames staged by fb_stage_frame: host-to-device copies on their own
+// stream into two buffers outside the arena, consumed in order by
+// fb_grab_frame.
+struct StagedInput {
+    cudaStream_t copy = nullptr;
+    uint16_t* depth[2] = {nullptr, nullptr};
+    uint8_t* rgb[2] = {nullptr, nullptr};
+    cudaEvent_t ready[2] = {nullptr, nullptr};   // copy done (copy stream)
+    cudaEvent_t freed[2] = {nullptr, nullptr};   // taken into the frame (session stream)
+    int head = 0, count = 0;
+};
+
 struct fb_session {
     fb_config cfg;
     cudaStream_t stream;
     bool own_stream;
+    StagedInput* staged = nullptr;
     int W[3], H[3];
     Intr K[3];
     FrameBuf fr[2];
@@ -356,8 +369,24 @@ void free_keys(fb_session* s) {
 
 void drop_graphs(fb_session* s);
 
+void free_staged(fb_session* s) {
+    StagedInput* g = s->staged;
+    if (!g) return;
+    if (g->copy) cudaStreamSynchronize(g->copy);
+    for (int i = 0; i < 2; ++i) {
+        if (g->depth[i]) cudaFree(g->depth[i]);
+        if (g->rgb[i]) cudaFree(g->rgb[i]);
+        if (g->ready[i]) cudaEventDestroy(g->ready[i]);
+        if (g->freed[i]) cudaEventDestroy(g->freed[i]);
+    }
+    if (g->copy) cudaStreamDestroy(g->copy);
+    delete g;
+    s->staged = nullptr;
+}
+
 void free_session(fb_session* s) {
     free_keys(s);
+    free_staged(s);
     drop_graphs(s);
     for (int i = 0; i <= kStages; ++i)
         if (s->ev[i]) cudaEventDestroy(s->ev[i]);
@@ -1337,10 +1366,60 @@ int fb_session_reset(fb_session* s) {
     return reset_session(s);
 }
 
+// The oldest staged frame into NextFrame's input buffers, on the session
+// stream once its copy has landed.
+int take_staged(fb_session* s) {
+    StagedInput* g = s->staged;
+    if (!g || g->count == 0) return FB_EINVAL;
+    const int k = g->head, W = s->W[0], H = s->H[0];
+    FrameBuf& N = s->fr[s->next];
+    FB_CUDA(cudaStreamWaitEvent(s->stream, g->ready[k], 0));
+    FB_CUDA(cudaMemcpyAsync(N.depth_in, g->depth[k], (size_t)W * H * 2, cudaMemcpyDeviceToDevice, s->stream));
+    FB_CUDA(cudaMemcpyAsync(N.rgb, g->rgb[k], (size_t)W * H * 3, cudaMemcpyDeviceToDevice, s->stream));
+    FB_CUDA(cudaEventRecord(g->freed[k], s->stream));
+    g->head ^= 1;
+    --g->count;
+    return FB_OK;
+}
+
+int fb_stage_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, const uint8_t* rgb, size_t rgb_pitch) {
+    if (!s || !depth || !rgb) return FB_EINVAL;
+    const int W = s->W[0], H = s->H[0];
+    if (depth_pitch < (size_t)W * 2 || rgb_pitch < (size_t)W * 3) return FB_EINVAL;
+    if (!s->staged) {
+        StagedInput* g = new (std::nothrow) StagedInput;
+        if (!g) return FB_ENOMEM;
+        s->staged = g;
+        cudaError_t e = cudaStreamCreateWithFlags(&g->copy, cudaStreamNonBlocking);
+        for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+            e = cudaMalloc(&g->depth[i], (size_t)W * H * 2);
+            if (e == cudaSuccess) e = cudaMalloc(&g->rgb[i], (size_t)W * H * 3);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->ready[i], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->freed[i], cudaEventDisableTiming);
+        }
+        if (e != cudaSuccess) {
+            free_staged(s);
+            cudaGetLastError();
+            return e == cudaErrorMemoryAllocation ? FB_ENOMEM : (cuda_ok(e) ? FB_OK : FB_ECUDA);
+        }
+    }
+    StagedInput* g = s->staged;
+    if (g->count == 2) return FB_EINVAL;   // two frames are waiting already
+    const int k = (g->head + g->count) & 1;
+    FB_CUDA(cudaStreamWaitEvent(g->copy, g->freed[k], 0));   // its previous frame has been taken
+    FB_CUDA(cudaMemcpy2DAsync(g->depth[k], (size_t)W * 2, depth, depth_pitch, (size_t)W * 2, H, cudaMemcpyHostToDevice,
+                              g->copy));
+    FB_CUDA(cudaMemcpy2DAsync(g->rgb[k], (size_t)W * 3, rgb, rgb_pitch, (size_t)W * 3, H, cudaMemcpyHostToDevice,
+                              g->copy));
+    FB_CUDA(cudaEventRecord(g->ready[k], g->copy));
+    ++g->count;
+    return FB_OK;
+}
+
 int fb_grab_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, const uint8_t* rgb, size_t rgb_pitch,
                   int on_device, fb_frame_result* out) {
-    if (!s || !depth || !rgb) return FB_EINVAL;
-    int rc = copy_frame_in(s, depth, depth_pitch, rgb, rgb_pitch, on_device, s->stream);
+    if (!s || (!depth) != (!rgb)) return FB_EINVAL;
+    int rc = depth ? copy_frame_in(s, depth, depth_pitch, rgb, rgb_pitch, on_device, s->stream) : take_staged(s);
     if (rc) return rc;
     if (s->keys) return grab_with_keys(s, out);
     const FramePlan p = plan_frame(s);

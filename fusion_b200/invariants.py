@@ -36,16 +36,13 @@ import numpy as np
 
 def bucket_of(x, y, z, num_buckets):
     """DeviceMap::Hash: ((x * 73856093) ^ (y * 19349669) ^ (z * 83492791))
-    % num_buckets in signed 32-bit arithmetic with wrap-around, C's truncated
-    remainder, plus num_buckets when negative."""
+    % NumBuckets, the products wrapping at 32 bits; NumBuckets is an unsigned
+    constant, so the remainder is taken of the 32-bit pattern as unsigned
+    (the reference's `res < 0` correction never applies)."""
     x, y, z = (np.asarray(v, np.int64) for v in (x, y, z))
-
-    def wrap(v):
-        return ((v + 2 ** 31) % 2 ** 32) - 2 ** 31
-
-    h = wrap(wrap(x * 73856093) ^ wrap(y * 19349669) ^ wrap(z * 83492791))
-    r = np.fmod(h, num_buckets)
-    return np.where(r < 0, r + num_buckets, r).astype(np.int64)
+    m = 0xFFFFFFFF
+    h = ((x * 73856093) & m) ^ ((y * 19349669) & m) ^ ((z * 83492791) & m)
+    return (h % int(num_buckets)).astype(np.int64)
 
 
 def check_map(entries, num_buckets, num_excess, num_blocks, heap_counter=None, entry_ptr=None, exhausted=False,

@@ -195,11 +195,23 @@ class Session:
             self.h, 1 if shared else 0, int(max_graphs), ctypes.byref(left)))
         return left.value
 
+    def stage(self, depth, rgb):
+        """Start copying a later frame (host numpy arrays, ideally pinned) to
+        the device (fb_stage_frame); grab(None, None) takes it."""
+        depth = np.ascontiguousarray(depth, np.uint16)
+        rgb = np.ascontiguousarray(rgb, np.uint8)
+        self._staged = getattr(self, "_staged", [])[-1:] + [(depth, rgb)]   # keep the host memory alive
+        check("fb_stage_frame", self.lib.fb_stage_frame(self.h, _p(depth), depth.strides[0], _p(rgb),
+                                                        rgb.strides[0]))
+
     def grab(self, depth, rgb, on_device=False):
         """One frame.  depth: u16 [H, W]; rgb: u8 [H, W, 3]; numpy arrays
-        (host) or, with on_device, objects with data_ptr() (device)."""
+        (host) or, with on_device, objects with data_ptr() (device); None and
+        None: the oldest frame given to stage()."""
         r = FrameResult()
-        if on_device:
+        if depth is None and rgb is None:
+            code = self.lib.fb_grab_frame(self.h, None, 0, None, 0, 0, ctypes.byref(r))
+        elif on_device:
             W = self.cfg.width
             code = self.lib.fb_grab_frame(self.h, depth.data_ptr(), 2 * W, rgb.data_ptr(), 3 * W, 1,
                                           ctypes.byref(r))

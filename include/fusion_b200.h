@@ -130,6 +130,18 @@ FB_API int fb_session_reset(fb_session* s);
  * pointers.  Synchronous: returns when the frame is done. */
 FB_API int fb_grab_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, const uint8_t* rgb,
                   size_t rgb_pitch, int on_device, fb_frame_result* out);
+/* No counterpart in the reference.  Starts the host-to-device copy of a
+ * later frame's depth and colour (host memory; pinned for the copy to run
+ * asynchronously) on a copy stream of the session and returns.  A
+ * fb_grab_frame call with depth = rgb = NULL takes the oldest staged frame
+ * instead of copying, so the copy overlaps the frames before it: stage
+ * frame k+1, then grab frame k.  At most two frames are staged at a time
+ * (FB_EINVAL beyond).  The host memory must stay unchanged until the
+ * fb_grab_frame that takes the frame has returned.  The staging buffers
+ * (2 x 5 bytes per pixel) are allocated at the first call, outside
+ * fb_session_bytes. */
+FB_API int fb_stage_frame(fb_session* s, const uint16_t* depth, size_t depth_pitch, const uint8_t* rgb,
+                          size_t rgb_pitch);
 
 /* Tracing (the reference has none; Utility/StopWatch.h is never called):
  * with profiling on, every frame records CUDA events around its stages and

@@ -55,14 +55,12 @@ def test_sound_table_passes():
     assert I.check_map(e, NB, NE, NS, heap_counter=hc, entry_ptr=ep) == []
 
 
-def test_hash_matches_signed_wrapping_modulo():
-    # ((x*73856093) ^ (y*19349669) ^ (z*83492791)) % n in int32, + n if negative
+def test_hash_is_the_unsigned_modulo_of_the_wrapped_products():
+    # int res = (...) % NumBuckets with NumBuckets unsigned: the 32-bit pattern
+    # of the xor of the wrapped products, modulo NumBuckets as unsigned
     def ref(x, y, z, n):
-        def w(v):
-            return ((v + 2 ** 31) % 2 ** 32) - 2 ** 31
-        h = w(w(x * 73856093) ^ w(y * 19349669) ^ w(z * 83492791))
-        r = abs(h) % n * (1 if h >= 0 else -1)
-        return r + n if r < 0 else r
+        h = (((x * 73856093) % 2 ** 32) ^ ((y * 19349669) % 2 ** 32) ^ ((z * 83492791) % 2 ** 32))
+        return h % n
     for x, y, z in [(0, 0, 0), (1, 2, 3), (-1, -2, -3), (4000, -5000, 60), (-32767, 32767, -1)]:
         for n in (64, 1000000, 1 << 20):
             assert int(I.bucket_of(x, y, z, n)) == ref(x, y, z, n)
@@ -117,3 +115,32 @@ def test_planted_defects_are_reported():
     # counters that disagree with the table
     msgs = _kinds(I.check_map(e, NB, NE, NS, heap_counter=hc + 1, entry_ptr=1))
     assert "heap_counter" in msgs and "entry_ptr" in msgs
+
+
+def test_reference_tables_show_its_allocator_races():
+    """The reference's own tables after one 128x96 frame (golden fixture from
+    its CUDA kernels, frames A and B): every head entry lies in the bucket
+    the checker's hash gives (the restatement of DeviceMap::Hash agrees with
+    the reference on every slot), and the reference's racy CreateBlock
+    (DeviceMap.cu:23-62: the bucket lock is released without a fence, the
+    entry written as a plain 32-byte store) shows as excess entries whose
+    chain link was overwritten, blocks entered more than once, and pool
+    blocks handed out by the heap that no entry holds."""
+    from tests import golden_util as G
+    fz = G.load("fuse_128x96.npz")
+    c = G.meta()["constants"]
+    NBr, NEr, NSr = int(c["num_buckets"]), int(c["num_excess"]), int(c["num_blocks"])
+    for p in "ab":
+        t = np.zeros((NBr + NEr, 5), np.int64)
+        t[:, 3] = -1
+        t[fz[p + "_slots"]] = fz[p + "_entries"]
+        hc, ep = (int(v) for v in fz[p + "_counters"])
+        msgs = I.check_map(t, NBr, NEr, NSr, heap_counter=hc, entry_ptr=ep, limit=10 ** 6)
+        unreached = [m for m in msgs if m.startswith("unreachable excess entry")]
+        repeated = [m for m in msgs if m.startswith("block ") and " entries" in m]
+        leaked = [m for m in msgs if m.startswith("allocated entries")]
+        print(p, len(unreached), "unreachable,", len(repeated), "repeated blocks,", leaked)
+        assert len(unreached) + len(repeated) + len(leaked) == len(msgs)   # nothing else, no foreign bucket
+        assert len(unreached) >= 20 and len(repeated) >= 40 and len(leaked) == 1
+        n_entries = len(fz[p + "_slots"])
+        assert NSr - 1 - hc > 1.5 * n_entries                              # most of the leak: lost entries
