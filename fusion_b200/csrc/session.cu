@@ -2552,6 +2552,8 @@ void clear_cache(fb_batch* b) {
 // kBatchSlots sessions, sessions share slots round-robin (their frames then
 // run one after the other on that slot, with the same results).
 constexpr int kBatchSlots = 32;
+// Steps of at most this many sessions run each frame as a session alone.
+constexpr int kBatchSharedMin = 2;
 
 int ensure_slots(fb_batch* b, int n) {
     while ((int)b->slots.size() < n) {
@@ -2693,10 +2695,13 @@ int fb_batch_step(fb_batch* b, fb_session* const* ss, int n, const fb_frame_inpu
                            b->origin);
         if (rc) return rc;
     }
-    // sessions of a batch run the tracking instance that leaves room for
-    // other sessions' frames (same results), also in a step of one session:
-    // its frame graphs are then the ones fb_session_prepare(s, 1) captured
-    for (int i = 0; i < n; ++i) ss[i]->shared_gpu = true;
+    // sessions of a step of more than kBatchSharedMin sessions run the
+    // tracking forms that leave room for the other sessions' frames (their
+    // frame graphs are the ones fb_session_prepare(s, 1) captures); smaller
+    // steps run the forms of a session alone (fb_session_prepare(s, 0)),
+    // which finish sooner.  Both give the same results.
+    const bool shared = n > kBatchSharedMin;
+    for (int i = 0; i < n; ++i) ss[i]->shared_gpu = shared;
     std::vector<FramePlan> plans(n);
     for (int i = 0; i < n; ++i) plans[i] = plan_frame(ss[i]);
     if (b->mode == 1) {

@@ -248,6 +248,7 @@ class Server:
                 adm.take(c)
                 c.session = Session(mixed_config(c.width, c.height, c.voxel), stream=self.stream)
                 c.session.prepare(shared=True)
+                c.session.prepare(shared=False)
                 warm.append(c)
             else:
                 waiting.append(c)
@@ -270,6 +271,7 @@ class Server:
                 group, held = [], adm.reserved
             g = Session(mixed_config(c.width, c.height, c.voxel), stream=self.stream)
             g.prepare(shared=True)
+            g.prepare(shared=False)
             group.append(g)
             held += need
         for g in group:
@@ -303,8 +305,12 @@ class Server:
             """One session creation or one graph capture."""
             t_s = time.perf_counter()
             if preparing:
+                # the graphs of steps with other sessions, then those of
+                # steps alone (batch steps of one or two sessions)
                 c = preparing[0]
-                if c.session.prepare_some(1, shared=True) == 0:
+                if c.session.prepare_some(0, shared=True) > 0:
+                    c.session.prepare_some(1, shared=True)
+                elif c.session.prepare_some(1, shared=False) == 0:
                     preparing.pop(0)
                     activate(c, now())
                 key = "capture_ms"
