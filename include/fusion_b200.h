@@ -165,9 +165,11 @@ FB_API int fb_session_launch_count(fb_session* s, uint64_t* launches);
 FB_API int fb_frame_transfer_bytes(const fb_config* cfg, size_t* h2d, size_t* d2h);
 
 /* Captures now every frame graph the session can use (tracker modes, fusion
- * on and off, both frame parities), for frames run alone (shared = 0) or in
- * batch steps with other sessions (shared = 1), so that later frames launch
- * without capture work on the host.  No reference counterpart. */
+ * on and off, both frame parities), for frames run alone and in batch steps
+ * of one or two sessions (shared = 0) or in batch steps of more sessions
+ * (shared = 1, tracking kernels that leave room for the other sessions'
+ * frames; the same results), so that later frames launch without capture
+ * work on the host.  No reference counterpart. */
 FB_API int fb_session_prepare(fb_session* s, int shared);
 /* As fb_session_prepare, capturing at most max_graphs graphs now;
  * *remaining = how many are still missing.  Lets a request loop spread the
