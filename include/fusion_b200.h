@@ -118,7 +118,9 @@ FB_API void fb_graph_exec_stats(long long* pooled, long long* updated, long long
 
 /* Replaces: System::System (Core/System.cc:16-73) -- Mapping::Create,
  * Tracker::Tracker, Frame::Create. stream: cudaStream_t or NULL (a stream is
- * created). */
+ * created).  FB_EINVAL for images outside width 16-4096, height 16-2048 or
+ * of 2^22 pixels or more (the photometric correspondences pack a 22-bit
+ * pixel index). */
 FB_API int fb_session_create(const fb_config* cfg, void* stream, fb_session** out);
 FB_API int fb_session_destroy(fb_session* s);
 /* Replaces: System::RebootSystem / Mapping::Reset + Tracker::ResetTracking. */
