@@ -23,8 +23,14 @@ Our arm prints one JSON line with
           for like with `value`) and the ragged mix (three resolutions, voxels
           4-20 mm) with autotuned raycast tiles; aggregate frames/s;
   served  the served form (N=1): clients arriving and leaving, 30 Hz Poisson
-          frames, HBM admission budget, continuous batching; aggregate
-          frames/s and p50/p99 latency from frame arrival to fusion.
+          frames, admission by HBM budget and calibrated GPU load,
+          continuous batching; aggregate frames/s and p50/p99 latency from
+          frame arrival to fusion, at 64 clients and (more_clients) at 256
+          clients plus arrivals, more than one GPU serves;
+  precision, mesh, keypoints, widened, reference_constants
+          the precision form, mesh extraction, frames with key points, the
+          top-down view / shading / snapshot / map-file timings, and this
+          build at the reference's compile-time constants.
 `--impl reference` times the CPU restatement of the reference's path (the
 reference itself is GPU-only code whose host classes need OpenCV/Eigen/Sophus)
 on all host cores on the same configuration.
