@@ -172,9 +172,14 @@ class Server:
     between steps: at most one session creation or one graph capture per
     iteration, so that no step waits for more than one slice (graph
     instantiation holds driver locks that a second host thread's launches
-    and copies would wait for, which showed as 100+ ms stalls).  A client
+    and copies would wait for, which showed as 100+ ms stalls).  A session
+    captures two sets of frame graphs: those of batch steps with other
+    sessions, then those of steps of one or two sessions (the library picks
+    the set by the step's size; both give the same results).  A client
     becomes active, and its frames start arriving, once its session is ready.
-    Clients present at the start are admitted before the clock starts."""
+    Clients present at the start are admitted before the clock starts.
+    Admission (class Admission) is by the HBM budget and, once calibrate()
+    has measured the per-resolution frame costs, by GPU load."""
 
     def __init__(self, pool, budget_bytes=120e9, mode=0, max_batch=256, frame_cost_ms=None, load_max=1.15):
         import torch
