@@ -2552,8 +2552,9 @@ void clear_cache(fb_batch* b) {
 // kBatchSlots sessions, sessions share slots round-robin (their frames then
 // run one after the other on that slot, with the same results).
 constexpr int kBatchSlots = 32;
-// Steps of at most this many sessions run each frame as a session alone.
-constexpr int kBatchSharedMin = 2;
+// Steps of at most this many sessions run each frame as a session alone
+// (served p50 at 64 clients on B200: 2.50 ms with 1, 2.25 with 2, 1.67 with 3).
+constexpr int kBatchSharedMin = 3;
 
 int ensure_slots(fb_batch* b, int n) {
     while ((int)b->slots.size() < n) {

@@ -174,7 +174,7 @@ class Server:
     instantiation holds driver locks that a second host thread's launches
     and copies would wait for, which showed as 100+ ms stalls).  A session
     captures two sets of frame graphs: those of batch steps with other
-    sessions, then those of steps of one or two sessions (the library picks
+    sessions, then those of steps of one to three sessions (the library picks
     the set by the step's size; both give the same results).  A client
     becomes active, and its frames start arriving, once its session is ready.
     Clients present at the start are admitted before the clock starts.
@@ -311,7 +311,7 @@ class Server:
             t_s = time.perf_counter()
             if preparing:
                 # the graphs of steps with other sessions, then those of
-                # steps alone (batch steps of one or two sessions)
+                # steps alone (batch steps of one to three sessions)
                 c = preparing[0]
                 if c.session.prepare_some(0, shared=True) > 0:
                     c.session.prepare_some(1, shared=True)

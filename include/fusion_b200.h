@@ -168,7 +168,7 @@ FB_API int fb_frame_transfer_bytes(const fb_config* cfg, size_t* h2d, size_t* d2
 
 /* Captures now every frame graph the session can use (tracker modes, fusion
  * on and off, both frame parities), for frames run alone and in batch steps
- * of one or two sessions (shared = 0) or in batch steps of more sessions
+ * of one to three sessions (shared = 0) or in batch steps of more sessions
  * (shared = 1, tracking kernels that leave room for the other sessions'
  * frames; the same results), so that later frames launch without capture
  * work on the host.  No reference counterpart. */

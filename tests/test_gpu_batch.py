@@ -1,10 +1,12 @@
 """Batched and served forms (fb_batch_*) through the C ABI.
 
 Each session's result in a batch must be the one the same session gives
-alone: the test runs ragged sessions (three resolutions, three voxel sizes,
+alone: the test runs ragged sessions (three resolutions, five voxel sizes,
 independent seeded sequences) once alone through fb_grab_frame and once
 together through fb_batch_step, in both batch modes, with sessions joining
-and skipping steps the way a server admits them, and compares every frame's
+and skipping steps the way a server admits them -- so that steps of more
+than three sessions (the group forms of the tracking kernels) and of three
+(the forms of a session alone) alternate -- and compares every frame's
 pose and counts and the final hash table and voxels bit for bit.
 """
 import hashlib
@@ -19,7 +21,8 @@ pytestmark = pytest.mark.gpu
 
 pytest.importorskip("torch")
 
-SPECS = [(160, 120, 0.012, 11), (320, 240, 0.007, 12), (640, 480, 0.005, 13)]
+SPECS = [(160, 120, 0.012, 11), (320, 240, 0.007, 12), (640, 480, 0.005, 13), (160, 120, 0.010, 14),
+         (320, 240, 0.009, 15)]
 N_FRAMES = 6
 
 
@@ -92,9 +95,12 @@ def frames():
     return [_frames(w, h, seed, N_FRAMES) for (w, h, _, seed) in SPECS]
 
 
-LOCKSTEP = [list(range(N_FRAMES))] * 3
-# session 1 joins at step 2, session 0 skips steps 3 and 4 (no frame arrived)
-STAGGERED = [[0, 1, 2, 5, 6, 7], [2, 3, 4, 5, 6, 7], [0, 1, 2, 3, 4, 5]]
+LOCKSTEP = [list(range(N_FRAMES))] * len(SPECS)
+# session 1 joins at step 2, session 0 skips steps 3 and 4 (no frame arrived);
+# steps of three sessions (steps 0 and 4: the tracking forms of sessions
+# alone) alternate with steps of four (the group forms)
+STAGGERED = [[0, 1, 2, 5, 6, 7], [2, 3, 4, 5, 6, 7], [0, 1, 2, 3, 4, 5], [0, 1, 3, 4, 6, 7],
+             [1, 2, 3, 5, 6, 7]]
 
 
 @pytest.mark.parametrize("mode", [0, 1])
