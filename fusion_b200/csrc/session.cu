@@ -226,7 +226,7 @@ struct fb_session {
     cudaGraphExec_t graph[3][2][2][2];
     int graph_kernels[3][2][2][2];
     int rc_bx, rc_by;          // raycast tile
-    bool shared_gpu;           // frames run beside other sessions' (batch steps)
+    bool shared_gpu;           // frames run beside other sessions (batch steps of more than three)
     // Tracker::mappingDisabled (set by System::ReadMapFromDisk): frames track
     // and render against the map without fusing into it
     bool mapping_disabled;
