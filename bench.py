@@ -62,8 +62,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-frames", type=int, default=6, help="frames in the CPU-oracle sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="reference arm: skip the timing of the reference's own CUDA kernels")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurements")
     ap.add_argument("--no-served", action="store_true", help="skip the served-form measurement")
     ap.add_argument("--batch-sessions", type=int, default=32)
@@ -165,25 +166,47 @@ def barrier(world):
         dist.barrier()
 
 
-def frames_for(cfg, seed, count):
-    from fusion_b200 import synth
-    p = synth.params(cfg.width, cfg.height, seed, fx=cfg.fx, fy=cfg.fy, cx=cfg.cx, cy=cfg.cy,
-                     depth_scale=cfg.depth_scale)
+# The full-size configuration as plain numbers, shared by both arms: the
+# reference arm builds its oracle configuration from these and never loads the
+# fusion library.  fusion_b200.system.config_c2() holds the same values.
+C2 = {"width": 640, "height": 480, "fx": 525.0, "fy": 525.0, "cx": 320.0, "cy": 240.0, "depth_scale": 5000.0,
+      "depth_cutoff": 4.0, "voxel_size": 0.005, "trunc_voxels": 4, "depth_min": 0.1, "depth_max": 4.0,
+      "num_buckets": 1 << 20, "num_excess": 1 << 18, "num_blocks": 1 << 18, "iters": (10, 5, 3)}
+C2_SEED = (2, 0)   # rgbd_synth.session_seed(config 2, session 0 + rank)
+
+
+def frames_c2(rank, count):
+    """The full-size sequence of one rank: `count` frames of the seeded room."""
+    import rgbd_synth as synth
+    seed = synth.session_seed(C2_SEED[0], C2_SEED[1] + rank)
+    p = synth.params(C2["width"], C2["height"], seed, fx=C2["fx"], fy=C2["fy"], cx=C2["cx"], cy=C2["cy"],
+                     depth_scale=C2["depth_scale"])
     d, c, _ = synth.render(p, 0, count)
     return d, c
 
 
-def cpu_oracle(cfg, depth, rgb, n_frames, budget_s=60.0):
-    """FP64 oracle on host cores: frames 0..n-1 of the sequence."""
+def oracle_config_c2():
     from oracle import oracle as O
-    oc = O.config(cfg.width, cfg.height, cfg.fx, cfg.fy, cfg.cx, cfg.cy, cfg.depth_scale, cfg.depth_cutoff,
-                  voxel_size=cfg.voxel_size, trunc_dist=cfg.trunc_dist, depth_min=cfg.depth_min,
-                  depth_max=cfg.depth_max, num_buckets=cfg.num_buckets, num_excess=cfg.num_excess,
-                  num_blocks=cfg.num_blocks, iters=tuple(cfg.iters), precision=64)
-    sysm = O.System(oc)
+    trunc = float(np.float32(C2["voxel_size"]) * np.float32(C2["trunc_voxels"]))
+    return O.config(C2["width"], C2["height"], C2["fx"], C2["fy"], C2["cx"], C2["cy"], C2["depth_scale"],
+                    C2["depth_cutoff"], voxel_size=C2["voxel_size"], trunc_dist=trunc, depth_min=C2["depth_min"],
+                    depth_max=C2["depth_max"], num_buckets=C2["num_buckets"], num_excess=C2["num_excess"],
+                    num_blocks=C2["num_blocks"], iters=C2["iters"], precision=64)
+
+
+def cpu_port_run(depth, rgb, W, K, budget_s=60.0):
+    """The FP64 CPU restatement of the reference's per-frame path on all host
+    threads: frames 0..W-1 untimed (they build the map and the tracker state),
+    then frames W..W+K-1 timed by the wall clock -- the same frames and the
+    same warm-up as the GPU arm's timed region.  Stops early after `budget_s`
+    seconds of timed work.  Returns (frames/s, frames timed, threads)."""
+    from oracle import oracle as O
+    sysm = O.System(oracle_config_c2())
+    for k in range(W):
+        sysm.grab(depth[k], rgb[k])
     t0 = time.perf_counter()
     done = 0
-    for k in range(n_frames):
+    for k in range(W, W + K):
         sysm.grab(depth[k], rgb[k])
         done += 1
         if time.perf_counter() - t0 > budget_s:
@@ -193,31 +216,52 @@ def cpu_oracle(cfg, depth, rgb, n_frames, budget_s=60.0):
     return done / dt, done, O.num_threads()
 
 
+def cpu_sample_text(W, done):
+    return (f"FP64 CPU restatement, all host threads: frames {W}..{W + done - 1} of the full-size sequence timed "
+            f"after frames 0..{W - 1} (the same frames and warm-up as the GPU arm's timed region)")
+
+
 def run_reference(args):
     """The reference arm: the CPU restatement of the reference's per-frame path
-    (FP64 oracle), all host threads, same configuration and sequence."""
+    (FP64 oracle) on all host threads, on the full-size configuration and the
+    frames the GPU arm times (--warmup frames untimed, then --steps frames).
+    It loads only the frame generator and oracle/ libraries.  Rank 0 runs it;
+    other ranks exit without work."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from fusion_b200 import system as S
-    cfg = S.config_c2()
-    from fusion_b200 import synth
-    budget = 120.0
-    n = max(2, min(args.steps + args.warmup, 40))
-    depth, rgb = frames_for(cfg, synth.session_seed(2, 0), n)
-    fps, done, cores = cpu_oracle(cfg, depth, rgb, n, budget_s=budget)
+    W, K = args.warmup, args.steps
+    depth, rgb = frames_c2(0, W + K)
+    fps, done, cores = cpu_port_run(depth, rgb, W, K, budget_s=150.0)
     line = {
         "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus,
-        "steps": done, "warmup": 0, "ms_per_step": 1000.0 / fps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural room)",
+        "steps": done, "warmup": W, "ms_per_step": 1000.0 / fps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural room, Kinect-like noise)",
         "config": {"workload": WORKLOAD, "parallelism": "host threads"},
         "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
-                         "sample": f"first {done} frames of the sequence (frame 0 initialises the map)"},
+                         "sample": cpu_sample_text(W, done)},
         "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "reference_cuda": reference_cuda(args),
+        "reference_cuda": None if args.no_reference_cuda else reference_cuda(args),
     }
     print(json.dumps(line))
     return 0
+
+
+def cpu_baseline_child(W, K):
+    """The CPU baseline of the GPU arm, measured exactly as the reference arm
+    measures it: a fresh process running `bench.py --impl reference` on the
+    same frames (an OpenMP team beside this process's CUDA and torch threads
+    runs the port measurably slower).  Returns the reference arm's
+    cpu_baseline object, or None if the child failed."""
+    env = dict(os.environ, RANK="0")
+    env.pop("WORLD_SIZE", None)
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", str(K),
+                          "--warmup", str(W), "--no-reference-cuda"], env=env, capture_output=True, text=True,
+                         timeout=600)
+    for ln in out.stdout.splitlines():
+        if ln.startswith("{"):
+            return json.loads(ln)["cpu_baseline"]
+    return None
 
 
 REF_CONSTANTS = ("the reference's compile-time map constants (6 mm voxels, truncation 48 mm, fusion depth "
@@ -241,10 +285,7 @@ def reference_cuda(args, frames=80, warmup=5):
             return None
     except Exception:
         return None
-    from fusion_b200 import synth
-    from fusion_b200 import system as S
-    cfg = S.config_c2()
-    depth, rgb = frames_for(cfg, synth.session_seed(2, 0), warmup + frames)
+    depth, rgb = frames_c2(0, warmup + frames)
     h = refharness.RefHarness(640, 480, 525.0, 525.0, 320.0, 240.0, 5000.0, 3.0)
     for i in range(warmup):
         h.grab(depth[i], rgb[i])
@@ -418,7 +459,8 @@ def _batched_run(specs, seeds, warmup, steps, tune=False):
     seeded sequence forwards and backwards).  Returns aggregate frames/s,
     ms per step, tracked fraction and the autotuned raycast tiles."""
     import torch
-    from fusion_b200 import Batch, Session, synth
+    import rgbd_synth as synth
+    from fusion_b200 import Batch, Session
     from fusion_b200.batch import autotune_raycast_tiles
     n_fr = 24
     seqs = {}
@@ -591,12 +633,18 @@ def main():
     rank, world, local = dist_setup(args.gpus)
     import torch
     torch.cuda.set_device(local)
-    from fusion_b200 import Session, synth
+    from fusion_b200 import Session
     from fusion_b200 import system as S
     cfg = S.config_c2()
+    for k, v in C2.items():
+        want = list(v) if k == "iters" else v
+        have = list(cfg.iters) if k == "iters" else (cfg.trunc_dist if k == "trunc_voxels" else getattr(cfg, k))
+        if k == "trunc_voxels":
+            want = float(np.float32(C2["voxel_size"]) * np.float32(v))
+        same = np.float32(have) == np.float32(want) if isinstance(want, float) else have == want
+        assert same, ("full-size configuration differs from config_c2()", k, have, want)
     W, K = args.warmup, args.steps
-    seed = synth.session_seed(2, rank)
-    depth, rgb = frames_for(cfg, seed, W + K)
+    depth, rgb = frames_c2(rank, W + K)
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
 
@@ -687,9 +735,11 @@ def main():
     # layout), and one read of the depth, colour and normal of every pixel
     bytes_launch = 2 * 8 * 512 * mean_vis + 32 * mean_vis + 23 * n_px
     achieved = bytes_launch / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
-    # DRAM bytes per launch: ncu's dram__bytes_read.sum + dram__bytes_write.sum
-    # of one full-size k_integrate launch, per visible block of that launch,
-    # scaled here to this run's mean visible-block count
+    # DRAM bytes per launch are not measurable inside this process (no
+    # profiler); the figure is ncu's dram__bytes_read.sum +
+    # dram__bytes_write.sum of one full-size k_integrate launch, per visible
+    # block of that launch (profiles/integration_traffic.txt), scaled to this
+    # run's mean visible-block count, and labelled as such in the line
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "integration_traffic.txt")
     if os.path.exists(tpath):
@@ -699,9 +749,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        fps_cpu, done, cores = cpu_oracle(cfg, depth, rgb, args.cpu_frames, budget_s=45.0)
-        cpu = {"value": fps_cpu, "unit": "frames/s", "cores": cores, "kind": "port",
-               "sample": f"FP64 oracle, first {done} frames of the same sequence (frame 0 initialises the map)"}
+        cpu = cpu_baseline_child(W, K)
 
     value = aggregate_value(K, world, ms)
     lat_ms = np.array(lat) * 1000.0
@@ -728,6 +776,8 @@ def main():
         "gpu_launches": int(launches),
         "roofline": {"kernel": "k_integrate", "bound": "hbm", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "traffic_source": "scaled: ncu DRAM bytes per visible block of one full-size launch "
+                                       "(profiles/integration_traffic.txt) x this run's mean visible blocks",
                      "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms},
         "cpu_baseline": cpu,
         "clocks": ck,

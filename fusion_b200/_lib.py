@@ -86,7 +86,6 @@ SIGNATURES = {
     "fb_get_pose": (_i, [_vp, _vp]),
     "fb_session_set_profiling": (_i, [_vp, _i]),
     "fb_session_set_graphs": (_i, [_vp, _i]),
-    "fb_session_set_persistent": (_i, [_vp, _i]),
     "fb_session_stage_times": (_i, [_vp, _vp, _vp, _i]),
     "fb_session_set_raycast_tile": (_i, [_vp, _i, _i]),
     "fb_session_prepare": (_i, [_vp, _i]),

@@ -1,7 +1,6 @@
 """Builds the native libraries of the package in-tree:
 
   fusion_b200/libfusion_b200.so  CUDA kernels + C ABI (nvcc, sm_100a)
-  fusion_b200/libfbsynth.so      seeded synthetic RGB-D generator (g++, OpenMP)
 
     python -m fusion_b200.build
 
@@ -20,11 +19,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
-CU_SOURCES = ["preprocess.cu", "track.cu", "map.cu", "raycast.cu", "session.cu", "shade.cu", "static_scratch.cu", "mesh.cu", "keypoints.cu"]
+CU_SOURCES = ["preprocess.cu", "track.cu", "map.cu", "raycast.cu", "session.cu", "keyframe_track.cu", "stage_api.cu",
+              "persist.cu", "batch_step.cu", "shade.cu", "static_scratch.cu", "mesh.cu", "keypoints.cu"]
 EXTRA_FLAGS = {"track.cu": ["-fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = os.path.join(HERE, "libfusion_b200.so")
-SYNTH = os.path.join(HERE, "libfbsynth.so")
 
 
 def _nvcc():
@@ -55,6 +54,7 @@ def _compile(src, verbose):
 def build_cuda(force=False, verbose=False):
     srcs = [os.path.join(CSRC, s) for s in CU_SOURCES]
     deps = srcs + [os.path.join(CSRC, "fb_common.cuh"), os.path.join(CSRC, "fb_internal.h"),
+                   os.path.join(CSRC, "session_internal.h"),
                    os.path.join(ROOT, "include", "fusion_b200.h"), os.path.abspath(__file__)]
     if not force and _newer(LIB, deps):
         return LIB
@@ -68,19 +68,7 @@ def build_cuda(force=False, verbose=False):
     return LIB
 
 
-def build_synth(force=False):
-    src = os.path.join(CSRC, "synth", "synth.cpp")
-    deps = [src, os.path.join(CSRC, "synth", "synth.h")]
-    if not force and _newer(SYNTH, deps):
-        return SYNTH
-    # the environment's CXX may lack OpenMP; the system g++ has it
-    subprocess.check_call(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
-                           "-o", SYNTH, src])
-    return SYNTH
-
-
 def build_all(force=False, verbose=False):
-    build_synth(force)
     build_cuda(force, verbose)
 
 

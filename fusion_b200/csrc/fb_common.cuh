@@ -156,7 +156,6 @@ enum ErrFlag : uint32_t {
     kErrNewListFull = 1u << 4,        // more new blocks in one frame than the pool
     kErrVisibleFull = 1u << 5,        // visible list capacity exceeded
     kErrSequentialInsert = 1u << 6,   // slow exact path taken (heap/excess edge cases)
-    kErrTimeout = 1u << 7,            // a bounded device wait gave up (frame not tracked)
 };
 
 }  // namespace fb

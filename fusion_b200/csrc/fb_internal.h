@@ -62,23 +62,8 @@ struct TrackState {
     float2 grp_rgb2[kTrackMaxGroups][32];
 };
 
-// All levels of one frame for the persistent tracking kernel.
-struct TrackFrame {
-    TrackLevel L[3];
-    int iters[3];
-    int min_count[3];
-    int last_level;
-    TrackState* st;
-    float* partials;       // 2 x kTrackMaxBlocks x 32 floats
-    int* residual;         // W0 x H0 ints (per-pixel correspondences)
-    unsigned int* bar;     // grid barrier: count, generation
-    int* err;              // barrier timeout flag
-};
-
 int track_grid(int n);
 int track_cluster_grid(int n);   // track_grid rounded up to whole clusters
-int track_frame_grid();
-int launch_track_frame(const TrackFrame& F, int grid, cudaStream_t s);
 int launch_track_begin(TrackState* st, cudaStream_t s);
 // residual: per-warp compact segments of photometric correspondences
 // (int2: pixel, packed last pixel + difference), capacity track_list_capacity;

@@ -511,30 +511,6 @@ __device__ void reduce_partials(const float* __restrict__ partials, int nb, int 
     }
 }
 
-// As reduce_partials, reading partials written by other blocks of the same
-// (cooperative) launch through L2.
-__device__ void reduce_partials_cg(const float* partials, int nb, int stride, int nv, double* out,
-                                   double* scratch) {
-    const int v = threadIdx.x & 31, c = threadIdx.x >> 5, nc = blockDim.x >> 5;
-    const int per = (nb + nc - 1) / nc;
-    for (int v0 = 0; v0 < nv; v0 += 32) {
-        double s = 0;
-        if (v0 + v < nv) {
-            const int b0 = c * per, b1 = min(nb, b0 + per);
-#pragma unroll 8
-            for (int b = b0; b < b1; ++b) s += (double)__ldcg(partials + (size_t)b * stride + v0 + v);
-        }
-        scratch[c * 32 + v] = s;
-        __syncthreads();
-        if (c == 0 && v0 + v < nv) {
-            double t = 0;
-            for (int q = 0; q < nc; ++q) t += scratch[q * 32 + v];
-            out[v0 + v] = t;
-        }
-        __syncthreads();
-    }
-}
-
 // Capacity of the per-warp correspondence segments for n pixels: every warp
 // of the pass-A grid gets as many slots as the pixels it visits.
 size_t track_list_capacity(int n) {
@@ -1173,150 +1149,6 @@ __device__ __forceinline__ void solve_step(TrackState* st, const double* s, int 
     __threadfence();
 }
 
-// ----------------------------------------------------- persistent tracking
-
-// Grid-wide barrier for a cooperative launch (all blocks co-resident).  The
-// wait is bounded: after kBarrierSpins polls the block records a timeout in
-// *err and returns false, and every later barrier returns false at once, so
-// the kernel ends instead of hanging.
-constexpr long long kBarrierSpins = 1ll << 24;   // ~1 s of 64 ns sleeps
-
-__device__ __forceinline__ bool grid_sync(unsigned int* bar, int* err) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned int* gen = bar + 1;
-        int ok = *(volatile int*)err == 0;
-        if (ok) {
-            const unsigned int g = *gen;
-            __threadfence();
-            const unsigned int arrived = atomicAdd(bar, 1u) + 1;
-            if (arrived == gridDim.x) {
-                bar[0] = 0;
-                __threadfence();
-                atomicAdd(bar + 1, 1u);
-            } else {
-                long long spins = 0;
-                while (*gen == g) {
-                    if (++spins > kBarrierSpins || *(volatile int*)err) {
-                        atomicExch(err, 1);
-                        ok = 0;
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-            }
-            __threadfence();
-        }
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok;
-}
-
-__device__ __forceinline__ DevPose load_pose_cg(const DevPose* p) {
-    DevPose d;
-    const float* src = (const float*)p;
-    float* dst = (float*)&d;
-#pragma unroll
-    for (int i = 0; i < (int)(sizeof(DevPose) / 4); ++i) dst[i] = __ldcg(src + i);
-    return d;
-}
-
-// Tracker::ComputeSE3 for one frame in a single cooperative launch: for every
-// level and iteration, pass A (ICP rows + RGB correspondences), pass B (RGB
-// rows), then block 0 reduces both passes in FP64 and solves; three grid
-// barriers per iteration.  Same arithmetic as k_track_a / k_track_b /
-// the staged solve of k_track_b.
-__global__ void __launch_bounds__(256, 2) k_track_frame(TrackFrame F) {
-    __shared__ float sm[32 * 29];
-    __shared__ long long smll[32];
-    __shared__ double scratch[8 * 32];
-    __shared__ double sums[64];
-    __shared__ float s_sigma;
-    TrackState* st = F.st;
-    const int G = gridDim.x;
-    float* icpp = F.partials;
-    float* rgbp = F.partials + (size_t)kTrackMaxBlocks * 32;
-    if (__ldcg(&st->failed)) return;
-    for (int l = 2; l >= 0; --l) {
-        const TrackLevel& L = F.L[l];
-        const int N = L.W * L.H;
-        for (int it = 0; it < F.iters[l]; ++it) {
-            const DevPose cur = load_pose_cg(&st->cur), last = load_pose_cg(&st->last);
-            // pass A
-            float acc[29];
-#pragma unroll
-            for (int k = 0; k < 29; ++k) acc[k] = 0.f;
-            long long rc = 0, rsq = 0;
-            for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += G * blockDim.x) {
-                const int y = p / L.W, x = p - y * L.W;
-                float row[7];
-                if (icp_row(L, cur, last, x, y, row)) add_products(row, acc);
-                int r = rgb_corresp(L, cur, last, x, y);
-                F.residual[p] = r;
-                if (r >= 0) {
-                    int d = (r & 511) - 255;
-                    rc += 1;
-                    rsq += d * d;
-                }
-            }
-            block_sum<29>(acc, sm);
-            long long bc = block_sum_ll(rc, smll);
-            long long bs = block_sum_ll(rsq, smll);
-            if (threadIdx.x == 0) {
-#pragma unroll
-                for (int k = 0; k < 29; ++k) icpp[(size_t)blockIdx.x * 32 + k] = acc[k];
-                st->scratch_cnt[blockIdx.x] = bc;
-                st->scratch_sq[blockIdx.x] = bs;
-            }
-            if (!grid_sync(F.bar, F.err)) return;
-            // pass B: sigma from every block's counts, in block order
-            long long c = 0, q = 0;
-            for (int b = threadIdx.x; b < G; b += blockDim.x) {
-                c += __ldcg(&st->scratch_cnt[b]);
-                q += __ldcg(&st->scratch_sq[b]);
-            }
-            c = block_sum_ll(c, smll);
-            q = block_sum_ll(q, smll);
-            if (threadIdx.x == 0) s_sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
-            __syncthreads();
-            const float sigma = s_sigma;
-#pragma unroll
-            for (int k = 0; k < 29; ++k) acc[k] = 0.f;
-            for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += G * blockDim.x) {
-                int r = F.residual[p];
-                if (r < 0) continue;
-                const int y = p / L.W, x = p - y * L.W;
-                float row[7];
-                rgb_row(L, cur, last, x, y, r, sigma, row);
-                add_products(row, acc);
-            }
-            block_sum<29>(acc, sm);
-            if (threadIdx.x == 0)
-#pragma unroll
-                for (int k = 0; k < 29; ++k) rgbp[(size_t)blockIdx.x * 32 + k] = acc[k];
-            if (!grid_sync(F.bar, F.err)) return;
-            if (blockIdx.x == 0) {
-                reduce_partials_cg(icpp, G, 32, 29, sums, scratch);
-                reduce_partials_cg(rgbp, G, 32, 29, sums + 32, scratch);
-                if (threadIdx.x < 29) {
-                    st->icp_sums[threadIdx.x] = sums[threadIdx.x];
-                    st->rgb_sums[threadIdx.x] = sums[32 + threadIdx.x];
-                }
-                if (threadIdx.x == 0) {
-                    st->rgb_cnt = c;
-                    st->rgb_sq = q;
-                    st->sigma = sigma;
-                    solve_step(st, sums, F.min_count[l], l == F.last_level && it == F.iters[l] - 1);
-                }
-            }
-            if (!grid_sync(F.bar, F.err)) return;
-            if (__ldcg(&st->failed)) return;
-        }
-    }
-}
-
 // Single-step entry points (the reference's ICPStep / RGBStep): reduce the
 // sums of one pass into out[29] (+ rgb count / sum of squares) in FP64.
 __global__ void __launch_bounds__(256) k_step_icp(TrackLevel L, DevPose cur, DevPose last, float* partials,
@@ -1480,36 +1312,6 @@ int launch_track_iter(const TrackLevel& L, TrackState* st, unsigned int* tickets
         k_track_b<2, false><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, fin);
     }
     return 2;
-}
-
-// Occupancy-limited grid of the cooperative tracking kernel (0: unavailable).
-int track_frame_grid() {
-    static int g = -1;
-    if (g < 0) {
-        int dev = 0, sms = 0, coop = 0, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_track_frame, 256, 0) != cudaSuccess) per = 0;
-        if (per > 2) per = 2;
-        g = coop && per > 0 ? per * sms : 0;
-        if (g > kTrackMaxBlocks) g = kTrackMaxBlocks;
-    }
-    return g;
-}
-
-int launch_track_frame(const TrackFrame& F, int grid, cudaStream_t s) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(256);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_track_frame, F);
-    return 1;
 }
 
 int launch_step_icp(const TrackLevel& L, const DevPose& cur, const DevPose& last, float* partials,

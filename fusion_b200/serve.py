@@ -27,7 +27,9 @@ import time
 
 import numpy as np
 
-from . import _lib, synth
+import rgbd_synth as synth
+
+from . import _lib
 from .batch import RESOLUTIONS, Batch, mixed_config
 
 

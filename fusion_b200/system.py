@@ -246,8 +246,6 @@ class Session:
     def set_graphs(self, on=True):
         check("fb_session_set_graphs", self.lib.fb_session_set_graphs(self.h, 1 if on else 0))
 
-    def set_persistent(self, on=True):
-        check("fb_session_set_persistent", self.lib.fb_session_set_persistent(self.h, 1 if on else 0))
 
     def launch_count(self):
         n = ctypes.c_uint64()
@@ -431,10 +429,10 @@ def rgb_step(gcurr, glast, vcurr, vlast, dx, dy, Rcurr, RcurrInv, Rlast, RlastIn
 def rgb_step_static(gcurr, glast, vcurr, vlast, dx, dy, Rcurr, RcurrInv, Rlast, RlastInv, tcurr, tlast, K,
                     stream=None):
     """rgb_step without a scratch argument: for callers that cannot allocate
-    device memory where they track (inside a CUDA graph capture, a frame loop
-    that cannot wait for cudaFree, a host that owns all device memory).  The
+    device memory where they track (a frame loop that cannot wait for
+    cudaFree, a plug-in in a host that owns all device memory).  The
     library's own fixed device buffer limits images to 640 x 480 pixels, and
-    calls that overlap on the GPU share that buffer."""
+    calls that overlap on the GPU share that buffer.  Synchronous."""
     res = np.zeros(2, np.float32)
     A = np.zeros(36)
     b = np.zeros(6)

@@ -49,7 +49,7 @@ extern "C" {
 #define FB_ERR_NEW_LIST_FULL 0x10u    /* more new blocks in one frame than the pool */
 #define FB_ERR_VISIBLE_FULL 0x20u     /* visible list full */
 #define FB_ERR_SEQUENTIAL_INSERT 0x40u /* pool/excess edge case: exact sequential insert used */
-#define FB_ERR_TIMEOUT 0x80u          /* a bounded device-side wait gave up; the frame was not tracked */
+#define FB_ERR_TIMEOUT 0x80u          /* reserved: no kernel of this library waits on another */
 
 /* Runtime form of the reference's compile-time constants:
  * Mapping/DeviceMap.h:135-151 (voxel size, truncation, depth range, table
@@ -156,10 +156,6 @@ FB_API int fb_session_stage_times(fb_session* s, double* ms, uint64_t* calls, in
  * mode and frame parity, made on first use).  Off: kernels launched one by
  * one.  Profiled frames always launch kernels one by one. */
 FB_API int fb_session_set_graphs(fb_session* s, int on);
-/* Tracking as one cooperative (persistent) kernel per frame with bounded
- * grid barriers, or (default) as kernels per Gauss-Newton iteration launched
- * from the frame's CUDA graph.  Same arithmetic. */
-FB_API int fb_session_set_persistent(fb_session* s, int on);
 /* Kernels this session has launched so far. */
 FB_API int fb_session_launch_count(fb_session* s, uint64_t* launches);
 /* Bytes fb_grab_frame moves per frame with host inputs: h2d = depth + rgb,
@@ -326,16 +322,16 @@ FB_API int fb_rgb_step(const fb_image* gcurr, const fb_image* glast, const fb_im
                 size_t scratch_bytes, float residual[2], double A[36], double b[6], void* stream);
 
 /* No counterpart in the reference.  fb_rgb_step for callers that cannot
- * allocate device memory when they track a frame -- code recording a CUDA
- * graph (cudaMalloc is not allowed during stream capture), frame loops that
- * cannot pay for cudaFree's device-wide wait, hosts whose device memory all
- * belongs to their own allocator.  Same arguments without the scratch: the
- * library keeps 1.25 MiB of device memory per GPU for it, so images may have
- * at most fb_rgb_step_static_max_pixels() (640 x 480) pixels; larger ones are
- * rejected with FB_EINVAL.  The first call on a device looks up that memory's
- * address and must not happen during a stream capture.  Every call shares the
- * memory: calls that overlap on the GPU (other streams, unordered threads)
- * corrupt each other's results.  Synchronous. */
+ * allocate device memory when they track a frame -- frame loops that cannot
+ * pay for cudaFree's device-wide wait, plug-ins in hosts whose device memory
+ * all belongs to the host's own allocator.  Same arguments without the
+ * scratch: the library keeps 1.25 MiB of device memory per GPU for it, so
+ * images may have at most fb_rgb_step_static_max_pixels() (640 x 480)
+ * pixels; larger ones are rejected with FB_EINVAL.  The first call on a
+ * device looks up that memory's address and should come before any stream
+ * capture.  Every call shares the memory: calls that overlap on the GPU
+ * (other streams, unordered threads) corrupt each other's results.
+ * Synchronous: returns once the sums are on the host. */
 FB_API int fb_rgb_step_static(const fb_image* gcurr, const fb_image* glast, const fb_image* vcurr,
                               const fb_image* vlast, const fb_image* dx, const fb_image* dy,
                               const float Rcurr[9], const float RcurrInv[9], const float Rlast[9],

@@ -1,4 +1,4 @@
-"""Seeded synthetic RGB-D sequences (ctypes wrapper of csrc/synth/synth.cpp).
+"""Seeded synthetic RGB-D sequences (ctypes wrapper of rgbd_synth/synth.cpp).
 
 The sequences stand in for the recorded RGB-D sequence the reference reads
 (MainTum.cc:78-96) and for its live camera (Core/Camera.cc:117-144): u16 depth
@@ -38,7 +38,7 @@ def _lib():
     if _LIB is None:
         path = os.path.join(_HERE, "libfbsynth.so")
         if not os.path.exists(path):
-            raise RuntimeError(f"{path} is missing: run fusion_b200.build.build_all() first")
+            raise RuntimeError(f"{path} is missing: run `python -m rgbd_synth.build` first")
         lib = ctypes.CDLL(path)
         lib.fbs_default_params.argtypes = [ctypes.POINTER(SynthParams), ctypes.c_int,
                                            ctypes.c_int, ctypes.c_uint64]

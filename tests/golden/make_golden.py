@@ -8,7 +8,7 @@ Workload ("ref-default"): the reference's compile-time map constants
 1e6 buckets, 5e5 excess entries, 7e5 blocks) on a 128x96 narrow-field camera
 (fx = fy = 420, principal point at the centre) so that the fixtures stay small,
 depth scale 5000 and depth cutoff 3.0 m.  Frames come from the seeded
-generator in fusion_b200/csrc/synth.
+generator in rgbd_synth.
 
     python tests/golden/make_golden.py --out tests/golden
 """
@@ -22,7 +22,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 
-from fusion_b200 import synth  # noqa: E402
+import rgbd_synth as synth  # noqa: E402
 from oracle.refharness import RefHarness  # noqa: E402
 
 W, H = 128, 96

@@ -14,7 +14,7 @@ import hashlib
 import numpy as np
 import pytest
 
-from fusion_b200 import synth
+import rgbd_synth as synth
 from fusion_b200.invariants import check_session
 
 pytestmark = pytest.mark.gpu

@@ -6,7 +6,7 @@ depth range."""
 import numpy as np
 import pytest
 
-from fusion_b200 import synth
+import rgbd_synth as synth
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu

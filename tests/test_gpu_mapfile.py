@@ -20,7 +20,7 @@ import shutil
 import numpy as np
 import pytest
 
-from fusion_b200 import synth
+import rgbd_synth as synth
 
 pytestmark = pytest.mark.gpu
 

@@ -13,7 +13,7 @@ The bounds are the measured values with headroom (printed by the test).
 import numpy as np
 import pytest
 
-from fusion_b200 import synth
+import rgbd_synth as synth
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu

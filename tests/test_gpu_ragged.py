@@ -9,7 +9,7 @@ oracle: bit for bit, except the bilateral filter (CUDA's expf vs the host's:
 import numpy as np
 import pytest
 
-from fusion_b200 import synth
+import rgbd_synth as synth
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu

@@ -13,7 +13,7 @@ shading of those maps."""
 import numpy as np
 import pytest
 
-from fusion_b200 import synth
+import rgbd_synth as synth
 
 pytestmark = pytest.mark.gpu
 

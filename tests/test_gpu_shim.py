@@ -15,7 +15,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from fusion_b200 import synth
+import rgbd_synth as synth
 
 pytestmark = pytest.mark.gpu
 

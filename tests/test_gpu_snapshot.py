@@ -8,7 +8,7 @@ import hashlib
 import numpy as np
 import pytest
 
-from fusion_b200 import synth
+import rgbd_synth as synth
 
 pytestmark = pytest.mark.gpu
 

@@ -5,7 +5,7 @@ when none is staged is refused."""
 import numpy as np
 import pytest
 
-from fusion_b200 import synth
+import rgbd_synth as synth
 
 pytestmark = pytest.mark.gpu
 

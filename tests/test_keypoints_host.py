@@ -6,7 +6,8 @@ import math
 
 import numpy as np
 
-from fusion_b200 import mixed_config, synth
+import rgbd_synth as synth
+from fusion_b200 import mixed_config
 from fusion_b200.system import pose_estimate
 from oracle import keypoints as OK
 from oracle import oracle as O

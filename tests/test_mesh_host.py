@@ -16,7 +16,7 @@ import collections
 import numpy as np
 import pytest
 
-from fusion_b200 import synth
+import rgbd_synth as synth
 from fusion_b200.system import mesh_case_table, write_ply
 from oracle import oracle as O
 

@@ -26,7 +26,7 @@ def _worker(rank, world, port, out):
     sys.path.insert(0, ROOT)
     import bench
     import torch.distributed as dist
-    from fusion_b200 import synth
+    import rgbd_synth as synth
     r, w, _ = bench.dist_setup(world)
     bench.barrier(w)
     ms = bench.max_over_ranks(100.0 + 10.0 * r, w)       # each rank's device time

@@ -17,7 +17,20 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = os.environ.get("FB_REFERENCE_DIR", "/root/reference")
+
+
+def _reference_dir():
+    """FB_REFERENCE_DIR, else the reference tree the last build() compiled
+    (recorded in oracle/_ref/REFERENCE_DIR); empty when neither exists."""
+    if os.environ.get("FB_REFERENCE_DIR"):
+        return os.environ["FB_REFERENCE_DIR"]
+    rec = os.path.join(ROOT, "oracle", "_ref", "REFERENCE_DIR")
+    if os.path.exists(rec):
+        return open(rec).read().strip()
+    return ""
+
+
+REF = _reference_dir()
 LIB = os.path.join(ROOT, "fusion_b200", "libfusion_b200.so")
 
 TU = r"""

@@ -1,4 +1,4 @@
-"""The seeded synthetic RGB-D generator (fusion_b200/csrc/synth) against its
+"""The seeded synthetic RGB-D generator (rgbd_synth) against its
 specification, on the host: seeds are splitmix64(config << 32 | session),
 sequences are deterministic, depth is u16 in 1/5000 m quantised to 1 mm,
 valid depths lie in 0.3-4 m, about 2 % of them drop out to 0, the noise has
@@ -6,7 +6,7 @@ the Kinect-like sigma 0.0012 + 0.0019 (z - 0.4)^2 m, and the camera moves at
 most 0.5 m/s and 30 deg/s at 30 Hz."""
 import numpy as np
 
-from fusion_b200 import synth
+import rgbd_synth as synth
 
 M64 = (1 << 64) - 1
 
