@@ -99,6 +99,11 @@ int fb_resize_map(const fb_image* vsrc, const fb_image* nsrc, fb_image* vdst, fb
     return check_launch();
 }
 
+int fb_track_reduction_grid(int pixels) {
+    if (pixels <= 0) return 0;
+    return track_cluster_grid(pixels);
+}
+
 size_t fb_step_scratch_bytes(int cols, int rows) {
     if (cols <= 0 || rows <= 0) return 0;
     // partials | tickets | out sums (32 doubles) | per-pixel correspondences

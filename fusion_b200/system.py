@@ -448,6 +448,12 @@ def step_scratch_bytes(cols, rows):
     return int(_lib.load().fb_step_scratch_bytes(cols, rows))
 
 
+def track_reduction_grids(cfg):
+    """The tracking kernels' grid at each pyramid level of cfg's camera
+    (fb_track_reduction_grid): the summation order of the normal equations."""
+    return tuple(int(_lib.load().fb_track_reduction_grid((cfg.width >> l) * (cfg.height >> l))) for l in range(3))
+
+
 def pose_parts(T):
     """Matrix3f rotation, its transpose and translation of a 4x4 pose, as
     Frame::GpuRotation / GpuInvRotation / GpuTranslation round them."""

@@ -303,6 +303,13 @@ FB_API int fb_resize_map(const fb_image* vsrc, const fb_image* nsrc, fb_image* v
  * (Tracking/Tracking.cc:29-34, Reduction.cu:572). */
 FB_API size_t fb_step_scratch_bytes(int cols, int rows);
 
+/* No counterpart in the reference.  The grid (blocks of 256 threads, a
+ * multiple of 4) of a session's per-iteration tracking kernels at a pyramid
+ * level of `pixels` pixels on the current device.  The normal equations are
+ * summed in a fixed order that depends only on this number, so a checker can
+ * sum in the same order and compare the tracker bit for bit.  0 on error. */
+FB_API int fb_track_reduction_grid(int pixels);
+
 /* Replaces: ICPStep (Tracking/Reduction.cu:319-375).  R* are row-major 3x3
  * (Matrix3f), t* 3-vectors, K = {fx, fy, cx, cy} of the level.  Outputs on
  * the host as the reference's: residual = {sum of squared point-to-plane

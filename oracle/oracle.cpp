@@ -265,52 +265,115 @@ void reduce_rows(int H, int nsum, double* out, F&& row_fn) {
         for (int k = 0; k < nsum; ++k) out[k] += part[(size_t)y * nsum + k];
 }
 
-// ICPReduce::searchPoint / getRow (Tracking/Reduction.cu:227-286), ICPStep
-// (Reduction.cu:319-375: angleThresh 0.6, distThresh 0.1)
+// ICPReduce::searchPoint / getRow (Tracking/Reduction.cu:227-286) of pixel
+// (x, y): the 7-wide point-to-plane row, or false without a correspondence
+// (ICPStep's angleThresh 0.6 and distThresh 0.1, Reduction.cu:319-375).
+template <class R>
+bool icp_pixel(int W, int H, const float* vc, const float* vl, const float* nc, const float* nl, const M3<R>& Rc,
+               const M3<R>& Rl, const M3<R>& RlInv, const V3<R>& tc, const V3<R>& tl, float fx, float fy, float cx,
+               float cy, int x, int y, R row[7]) {
+    const R angleThresh = (R)0.6f, distThresh = (R)0.1f;
+    size_t i = (size_t)y * W + x;
+    V3<R> vcurr_c = xyz(cv4<R>(ld4(vc, i)));
+    if (isnan_(vcurr_c.x) || (double)vcurr_c.z < 1e-3) return false;
+    V3<R> vcurr_g = add(mv(Rc, vcurr_c), tc);
+    V3<R> vcurr_p = mv(RlInv, sub(vcurr_g, tl));
+    R invz = (R)(1.0 / (double)vcurr_p.z);
+    int u = (int)((double)(vcurr_p.x * invz * (R)fx + (R)cx) + 0.5);
+    int v = (int)((double)(vcurr_p.y * invz * (R)fy + (R)cy) + 0.5);
+    if (u < 0 || v < 0 || u >= W || v >= H) return false;
+    size_t j = (size_t)v * W + u;
+    V3<R> vlast_c = xyz(cv4<R>(ld4(vl, j)));
+    V3<R> vlast_g = add(mv(Rl, vlast_c), tl);
+    V3<R> ncurr_c = xyz(cv4<R>(ld4(nc, i)));
+    V3<R> ncurr_g = mv(Rc, ncurr_c);
+    V3<R> nlast_c = xyz(cv4<R>(ld4(nl, j)));
+    V3<R> nlast_g = mv(Rl, nlast_c);
+    R dist = norm3(sub(vlast_g, vcurr_g));
+    R sine = norm3(cross(ncurr_g, nlast_g));
+    if (!(sine < angleThresh && dist <= distThresh && !isnan_(ncurr_c.x) && !isnan_(nlast_c.x))) return false;
+    V3<R> nlast = mv(RlInv, nlast_g);
+    V3<R> vcurr = mv(RlInv, sub(vcurr_g, tl));
+    V3<R> vlast = mv(RlInv, sub(vlast_g, tl));
+    V3<R> a = neg(nlast), b = cross(nlast, vlast);
+    row[0] = a.x; row[1] = a.y; row[2] = a.z; row[3] = b.x; row[4] = b.y; row[5] = b.z;
+    row[6] = dot3(neg(nlast), sub(vcurr, vlast));
+    return true;
+}
+
+// ICPStep (Reduction.cu:319-375): the 29 sums of all pixels' rows.
 template <class R>
 void icp_step(int W, int H, const float* vc, const float* vl, const float* nc, const float* nl,
               const double* Tc, const double* Tl, float fx, float fy, float cx, float cy,
               double* sums) {
     const M3<R> Rc = rot<R>(Tc), Rl = rot<R>(Tl), RlInv = rot_inv<R>(Tl);
     const V3<R> tc = trans<R>(Tc), tl = trans<R>(Tl);
-    const R angleThresh = (R)0.6f, distThresh = (R)0.1f;
     reduce_rows(H, 29, sums, [&](int y, double* s) {
         for (int x = 0; x < W; ++x) {
-            size_t i = (size_t)y * W + x;
-            V3<R> vcurr_c = xyz(cv4<R>(ld4(vc, i)));
-            if (isnan_(vcurr_c.x) || (double)vcurr_c.z < 1e-3) continue;
-            V3<R> vcurr_g = add(mv(Rc, vcurr_c), tc);
-            V3<R> vcurr_p = mv(RlInv, sub(vcurr_g, tl));
-            R invz = (R)(1.0 / (double)vcurr_p.z);
-            int u = (int)((double)(vcurr_p.x * invz * (R)fx + (R)cx) + 0.5);
-            int v = (int)((double)(vcurr_p.y * invz * (R)fy + (R)cy) + 0.5);
-            if (u < 0 || v < 0 || u >= W || v >= H) continue;
-            size_t j = (size_t)v * W + u;
-            V3<R> vlast_c = xyz(cv4<R>(ld4(vl, j)));
-            V3<R> vlast_g = add(mv(Rl, vlast_c), tl);
-            V3<R> ncurr_c = xyz(cv4<R>(ld4(nc, i)));
-            V3<R> ncurr_g = mv(Rc, ncurr_c);
-            V3<R> nlast_c = xyz(cv4<R>(ld4(nl, j)));
-            V3<R> nlast_g = mv(Rl, nlast_c);
-            R dist = norm3(sub(vlast_g, vcurr_g));
-            R sine = norm3(cross(ncurr_g, nlast_g));
-            if (!(sine < angleThresh && dist <= distThresh && !isnan_(ncurr_c.x) &&
-                  !isnan_(nlast_c.x)))
-                continue;
-            V3<R> nlast = mv(RlInv, nlast_g);
-            V3<R> vcurr = mv(RlInv, sub(vcurr_g, tl));
-            V3<R> vlast = mv(RlInv, sub(vlast_g, tl));
-            V3<R> a = neg(nlast), b = cross(nlast, vlast);
-            R row[7] = {a.x, a.y, a.z, b.x, b.y, b.z, dot3(neg(nlast), sub(vcurr, vlast))};
+            R row[7];
+            if (!icp_pixel<R>(W, H, vc, vl, nc, nl, Rc, Rl, RlInv, tc, tl, fx, fy, cx, cy, x, y, row)) continue;
             add_products(row, s);
             s[28] += 1;
         }
     });
 }
 
-// RGBReduction::FindCorresp / GetRow (Tracking/Reduction.cu:404-508), RGBStep
-// (Reduction.cu:547-627).  The two integer sums are kept in 64 bits (the
-// reference sums diff^2 in int32 and would wrap beyond 2^31).
+// RGBReduction::FindCorresp (Tracking/Reduction.cu:404-451) of pixel (x, y):
+// the last-frame pixel and the intensity difference, or false.
+struct RgbCorr { int diff; int cx, cy, lx, ly; };
+
+template <class R>
+bool rgb_corresp(int W, int H, const uint8_t* gc, const uint8_t* gl, const float* vc, const float* vl,
+                 const int16_t* dxm, const int16_t* dym, const M3<R>& Rc, const M3<R>& RlInv, const V3<R>& tc,
+                 const V3<R>& tl, float fx, float fy, float cx, float cy, int x, int y, RgbCorr& r) {
+    size_t k = (size_t)y * W + x;
+    if (!(x >= 5 && x < W - 5 && y >= 5 && y < H - 5)) return false;
+    for (int u = std::max(y - 2, 0); u < std::min(y + 2, H); ++u)
+        for (int v = std::max(x - 2, 0); v < std::min(x + 2, W); ++v)
+            if (!(gc[u * W + v] > 0)) return false;
+    int gx = dxm[k], gy = dym[k];
+    if (!(std::sqrt((float)(gx * gx + gy * gy)) > 0)) return false;
+    V4<R> vcurr = cv4<R>(ld4(vc, k));
+    if (isnan_(vcurr.x)) return false;
+    V3<R> vcurr_g = add(mv(Rc, xyz(vcurr)), tc);
+    V3<R> vcl = mv(RlInv, sub(vcurr_g, tl));
+    R pu = (R)fx * vcl.x / vcl.z + (R)cx;
+    R pv = (R)fy * vcl.y / vcl.z + (R)cy;
+    int u = (int)std::floor((R)((double)pu + 0.5));
+    int v = (int)std::floor((R)((double)pv + 0.5));
+    if (!(u >= 0 && v >= 0 && u < W && v < H)) return false;
+    size_t j = (size_t)v * W + u;
+    V4<R> vlast = cv4<R>(ld4(vl, j));
+    V4<R> dd = {vlast.x - vcurr.x, vlast.y - vcurr.y, vlast.z - vcurr.z, vlast.w - vcurr.w};
+    if (!(!isnan_(vlast.x) && (double)norm4(dd) < 0.1 && gl[j] != 0)) return false;
+    r.diff = (int)gc[k] - (int)gl[j];
+    r.cx = x; r.cy = y; r.lx = u; r.ly = v;
+    return true;
+}
+
+// RGBReduction::GetRow (Reduction.cu:471-508) of one correspondence.
+template <class R>
+void rgb_row(int W, const float* vl, const int16_t* dxm, const int16_t* dym, const M3<R>& RcInv, const M3<R>& Rl,
+             const V3<R>& tc, const V3<R>& tl, float fx, float fy, float sigma, const RgbCorr& r, R row[7]) {
+    R w = (R)sigma + (R)std::abs(r.diff);
+    w = (double)w < 1e-3 ? (R)1 : (R)1 / w;
+    if ((double)sigma < 1e-6) w = 1;
+    V3<R> vlast = xyz(cv4<R>(ld4(vl, (size_t)r.ly * W + r.lx)));
+    V3<R> point = mv(RcInv, sub(add(mv(Rl, vlast), tl), tc));
+    R gx = (R)(float)((double)(float)dxm[(size_t)r.cy * W + r.cx] / 9.0);
+    R gy = (R)(float)((double)(float)dym[(size_t)r.cy * W + r.cx] / 9.0);
+    R invz = (R)1 / point.z;
+    V3<R> left;
+    left.x = gx * (R)fx * invz;
+    left.y = gy * (R)fy * invz;
+    left.z = -(left.x * point.x + left.y * point.y) * invz;
+    V3<R> a = mul(w, left), b = mul(w, cross(point, left));
+    row[0] = a.x; row[1] = a.y; row[2] = a.z; row[3] = b.x; row[4] = b.y; row[5] = b.z;
+    row[6] = -w * (R)r.diff;
+}
+
+// RGBStep (Reduction.cu:547-627).  The two integer sums are kept in 64 bits
+// (the reference sums diff^2 in int32 and would wrap beyond 2^31).
 template <class R>
 void rgb_step(int W, int H, const uint8_t* gc, const uint8_t* gl, const float* vc,
               const float* vl, const int16_t* dxm, const int16_t* dym, const double* Tc,
@@ -318,43 +381,20 @@ void rgb_step(int W, int H, const uint8_t* gc, const uint8_t* gl, const float* v
               int64_t* res2) {
     const M3<R> Rc = rot<R>(Tc), RcInv = rot_inv<R>(Tc), Rl = rot<R>(Tl), RlInv = rot_inv<R>(Tl);
     const V3<R> tc = trans<R>(Tc), tl = trans<R>(Tl);
-    struct Res { int diff; int cx, cy, lx, ly; };
-    std::vector<Res> res((size_t)W * H);
+    std::vector<RgbCorr> res((size_t)W * H);
     std::vector<unsigned char> valid((size_t)W * H, 0);
     std::vector<int64_t> rc((size_t)H * 2, 0);
 #pragma omp parallel for schedule(dynamic, 4)
     for (int y = 0; y < H; ++y) {
         for (int x = 0; x < W; ++x) {
             size_t k = (size_t)y * W + x;
-            if (!(x >= 5 && x < W - 5 && y >= 5 && y < H - 5)) continue;
-            bool ok = true;
-            for (int u = std::max(y - 2, 0); u < std::min(y + 2, H); ++u)
-                for (int v = std::max(x - 2, 0); v < std::min(x + 2, W); ++v)
-                    ok = ok && (gc[u * W + v] > 0);
-            if (!ok) continue;
-            int gx = dxm[k], gy = dym[k];
-            if (!(std::sqrt((float)(gx * gx + gy * gy)) > 0)) continue;
-            V4<R> vcurr = cv4<R>(ld4(vc, k));
-            if (isnan_(vcurr.x)) continue;
-            V3<R> vcurr_g = add(mv(Rc, xyz(vcurr)), tc);
-            V3<R> vcl = mv(RlInv, sub(vcurr_g, tl));
-            R pu = (R)fx * vcl.x / vcl.z + (R)cx;
-            R pv = (R)fy * vcl.y / vcl.z + (R)cy;
-            int u = (int)std::floor((R)((double)pu + 0.5));
-            int v = (int)std::floor((R)((double)pv + 0.5));
-            if (!(u >= 0 && v >= 0 && u < W && v < H)) continue;
-            size_t j = (size_t)v * W + u;
-            V4<R> vlast = cv4<R>(ld4(vl, j));
-            V4<R> dd = {vlast.x - vcurr.x, vlast.y - vcurr.y, vlast.z - vcurr.z, vlast.w - vcurr.w};
-            if (!isnan_(vlast.x) && (double)norm4(dd) < 0.1 && gl[j] != 0) {
-                Res r;
-                r.diff = (int)gc[k] - (int)gl[j];
-                r.cx = x; r.cy = y; r.lx = u; r.ly = v;
-                res[k] = r;
-                valid[k] = 1;
-                rc[(size_t)y * 2] += 1;
-                rc[(size_t)y * 2 + 1] += (int64_t)r.diff * r.diff;
-            }
+            RgbCorr r;
+            if (!rgb_corresp<R>(W, H, gc, gl, vc, vl, dxm, dym, Rc, RlInv, tc, tl, fx, fy, cx, cy, x, y, r))
+                continue;
+            res[k] = r;
+            valid[k] = 1;
+            rc[(size_t)y * 2] += 1;
+            rc[(size_t)y * 2 + 1] += (int64_t)r.diff * r.diff;
         }
     }
     res2[0] = res2[1] = 0;
@@ -365,26 +405,173 @@ void rgb_step(int W, int H, const uint8_t* gc, const uint8_t* gl, const float* v
         for (int x = 0; x < W; ++x) {
             size_t k = (size_t)y * W + x;
             if (!valid[k]) continue;
-            const Res& r = res[k];
-            R w = (R)sigma + (R)std::abs(r.diff);
-            w = (double)w < 1e-3 ? (R)1 : (R)1 / w;
-            if ((double)sigma < 1e-6) w = 1;
-            V3<R> vlast = xyz(cv4<R>(ld4(vl, (size_t)r.ly * W + r.lx)));
-            V3<R> point = mv(RcInv, sub(add(mv(Rl, vlast), tl), tc));
-            R gx = (R)(float)((double)(float)dxm[(size_t)r.cy * W + r.cx] / 9.0);
-            R gy = (R)(float)((double)(float)dym[(size_t)r.cy * W + r.cx] / 9.0);
-            R invz = (R)1 / point.z;
-            V3<R> left;
-            left.x = gx * (R)fx * invz;
-            left.y = gy * (R)fy * invz;
-            left.z = -(left.x * point.x + left.y * point.y) * invz;
-            V3<R> a = mul(w, left), b = mul(w, cross(point, left));
-            R row[7] = {a.x, a.y, a.z, b.x, b.y, b.z, -w * (R)r.diff};
+            R row[7];
+            rgb_row<R>(W, vl, dxm, dym, RcInv, Rl, tc, tl, fx, fy, sigma, res[k], row);
             add_products(row, s);
             s[28] += 1;
         }
     });
 }
+
+// ------------------------------------------- the GPU kernels' summation order
+//
+// Reference precision only.  The library's tracking kernels sum the 29
+// normal-equation values in a fixed order that depends only on the grid size
+// G (a multiple of 4 blocks of 256 threads; fb_track_reduction_grid reports
+// it per pyramid level):
+//   pass A (ICP rows): thread t of block b visits pixels p = 256 b + t +
+//     256 G k, k = 0, 1, ..., and adds each valid row's products into float
+//     accumulators (product rounded, then added);
+//   pass B (photometric rows): warp w of block b lists its correspondences in
+//     pass A's visiting order (k, then lane); lane l of that warp then adds
+//     the rows of entries l, l + 32, l + 64, ... in float;
+//   each block: a transposed butterfly over the warp's 32 lanes (at distance
+//     16, 8, 4, 2, 1 a lane keeps one half of its values and adds its
+//     partner's copy of that half), then the 8 warp sums in warp order (float,
+//     from 0);
+//   each cluster of 4 consecutive blocks: the block sums in rank order (FP64,
+//     from 0); then the NG = G / 4 cluster sums in four consecutive ranges of
+//     ceil(NG / 4) clusters (FP64, from 0), and the ranges added as
+//     ((r0 + r1) + r2) + r3.
+// Summing in that order makes the oracle's sums equal the GPU's bit for bit,
+// so the tracker can be compared bit for bit on every frame.
+namespace gpuorder {
+
+constexpr int kThreads = 256, kWarps = 8, kCluster = 4;
+
+// One block's sums of thread accumulators acc[256][29] (float).
+void block_sum(const float* acc, float* out) {
+    float bs[kWarps][32];
+    for (int w = 0; w < kWarps; ++w) {
+        float a[32][32];
+        int id[32][32];
+        for (int l = 0; l < 32; ++l)
+            for (int k = 0; k < 32; ++k) {
+                a[l][k] = k < 29 ? acc[(size_t)(w * 32 + l) * 29 + k] : 0.f;
+                id[l][k] = k;
+            }
+        for (int off = 16; off >= 1; off >>= 1) {
+            float na[32][16];
+            int nid[32][16];
+            for (int l = 0; l < 32; ++l) {
+                const bool up = (l & off) != 0;
+                const int p = l ^ off;
+                for (int k = 0; k < off; ++k) {
+                    const int q = up ? k + off : k;
+                    na[l][k] = a[l][q] + a[p][q];
+                    nid[l][k] = id[l][q];
+                }
+            }
+            for (int l = 0; l < 32; ++l)
+                for (int k = 0; k < off; ++k) {
+                    a[l][k] = na[l][k];
+                    id[l][k] = nid[l][k];
+                }
+        }
+        for (int l = 0; l < 32; ++l) bs[w][id[l][0]] = a[l][0];
+    }
+    for (int v = 0; v < 29; ++v) {
+        float r = 0.f;
+        for (int w = 0; w < kWarps; ++w) r += bs[w][v];
+        out[v] = r;
+    }
+}
+
+// The 29 sums of per-thread accumulators acc[G * 256][29].
+void grid_sum(const std::vector<float>& acc, int G, double* sums) {
+    std::vector<float> bsum((size_t)G * 29);
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < G; ++b) block_sum(&acc[(size_t)b * kThreads * 29], &bsum[(size_t)b * 29]);
+    const int NG = G / kCluster, per = (NG + 3) / 4;
+    for (int v = 0; v < 29; ++v) {
+        double part[4];
+        for (int q = 0; q < 4; ++q) {
+            double t = 0;
+            for (int g = q * per; g < std::min(NG, (q + 1) * per); ++g) {
+                double c = 0;
+                for (int r = 0; r < kCluster; ++r) c += (double)bsum[(size_t)(g * kCluster + r) * 29 + v];
+                t += c;
+            }
+            part[q] = t;
+        }
+        sums[v] = ((part[0] + part[1]) + part[2]) + part[3];
+    }
+}
+
+inline void add_row(const float row[7], float* acc) {
+    int n = 0;
+    for (int i = 0; i < 7; ++i)
+        for (int j = i; j < 7; ++j) acc[n++] += row[i] * row[j];
+    acc[28] += 1.0f;
+}
+
+void icp_step(int W, int H, const float* vc, const float* vl, const float* nc, const float* nl, const double* Tc,
+              const double* Tl, float fx, float fy, float cx, float cy, int G, double* sums) {
+    const M3<float> Rc = rot<float>(Tc), Rl = rot<float>(Tl), RlInv = rot_inv<float>(Tl);
+    const V3<float> tc = trans<float>(Tc), tl = trans<float>(Tl);
+    const int N = W * H, stride = G * kThreads, iters = (N + stride - 1) / stride;
+    std::vector<float> acc((size_t)stride * 29, 0.f);
+#pragma omp parallel for schedule(static)
+    for (int th = 0; th < stride; ++th) {
+        float* a = &acc[(size_t)th * 29];
+        for (int k = 0; k < iters; ++k) {
+            const int p = th + k * stride;
+            if (p >= N) break;
+            float row[7];
+            if (icp_pixel<float>(W, H, vc, vl, nc, nl, Rc, Rl, RlInv, tc, tl, fx, fy, cx, cy, p % W, p / W, row))
+                add_row(row, a);
+        }
+    }
+    grid_sum(acc, G, sums);
+}
+
+void rgb_step(int W, int H, const uint8_t* gc, const uint8_t* gl, const float* vc, const float* vl,
+              const int16_t* dxm, const int16_t* dym, const double* Tc, const double* Tl, float fx, float fy,
+              float cx, float cy, int G, double* sums, int64_t* res2) {
+    const M3<float> Rc = rot<float>(Tc), RcInv = rot_inv<float>(Tc), Rl = rot<float>(Tl),
+                    RlInv = rot_inv<float>(Tl);
+    const V3<float> tc = trans<float>(Tc), tl = trans<float>(Tl);
+    const int N = W * H, stride = G * kThreads, iters = (N + stride - 1) / stride;
+    const int nwarps = G * kWarps;
+    std::vector<std::vector<RgbCorr>> seg(nwarps);
+    std::vector<int64_t> cnt(nwarps, 0), sq(nwarps, 0);
+#pragma omp parallel for schedule(static)
+    for (int gw = 0; gw < nwarps; ++gw) {
+        const int b = gw / kWarps, w = gw % kWarps;
+        for (int k = 0; k < iters; ++k)
+            for (int lane = 0; lane < 32; ++lane) {
+                const int p = b * kThreads + w * 32 + lane + k * stride;
+                if (p >= N) continue;
+                RgbCorr r;
+                if (!rgb_corresp<float>(W, H, gc, gl, vc, vl, dxm, dym, Rc, RlInv, tc, tl, fx, fy, cx, cy, p % W,
+                                        p / W, r))
+                    continue;
+                seg[gw].push_back(r);
+                cnt[gw] += 1;
+                sq[gw] += (int64_t)r.diff * r.diff;
+            }
+    }
+    res2[0] = res2[1] = 0;
+    for (int gw = 0; gw < nwarps; ++gw) {
+        res2[0] += cnt[gw];
+        res2[1] += sq[gw];
+    }
+    const float sigma = std::sqrt((float)res2[1] / (float)(res2[0] == 0 ? 1 : res2[0]));
+    std::vector<float> acc((size_t)stride * 29, 0.f);
+#pragma omp parallel for schedule(static)
+    for (int gw = 0; gw < nwarps; ++gw)
+        for (int lane = 0; lane < 32; ++lane) {
+            float* a = &acc[(size_t)(gw * 32 + lane) * 29];
+            for (size_t i = lane; i < seg[gw].size(); i += 32) {
+                float row[7];
+                rgb_row<float>(W, vl, dxm, dym, RcInv, Rl, tc, tl, fx, fy, sigma, seg[gw][i], row);
+                add_row(row, a);
+            }
+        }
+    grid_sum(acc, G, sums);
+}
+
+}  // namespace gpuorder
 
 // ------------------------------------------------------------------- map --
 
@@ -913,8 +1100,12 @@ template <class R> void resize_images(Frame& f) {
                       f.lv[i].vmap.data(), f.lv[i].nmap.data());
 }
 
-// Tracker::ComputeSE3(false, ITERATIONS_SE3, THRESH_ICP_SE3) (Tracking.cc:296-409)
-template <class R> bool compute_se3(System& s) {
+// Tracker::ComputeSE3(false, ITERATIONS_SE3, THRESH_ICP_SE3) (Tracking.cc:296-409).
+// grid (reference precision only, else null): the library's tracking grid per
+// pyramid level; the normal equations are then summed in its kernels' order
+// (gpuorder above) and solved in its solver's order (pivot-free LDL^T, rigid
+// inverses), so that the result equals the library's bit for bit.
+template <class R> bool compute_se3(System& s, const int* grid = nullptr) {
     const int minCount[3] = {2000, 1000, 100};   // Tracking.h:102
     double lastPose[16], pose[16], delta[16];
     std::memcpy(lastPose, s.last->pose, sizeof lastPose);
@@ -926,9 +1117,14 @@ template <class R> bool compute_se3(System& s) {
         for (int j = 0; j < s.cfg.iters[i]; ++j) {
             double sr[29], si[29], Ar[36], br[6], Ai[36], bi[6];
             int64_t res2[2];
-            rgb_step<R>(N.W, N.H, N.image.data(), L.image.data(), N.vmap.data(), L.vmap.data(),
-                        N.dx.data(), N.dy.data(), s.next->pose, s.last->pose, s.fx(i), s.fy(i),
-                        s.cx(i), s.cy(i), sr, res2);
+            if (grid)
+                gpuorder::rgb_step(N.W, N.H, N.image.data(), L.image.data(), N.vmap.data(), L.vmap.data(),
+                                   N.dx.data(), N.dy.data(), s.next->pose, s.last->pose, s.fx(i), s.fy(i), s.cx(i),
+                                   s.cy(i), grid[i], sr, res2);
+            else
+                rgb_step<R>(N.W, N.H, N.image.data(), L.image.data(), N.vmap.data(), L.vmap.data(),
+                            N.dx.data(), N.dy.data(), s.next->pose, s.last->pose, s.fx(i), s.fy(i),
+                            s.cx(i), s.cy(i), sr, res2);
             float r0 = (float)sr[27], r1 = (float)sr[28];
             float rgbError = std::sqrt(r0) / r1;
             s.lastRgbError = rgbError;
@@ -937,8 +1133,12 @@ template <class R> bool compute_se3(System& s) {
                 std::memcpy(s.next->pose, lastPose, sizeof lastPose);
                 return false;
             }
-            icp_step<R>(N.W, N.H, N.vmap.data(), L.vmap.data(), N.nmap.data(), L.nmap.data(),
-                        s.next->pose, s.last->pose, s.fx(i), s.fy(i), s.cx(i), s.cy(i), si);
+            if (grid)
+                gpuorder::icp_step(N.W, N.H, N.vmap.data(), L.vmap.data(), N.nmap.data(), L.nmap.data(),
+                                   s.next->pose, s.last->pose, s.fx(i), s.fy(i), s.cx(i), s.cy(i), grid[i], si);
+            else
+                icp_step<R>(N.W, N.H, N.vmap.data(), L.vmap.data(), N.nmap.data(), L.nmap.data(),
+                            s.next->pose, s.last->pose, s.fx(i), s.fy(i), s.cx(i), s.cy(i), si);
             float q0 = (float)si[27], q1 = (float)si[28];
             icpError = std::sqrt(q0) / q1;
             s.lastIcpError = icpError;
@@ -953,15 +1153,24 @@ template <class R> bool compute_se3(System& s) {
             const float w = 1e-4f;
             for (int k = 0; k < 36; ++k) A[k] = Ar[k] * w + Ai[k];
             for (int k = 0; k < 6; ++k) b[k] = br[k] * w + bi[k];
-            fbo::ldlt_solve(A, b, xi);
+            if (grid)
+                fbo::ldlt_solve_nopivot(A, b, xi);
+            else
+                fbo::ldlt_solve(A, b, xi);
             fbo::se3_exp(xi, dT);
             fbo::mat4_mul(dT, delta, delta);
-            fbo::mat4_inv(delta, dinv);
+            if (grid)
+                fbo::mat4_rigid_inv(delta, dinv);
+            else
+                fbo::mat4_inv(delta, dinv);
             fbo::mat4_mul(lastPose, dinv, s.next->pose);
         }
     }
     double pinv[16], p[16];
-    fbo::mat4_inv(pose, pinv);
+    if (grid)
+        fbo::mat4_rigid_inv(pose, pinv);
+    else
+        fbo::mat4_inv(pose, pinv);
     fbo::mat4_mul(pinv, s.next->pose, p);
     double tn = std::sqrt(p[3] * p[3] + p[7] * p[7] + p[11] * p[11]);
     if (icpError < 0.0001f && fbo::euler_sin_norm(p) <= 0.1 && tn <= 0.1) return true;
@@ -1353,6 +1562,42 @@ int fbo_track(const fbo_config* c, const float* const* nv, const float* const* n
     std::memcpy(s.last->pose, last_pose, 16 * sizeof(double));
     std::memcpy(s.next->pose, last_pose, 16 * sizeof(double));
     bool ok = c->precision == 32 ? compute_se3<float>(s) : compute_se3<double>(s);
+    std::memcpy(out_pose, s.next->pose, 16 * sizeof(double));
+    if (info) {
+        info[0] = ok; info[1] = s.lastIcpError; info[2] = s.lastIcpCount; info[3] = s.lastRgbError;
+        info[4] = s.lastRgbCount;
+    }
+    return 0;
+}
+
+// fbo_track in reference precision with the normal equations summed and
+// solved in the order of the library's kernels for the tracking grid
+// grid[level] (see gpuorder).
+int fbo_track_gpu_order(const fbo_config* c, const int* grid, const float* const* nv, const float* const* nn,
+                        const uint8_t* const* ng, const int16_t* const* ndx, const int16_t* const* ndy,
+                        const float* const* lv, const float* const* ln, const uint8_t* const* lg,
+                        const double* last_pose, double* out_pose, double* info) {
+    fbo_config cc = *c;
+    cc.num_buckets = 1;
+    cc.num_excess = 0;
+    cc.num_blocks = 1;
+    System s(cc);
+    for (int l = 0; l < 3; ++l) {
+        if (c->iters[l] > 0 && (grid[l] <= 0 || grid[l] % gpuorder::kCluster)) return -1;
+        Level &N = s.next->lv[l], &L = s.last->lv[l];
+        size_t n = (size_t)N.W * N.H;
+        std::memcpy(N.vmap.data(), nv[l], 16 * n);
+        std::memcpy(N.nmap.data(), nn[l], 16 * n);
+        std::memcpy(N.image.data(), ng[l], n);
+        std::memcpy(N.dx.data(), ndx[l], 2 * n);
+        std::memcpy(N.dy.data(), ndy[l], 2 * n);
+        std::memcpy(L.vmap.data(), lv[l], 16 * n);
+        std::memcpy(L.nmap.data(), ln[l], 16 * n);
+        std::memcpy(L.image.data(), lg[l], n);
+    }
+    std::memcpy(s.last->pose, last_pose, 16 * sizeof(double));
+    std::memcpy(s.next->pose, last_pose, 16 * sizeof(double));
+    bool ok = compute_se3<float>(s, grid);
     std::memcpy(out_pose, s.next->pose, 16 * sizeof(double));
     if (info) {
         info[0] = ok; info[1] = s.lastIcpError; info[2] = s.lastIcpCount; info[3] = s.lastRgbError;

@@ -124,6 +124,15 @@ int fbo_track(const fbo_config* cfg, const float* const* next_vmap, const float*
               const int16_t* const* next_dy, const float* const* last_vmap,
               const float* const* last_nmap, const uint8_t* const* last_gray,
               const double* last_pose, double* out_pose, double* info);
+// fbo_track in reference precision, summing the normal equations in the order
+// of the library's tracking kernels for their grid size grid[level] (a
+// multiple of 4) and solving in its solver's order; -1 on a bad grid.
+int fbo_track_gpu_order(const fbo_config* cfg, const int* grid, const float* const* next_vmap,
+                        const float* const* next_nmap, const uint8_t* const* next_gray,
+                        const int16_t* const* next_dx, const int16_t* const* next_dy,
+                        const float* const* last_vmap, const float* const* last_nmap,
+                        const uint8_t* const* last_gray, const double* last_pose, double* out_pose,
+                        double* info);
 int fbo_num_threads(void);
 }
 

@@ -325,10 +325,13 @@ class System:
         return out
 
 
-def track(cfg, nxt, last, last_pose):
+def track(cfg, nxt, last, last_pose, grid=None):
     """Tracker::ComputeSE3 on given inputs.  nxt / last: lists of three dicts
     (levels 0-2) with vmap, nmap, image (+ dx, dy for nxt).  Returns
-    (pose, info[ok, icp_err, icp_count, rgb_err, rgb_count])."""
+    (pose, info[ok, icp_err, icp_count, rgb_err, rgb_count]).
+    grid (reference precision only): the library's tracking grid per level
+    (fb_track_reduction_grid); the normal equations are then summed and
+    solved in the order of its kernels, for a bit-for-bit comparison."""
     keep = []
 
     def arr(lst, key, dtype):
@@ -340,10 +343,17 @@ def track(cfg, nxt, last, last_pose):
         return ptrs
     out = np.zeros((4, 4), np.float64)
     info = np.zeros(5, np.float64)
-    lib().fbo_track(ctypes.byref(cfg), arr(nxt, "vmap", np.float32), arr(nxt, "nmap", np.float32),
-                    arr(nxt, "image", np.uint8), arr(nxt, "dx", np.int16), arr(nxt, "dy", np.int16),
-                    arr(last, "vmap", np.float32), arr(last, "nmap", np.float32), arr(last, "image", np.uint8),
-                    _p(np.ascontiguousarray(last_pose, np.float64)), _p(out), _p(info))
+    args = [arr(nxt, "vmap", np.float32), arr(nxt, "nmap", np.float32), arr(nxt, "image", np.uint8),
+            arr(nxt, "dx", np.int16), arr(nxt, "dy", np.int16), arr(last, "vmap", np.float32),
+            arr(last, "nmap", np.float32), arr(last, "image", np.uint8),
+            _p(np.ascontiguousarray(last_pose, np.float64)), _p(out), _p(info)]
+    if grid is None:
+        lib().fbo_track(ctypes.byref(cfg), *args)
+    else:
+        assert cfg.precision == 32, "the kernels' summation order is a reference-precision mode"
+        g = (ctypes.c_int * 3)(*[int(x) for x in grid])
+        if lib().fbo_track_gpu_order(ctypes.byref(cfg), g, *args) != 0:
+            raise ValueError(f"bad tracking grid {list(grid)}")
     return out, info
 
 

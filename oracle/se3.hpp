@@ -126,6 +126,38 @@ inline bool ldlt_solve(const double* Ain, const double* bin, double* x, int n = 
     return true;
 }
 
+// The same solve without pivoting, in the operation order of the library's
+// device solver (the normal matrix is symmetric positive definite, so no
+// pivot is needed): D and L column by column with L = t * (1 / d), forward
+// substitution, scaling by 1 / D, back substitution.  Used to compare the
+// library's tracker bit for bit.
+inline void ldlt_solve_nopivot(const double* A, const double* b, double* x) {
+    double L[6][6] = {}, D[6], Dinv[6], y[6];
+    for (int k = 0; k < 6; ++k) {
+        double d = A[k * 6 + k];
+        for (int j = 0; j < k; ++j) d -= L[k][j] * L[k][j] * D[j];
+        D[k] = d;
+        const double inv = 1.0 / d;
+        Dinv[k] = inv;
+        for (int i = k + 1; i < 6; ++i) {
+            double t = A[i * 6 + k];
+            for (int j = 0; j < k; ++j) t -= L[i][j] * L[k][j] * D[j];
+            L[i][k] = t * inv;
+        }
+    }
+    for (int i = 0; i < 6; ++i) {
+        double t = b[i];
+        for (int j = 0; j < i; ++j) t -= L[i][j] * y[j];
+        y[i] = t;
+    }
+    for (int i = 0; i < 6; ++i) y[i] *= Dinv[i];
+    for (int i = 5; i >= 0; --i) {
+        double t = y[i];
+        for (int j = i + 1; j < 6; ++j) t -= L[j][i] * x[j];
+        x[i] = t;
+    }
+}
+
 // exp of the se(3) tangent (upsilon[3], omega[3]) into a 4x4 row-major matrix.
 inline void se3_exp(const double* xi, double* T) {
     const double* u = xi;

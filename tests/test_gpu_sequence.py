@@ -4,17 +4,22 @@ oracle, through the C ABI session, on seeded synthetic sequences.
 Pose grading is teacher-forced: before each frame the GPU's model (the last
 frame's raycast maps and gray pyramid) and its last pose are handed to the
 oracle's ComputeSE3 together with the new frame's pyramid, so both trackers
-start from identical inputs.  Bars per frame: the same tracking outcome; pose
-within 1e-5 rad / 1e-5 m of the reference-precision oracle on the median
-frame and 5e-5 on every frame (the GPU sums in float trees where the oracle
-sums in double, so now and then one pixel lands on a neighbouring
-correspondence in one iteration); against the FP64
-oracle within 1e-5 on the median frame and 1e-3 on every frame.  (The
-reference's Gauss-Newton runs a fixed number of iterations and has not
-converged when it stops -- its last step is still ~1e-4 -- so rounding
-differences that flip a few pixel correspondences move its final pose by up
-to ~1e-4 on some frames: the oracle's own float and double modes differ by
-that much with identical inputs.)
+start from identical inputs.
+
+The reference-precision oracle sums the normal equations in the order of the
+library's tracking kernels (the grid per level comes from
+fb_track_reduction_grid) and solves them in its solver's order, so the GPU's
+tracker must agree with it bit for bit on every frame: the same outcome, the
+same correspondence counts, and the same pose up to the last bits of the
+host's and the device's sin / cos in the SE(3) exponential (bar 1e-12).
+
+Against the FP64 oracle the pose differences are a stated error, printed as
+a per-frame distribution; the bar is 1e-5 rad / 1e-5 m on every frame
+(measured: at most 2.2e-6 rad / 2.7e-6 m over the 50 full-size frames,
+8.8e-6 rad / 6.1e-6 m on the 320x240 case).  The reference's Gauss-Newton
+runs a fixed number of iterations and has not converged when it stops (its
+last step is still ~1e-4), so these are rounding differences that flip a few
+pixel correspondences, not a convergence tolerance.
 """
 import numpy as np
 import pytest
@@ -67,10 +72,12 @@ def _model(sess):
 
 def _teacher_forced(cfg, seed, n_frames):
     from fusion_b200 import Session
+    from fusion_b200 import system as S
     p = synth.params(cfg.width, cfg.height, seed, fx=cfg.fx, fy=cfg.fy, cx=cfg.cx, cy=cfg.cy,
                      depth_scale=cfg.depth_scale)
     depth, rgb, _ = synth.render(p, 0, n_frames)
     sess = Session(cfg)
+    grids = S.track_reduction_grids(cfg)
     c32, c64 = _oracle_cfg(cfg, 32), _oracle_cfg(cfg, 64)
     rows = []
     r = sess.grab(depth[0], rgb[0])
@@ -79,13 +86,13 @@ def _teacher_forced(cfg, seed, n_frames):
         last_pose = sess.pose()
         r = sess.grab(depth[k], rgb[k])
         frame = _frame_inputs(sess, cfg, 0 if r.tracked else 1)
-        P32, i32 = O.track(c32, frame, model, last_pose)
+        Pk, ik = O.track(c32, frame, model, last_pose, grid=grids)
         P64, i64 = O.track(c64, frame, model, last_pose)
         Pg = np.array(r.pose[:]).reshape(4, 4)
-        rows.append(dict(k=k, tracked=(int(r.tracked), int(i32[0]), int(i64[0])),
-                         rot32=rot_err(Pg, P32), t32=float(np.abs(Pg[:3, 3] - P32[:3, 3]).max()),
-                         rot64=rot_err(Pg, P64), t64=float(np.abs(Pg[:3, 3] - P64[:3, 3]).max()),
-                         icp=(r.icp_count, i32[2]), rgb=(r.rgb_count, i32[4])))
+        rows.append(dict(k=k, tracked=(int(r.tracked), int(ik[0]), int(i64[0])),
+                         exact=float(np.abs(Pg - Pk).max()),
+                         counts=((r.icp_count, ik[2]), (r.rgb_count, ik[4])),
+                         rot64=rot_err(Pg, P64), t64=float(np.abs(Pg[:3, 3] - P64[:3, 3]).max())))
     sess.close()
     return rows
 
@@ -93,8 +100,8 @@ def _teacher_forced(cfg, seed, n_frames):
 CASES = {
     # the reference's own constants on a 320x240 camera (fx = fy = 525)
     "ref_320x240": ("ref", 0x5EEDF00D, 8),
-    # the full-size plain configuration, 640x480, 5 mm voxels
-    "c2_640x480": ("c2", None, 5),
+    # the full-size plain configuration, 640x480, 5 mm voxels, 50 frames
+    "c2_640x480": ("c2", None, 51),
     # a ragged camera: levels 322x242, 161x121, 80x60 (odd sizes, rows and
     # columns that are not multiples of 8)
     "ragged_322x242": ("ragged", 0x0DDC0FFE, 6),
@@ -114,16 +121,23 @@ def test_teacher_forced_tracking(name):
         cfg = S.config_c2()
         seed = synth.session_seed(2, 0)
     rows = _teacher_forced(cfg, seed, n)
-    print(name, rows)
     for r in rows:
+        print(name, r)
+    for r in rows:
+        # the kernels' summation order: bit for bit
         assert r["tracked"][0] == r["tracked"][1], r
-        assert r["rot32"] <= 5e-5 and r["t32"] <= 5e-5, r
-        assert r["rot64"] <= 1e-3 and r["t64"] <= 1e-3, r
+        assert r["counts"][0][0] == r["counts"][0][1] and r["counts"][1][0] == r["counts"][1][1], r
+        assert r["exact"] <= 1e-12, r
     assert sum(r["tracked"][0] for r in rows) >= len(rows) - 1
-    assert np.median([r["rot32"] for r in rows]) <= 1e-5
-    assert np.median([r["t32"] for r in rows]) <= 1e-5
-    assert np.median([r["rot64"] for r in rows]) <= 1e-5
-    assert np.median([r["t64"] for r in rows]) <= 1e-5
+    both = [r for r in rows if r["tracked"][0] and r["tracked"][2]]
+    assert len(both) >= 0.9 * len(rows)
+    rot = np.array([r["rot64"] for r in both])
+    tra = np.array([r["t64"] for r in both])
+    print(name, "pose vs FP64 over %d frames: rotation median %.2e p90 %.2e max %.2e rad; translation median "
+          "%.2e p90 %.2e max %.2e m; frames within 1e-5: %d / %d" %
+          (len(both), np.median(rot), np.percentile(rot, 90), rot.max(), np.median(tra), np.percentile(tra, 90),
+           tra.max(), int(np.sum((rot <= 1e-5) & (tra <= 1e-5))), len(both)))
+    assert rot.max() <= 1e-5 and tra.max() <= 1e-5
 
 
 def test_c1_loses_tracking_like_the_oracle():
