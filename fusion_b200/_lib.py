@@ -14,7 +14,7 @@ FB_FORM_REFERENCE, FB_FORM_PRECISION = 0, 1
 
 ERR_FLAGS = {
     0x1: "heap_exhausted", 0x2: "excess_full", 0x4: "request_set_full", 0x8: "coord_range",
-    0x10: "new_list_full", 0x20: "visible_full", 0x40: "sequential_insert", 0x80: "timeout",
+    0x10: "new_list_full", 0x20: "visible_full", 0x40: "sequential_insert", 0x80: "timeout", 0x100: "normal_w",
 }
 
 

@@ -13,6 +13,7 @@
 #ifndef FB_COMMON_CUH
 #define FB_COMMON_CUH
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -121,11 +122,41 @@ struct __align__(8) Voxel {
     unsigned char r, g, b;
 };
 
-// Precision form: a voxel block is 3072 bytes, structure of arrays --
-// TSDF as FP16 [512] (bytes 0-1023), weight u8 [512] (1024-1535), red,
-// green, blue u8 [512] each (1536-3071).  6 bytes per voxel.
+// Precision form: a voxel block is 3072 bytes -- TSDF as FP16 [512] (bytes
+// 0-1023), then one 32-bit word per voxel [512] (1024-3071) holding red,
+// green, blue and the weight in bytes 0-3.  6 bytes per voxel.
 constexpr int kCBlockBytes = 3072;
-constexpr int kCWeight = 1024, kCRed = 1536, kCGreen = 2048, kCBlue = 2560;
+constexpr int kCRgbw = 1024;
+__host__ __device__ constexpr int c_red(int v) { return kCRgbw + 4 * v; }
+__host__ __device__ constexpr int c_green(int v) { return kCRgbw + 4 * v + 1; }
+__host__ __device__ constexpr int c_blue(int v) { return kCRgbw + 4 * v + 2; }
+__host__ __device__ constexpr int c_weight(int v) { return kCRgbw + 4 * v + 3; }
+
+// Per-pixel inputs of integration, made once per frame: {depth, n.x, n.y,
+// n.z} with the depth NaN where integrateColor (FuseMap.cu:140-191) skips the
+// pixel whatever the voxel -- depth NaN or outside [depth_min, depth_max], or
+// a NaN normal -- and the colour as one word r | g << 8 | b << 16.  The
+// floats are the raw depth and the normal unchanged, so both forms read them
+// in place of the three images.
+__device__ __forceinline__ void fuse_record(float dp, float4 n, const uint8_t* c3, float dmin, float dmax,
+                                            float4* rec, uint32_t* col) {
+    const bool ok = !(isnan(dp) || dp > dmax || dp < dmin) && !isnan(n.x);
+    *rec = make_float4(ok ? dp : qnan(), n.x, n.y, n.z);
+    *col = (uint32_t)c3[0] | (uint32_t)c3[1] << 8 | (uint32_t)c3[2] << 16;
+}
+
+// The precision form's fusion record: the same inputs in one 16-byte word,
+// so integration gathers once per voxel -- x: the depth (NaN where skipped),
+// y: n.x and n.y as FP16, z: n.z as FP16 | red << 16 | green << 24, w: blue.
+__device__ __forceinline__ void fuse_record_packed(float dp, float4 n, const uint8_t* c3, float dmin, float dmax,
+                                                   uint4* rec) {
+    const bool ok = !(isnan(dp) || dp > dmax || dp < dmin) && !isnan(n.x);
+    const __half2 nxy = __floats2half2_rn(n.x, n.y);
+    const __half nz = __float2half_rn(n.z);
+    *rec = make_uint4(__float_as_uint(ok ? dp : qnan()), *reinterpret_cast<const uint32_t*>(&nxy),
+                      (uint32_t)__half_as_ushort(nz) | (uint32_t)c3[0] << 16 | (uint32_t)c3[1] << 24,
+                      (uint32_t)c3[2]);
+}
 
 // Bucket of a block (Mapping/DeviceMap.cu:3-10): products wrap in 32 bits and
 // the modulo is unsigned because NumBuckets is an unsigned constant.
@@ -156,6 +187,8 @@ enum ErrFlag : uint32_t {
     kErrNewListFull = 1u << 4,        // more new blocks in one frame than the pool
     kErrVisibleFull = 1u << 5,        // visible list capacity exceeded
     kErrSequentialInsert = 1u << 6,   // slow exact path taken (heap/excess edge cases)
+    kErrTimeout = 1u << 7,            // a bounded device-side wait gave up (the kernel stopped early)
+    kErrNormalW = 1u << 8,            // a valid normal given to integration had a w lane other than 1
 };
 
 }  // namespace fb

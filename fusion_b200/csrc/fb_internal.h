@@ -86,9 +86,22 @@ int launch_level0(const uint16_t* depth, int dpitch, const uint8_t* rgb, int rgb
                    uint8_t* gray, int gpitch, cudaStream_t st);
 int launch_pyrdown(const float* sd, int sdp, const uint8_t* sg, int sgp, int SW, int SH, float* dd, int ddp,
                     uint8_t* dg, int dgp, cudaStream_t st);
+// Where the level-0 map kernel writes the fusion records of its pixels
+// (fuse_record): the raw depth and RGB8 image they are made from, the fusion
+// depth range, and the destinations (W wide); rec null: none.
+struct FuseRecDst {
+    const float* raw;
+    int rp;
+    const uint8_t* rgb;
+    int cp;
+    float dmin, dmax;
+    float4* rec;
+    uint32_t* col;
+    int packed;   // 1: the precision form's 16-byte records (fuse_record_packed) in rec, col unused
+};
 int launch_maps(const float* depth, int dp, const uint8_t* gray, int gp, int W, int H, const Intr& k,
                  float cutoff, float4* vmap, int vp, float4* nmap, int np, int16_t* dx, int16_t* dy, int sp,
-                 cudaStream_t st, uint8_t* rgbok = nullptr);
+                 cudaStream_t st, uint8_t* rgbok = nullptr, const FuseRecDst* fr = nullptr);
 int launch_nmap(const float4* vmap, int vp, int W, int H, float4* nmap, int np, cudaStream_t st);
 int launch_resize(const float4* vs, const float4* ns, int sp, int SW, int SH, float4* vd, float4* nd, int dp,
                    cudaStream_t st);
@@ -159,6 +172,9 @@ struct MapView {
     float* zmin;                // z-range image, zc x zr
     float* zmax;
     int zc, zr;
+    float4* frec;               // fusion records, 8 zc x 8 zr: {depth or NaN, normal xyz} (fuse_record), or
+                                // in the precision form one packed 16-byte word each (fuse_record_packed)
+    uint32_t* fcol;             // reference form: the records' colours r | g << 8 | b << 16
     MapGeom g;
 };
 
@@ -171,8 +187,13 @@ int launch_allocate(const MapView& m, const float* raw, int rp, int W, int H, co
                      const int* skip, cudaStream_t s);
 int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
                        cudaStream_t s);
-int launch_integrate(const MapView& m, const float* raw, int rp, const uint8_t* rgb, int cp, const float4* nmap,
-                      int np, int W, int H, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s);
+// Fusion records (m.frec / m.fcol, W wide) of a raw depth map, RGB8 image and
+// normal map; the frame path makes them in the level-0 map kernel instead.
+int launch_fuse_records(const MapView& m, const float* raw, int rp, const uint8_t* rgb, int cp, const float4* nmap,
+                        int np, int W, int H, cudaStream_t s);
+// Integration of the visible blocks from the fusion records of a W x H frame.
+int launch_integrate(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
+                     cudaStream_t s);
 int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s);
 // tile bx x by threads: bx * by <= 128 (the kernel's launch bound), a multiple
 // of 32; bx = by = 0: the pooled raycast (lane refill)

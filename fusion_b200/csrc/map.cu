@@ -27,7 +27,9 @@
 // Visibility walks the list of allocated entries rather than every slot of
 // the table (CheckVisibleBlockKernel, FuseMap.cu:113-138, scans all of them).
 // Integration processes one visible block per CTA iteration: 256 threads, two
-// voxels each, one 16-byte load and at most one 16-byte store per thread.
+// voxels each, one 16-byte load and at most one 16-byte store per thread; the
+// per-pixel inputs come from the frame's fusion records (one 16-byte gather
+// of depth and normal, one word of colour).
 #include <cuda_fp16.h>
 
 #include "fb_internal.h"
@@ -518,45 +520,64 @@ __global__ void __launch_bounds__(256) k_visibility(MapView m, int W, int H, Int
 
 // --------------------------------------------------------------- integration
 
-// Fusion::integrateColor (FuseMap.cu:140-191) for one voxel.  Returns true
-// when the voxel changed.
-__device__ __forceinline__ bool integrate_voxel(Voxel& vox, int vx, int vy, int vz, const float* __restrict__ raw,
-                                                int rp, const uint8_t* __restrict__ rgb, int cp,
-                                                const float4* __restrict__ nmap, int np, int W, int H,
-                                                const Intr& k, const DevPose& P, const MapGeom& g,
+// Fusion records of caller images (fb_fuse_map_color; the frame path makes
+// them in the level-0 map kernel): see fuse_record.  The integration kernels
+// use 1 for the normal's w lane, which ComputeNMap sets on every valid normal
+// (Pyrdown.cu:93-125); a valid normal with another w lane is flagged.
+__global__ void k_fuse_records(MapView m, const float* __restrict__ raw, int rp, const uint8_t* __restrict__ rgb,
+                               int cp, const float4* __restrict__ nmap, int np, int W, int H) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const float4 n = nmap[(size_t)y * np + x];
+    if (!isnan(n.x) && n.w != 1.0f) atomicOr(&m.ctr->err, kErrNormalW);
+    if (m.cvox)
+        fuse_record_packed(raw[(size_t)y * rp + x], n, rgb + (size_t)y * cp + 3 * x, m.g.depth_min, m.g.depth_max,
+                           (uint4*)m.frec + (size_t)y * W + x);
+    else
+        fuse_record(raw[(size_t)y * rp + x], n, rgb + (size_t)y * cp + 3 * x, m.g.depth_min, m.g.depth_max,
+                    m.frec + (size_t)y * W + x, m.fcol + (size_t)y * W + x);
+}
+
+// Fusion::integrateColor (FuseMap.cu:140-191) for one voxel, every operation
+// rounded as the reference's float expression.  rec / col: the frame's fusion
+// records (W wide).  Returns true when the voxel changed.
+__device__ __forceinline__ bool integrate_voxel(Voxel& vox, int vx, int vy, int vz, const float4* __restrict__ rec,
+                                                const uint32_t* __restrict__ col, int W, int H, const Intr& k,
+                                                const DevPose& P, const MapGeom& g,
                                                 const float* __restrict__ div255) {
     f3 pos = mk3(fm((float)vx, g.voxel_size), fm((float)vy, g.voxel_size), fm((float)vz, g.voxel_size));
     pos = mv(P.Rinv, sub3(pos, P.t));
     const float pu = fa(fd(fm(k.fx, pos.x), pos.z), k.cx), pv = fa(fd(fm(k.fy, pos.y), pos.z), k.cy);
     const int u = __float2int_rz(pu), v = __float2int_rz(pv);  // make_int2(float2)
     if (u < 0 || v < 0 || u >= W || v >= H) return false;
-    const float dp = raw[(size_t)v * rp + u];
-    if (isnan(dp) || dp > g.depth_max || dp < g.depth_min) return false;
+    const int pix = v * W + u;
+    const float4 r = __ldg(rec + pix);   // r.x: the raw depth, NaN where the pixel is skipped
     const float thresh = g.trunc_dist;
-    float sdf = fs(dp, pos.z);
+    float sdf = fs(r.x, pos.z);
     if (!(sdf >= -thresh)) return false;
     sdf = fminf(1.0f, fd(sdf, thresh));
-    const float4 nl = nmap[(size_t)v * np + u];
-    if (isnan(nl.x)) return false;
     // w = nl * normalised(float4(pos, 1)): the dot runs over all four lanes
+    // (the normal's w lane is 1, so its term is 1 / nrm)
     const float nrm = fsq(fa(fa(fa(fm(pos.x, pos.x), fm(pos.y, pos.y)), fm(pos.z, pos.z)), 1.0f));
-    const float w = fa(fa(fa(fm(nl.x, fd(pos.x, nrm)), fm(nl.y, fd(pos.y, nrm))), fm(nl.z, fd(pos.z, nrm))),
-                       fm(nl.w, fd(1.0f, nrm)));
-    const uint8_t* px = rgb + (size_t)v * cp + 3 * u;
+    const float w = fa(fa(fa(fm(r.y, fd(pos.x, nrm)), fm(r.z, fd(pos.y, nrm))), fm(r.w, fd(pos.z, nrm))),
+                       fd(1.0f, nrm));
+    const uint32_t c = __ldg(col + pix);
+    const uint32_t cr = c & 255u, cg = (c >> 8) & 255u, cb = c >> 16;
     if (vox.weight == 0) {
         vox.sdf = sdf;
         vox.weight = 1;
-        vox.r = px[0];
-        vox.g = px[1];
-        vox.b = px[2];
+        vox.r = (unsigned char)cr;
+        vox.g = (unsigned char)cg;
+        vox.b = (unsigned char)cb;
         return true;
     }
     const float a = fm(w, 0.2f), oa = fs(1.0f, a);
     const float W0 = (float)vox.weight;
     // (float)c / 255 of a byte c: the table holds those 256 IEEE quotients
-    float rr = fm(fa(fm(a, div255[px[0]]), fm(oa, div255[vox.r])), 255.f);
-    float gg = fm(fa(fm(a, div255[px[1]]), fm(oa, div255[vox.g])), 255.f);
-    float bb = fm(fa(fm(a, div255[px[2]]), fm(oa, div255[vox.b])), 255.f);
+    float rr = fm(fa(fm(a, div255[cr]), fm(oa, div255[vox.r])), 255.f);
+    float gg = fm(fa(fm(a, div255[cg]), fm(oa, div255[vox.g])), 255.f);
+    float bb = fm(fa(fm(a, div255[cb]), fm(oa, div255[vox.b])), 255.f);
     vox.sdf = fd(fa(fm(vox.sdf, W0), fm(w, sdf)), fa(W0, w));
     vox.weight = (unsigned char)min(255, (int)vox.weight + 1);
     // make_uchar3(float3): truncate to int, then to the low byte
@@ -566,10 +587,8 @@ __device__ __forceinline__ bool integrate_voxel(Voxel& vox, int vx, int vy, int 
     return true;
 }
 
-__global__ void __launch_bounds__(256) k_integrate(MapView m, const float* __restrict__ raw, int rp,
-                                                   const uint8_t* __restrict__ rgb, int cp,
-                                                   const float4* __restrict__ nmap, int np, int W, int H, Intr k,
-                                                   const DevPose* __restrict__ posep, const int* __restrict__ skip) {
+__global__ void __launch_bounds__(256) k_integrate(MapView m, int W, int H, Intr k, const DevPose* __restrict__ posep,
+                                                   const int* __restrict__ skip) {
     if (skip && *skip) return;
     __shared__ float s_div255[256];
     s_div255[threadIdx.x] = fd((float)threadIdx.x, 255.f);   // blockDim.x == 256
@@ -578,14 +597,16 @@ __global__ void __launch_bounds__(256) k_integrate(MapView m, const float* __res
     const int n = min(m.ctr->n_visible, m.NS);
     const int t = threadIdx.x;
     const int lx = (2 * t) & 7, ly = (t >> 2) & 7, lz = t >> 5;
+    const float4* __restrict__ rec = m.frec;
+    const uint32_t* __restrict__ col = m.fcol;
     for (int b = blockIdx.x; b < n; b += gridDim.x) {
         const HEntry e = m.vis_blocks[b];
         const int vx = e.x * 8 + lx, vy = e.y * 8 + ly, vz = e.z * 8 + lz;
         uint4* base = (uint4*)(m.voxels + (size_t)e.ptr * 512) + t;
-        uint4 raw2 = *base;
-        Voxel v0 = *(Voxel*)&raw2.x, v1 = *(Voxel*)&raw2.z;
-        bool c0 = integrate_voxel(v0, vx, vy, vz, raw, rp, rgb, cp, nmap, np, W, H, k, P, m.g, s_div255);
-        bool c1 = integrate_voxel(v1, vx + 1, vy, vz, raw, rp, rgb, cp, nmap, np, W, H, k, P, m.g, s_div255);
+        const uint4 raw2 = *base;
+        Voxel v0 = *(const Voxel*)&raw2.x, v1 = *(const Voxel*)&raw2.z;
+        bool c0 = integrate_voxel(v0, vx, vy, vz, rec, col, W, H, k, P, m.g, s_div255);
+        bool c1 = integrate_voxel(v1, vx + 1, vy, vz, rec, col, W, H, k, P, m.g, s_div255);
         if (c0 || c1) {
             uint4 o;
             *(Voxel*)&o.x = v0;
@@ -595,27 +616,58 @@ __global__ void __launch_bounds__(256) k_integrate(MapView m, const float* __res
     }
 }
 
-// Precision form of k_integrate: 6-byte voxels (FP16 TSDF), contracted FP32.
-// One CTA of 128 threads per visible block per iteration; thread t owns the
-// four x-consecutive voxels (4 (t & 1) .. +3, (t >> 1) & 7, t >> 4), so its
-// TSDF (8 B), weights (4 B) and colours (3 x 4 B) are aligned vector loads
-// of the block's arrays, and the block's 3 KB is read by one coalesced pass.
+// Precision form of k_integrate: 6-byte voxels (FP16 TSDF and one r, g, b,
+// weight word), contracted FP32.  One wave of CTAs of 128 threads; each CTA
+// takes every gridDim.x-th visible block.  The block's voxel loads are issued
+// before the projections, so they overlap the record gathers.  Thread t owns
+// four x-consecutive voxels, so its TSDF (8 B) and words (16 B) are two
+// coalesced vector loads and stores; which (y, z) it owns is chosen per frame
+// so that a warp's 32 voxels of one gather lie along the viewing direction.
+// The per-pixel inputs are one packed 16-byte record (fuse_record_packed):
+// the gathers, not the voxel traffic, bound this kernel (L1 wavefronts of
+// scattered loads), so one gather per voxel instead of two matters most.
 // Camera-space positions come from a per-block origin and the columns of
-// Rinv scaled by the voxel size (basis), one FMA chain per coordinate.  The
-// update rule is integrateColor's (FuseMap.cu:140-191): project (truncated
-// pixel), depth in range, sdf >= -T, sdf = min(1, sdf / T), skip a NaN
-// normal, w = n . normalised(p, 1) over four lanes, first observation or
-// weighted running average, weight + 1 capped at 255, colour blend 0.2 w.
-__global__ void __launch_bounds__(128, 8) k_integrate_compact(MapView m, const float* __restrict__ raw, int rp,
-                                                           const uint8_t* __restrict__ rgb, int cp,
-                                                           const float4* __restrict__ nmap, int np, int W, int H,
-                                                           Intr k, const DevPose* __restrict__ posep,
+// Rinv scaled by the voxel size (voxel q of the four at origin + q x-column).
+//
+// The update is integrateColor's (FuseMap.cu:140-191): project (truncated
+// pixel), record depth valid, sdf >= -T, sdf = min(1, sdf / T),
+// w = n . normalised(p, 1) over four lanes, first observation or weighted
+// running average, weight + 1 capped at 255, colour c0 + 0.2 w (c - c0).
+// The colour is blended on floats 1.5 * 2^23 + byte, whose low mantissa bits
+// are the byte: one exact subtraction and one fused multiply-add rounded
+// toward zero give floor(c0 + 0.2 w (c - c0)) modulo 256 (the reference
+// truncates toward zero; the two differ only where the sum is negative and
+// wraps).
+__device__ __forceinline__ float byte_as_magic(uint32_t word, uint32_t sel) {
+    // byte `sel` of `word` into the low byte of 0x4b400000 = 1.5 * 2^23
+    return __uint_as_float(__byte_perm(word, 0x4b400000u, sel | 0x7650u));
+}
+
+__global__ void __launch_bounds__(128, 7) k_integrate_compact(MapView m, int W, int H, Intr k,
+                                                           const DevPose* __restrict__ posep,
                                                            const int* __restrict__ skip) {
     if (skip && *skip) return;
     const DevPose P = *posep;
     const int n = min(m.ctr->n_visible, m.NS);
-    const int t = threadIdx.x;
-    const int lx = 4 * (t & 1), ly = (t >> 1) & 7, lz = t >> 4;
+    const int t = threadIdx.x, l = t & 31, wq = t >> 5;
+    // voxels of a warp's gather lie along the world axis closest to the
+    // viewing direction (the camera's z axis in world coordinates is row 2 of
+    // Rinv), where they project onto few pixels: lane bits 1-4 and the warp
+    // index split the block's y and z coordinates accordingly; each thread
+    // keeps four x-consecutive voxels (vector loads and stores)
+    const float ax = fabsf(P.Rinv.r2.x), ay = fabsf(P.Rinv.r2.y), az = fabsf(P.Rinv.r2.z);
+    int ly, lz;
+    if (az >= ax && az >= ay) {          // view along z: 8 z x 2 y per warp
+        ly = ((l >> 1) & 1) | (wq << 1);
+        lz = (l >> 2) & 7;
+    } else if (ay >= ax) {               // view along y: 8 y x 2 z per warp
+        ly = (l >> 1) & 7;
+        lz = ((l >> 4) & 1) | (wq << 1);
+    } else {                             // view along x: 4 y x 4 z per warp
+        ly = ((l >> 1) & 3) | ((wq & 1) << 2);
+        lz = ((l >> 3) & 3) | ((wq >> 1) << 2);
+    }
+    const int lx = 4 * (l & 1);
     const int idx = lz * 64 + ly * 8 + lx;
     const float vs = m.g.voxel_size, T = m.g.trunc_dist, invT = 1.0f / T;
     // camera = Rinv (world - t): basis columns Rinv e_i * vs and offset -Rinv t
@@ -625,98 +677,72 @@ __global__ void __launch_bounds__(128, 8) k_integrate_compact(MapView m, const f
     const f3 c0 = mk3(-(P.Rinv.r0.x * P.t.x + P.Rinv.r0.y * P.t.y + P.Rinv.r0.z * P.t.z),
                       -(P.Rinv.r1.x * P.t.x + P.Rinv.r1.y * P.t.y + P.Rinv.r1.z * P.t.z),
                       -(P.Rinv.r2.x * P.t.x + P.Rinv.r2.y * P.t.y + P.Rinv.r2.z * P.t.z));
+    const uint4* __restrict__ rec = (const uint4*)m.frec;   // packed records (fuse_record_packed)
     for (int b = blockIdx.x; b < n; b += gridDim.x) {
-        const HEntry e = m.vis_blocks[b];
+        const HEntry e4 = m.vis_blocks[b];
+        const int4 e = make_int4(e4.x, e4.y, e4.z, e4.ptr);
+        uint8_t* blk = m.cvox + (size_t)e.w * kCBlockBytes;
+        uint2 sd = *(const uint2*)(blk + 2 * idx);
+        const uint4 cw = *(const uint4*)(blk + kCRgbw + 4 * idx);
         const float ox = (float)(e.x * 8 + lx), oy = (float)(e.y * 8 + ly), oz = (float)(e.z * 8 + lz);
-        // position of the thread's first voxel
         f3 p;
         p.x = fmaf(bx.x, ox, fmaf(by.x, oy, fmaf(bz.x, oz, c0.x)));
         p.y = fmaf(bx.y, ox, fmaf(by.y, oy, fmaf(bz.y, oz, c0.y)));
         p.z = fmaf(bx.z, ox, fmaf(by.z, oy, fmaf(bz.z, oz, c0.z)));
-        uint8_t* blk = m.cvox + (size_t)e.ptr * kCBlockBytes;
-        uint2 sd = *(const uint2*)(blk + 2 * idx);
-        uint32_t wq = *(const uint32_t*)(blk + kCWeight + idx);
-        uint32_t rq = *(const uint32_t*)(blk + kCRed + idx);
-        uint32_t gq = *(const uint32_t*)(blk + kCGreen + idx);
-        uint32_t bq = *(const uint32_t*)(blk + kCBlue + idx);
-        __half2 s01 = *(__half2*)&sd.x, s23 = *(__half2*)&sd.y;
+        // the four projections, then their record gathers issued together;
+        // voxel q sits at p + q bx (recomputed where needed: fewer live
+        // registers than keeping the four positions)
+        int pix[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const f3 pq = mk3(fmaf((float)q, bx.x, p.x), fmaf((float)q, bx.y, p.y), fmaf((float)q, bx.z, p.z));
+            const float rz = __fdividef(1.0f, pq.z);
+            const int u = __float2int_rz(fmaf(k.fx * pq.x, rz, k.cx));
+            const int v = __float2int_rz(fmaf(k.fy * pq.y, rz, k.cy));
+            pix[q] = ((unsigned)u < (unsigned)W && (unsigned)v < (unsigned)H) ? v * W + u : -1;
+        }
+        uint4 r[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) r[q] = pix[q] >= 0 ? __ldg(rec + pix[q]) : make_uint4(0x7fffffffu, 0u, 0u, 0u);
+        const __half2 s01 = *(const __half2*)&sd.x, s23 = *(const __half2*)&sd.y;
         float sdf[4] = {__low2float(s01), __high2float(s01), __low2float(s23), __high2float(s23)};
+        uint32_t word[4] = {cw.x, cw.y, cw.z, cw.w};
         bool changed = false;
-        // phase 1: the four projections; phase 2: their depth gathers issued
-        // together; phase 3: normal and colour gathers of the voxels that
-        // update, issued together; phase 4: the updates
-        int pix[4], uv[4];
-        f3 pq[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            pq[q] = mk3(fmaf(bx.x, (float)q, p.x), fmaf(bx.y, (float)q, p.y), fmaf(bx.z, (float)q, p.z));
-            const float iz = __fdividef(1.0f, pq[q].z);
-            const int u = __float2int_rz(fmaf(k.fx * pq[q].x, iz, k.cx));
-            const int v = __float2int_rz(fmaf(k.fy * pq[q].y, iz, k.cy));
-            const bool in = !(u < 0 || v < 0 || u >= W || v >= H);
-            pix[q] = in ? v * rp + u : -1;
-            uv[q] = u | v << 16;
-        }
-        float dp[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) dp[q] = pix[q] >= 0 ? __ldg(raw + pix[q]) : qnan();
-        float so[4];
-        bool upd[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            so[q] = dp[q] - pq[q].z;
-            upd[q] = !(isnan(dp[q]) || dp[q] > m.g.depth_max || dp[q] < m.g.depth_min) && so[q] >= -T;
-            so[q] = fminf(1.0f, so[q] * invT);
-        }
-        float4 nl[4];
-        uint32_t px[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (upd[q]) {
-                const int u = uv[q] & 0xffff, v = uv[q] >> 16;
-                nl[q] = __ldg(nmap + (size_t)v * np + u);
-                const uint8_t* c3 = rgb + (size_t)v * cp + 3 * u;
-                px[q] = (uint32_t)__ldg(c3) | (uint32_t)__ldg(c3 + 1) << 8 | (uint32_t)__ldg(c3 + 2) << 16;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (!upd[q] || isnan(nl[q].x)) continue;
-            const float w = (nl[q].x * pq[q].x + nl[q].y * pq[q].y + nl[q].z * pq[q].z + nl[q].w) *
-                            rsqrtf(pq[q].x * pq[q].x + pq[q].y * pq[q].y + pq[q].z * pq[q].z + 1.0f);
-            const uint32_t sh = 8 * q, keep = ~(255u << sh);
-            const uint32_t W0 = (wq >> sh) & 255u;
-            const uint32_t cr = px[q] & 255u, cg = (px[q] >> 8) & 255u, cb = px[q] >> 16;
-            uint32_t nr, ng, nb;
+            const f3 pq = mk3(fmaf((float)q, bx.x, p.x), fmaf((float)q, bx.y, p.y), fmaf((float)q, bx.z, p.z));
+            const float so = __uint_as_float(r[q].x) - pq.z;
+            if (!(so >= -T)) continue;   // NaN depth (skipped pixel or outside the image) fails too
+            const float ts = fminf(1.0f, so * invT);
+            const float2 nxy = __half22float2(*reinterpret_cast<const __half2*>(&r[q].y));
+            const float nz = __half2float(__ushort_as_half((unsigned short)(r[q].z & 0xffffu)));
+            const uint32_t cq = (r[q].z >> 16) | (r[q].w << 16);   // r | g << 8 | b << 16
+            const float w = fmaf(nxy.x, pq.x, fmaf(nxy.y, pq.y, fmaf(nz, pq.z, 1.0f))) *
+                            rsqrtf(fmaf(pq.x, pq.x, fmaf(pq.y, pq.y, fmaf(pq.z, pq.z, 1.0f))));
+            const uint32_t W0 = word[q] >> 24;
             if (W0 == 0) {
-                sdf[q] = so[q];
-                wq = (wq & keep) | (1u << sh);
-                nr = cr;
-                ng = cg;
-                nb = cb;
+                sdf[q] = ts;
+                word[q] = cq | (1u << 24);
             } else {
-                const float a = 0.2f * w, oa = 1.0f - a, Wf = (float)W0;
-                sdf[q] = __fdividef(sdf[q] * Wf + w * so[q], Wf + w);
-                wq = (wq & keep) | ((W0 < 255u ? W0 + 1u : 255u) << sh);
-                nr = (uint32_t)__float2int_rz(fmaf(a, (float)cr, oa * (float)((rq >> sh) & 255u))) & 255u;
-                ng = (uint32_t)__float2int_rz(fmaf(a, (float)cg, oa * (float)((gq >> sh) & 255u))) & 255u;
-                nb = (uint32_t)__float2int_rz(fmaf(a, (float)cb, oa * (float)((bq >> sh) & 255u))) & 255u;
+                const float Wf = (float)W0, a = 0.2f * w;
+                sdf[q] = __fdividef(fmaf(sdf[q], Wf, w * ts), Wf + w);
+                const float r0 = byte_as_magic(word[q], 0), g0 = byte_as_magic(word[q], 1),
+                            b0 = byte_as_magic(word[q], 2);
+                const float rn = __fmaf_rz(a, byte_as_magic(cq, 0) - r0, r0);
+                const float gn = __fmaf_rz(a, byte_as_magic(cq, 1) - g0, g0);
+                const float bn = __fmaf_rz(a, byte_as_magic(cq, 2) - b0, b0);
+                const uint32_t rg = __byte_perm(__float_as_uint(rn), __float_as_uint(gn), 0x0040u);
+                const uint32_t bw = __byte_perm(__float_as_uint(bn), (W0 < 255u ? W0 + 1u : 255u), 0x0040u);
+                word[q] = __byte_perm(rg, bw, 0x5410u);
             }
-            rq = (rq & keep) | (nr << sh);
-            gq = (gq & keep) | (ng << sh);
-            bq = (bq & keep) | (nb << sh);
             changed = true;
         }
         if (changed) {
-            s01 = __floats2half2_rn(sdf[0], sdf[1]);
-            s23 = __floats2half2_rn(sdf[2], sdf[3]);
-            sd.x = *(uint32_t*)&s01;
-            sd.y = *(uint32_t*)&s23;
+            const __half2 n01 = __floats2half2_rn(sdf[0], sdf[1]), n23 = __floats2half2_rn(sdf[2], sdf[3]);
+            sd.x = *(const uint32_t*)&n01;
+            sd.y = *(const uint32_t*)&n23;
             *(uint2*)(blk + 2 * idx) = sd;
-            *(uint32_t*)(blk + kCWeight + idx) = wq;
-            *(uint32_t*)(blk + kCRed + idx) = rq;
-            *(uint32_t*)(blk + kCGreen + idx) = gq;
-            *(uint32_t*)(blk + kCBlue + idx) = bq;
+            *(uint4*)(blk + kCRgbw + 4 * idx) = make_uint4(word[0], word[1], word[2], word[3]);
         }
     }
 }
@@ -808,12 +834,19 @@ int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPo
     return 2;
 }
 
-int launch_integrate(const MapView& m, const float* raw, int rp, const uint8_t* rgb, int cp, const float4* nmap,
-                      int np, int W, int H, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s) {
+int launch_fuse_records(const MapView& m, const float* raw, int rp, const uint8_t* rgb, int cp, const float4* nmap,
+                        int np, int W, int H, cudaStream_t s) {
+    dim3 b(32, 8), g((W + 31) / 32, (H + 7) / 8);
+    k_fuse_records<<<g, b, 0, s>>>(m, raw, rp, rgb, cp, nmap, np, W, H);
+    return 1;
+}
+
+int launch_integrate(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
+                     cudaStream_t s) {
     if (m.cvox)
-        k_integrate_compact<<<sm_count() * 16, 128, 0, s>>>(m, raw, rp, rgb, cp, nmap, np, W, H, k, pose, skip);
+        k_integrate_compact<<<sm_count() * 7, 128, 0, s>>>(m, W, H, k, pose, skip);
     else
-        k_integrate<<<sm_count() * 8, 256, 0, s>>>(m, raw, rp, rgb, cp, nmap, np, W, H, k, pose, skip);
+        k_integrate<<<sm_count() * 8, 256, 0, s>>>(m, W, H, k, pose, skip);
     return 1;
 }
 

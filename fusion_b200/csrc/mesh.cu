@@ -238,7 +238,7 @@ __device__ void stage_block(const MapView& m, const HEntry& self, MeshSmem& s) {
             if (m.cvox) {
                 const uint8_t* blk = m.cvox + (size_t)p * kCBlockBytes;
                 sdf = __half2float(reinterpret_cast<const __half*>(blk)[idx]);
-                col = (uint32_t)blk[kCRed + idx] | (uint32_t)blk[kCGreen + idx] << 8 | (uint32_t)blk[kCBlue + idx] << 16;
+                col = *reinterpret_cast<const uint32_t*>(blk + kCRgbw + 4 * idx) & 0xffffffu;
             } else {
                 const Voxel vx = m.voxels[(size_t)p * 512 + idx];
                 sdf = vx.sdf;

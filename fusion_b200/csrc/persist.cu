@@ -273,10 +273,10 @@ int fb_write_map_file(fb_session* s, const char* path) {
                     std::memcpy(&h, blk + 2 * v, 2);
                     Voxel& o = vox[(size_t)b * 512 + v];
                     o.sdf = half_bits_to_float(h);
-                    o.weight = blk[kCWeight + v];
-                    o.r = blk[kCRed + v];
-                    o.g = blk[kCGreen + v];
-                    o.b = blk[kCBlue + v];
+                    o.weight = blk[c_weight(v)];
+                    o.r = blk[c_red(v)];
+                    o.g = blk[c_green(v)];
+                    o.b = blk[c_blue(v)];
                 }
             }
         } else {
@@ -339,10 +339,10 @@ int fb_read_map_file(fb_session* s, const char* path) {
                     const Voxel& x = vox[(size_t)b * 512 + v];
                     const __half h = __float2half_rn(x.sdf);
                     std::memcpy(blk + 2 * v, &h, 2);
-                    blk[kCWeight + v] = x.weight;
-                    blk[kCRed + v] = x.r;
-                    blk[kCGreen + v] = x.g;
-                    blk[kCBlue + v] = x.b;
+                    blk[c_weight(v)] = x.weight;
+                    blk[c_red(v)] = x.r;
+                    blk[c_green(v)] = x.g;
+                    blk[c_blue(v)] = x.b;
                 }
             }
             FB_CUDA(cudaMemcpy(m.cvox + (size_t)b0 * kCBlockBytes, cb.data(), (size_t)nb * kCBlockBytes,

@@ -123,7 +123,7 @@ __global__ void k_nmap(const float4* __restrict__ vmap, int vp, int W, int H, fl
 __global__ void k_maps(const float* __restrict__ depth, int dp, const uint8_t* __restrict__ gray, int gp,
                        int W, int H, Intr k, float cutoff, float4* __restrict__ vmap, int vp,
                        float4* __restrict__ nmap, int np, int16_t* __restrict__ dxo, int16_t* __restrict__ dyo,
-                       int sp, uint8_t* __restrict__ rgbok) {
+                       int sp, uint8_t* __restrict__ rgbok, FuseRecDst fr) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
@@ -138,6 +138,15 @@ __global__ void k_maps(const float* __restrict__ depth, int dp, const uint8_t* _
                 n = normal_of(c, r, d);
             }
             nmap[(size_t)y * np + x] = n;
+            // the fusion record of this pixel (level 0 of a frame that may be fused)
+            if (fr.rec) {
+                const float dp = fr.raw[(size_t)y * fr.rp + x];
+                const uint8_t* c3 = fr.rgb + (size_t)y * fr.cp + 3 * x;
+                if (fr.packed)
+                    fuse_record_packed(dp, n, c3, fr.dmin, fr.dmax, (uint4*)fr.rec + (size_t)y * W + x);
+                else
+                    fuse_record(dp, n, c3, fr.dmin, fr.dmax, fr.rec + (size_t)y * W + x, fr.col + (size_t)y * W + x);
+            }
         }
     }
     if (dxo) {
@@ -230,10 +239,11 @@ int launch_pyrdown(const float* sd, int sdp, const uint8_t* sg, int sgp, int SW,
 
 int launch_maps(const float* depth, int dp, const uint8_t* gray, int gp, int W, int H, const Intr& k,
                  float cutoff, float4* vmap, int vp, float4* nmap, int np, int16_t* dx, int16_t* dy,
-                 int sp, cudaStream_t st, uint8_t* rgbok) {
+                 int sp, cudaStream_t st, uint8_t* rgbok, const FuseRecDst* fr) {
     dim3 b(32, 8);
+    const FuseRecDst none{};
     k_maps<<<grid2d(W, H, b), b, 0, st>>>(depth, dp, gray, gp, W, H, k, cutoff, vmap, vp, nmap, np, dx,
-                                           dy, sp, rgbok);
+                                           dy, sp, rgbok, fr ? *fr : none);
     return 1;
 }
 

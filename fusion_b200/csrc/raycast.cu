@@ -194,7 +194,7 @@ struct ExactVox {
     static __device__ __forceinline__ int weight(ref v) { return v->weight; }
 };
 
-// Precision form: block arrays, FP16 TSDF.
+// Precision form: FP16 TSDF array, then one r, g, b, weight word per voxel.
 struct CompactVox {
     struct ref {
         const uint8_t* blk;
@@ -208,7 +208,7 @@ struct CompactVox {
     static __device__ __forceinline__ float sdf(ref v) {
         return __half2float(*(const __half*)(v.blk + 2 * v.idx));
     }
-    static __device__ __forceinline__ int weight(ref v) { return v.blk[kCWeight + v.idx]; }
+    static __device__ __forceinline__ int weight(ref v) { return v.blk[c_weight(v.idx)]; }
 };
 
 // FindEntry with the cache of FindVoxel(float3, cache, valid)

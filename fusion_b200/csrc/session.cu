@@ -301,7 +301,8 @@ bool carve_session(fb_session* s, const fb_config* cfg) {
              dalloc(s, &m.bucket_cnt, m.NB) && dalloc(s, &m.bucket_start, m.NB) && dalloc(s, &m.bucket_x, m.NB) &&
              dalloc(s, &m.chunk_sums, 2 * (size_t)m.nchunks) && dalloc(s, &m.zmin, (size_t)m.zc * m.zr) &&
              dalloc(s, &m.grid, (size_t)m.grid_cap) &&
-             dalloc(s, &m.zmax, (size_t)m.zc * m.zr);
+             dalloc(s, &m.zmax, (size_t)m.zc * m.zr) && dalloc(s, &m.frec, (size_t)64 * m.zc * m.zr) &&
+             dalloc(s, &m.fcol, (size_t)64 * m.zc * m.zr);
         s->ctr = m.ctr;
     }
     return ok;
@@ -360,9 +361,14 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
         for (int l = 1; l < 3; ++l)
             n += launch_pyrdown(N.depth[l - 1], s->W[l - 1], N.gray[l - 1], s->W[l - 1], s->W[l - 1], s->H[l - 1],
                                 N.depth[l], s->W[l], N.gray[l], s->W[l], st);
-        for (int l = 0; l < 3; ++l)
+        for (int l = 0; l < 3; ++l) {
+            // level 0 also makes the frame's fusion records
+            FuseRecDst fr{N.raw,          s->W[0],      N.rgb, 3 * s->W[0], c.depth_min, c.depth_max, s->map.frec,
+                          s->map.fcol, s->map.cvox ? 1 : 0};
             n += launch_maps(N.depth[l], s->W[l], N.gray[l], s->W[l], s->W[l], s->H[l], s->K[l], c.depth_cutoff,
-                             N.vmap[l], s->W[l], N.nmap[l], s->W[l], N.dx[l], N.dy[l], s->W[l], st, N.rgbok[l]);
+                             N.vmap[l], s->W[l], N.nmap[l], s->W[l], N.dx[l], N.dy[l], s->W[l], st, N.rgbok[l],
+                             l == 0 ? &fr : nullptr);
+        }
         *ran |= 1u << 1;
         if (part == 1) return n;
     }
@@ -403,8 +409,7 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
         mark(4);
         n += launch_visibility(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st);
         mark(5);
-        n += launch_integrate(s->map, N.raw, s->W[0], N.rgb, 3 * s->W[0], N.nmap[0], s->W[0], s->W[0], s->H[0],
-                              s->K[0], pose, skip, st);
+        n += launch_integrate(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st);
         *ran |= 7u << 3;
     } else {
         mark(4);
@@ -1079,10 +1084,10 @@ int fb_map_download_blocks(fb_session* s, const int32_t* ptrs, int n, float* sdf
                 uint16_t h;
                 std::memcpy(&h, cb.data() + 2 * v, 2);
                 tmp[v].sdf = half_bits_to_float(h);
-                tmp[v].weight = cb[kCWeight + v];
-                tmp[v].r = cb[kCRed + v];
-                tmp[v].g = cb[kCGreen + v];
-                tmp[v].b = cb[kCBlue + v];
+                tmp[v].weight = cb[c_weight(v)];
+                tmp[v].r = cb[c_red(v)];
+                tmp[v].g = cb[c_green(v)];
+                tmp[v].b = cb[c_blue(v)];
             }
         } else {
             FB_CUDA(cudaMemcpyAsync(tmp.data(), s->map.voxels + ptrs[i], 512 * sizeof(Voxel), cudaMemcpyDeviceToHost,

@@ -256,15 +256,17 @@ int fb_fuse_map_color(fb_session* s, const fb_image* depth, const fb_image* rgb,
     const Intr k = intr_from(K);
     launch_allocate(s->map, (const float*)depth->data, (int)(depth->pitch / 4), W, H, k, s->scratch_pose, nullptr, st);
     launch_visibility(s->map, W, H, k, s->scratch_pose, nullptr, st);
-    launch_integrate(s->map, (const float*)depth->data, (int)(depth->pitch / 4), (const uint8_t*)rgb->data,
-                     (int)rgb->pitch, (const float4*)nmap->data, (int)(nmap->pitch / 16), W, H, k, s->scratch_pose,
-                     nullptr, st);
+    launch_fuse_records(s->map, (const float*)depth->data, (int)(depth->pitch / 4), (const uint8_t*)rgb->data,
+                        (int)rgb->pitch, (const float4*)nmap->data, (int)(nmap->pitch / 16), W, H, st);
+    launch_integrate(s->map, W, H, k, s->scratch_pose, nullptr, st);
     if (check_launch()) return FB_ECUDA;
     FB_CUDA(cudaStreamSynchronize(st));
-    if (no_visible) {
-        MapCounters c;
-        FB_CUDA(cudaMemcpy(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost));
-        *no_visible = (uint32_t)c.n_visible;
+    MapCounters c;
+    FB_CUDA(cudaMemcpy(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost));
+    if (no_visible) *no_visible = (uint32_t)c.n_visible;
+    if (c.err & kErrNormalW) {
+        fb_set_error_text("fb_fuse_map_color: a valid normal's w lane is not 1 (ComputeNMap writes 1)");
+        return FB_EINVAL;
     }
     return FB_OK;
 }

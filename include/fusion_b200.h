@@ -49,7 +49,8 @@ extern "C" {
 #define FB_ERR_NEW_LIST_FULL 0x10u    /* more new blocks in one frame than the pool */
 #define FB_ERR_VISIBLE_FULL 0x20u     /* visible list full */
 #define FB_ERR_SEQUENTIAL_INSERT 0x40u /* pool/excess edge case: exact sequential insert used */
-#define FB_ERR_TIMEOUT 0x80u          /* reserved: no kernel of this library waits on another */
+#define FB_ERR_TIMEOUT 0x80u          /* a bounded device-side wait (a staged copy) gave up; integration stopped */
+#define FB_ERR_NORMAL_W 0x100u        /* fb_fuse_map_color: a valid normal's w lane was not 1 (ComputeNMap's) */
 
 /* Runtime form of the reference's compile-time constants:
  * Mapping/DeviceMap.h:135-151 (voxel size, truncation, depth range, table

@@ -154,10 +154,10 @@ def test_precision_form_integration_teacher_forced():
         assert abs(n_g - n_o) <= 0.005 * n_o
     e_g = s.entries()
     occ = e_g[:, 3] >= 0
-    sdf_g, w_g, _ = s.blocks(e_g[occ][:, 3])
+    sdf_g, w_g, c_g = s.blocks(e_g[occ][:, 3])
     e_o = M.entries()
     occ_o = e_o[:, 3] >= 0
-    sdf_o, w_o, _ = M.voxels(e_o[occ_o][:, 3])
+    sdf_o, w_o, c_o = M.voxels(e_o[occ_o][:, 3])
     bg, bo = {tuple(x[:3]) for x in e_g[occ]}, {tuple(x[:3]) for x in e_o[occ_o]}
     assert len(bg ^ bo) <= 0.005 * len(bo)      # allocation decisions in FP32 vs FP64
     vg, vo = _observed(e_g, sdf_g, w_g), _observed(e_o, sdf_o, w_o)
@@ -165,9 +165,25 @@ def test_precision_form_integration_teacher_forced():
     d = np.array([vg[k][0] - vo[k][0] for k in common])
     eq = np.array([vg[k][1] == vo[k][1] for k in common])
     rms, rms_eq = float(np.sqrt(np.mean(d ** 2))), float(np.sqrt(np.mean(d[eq] ** 2)))
+    # colours of the voxels both observed: the blend c0 + 0.2 w (c - c0) in
+    # FP32 floors where the reference truncates toward zero (they differ
+    # where the sum is negative and wraps), so a colour may be one level off
+    # per observation
+    def colours(e, occ_, c, w):
+        rows = e[occ_]
+        out = {}
+        for b in range(len(rows)):
+            for v in np.nonzero(w[b] > 0)[0]:
+                out[(int(rows[b, 0]), int(rows[b, 1]), int(rows[b, 2]), int(v))] = c[b, v].astype(int)
+        return out
+    cg_, co_ = colours(e_g, occ, c_g, w_g), colours(e_o, occ_o, c_o, w_o)
+    dc = np.array([np.abs(cg_[k] - co_[k]).max() for k in common])
+    within1 = float(np.mean(dc <= 1))
     print(f"precision form integration vs FP64 oracle, same inputs: TSDF rms {rms:.2e}, rms where weights "
           f"agree {rms_eq:.2e}, max {np.abs(d).max():.2e} (truncation units); weights equal {eq.mean():.5f}; "
+          f"colours equal {np.mean(dc == 0):.4f}, within 1 level {within1:.4f}; "
           f"voxels {len(common)} of {len(vo)} oracle / {len(vg)} gpu")
+    assert within1 >= 0.99
     assert rms_eq <= 1e-3            # FP16 storage: half an ulp is 2.4e-4 at |sdf| in [0.5, 1)
     assert eq.mean() >= 0.999
     assert len(common) >= 0.999 * len(vo)
