@@ -135,6 +135,9 @@ SIGNATURES = {
     "fb_resize_map": (_i, [ctypes.POINTER(Image)] * 4 + [_vp]),
     "fb_step_scratch_bytes": (_sz, [_i, _i]),
     "fb_track_reduction_grid": (_i, [_i]),
+    "fb_create_rendering_blocks": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "fb_map_export_visible": (_i, [_vp, _vp, ctypes.c_uint32, _vp, _vp]),
+    "fb_map_export_reference": (_i, [_vp, _vp, _sz, _vp, _sz, _vp, _sz, _vp, _vp, _vp]),
     "fb_icp_step": (_i, [ctypes.POINTER(Image)] * 4 + [_vp] * 6 + [_vp, _sz, _vp, _vp, _vp, _vp]),
     "fb_rgb_step": (_i, [ctypes.POINTER(Image)] * 6 + [_vp] * 7 + [_vp, _sz, _vp, _vp, _vp, _vp]),
     "fb_rgb_step_static": (_i, [ctypes.POINTER(Image)] * 6 + [_vp] * 7 + [_vp, _vp, _vp, _vp]),

@@ -187,6 +187,13 @@ int launch_allocate(const MapView& m, const float* raw, int rp, int W, int H, co
                      const int* skip, cudaStream_t s);
 int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
                        cudaStream_t s);
+// The visible entries (at most `capacity`) in the reference's 32-byte
+// HashEntry layout at dst; the table, voxels and counters in the reference's
+// layouts (the reference form's voxels are the reference's already: the
+// caller copies them).
+int launch_export_visible(const MapView& m, void* dst, int capacity, cudaStream_t s);
+int launch_export_reference(const MapView& m, void* entries, void* voxels, int* heap_counter, int* entry_ptr,
+                            cudaStream_t s);
 // Fusion records (m.frec / m.fcol, W wide) of a raw depth map, RGB8 image and
 // normal map; the frame path makes them in the level-0 map kernel instead.
 int launch_fuse_records(const MapView& m, const float* raw, int rp, const uint8_t* rgb, int cp, const float4* nmap,

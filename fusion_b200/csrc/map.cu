@@ -747,6 +747,58 @@ __global__ void __launch_bounds__(128, 7) k_integrate_compact(MapView m, int W, 
     }
 }
 
+// ------------------------------------------------- the reference's layouts
+
+// The reference's HashEntry (Mapping/DeviceMap.h:17-59, __align__(16): 32
+// bytes): block position, voxel index of the block (block * 512) or -1, and
+// the chain offset.
+struct RefHashEntry {
+    int x, y, z, ptr, offset, pad[3];
+};
+static_assert(sizeof(RefHashEntry) == 32, "the reference's HashEntry");
+
+__device__ __forceinline__ RefHashEntry to_ref_entry(const HEntry& e) {
+    RefHashEntry r;
+    r.x = e.x;
+    r.y = e.y;
+    r.z = e.z;
+    r.ptr = e.ptr >= 0 ? e.ptr * 512 : -1;
+    r.offset = e.offset;
+    r.pad[0] = r.pad[1] = r.pad[2] = 0;
+    return r;
+}
+
+// n entries (from a table or the visible list) in the reference's layout.
+__global__ void k_export_ref_entries(const HEntry* __restrict__ src, const int* __restrict__ count, int n,
+                                     RefHashEntry* __restrict__ dst) {
+    const int lim = count ? min(*count, n) : n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < lim; i += gridDim.x * blockDim.x)
+        dst[i] = to_ref_entry(src[i]);
+}
+
+// Precision-form voxels in the reference's 8-byte Voxel layout (FP16 TSDF
+// widened to float).
+__global__ void k_export_ref_voxels(MapView m, Voxel* __restrict__ dst) {
+    const size_t n = (size_t)m.NS * 512;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint8_t* blk = m.cvox + (i / 512) * kCBlockBytes;
+        const int v = (int)(i % 512);
+        Voxel o;
+        o.sdf = __half2float(reinterpret_cast<const __half*>(blk)[v]);
+        const uint32_t w = *reinterpret_cast<const uint32_t*>(blk + kCRgbw + 4 * v);
+        o.weight = (uint8_t)(w >> 24);
+        o.r = (uint8_t)w;
+        o.g = (uint8_t)(w >> 8);
+        o.b = (uint8_t)(w >> 16);
+        dst[i] = o;
+    }
+}
+
+__global__ void k_export_ref_counters(const MapCounters* __restrict__ c, int* heap_counter, int* entry_ptr) {
+    if (heap_counter) *heap_counter = c->heap_counter;
+    if (entry_ptr) *entry_ptr = c->entry_ptr;
+}
+
 // ---------------------------------------------------------------------- reset
 
 // ResetHashKernel / ResetSdfBlockKernel (FuseMap.cu:321-350) on all of the
@@ -832,6 +884,20 @@ int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPo
     k_reset_visible<<<1, 1, 0, s>>>(m.ctr);
     k_visibility<<<sm_count() * 4, 256, 0, s>>>(m, W, H, k, pose, skip);
     return 2;
+}
+
+int launch_export_visible(const MapView& m, void* dst, int capacity, cudaStream_t s) {
+    k_export_ref_entries<<<sm_count() * 2, 256, 0, s>>>(m.vis_blocks, &m.ctr->n_visible, min(capacity, m.NS),
+                                                          (RefHashEntry*)dst);
+    return 1;
+}
+
+int launch_export_reference(const MapView& m, void* entries, void* voxels, int* heap_counter, int* entry_ptr,
+                            cudaStream_t s) {
+    k_export_ref_entries<<<sm_count() * 8, 256, 0, s>>>(m.entries, nullptr, m.NB + m.NE, (RefHashEntry*)entries);
+    if (m.cvox) k_export_ref_voxels<<<sm_count() * 8, 256, 0, s>>>(m, (Voxel*)voxels);
+    k_export_ref_counters<<<1, 1, 0, s>>>(m.ctr, heap_counter, entry_ptr);
+    return m.cvox ? 3 : 2;
 }
 
 int launch_fuse_records(const MapView& m, const float* raw, int rp, const uint8_t* rgb, int cp, const float4* nmap,

@@ -26,7 +26,10 @@ __global__ void k_zrange_init(MapView m, const int* __restrict__ skip) {
         m.ctr->bmin[threadIdx.x] = 0x7fffffff;
         m.ctr->bmax[threadIdx.x] = -0x7fffffff;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) m.ctr->ray_next = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        m.ctr->ray_next = 0;
+        m.ctr->n_tiles = 0;   // counted again by each z-range pass
+    }
     const int n = m.zc * m.zr;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         m.zmin[i] = 100.f;   // CreateRenderingBlocks uploads 100 (RenderScene.cu:245-251)

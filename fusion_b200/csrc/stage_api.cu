@@ -287,6 +287,67 @@ int fb_check_block_visibility(fb_session* s, const float Rview[9], const float R
     return FB_OK;
 }
 
+int fb_create_rendering_blocks(fb_session* s, const float RviewInv[9], const float tview[3], const float K[4],
+                               fb_image* zmin, fb_image* zmax, uint32_t* no_tiles, void* stream) {
+    if (!s || !RviewInv || !tview || !K || !image_ok(zmin, 4) || !image_ok(zmax, 4)) return FB_EINVAL;
+    const MapView& m = s->map;
+    if (zmin->cols < m.zc || zmin->rows < m.zr || zmax->cols < m.zc || zmax->rows < m.zr) return FB_EINVAL;
+    // the view's rotation is the transpose of RviewInv
+    const float R[9] = {RviewInv[0], RviewInv[3], RviewInv[6], RviewInv[1], RviewInv[4],
+                        RviewInv[7], RviewInv[2], RviewInv[5], RviewInv[8]};
+    cudaStream_t st = stream ? as_stream(stream) : s->stream;
+    k_set_pose<<<1, 1, 0, st>>>(s->scratch_pose, pose_from(R, RviewInv, tview));
+    launch_zrange(m, intr_from(K), s->scratch_pose, nullptr, st);
+    if (check_launch()) return FB_ECUDA;
+    FB_CUDA(cudaMemcpy2DAsync(zmin->data, zmin->pitch, m.zmin, (size_t)m.zc * 4, (size_t)m.zc * 4, m.zr,
+                              cudaMemcpyDeviceToDevice, st));
+    FB_CUDA(cudaMemcpy2DAsync(zmax->data, zmax->pitch, m.zmax, (size_t)m.zc * 4, (size_t)m.zc * 4, m.zr,
+                              cudaMemcpyDeviceToDevice, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    if (no_tiles) {
+        MapCounters c;
+        FB_CUDA(cudaMemcpy(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost));
+        *no_tiles = (uint32_t)c.n_tiles;
+    }
+    return FB_OK;
+}
+
+int fb_map_export_visible(fb_session* s, void* entries, uint32_t capacity, uint32_t* n, void* stream) {
+    if (!s || (capacity && !entries) || ((uintptr_t)entries & 15)) return FB_EINVAL;
+    cudaStream_t st = stream ? as_stream(stream) : s->stream;
+    if (capacity) launch_export_visible(s->map, entries, (int)(capacity > (uint32_t)INT32_MAX ? INT32_MAX : capacity), st);
+    if (check_launch()) return FB_ECUDA;
+    FB_CUDA(cudaStreamSynchronize(st));
+    MapCounters c;
+    FB_CUDA(cudaMemcpy(&c, s->ctr, sizeof c, cudaMemcpyDeviceToHost));
+    const uint32_t nv = (uint32_t)(c.n_visible < 0 ? 0 : c.n_visible < s->map.NS ? c.n_visible : s->map.NS);
+    if (n) *n = nv;
+    if (nv > capacity) {
+        fb_set_error_text("fb_map_export_visible: more visible entries than the destination holds");
+        return FB_EINVAL;
+    }
+    return FB_OK;
+}
+
+int fb_map_export_reference(fb_session* s, void* hash_entries, size_t n_entries, void* voxels, size_t n_voxels,
+                            int32_t* heap, size_t n_heap, int32_t* heap_counter, int32_t* entry_ptr, void* stream) {
+    if (!s || !hash_entries || !voxels || !heap || !heap_counter || !entry_ptr) return FB_EINVAL;
+    const MapView& m = s->map;
+    if (n_entries != (size_t)m.NB + m.NE || n_voxels != (size_t)m.NS * 512 || n_heap != (size_t)m.NS ||
+        ((uintptr_t)hash_entries & 15) || ((uintptr_t)voxels & 7)) {
+        fb_set_error_text("fb_map_export_reference: the buffers' sizes differ from the session's map");
+        return FB_EINVAL;
+    }
+    cudaStream_t st = stream ? as_stream(stream) : s->stream;
+    launch_export_reference(m, hash_entries, voxels, heap_counter, entry_ptr, st);
+    if (check_launch()) return FB_ECUDA;
+    if (!m.cvox)
+        FB_CUDA(cudaMemcpyAsync(voxels, m.voxels, n_voxels * sizeof(Voxel), cudaMemcpyDeviceToDevice, st));
+    FB_CUDA(cudaMemcpyAsync(heap, m.heap, n_heap * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    return FB_OK;
+}
+
 int fb_raycast(fb_session* s, fb_image* vmap, fb_image* nmap, const float Rview[9], const float RviewInv[9],
                const float tview[3], const float K[4], int* rendered, void* stream) {
     if (!s || !image_ok(vmap, 16) || !image_ok(nmap, 16) || vmap->pitch != nmap->pitch || !Rview || !RviewInv ||

@@ -365,6 +365,39 @@ FB_API int fb_check_block_visibility(fb_session* s, const float Rview[9], const 
                               const float tview[3], int cols, int rows, const float K[4],
                               uint32_t* no_visible, void* stream);
 
+/* Replaces: CreateRenderingBlocks (Mapping/RenderScene.cu:199-276, declared
+ * at Mapping/RenderScene.h:20-27): the z ranges of the session's visible
+ * blocks seen from (RviewInv, tview) with intrinsics K, written into the
+ * caller's z-range images zmin / zmax (float, at least ceil(W/8) x ceil(H/8)
+ * of the session's camera; tiles with no block hold 100 and 0, as the
+ * reference initialises them), and the number of rendering tiles.  The
+ * reference's RenderingBlock list is an intermediate of its own; the library
+ * keeps a dense block index instead and writes no list. */
+FB_API int fb_create_rendering_blocks(fb_session* s, const float RviewInv[9], const float tview[3],
+                                      const float K[4], fb_image* zmin, fb_image* zmax, uint32_t* no_tiles,
+                                      void* stream);
+
+/* Replaces the visibleEntries array that CheckBlockVisibility and
+ * FuseMapColor fill in the reference (Mapping/FuseMap.cu:206-249): the
+ * session's visible entries, in order, written to device memory `entries`
+ * (16-byte aligned) in the reference's 32-byte HashEntry layout
+ * (Mapping/DeviceMap.h:17-59: int3 pos, int ptr = voxel index or -1, int
+ * offset, padding).  *n = the number of visible entries; FB_EINVAL when more
+ * than `capacity`. */
+FB_API int fb_map_export_visible(fb_session* s, void* entries, uint32_t capacity, uint32_t* n, void* stream);
+
+/* The session's map written into the reference's own device buffers -- the
+ * DeviceMap views Mapping::operator DeviceMap passes (Mapping/Mapping.cc:
+ * 311-325): hashEntries (NumBuckets + NumExcess HashEntry), voxelBlocks
+ * (NumSdfBlocks * 512 Voxel of 8 bytes; the precision form's FP16 TSDF
+ * widened), heapMem (NumSdfBlocks int), heapCounter and entryPtr (one int
+ * each).  The library keeps its map in its own layout; code that reads
+ * Mapping's buffers directly (System::WriteMapToDisk, Core/System.cc:195-231)
+ * calls this first.  The sizes must be the session's. */
+FB_API int fb_map_export_reference(fb_session* s, void* hash_entries, size_t n_entries, void* voxels,
+                                   size_t n_voxels, int32_t* heap, size_t n_heap, int32_t* heap_counter,
+                                   int32_t* entry_ptr, void* stream);
+
 /* Replaces: CreateRenderingBlocks + Raycast (Mapping/RenderScene.cu:199-276,
  * 447-489) as called by Mapping::RayTrace (Mapping/Mapping.cc:98-109): z
  * ranges of the visible blocks, then the raycast into vmap/nmap (float4,

@@ -21,16 +21,26 @@
  *   normal equations on the host, synchronously, as the reference's do; their
  *   reduction buffers (sum, out, sumRes, outRes) are not used.
  * - The map: the library keeps the hash table and the voxel blocks in its own
- *   layout inside an fb_session.  The first FuseMapColor or
- *   CheckBlockVisibility creates that session with the reference's map
- *   constants (fb_default_config) and the camera of the call; every later
- *   map call -- on the reference's one DeviceMap -- goes to it.  The
- *   reference's DeviceMap buffers stay allocated by Mapping and are not read.
- *   Mapping::RayTrace calls CreateRenderingBlocks and then Raycast;
- *   fb_raycast does both (z ranges, then the rays), so CreateRenderingBlocks
- *   only records the camera and reports whether any block is visible, and
- *   Raycast leaves the maps untouched when no rendering rectangle results,
- *   as the reference does when CreateRenderingBlocks returns false.
+ *   layout inside an fb_session, one per DeviceMap -- keyed by the address of
+ *   the DeviceMap's hashEntries buffer, i.e. one per Mapping.  The first
+ *   FuseMapColor or CheckBlockVisibility on a DeviceMap creates its session
+ *   with the reference's map constants (fb_default_config) and the camera of
+ *   the call.  What the reference's callers read back is written into their
+ *   own buffers:
+ *     - FuseMapColor and CheckBlockVisibility fill the DeviceMap's
+ *       visibleEntries (the reference's 32-byte HashEntry layout, in order)
+ *       and its noVisibleBlocks counter, and return the count in host_data;
+ *     - CreateRenderingBlocks fills the caller's zRangeX / zRangeY images and
+ *       the rendering-tile count in noRenderingBlocks (the RenderingBlock list
+ *       itself is the reference's intermediate: not written), and returns
+ *       false when there is no tile, as the reference does;
+ *     - Raycast writes vmap / nmap (it recomputes the z ranges itself);
+ *     - ResetMap empties the session's map.
+ *   The hash table, heap, counters and voxel blocks of the DeviceMap are not
+ *   kept up to date frame by frame (that would copy the whole map every
+ *   frame): code that reads them directly, such as System::WriteMapToDisk,
+ *   calls fusion_b200_shim::ExportMap(mapping) first, which writes the
+ *   session's map into them in the reference's layouts.
  * - Errors print the library's message and exit(0), as the reference's
  *   SafeCall does.
  * - Not provided by the library, defined here as such: SO3Step (its only
@@ -46,6 +56,7 @@
 
 #include <cstdlib>
 #include <iostream>
+#include <map>
 
 #include "fusion_b200.h"
 
@@ -91,21 +102,34 @@ inline void* step_scratch(int cols, int rows_, size_t* bytes) {
     return buf;
 }
 
-// The session holding the map, and the camera of the last
+// The session holding one DeviceMap's map, and the camera of its last
 // CreateRenderingBlocks call (Raycast receives only 1/fx and 1/fy).
 struct MapState {
     fb_session* session = nullptr;
     float K[4] = {0.f, 0.f, 0.f, 0.f};
 };
 
-inline MapState& map_state() {
-    static MapState m;
+// Sessions by the address of the DeviceMap's hashEntries buffer, and the
+// same sessions by the address of its visibleEntries buffer (what
+// CreateRenderingBlocks receives).
+inline std::map<const void*, MapState>& map_states() {
+    static std::map<const void*, MapState> m;
     return m;
 }
 
-inline fb_session* bind_map(int cols, int rows_, float fx, float fy, float cx, float cy, float depthMin,
-                            float depthMax) {
-    MapState& m = map_state();
+inline std::map<const void*, MapState*>& by_visible() {
+    static std::map<const void*, MapState*> m;
+    return m;
+}
+
+inline MapState* find_map(const DeviceMap& map) {
+    auto it = map_states().find((const void*)map.hashEntries.data);
+    return it == map_states().end() ? nullptr : &it->second;
+}
+
+inline MapState& bind_map(const DeviceMap& map, int cols, int rows_, float fx, float fy, float cx, float cy,
+                          float depthMin, float depthMax) {
+    MapState& m = map_states()[(const void*)map.hashEntries.data];
     if (!m.session) {
         fb_config c;
         fb_default_config(&c, cols, rows_);
@@ -116,8 +140,35 @@ inline fb_session* bind_map(int cols, int rows_, float fx, float fy, float cx, f
         c.depth_min = depthMin;
         c.depth_max = depthMax;
         check(fb_session_create(&c, legacy(), &m.session), "fb_session_create");
+        by_visible()[(const void*)map.visibleEntries.data] = &m;
     }
-    return m.session;
+    return m;
+}
+
+// After visibility: the DeviceMap's visibleEntries and noVisibleBlocks, as
+// the reference's CheckBlockVisibility leaves them.
+inline void write_visible(const DeviceMap& map, fb_session* s) {
+    if (!map.visibleEntries.data) return;   // a DeviceMap without buffers
+    uint32_t n = 0;
+    check(fb_map_export_visible(s, map.visibleEntries.data, (uint32_t)map.visibleEntries.size, &n, legacy()),
+          "visible entries");
+    if (map.noVisibleBlocks.data)
+        cudaMemcpyAsync(map.noVisibleBlocks.data, &n, sizeof n, cudaMemcpyHostToDevice, cudaStreamLegacy);
+    cudaStreamSynchronize(cudaStreamLegacy);
+}
+
+// The session's whole map written into the DeviceMap's own buffers
+// (hashEntries, voxelBlocks, heapMem, heapCounter, entryPtr, and the visible
+// list), in the reference's layouts.  Call it before code that reads
+// Mapping's device buffers directly, such as System::WriteMapToDisk.
+inline void ExportMap(const DeviceMap& map) {
+    MapState* m = find_map(map);
+    if (!m) return;
+    check(fb_map_export_reference(m->session, map.hashEntries.data, map.hashEntries.size, map.voxelBlocks.data,
+                                  map.voxelBlocks.size, map.heapMem.data, map.heapMem.size, map.heapCounter.data,
+                                  map.entryPtr.data, legacy()),
+          "ExportMap");
+    write_visible(map, m->session);
 }
 
 }  // namespace fusion_b200_shim
@@ -239,10 +290,10 @@ void RGBStep(const DeviceArray2D<unsigned char>& nextImage, const DeviceArray2D<
 
 // ------------------------------------------------ Mapping/RenderScene.h
 
-void ResetMap(DeviceMap) {
+void ResetMap(DeviceMap map) {
     using namespace fusion_b200_shim;
-    // before the first frame there is no session yet: it starts empty
-    if (map_state().session) check(fb_reset_map(map_state().session), "ResetMap");
+    // a DeviceMap without a session yet (before its first frame) is empty
+    if (MapState* m = find_map(map)) check(fb_reset_map(m->session), "ResetMap");
 }
 
 void ResetKeyPoints(KeyMap) {}
@@ -254,64 +305,79 @@ void CollectKeyPoints(KeyMap, DeviceArray<SURF>&, DeviceArray<uint>& noKeys) {
     cudaMemcpy(noKeys.data, &zero, sizeof zero, cudaMemcpyHostToDevice);
 }
 
-void CheckBlockVisibility(DeviceMap, DeviceArray<uint>&, Matrix3f Rview, Matrix3f RviewInv, float3 tview, int cols,
-                          int rows_, float fx, float fy, float cx, float cy, float depthMax, float depthMin,
-                          uint* host_data) {
+void CheckBlockVisibility(DeviceMap map, DeviceArray<uint>& noVisibleBlocks, Matrix3f Rview, Matrix3f RviewInv,
+                          float3 tview, int cols, int rows_, float fx, float fy, float cx, float cy, float depthMax,
+                          float depthMin, uint* host_data) {
     using namespace fusion_b200_shim;
-    fb_session* s = bind_map(cols, rows_, fx, fy, cx, cy, depthMin, depthMax);
+    fb_session* s = bind_map(map, cols, rows_, fx, fy, cx, cy, depthMin, depthMax).session;
     const float k[4] = {fx, fy, cx, cy};
     uint32_t n = 0;
     check(fb_check_block_visibility(s, rows(Rview), rows(RviewInv), &tview.x, cols, rows_, k, &n, legacy()),
           "CheckBlockVisibility");
+    write_visible(map, s);
+    if (noVisibleBlocks.data && noVisibleBlocks.data != map.noVisibleBlocks.data)
+        cudaMemcpy(noVisibleBlocks.data, &n, sizeof n, cudaMemcpyHostToDevice);
     if (host_data) *host_data = n;
 }
 
 void FuseMapColor(const DeviceArray2D<float>& depth, const DeviceArray2D<uchar3>& color,
-                  const DeviceArray2D<float4>& nmap, DeviceArray<uint>&, Matrix3f Rview, Matrix3f RviewInv,
-                  float3 tview, DeviceMap, float fx, float fy, float cx, float cy, float depthMax, float depthMin,
-                  uint* host_data) {
+                  const DeviceArray2D<float4>& nmap, DeviceArray<uint>& noVisibleBlocks, Matrix3f Rview,
+                  Matrix3f RviewInv, float3 tview, DeviceMap map, float fx, float fy, float cx, float cy,
+                  float depthMax, float depthMin, uint* host_data) {
     using namespace fusion_b200_shim;
-    fb_session* s = bind_map(depth.cols, depth.rows, fx, fy, cx, cy, depthMin, depthMax);
+    fb_session* s = bind_map(map, depth.cols, depth.rows, fx, fy, cx, cy, depthMin, depthMax).session;
     fb_image d = img(depth), c = img(color), n = img(nmap);
     const float k[4] = {fx, fy, cx, cy};
     uint32_t no = 0;
     check(fb_fuse_map_color(s, &d, &c, &n, rows(Rview), rows(RviewInv), &tview.x, k, &no, legacy()),
           "FuseMapColor");
+    write_visible(map, s);
+    if (noVisibleBlocks.data && noVisibleBlocks.data != map.noVisibleBlocks.data)
+        cudaMemcpy(noVisibleBlocks.data, &no, sizeof no, cudaMemcpyHostToDevice);
     if (host_data) *host_data = no;
 }
 
-bool CreateRenderingBlocks(const DeviceArray<HashEntry>&, DeviceArray2D<float>&, DeviceArray2D<float>&,
-                           const float&, const float&, DeviceArray<RenderingBlock>&, DeviceArray<uint>&, Matrix3f,
-                           float3, uint noVisibleBlocks, float fx, float fy, float cx, float cy) {
-    fusion_b200_shim::MapState& m = fusion_b200_shim::map_state();
+bool CreateRenderingBlocks(const DeviceArray<HashEntry>& visibleBlocks, DeviceArray2D<float>& zRangeX,
+                           DeviceArray2D<float>& zRangeY, const float&, const float&, DeviceArray<RenderingBlock>&,
+                           DeviceArray<uint>& noRenderingBlocks, Matrix3f RviewInv, float3 tview,
+                           uint noVisibleBlocks, float fx, float fy, float cx, float cy) {
+    using namespace fusion_b200_shim;
+    auto it = by_visible().find((const void*)visibleBlocks.data);
+    if (it == by_visible().end() || noVisibleBlocks == 0) return false;
+    MapState& m = *it->second;
     m.K[0] = fx;
     m.K[1] = fy;
     m.K[2] = cx;
     m.K[3] = cy;
-    return m.session != nullptr && noVisibleBlocks > 0;
+    fb_image zx = img(zRangeX), zy = img(zRangeY);
+    uint32_t tiles = 0;
+    check(fb_create_rendering_blocks(m.session, rows(RviewInv), &tview.x, m.K, &zx, &zy, &tiles, legacy()),
+          "CreateRenderingBlocks");
+    if (noRenderingBlocks.data) cudaMemcpy(noRenderingBlocks.data, &tiles, sizeof tiles, cudaMemcpyHostToDevice);
+    return tiles > 0;
 }
 
-void Raycast(DeviceMap, DeviceArray2D<float4>& vmap, DeviceArray2D<float4>& nmap, DeviceArray2D<float>&,
+void Raycast(DeviceMap map, DeviceArray2D<float4>& vmap, DeviceArray2D<float4>& nmap, DeviceArray2D<float>&,
              DeviceArray2D<float>&, Matrix3f Rview, Matrix3f RviewInv, float3 tview, float, float, float, float) {
     using namespace fusion_b200_shim;
-    MapState& m = map_state();
-    if (!m.session) return;
+    MapState* m = find_map(map);
+    if (!m) return;
     fb_image v = img(vmap), n = img(nmap);
     int rendered = 0;
-    check(fb_raycast(m.session, &v, &n, rows(Rview), rows(RviewInv), &tview.x, m.K, &rendered, legacy()),
+    check(fb_raycast(m->session, &v, &n, rows(Rview), rows(RviewInv), &tview.x, m->K, &rendered, legacy()),
           "Raycast");
 }
 
-uint MeshScene(DeviceArray<uint>&, DeviceArray<uint>&, DeviceMap, const DeviceArray<int>&, const DeviceArray<int>&,
-               const DeviceArray2D<int>&, DeviceArray<float3>& normal, DeviceArray<float3>& vertex,
-               DeviceArray<uchar3>& color, DeviceArray<int3>&) {
+uint MeshScene(DeviceArray<uint>&, DeviceArray<uint>&, DeviceMap map, const DeviceArray<int>&,
+               const DeviceArray<int>&, const DeviceArray2D<int>&, DeviceArray<float3>& normal,
+               DeviceArray<float3>& vertex, DeviceArray<uchar3>& color, DeviceArray<int3>&) {
     using namespace fusion_b200_shim;
-    MapState& m = map_state();
-    if (!m.session) return 0;
+    MapState* m = find_map(map);
+    if (!m) return 0;
     size_t cap = vertex.size < normal.size ? vertex.size : normal.size;
     if (color.size < cap) cap = color.size;
     uint64_t n = 0;
-    check(fb_mesh_scene(m.session, (float*)vertex.data, (float*)normal.data, (uint8_t*)color.data, cap / 3, &n,
+    check(fb_mesh_scene(m->session, (float*)vertex.data, (float*)normal.data, (uint8_t*)color.data, cap / 3, &n,
                         legacy()),
           "MeshScene");
     return (uint)(n < cap / 3 ? n : cap / 3);
