@@ -465,11 +465,12 @@ def ours_at_reference_constants(depth, rgb, frames=80, warmup=5):
             "mesh": mesh}
 
 
-def _batched_run(specs, seeds, warmup, steps, tune=False):
+def _batched_run(specs, seeds, warmup, steps, tune=False, mode=0):
     """Sessions `specs` [(w, h, voxel, config)] stepped together through
-    fb_batch_step, frames resident in HBM (each session plays a pre-rendered
-    seeded sequence forwards and backwards).  Returns aggregate frames/s,
-    ms per step, tracked fraction and the autotuned raycast tiles."""
+    fb_batch_step in batch mode `mode`, frames resident in HBM (each session
+    plays a pre-rendered seeded sequence forwards and backwards).  Returns
+    aggregate frames/s, ms per step, tracked fraction, the autotuned raycast
+    tiles and (mode 2) the kernel launches of a step."""
     import torch
     import rgbd_synth as synth
     from fusion_b200 import Batch, Session
@@ -494,7 +495,7 @@ def _batched_run(specs, seeds, warmup, steps, tune=False):
         j = j if j < n_fr else 2 * n_fr - 2 - j
         return [(seqs[k][0][j], seqs[k][1][j]) for k in keys]
 
-    b = Batch(mode=0)
+    b = Batch(mode=mode)
     for _ in range(warmup):
         b.step(sess, frames(), on_device=True)
     tiles = None
@@ -507,13 +508,18 @@ def _batched_run(specs, seeds, warmup, steps, tune=False):
     for _ in range(steps):
         tracked += sum(r.tracked for r in b.step(sess, frames(), on_device=True))
     dt = time.perf_counter() - t0
+    launches = b.launch_stats() if mode == 2 else None
     b.close()
     for s in sess:
         s.close()
     n = len(specs)
-    return {"value": n * steps / dt, "unit": "frames/s", "ms_per_step": dt / steps * 1e3, "sessions": n,
-            "steps": steps, "warmup": warmup, "tracked_fraction": tracked / (n * steps),
-            "raycast_tiles": {f"{w}x{h}": list(t) for (w, h), t in tiles.items()} if tiles else None}
+    out = {"value": n * steps / dt, "unit": "frames/s", "ms_per_step": dt / steps * 1e3, "sessions": n,
+           "steps": steps, "warmup": warmup, "tracked_fraction": tracked / (n * steps), "batch_mode": mode,
+           "raycast_tiles": {f"{w}x{h}": list(t) for (w, h), t in tiles.items()} if tiles else None}
+    if launches:
+        out["launches_per_step"] = launches[0]
+        out["per_session_kernels_per_step"] = launches[1]
+    return out
 
 
 def precision_form(depth, rgb, W, K, plain_value, peak, peak_kind):
@@ -601,7 +607,15 @@ def batched_forms(args, rank, plain_value):
     mix["workload"] = (f"{n} ragged sessions: resolution uniform over 160x120/320x240/640x480, voxel "
                        "uniform 4-20 mm, truncation 4 voxels, maps sized per voxel size")
     mix["vs_plain"] = mix["value"] / plain_value
-    return {"same_config": c2, "mixed": mix}
+    # fused launches (batch mode 2): one launch per stage kernel for all sessions
+    c2f = _batched_run([(640, 480, 0.005, S.config_c2())] * n, seeds, 3, 8, mode=2)
+    c2f["workload"] = c2["workload"] + "; fused launches"
+    c2f["vs_plain"] = c2f["value"] / plain_value
+    mixf = _batched_run([(w, h, v, mixed_config(w, h, v)) for (w, h, v) in mixed_population(n, 1234 + rank)],
+                        seeds, 3, 10, mode=2)
+    mixf["workload"] = mix["workload"] + "; fused launches"
+    mixf["vs_plain"] = mixf["value"] / plain_value
+    return {"same_config": c2, "mixed": mix, "same_config_fused": c2f, "mixed_fused": mixf}
 
 
 def served_form(args, rank, plain_value):

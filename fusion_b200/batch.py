@@ -56,7 +56,8 @@ def mixed_population(n, seed):
 
 class Batch:
     """fb_batch: mode 0 launches each session's frame graph on its own stream;
-    mode 1 captures one graph per composition of the step."""
+    mode 1 captures one graph per composition of the step; mode 2 (fused)
+    runs each stage kernel once for all sessions of the step."""
 
     def __init__(self, mode=0, stream=None):
         self.lib = _lib.load()
@@ -112,6 +113,13 @@ class Batch:
         steps, caps = ctypes.c_uint64(), ctypes.c_uint64()
         check("fb_batch_stats", self.lib.fb_batch_stats(self.h, ctypes.byref(steps), ctypes.byref(caps)))
         return steps.value, caps.value
+
+    def launch_stats(self):
+        """Mode 2: (kernel launches of the last step, per-session kernels they carried)."""
+        launches, kernels = ctypes.c_int(), ctypes.c_int()
+        check("fb_batch_launch_stats",
+              self.lib.fb_batch_launch_stats(self.h, ctypes.byref(launches), ctypes.byref(kernels)))
+        return launches.value, kernels.value
 
 
 def set_raycast_tile(session, bx, by):

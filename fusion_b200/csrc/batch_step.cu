@@ -1,8 +1,12 @@
 // Batched steps (fb_batch_*): one frame of each of n independent sessions
-// with all frames in flight together, each session's cached frame graph on
-// its own stream of the batch, or one composite graph per composition.
+// with all frames in flight together -- each session's cached frame graph on
+// its own stream of the batch (mode 0), one composite graph per composition
+// (mode 1), or fused launches (mode 2): every stage kernel runs once for all
+// sessions of the step, as one launch whose grid is the concatenation of the
+// sessions' grids (fb_fused.cuh), captured as one graph per composition.
 #include <algorithm>
 #include <cstring>
+#include <tuple>
 #include <map>
 #include <new>
 #include <vector>
@@ -10,6 +14,27 @@
 #include "session_internal.h"
 
 // ------------------------------------------------------------------ batches
+
+// One merged launch of a fused step: the fused kernel over n parts (one per
+// session that issued this launch), its parts and argument tuples at byte
+// offsets of the plan's device buffer.
+struct FusedLaunch {
+    const void* fused;
+    dim3 block;
+    size_t smem;
+    int n, blocks;
+    size_t parts_off, args_off;
+};
+
+// The fused launches of one composition, their device-side arguments and,
+// once the composition repeats, their graph.
+struct FusedPlan {
+    void* dev = nullptr;
+    std::vector<FusedLaunch> launches;
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;      // per-session kernel launches the merged ones replace
+    uint64_t uses = 0;
+};
 
 struct fb_batch {
     cudaStream_t origin = nullptr;
@@ -21,6 +46,11 @@ struct fb_batch {
     // mode 1: one graph per composition
     std::map<std::vector<uint64_t>, std::pair<cudaGraphExec_t, int>> cache;
     uint64_t steps = 0, captures = 0;
+    // mode 2: fused plans by composition, the recorders of a step's frames
+    std::map<std::vector<uint64_t>, FusedPlan> fused;
+    std::vector<LaunchRecorder> recs;
+    std::vector<unsigned char> blob;
+    int last_launches = 0, last_kernels = 0;   // of the last fused step
 };
 
 namespace {
@@ -30,6 +60,190 @@ constexpr size_t kBatchCacheMax = 32;
 void clear_cache(fb_batch* b) {
     for (auto& kv : b->cache) cudaGraphExecDestroy(kv.second.first);
     b->cache.clear();
+}
+
+constexpr size_t kFusedCacheMax = 64;
+
+void clear_fused(fb_batch* b) {
+    if (b->fused.empty()) return;
+    cudaStreamSynchronize(b->origin);
+    for (auto& kv : b->fused) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (kv.second.dev) cudaFreeAsync(kv.second.dev, b->origin);
+    }
+    b->fused.clear();
+}
+
+// The composition of a step: each session with what decides its launches
+// (tracker mode, fusion, frame parity, map form options, raycast tile).
+std::vector<uint64_t> composition(fb_session* const* ss, int n, const FramePlan* plans) {
+    std::vector<uint64_t> key;
+    key.reserve(2 * n);
+    for (int i = 0; i < n; ++i) {
+        const fb_session* s = ss[i];
+        key.push_back((uint64_t)(uintptr_t)s);
+        key.push_back((uint64_t)plans[i].mode | (uint64_t)plans[i].fuse << 2 | (uint64_t)s->next << 3 |
+                      (uint64_t)s->shared_gpu << 5 | (uint64_t)s->mapping_disabled << 6 |
+                      (uint64_t)s->rc_bx << 8 | (uint64_t)s->rc_by << 20);
+    }
+    return key;
+}
+
+// Records every session's frame (and its result read-back), merges the
+// launches of the same slot and kernel across sessions, and uploads the
+// merged launches' parts and argument tuples.
+int build_fused(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plans, FusedPlan& out) {
+    if ((int)b->recs.size() < n) b->recs.resize(n);
+    int kernels = 0;
+    for (int i = 0; i < n; ++i)
+        if (!ss[i]->h_out_dev) {
+            fb_set_error_text("fused batch step: a session's pinned result has no device address");
+            return FB_ECUDA;
+        }
+    for (int i = 0; i < n; ++i) {
+        fb_session* s = ss[i];
+        LaunchRecorder& r = b->recs[i];
+        r.clear();
+        const bool prof = s->profile;
+        s->profile = false;   // no stage events inside fused launches
+        launch_recorder() = &r;
+        unsigned ran = 0;
+        const int issued = issue_frame(s, plans[i].track, plans[i].fuse, plans[i].render, plans[i].init, &ran);
+        launch_slot(kSlotOut);
+        launch_result_out(s, b->origin);
+        launch_recorder() = nullptr;
+        s->profile = prof;
+        // every kernel of the frame went through the recorder, in slot order
+        if ((int)r.recs.size() != issued + 1) {
+            fb_set_error_text("fused batch step: a frame kernel was not recorded");
+            return FB_ECUDA;
+        }
+        for (size_t k = 1; k < r.recs.size(); ++k)
+            if (r.recs[k].slot <= r.recs[k - 1].slot) {
+                fb_set_error_text("fused batch step: frame launches out of slot order");
+                return FB_ECUDA;
+            }
+        kernels += (int)r.recs.size();
+    }
+    // (slot, kernel, block shape, shared memory, session): launches of one
+    // slot and kernel merge; the sessions' parts keep session order
+    using Ent = std::tuple<uint64_t, uintptr_t, unsigned, unsigned, unsigned, size_t, int, int>;
+    std::vector<Ent> ents;
+    ents.reserve((size_t)kernels);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < (int)b->recs[i].recs.size(); ++k) {
+            const LaunchRec& r = b->recs[i].recs[k];
+            if (r.grid.z != 1 || r.block.z != 1) {
+                fb_set_error_text("fused batch step: 3-D grid");
+                return FB_ECUDA;
+            }
+            ents.emplace_back(r.slot, (uintptr_t)r.fused, r.block.x, r.block.y, r.block.z, r.smem, i, k);
+        }
+    std::sort(ents.begin(), ents.end());
+    std::vector<FusedLaunch> launches;
+    std::vector<std::pair<size_t, size_t>> groups;   // [first, last) in ents
+    size_t bytes = 0;
+    for (size_t e = 0; e < ents.size();) {
+        size_t f = e + 1;
+        while (f < ents.size() && std::get<0>(ents[f]) == std::get<0>(ents[e]) &&
+               std::get<1>(ents[f]) == std::get<1>(ents[e]) && std::get<2>(ents[f]) == std::get<2>(ents[e]) &&
+               std::get<3>(ents[f]) == std::get<3>(ents[e]) && std::get<5>(ents[f]) == std::get<5>(ents[e]))
+            ++f;
+        const LaunchRec& r0 = b->recs[std::get<6>(ents[e])].recs[std::get<7>(ents[e])];
+        FusedLaunch L;
+        L.fused = r0.fused;
+        L.block = r0.block;
+        L.smem = r0.smem;
+        L.n = (int)(f - e);
+        L.blocks = 0;
+        L.parts_off = (bytes + 15) & ~(size_t)15;
+        bytes = L.parts_off + sizeof(FusedPart) * L.n;
+        L.args_off = (bytes + 15) & ~(size_t)15;
+        bytes = L.args_off + r0.size * L.n;
+        launches.push_back(L);
+        groups.emplace_back(e, f);
+        e = f;
+    }
+    b->blob.assign(bytes, 0);
+    for (size_t g = 0; g < launches.size(); ++g) {
+        FusedLaunch& L = launches[g];
+        FusedPart* parts = (FusedPart*)(b->blob.data() + L.parts_off);
+        size_t size0 = 0;
+        for (size_t e = groups[g].first; e < groups[g].second; ++e) {
+            const LaunchRec& r = b->recs[std::get<6>(ents[e])].recs[std::get<7>(ents[e])];
+            if (e == groups[g].first) size0 = r.size;
+            if (r.size != size0) {
+                fb_set_error_text("fused batch step: argument tuples of one kernel differ in size");
+                return FB_ECUDA;
+            }
+            const int j = (int)(e - groups[g].first);
+            const long long nb = (long long)r.grid.x * r.grid.y;
+            if (nb <= 0 || L.blocks + nb > 0x7fffffffLL) {
+                fb_set_error_text("fused batch step: grid too large");
+                return FB_ECUDA;
+            }
+            parts[j] = FusedPart{L.blocks, (int)r.grid.x, (int)r.grid.y, 0};
+            L.blocks += (int)nb;
+            const unsigned char* src = b->recs[std::get<6>(ents[e])].bytes.data() + r.off;
+            std::memcpy(b->blob.data() + L.args_off + (size_t)j * r.size, src, r.size);
+        }
+    }
+    FB_CUDA(cudaMallocAsync(&out.dev, bytes ? bytes : 16, b->origin));
+    if (bytes) FB_CUDA(cudaMemcpyAsync(out.dev, b->blob.data(), bytes, cudaMemcpyHostToDevice, b->origin));
+    out.launches = std::move(launches);
+    out.kernels = kernels;
+    return FB_OK;
+}
+
+int launch_fused(fb_batch* b, const FusedPlan& p) {
+    for (const FusedLaunch& L : p.launches) {
+        FusedArgs fa;
+        fa.parts = (const FusedPart*)((const char*)p.dev + L.parts_off);
+        fa.args = (const char*)p.dev + L.args_off;
+        fa.n = L.n;
+        void* kargs[] = {&fa};
+        FB_CUDA(cudaLaunchKernel(L.fused, dim3((unsigned)L.blocks), L.block, kargs, L.smem, b->origin));
+    }
+    return FB_OK;
+}
+
+// One fused step: the plan of this composition (built on first sight), its
+// graph from the second use on (a composition seen once is launched
+// directly: no instantiation for one-off mixes of the served form).
+int fused_step(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plans) {
+    std::vector<uint64_t> key = composition(ss, n, plans);
+    auto it = b->fused.find(key);
+    if (it == b->fused.end()) {
+        if (b->fused.size() >= kFusedCacheMax) clear_fused(b);
+        FusedPlan p;
+        int rc = build_fused(b, ss, n, plans, p);
+        if (rc) {
+            if (p.dev) cudaFreeAsync(p.dev, b->origin);
+            return rc;
+        }
+        it = b->fused.emplace(std::move(key), std::move(p)).first;
+    }
+    FusedPlan& p = it->second;
+    if (p.uses > 0 && !p.exec) {
+        cudaGraph_t graph = nullptr;
+        FB_CUDA(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
+        int rc = launch_fused(b, p);
+        cudaError_t e = cudaStreamEndCapture(b->origin, &graph);
+        if (rc == FB_OK && e == cudaSuccess) e = cudaGraphInstantiate(&p.exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (rc) return rc;
+        FB_CUDA(e);
+        b->captures++;
+    }
+    if (p.exec)
+        FB_CUDA(cudaGraphLaunch(p.exec, b->origin));
+    else if (int rc = launch_fused(b, p))
+        return rc;
+    p.uses++;
+    b->last_launches = (int)p.launches.size();
+    b->last_kernels = p.kernels;
+    ss[0]->launches += (uint64_t)p.launches.size();
+    return check_launch();
 }
 
 // Slot streams of a batch: a fixed set, created with the batch.  Creating a
@@ -132,6 +346,7 @@ int fb_batch_destroy(fb_batch* b) {
     if (!b) return FB_EINVAL;
     cudaStreamSynchronize(b->origin);
     clear_cache(b);
+    clear_fused(b);
     for (size_t i = 0; i < b->slots.size(); ++i) {
         cudaStreamSynchronize(b->slots[i]);
         cudaStreamDestroy(b->slots[i]);
@@ -154,8 +369,15 @@ int fb_batch_reserve(fb_batch* b, size_t bytes) {
 }
 
 int fb_batch_set_mode(fb_batch* b, int mode) {
-    if (!b || mode < 0 || mode > 1) return FB_EINVAL;
+    if (!b || mode < 0 || mode > 2) return FB_EINVAL;
     b->mode = mode;
+    return FB_OK;
+}
+
+int fb_batch_launch_stats(fb_batch* b, int* launches, int* kernels) {
+    if (!b) return FB_EINVAL;
+    if (launches) *launches = b->last_launches;
+    if (kernels) *kernels = b->last_kernels;
     return FB_OK;
 }
 
@@ -187,21 +409,20 @@ int fb_batch_step(fb_batch* b, fb_session* const* ss, int n, const fb_frame_inpu
     // frame graphs are the ones fb_session_prepare(s, 1) captures); smaller
     // steps run the forms of a session alone (fb_session_prepare(s, 0)),
     // which finish sooner.  Both give the same results.
-    const bool shared = n > kBatchSharedMin;
+    // fused steps always run the group forms (clusters do not span the parts
+    // of a fused grid)
+    const bool shared = n > kBatchSharedMin || b->mode == 2;
     for (int i = 0; i < n; ++i) ss[i]->shared_gpu = shared;
     std::vector<FramePlan> plans(n);
     for (int i = 0; i < n; ++i) plans[i] = plan_frame(ss[i]);
-    if (b->mode == 1) {
-        std::vector<uint64_t> key;
-        key.reserve(2 * n);
-        for (int i = 0; i < n; ++i) {
-            const fb_session* s = ss[i];
-            key.push_back((uint64_t)(uintptr_t)s);
-            key.push_back((uint64_t)plans[i].mode | (uint64_t)plans[i].fuse << 2 | (uint64_t)s->next << 3 |
-                          (uint64_t)s->shared_gpu << 5 |
-                          (uint64_t)s->mapping_disabled << 6 | (uint64_t)s->rc_bx << 8 |
-                          (uint64_t)s->rc_by << 20);
+    if (b->mode == 2) {
+        rc = fused_step(b, ss, n, plans.data());
+        if (rc) {
+            for (int i = 0; i < n; ++i) ss[i]->shared_gpu = false;
+            return rc;
         }
+    } else if (b->mode == 1) {
+        std::vector<uint64_t> key = composition(ss, n, plans.data());
         auto it = b->cache.find(key);
         if (it == b->cache.end()) {
             if (b->cache.size() >= kBatchCacheMax) clear_cache(b);

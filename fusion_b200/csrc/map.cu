@@ -32,6 +32,7 @@
 // of depth and normal, one word of colour).
 #include <cuda_fp16.h>
 
+#include "fb_fused.cuh"
 #include "fb_internal.h"
 
 namespace fb {
@@ -101,12 +102,12 @@ __device__ __forceinline__ void request_block(const MapView& m, int x, int y, in
 }
 
 // Fusion::CreateBlocks (FuseMap.cu:80-111) for one pixel of the raw depth map.
-__global__ void __launch_bounds__(256) k_alloc_requests(MapView m, const float* __restrict__ raw, int rp, int W,
-                                                        int H, Intr k, const DevPose* __restrict__ posep,
-                                                        const int* __restrict__ skip) {
+__device__ __forceinline__ void alloc_requests_body(const BlockCtx& ctx, MapView m, const float* __restrict__ raw,
+                                                    int rp, int W, int H, Intr k, const DevPose* __restrict__ posep,
+                                                    const int* __restrict__ skip) {
     if (skip && *skip) return;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int x = ctx.bx * blockDim.x + threadIdx.x;
+    const int y = ctx.by * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
     const float z = raw[(size_t)y * rp + x];
     const float dmin = m.g.depth_min, dmax = m.g.depth_max;
@@ -141,18 +142,29 @@ __global__ void __launch_bounds__(256) k_alloc_requests(MapView m, const float* 
     }
 }
 
-__global__ void k_alloc_count(MapView m) {
+__global__ void __launch_bounds__(256) k_alloc_requests(MapView m, const float* __restrict__ raw, int rp, int W,
+                                  int H, Intr k, const DevPose* __restrict__ posep, const int* __restrict__ skip) {
+    alloc_requests_body(own_ctx(), m, raw, rp, W, H, k, posep, skip);
+}
+FB_FUSED_KERNEL(k_alloc_requests, alloc_requests_body, 256)
+
+__device__ __forceinline__ void alloc_count_body(const BlockCtx& ctx, MapView m) {
     const int M = min(m.ctr->n_req, m.newcap);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x)
+    for (int i = ctx.bx * blockDim.x + threadIdx.x; i < M; i += ctx.gx * blockDim.x)
         m.newblk[i].j = atomicAdd(&m.bucket_cnt[m.newblk[i].bucket], 1);
 }
 
+__global__ void __launch_bounds__(256) k_alloc_count(MapView m) {
+    alloc_count_body(own_ctx(), m);
+}
+FB_FUSED_KERNEL(k_alloc_count, alloc_count_body, 256)
+
 // Per chunk of kScanChunk buckets: number of new blocks, and of those that go
 // to the excess list (all but the first when the bucket's head slot is empty).
-__global__ void __launch_bounds__(256) k_scan_chunks(MapView m) {
+__device__ __forceinline__ void scan_chunks_body(const BlockCtx& ctx, MapView m) {
     if (m.ctr->n_req == 0) return;
     __shared__ int s_c[256], s_x[256];
-    const int base = blockIdx.x * kScanChunk;
+    const int base = ctx.bx * kScanChunk;
     int c = 0, xs = 0;
     for (int q = threadIdx.x; q < kScanChunk; q += 256) {
         int b = base + q;
@@ -175,15 +187,20 @@ __global__ void __launch_bounds__(256) k_scan_chunks(MapView m) {
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        m.chunk_sums[2 * blockIdx.x] = s_c[0];
-        m.chunk_sums[2 * blockIdx.x + 1] = s_x[0];
+        m.chunk_sums[2 * ctx.bx] = s_c[0];
+        m.chunk_sums[2 * ctx.bx + 1] = s_x[0];
     }
 }
+
+__global__ void __launch_bounds__(256) k_scan_chunks(MapView m) {
+    scan_chunks_body(own_ctx(), m);
+}
+FB_FUSED_KERNEL(k_scan_chunks, scan_chunks_body, 256)
 
 // Exclusive scan over the chunk sums (one block of 1024 threads, chunks in
 // order); snapshot of the counters and choice of the parallel or sequential
 // insertion path.
-__global__ void __launch_bounds__(1024) k_scan_top(MapView m) {
+__device__ __forceinline__ void scan_top_body(const BlockCtx& ctx, MapView m) {
     MapCounters* c = m.ctr;
     const int M = min(c->n_req, m.newcap);
     __shared__ int s_a[1024], s_e[1024];
@@ -235,13 +252,18 @@ __global__ void __launch_bounds__(1024) k_scan_top(MapView m) {
     }
 }
 
+__global__ void __launch_bounds__(1024) k_scan_top(MapView m) {
+    scan_top_body(own_ctx(), m);
+}
+FB_FUSED_KERNEL(k_scan_top, scan_top_body, 1024)
+
 // Per chunk: exclusive scan of the per-bucket counts into segment starts and
 // excess starts.
-__global__ void __launch_bounds__(256) k_scan_apply(MapView m) {
+__device__ __forceinline__ void scan_apply_body(const BlockCtx& ctx, MapView m) {
     if (m.ctr->snap_M == 0) return;
     __shared__ int s_c[256], s_x[256];
     constexpr int per = kScanChunk / 256;
-    const int base = blockIdx.x * kScanChunk + threadIdx.x * per;
+    const int base = ctx.bx * kScanChunk + threadIdx.x * per;
     int cnt[per], he[per];
     int c = 0, xs = 0;
 #pragma unroll
@@ -268,8 +290,8 @@ __global__ void __launch_bounds__(256) k_scan_apply(MapView m) {
         s_x[threadIdx.x] += ax;
         __syncthreads();
     }
-    int run_c = m.chunk_sums[2 * blockIdx.x] + s_c[threadIdx.x] - c;
-    int run_x = m.chunk_sums[2 * blockIdx.x + 1] + s_x[threadIdx.x] - xs;
+    int run_c = m.chunk_sums[2 * ctx.bx] + s_c[threadIdx.x] - c;
+    int run_x = m.chunk_sums[2 * ctx.bx + 1] + s_x[threadIdx.x] - xs;
 #pragma unroll
     for (int q = 0; q < per; ++q) {
         int b = base + q;
@@ -282,13 +304,23 @@ __global__ void __launch_bounds__(256) k_scan_apply(MapView m) {
     }
 }
 
-__global__ void k_alloc_place(MapView m) {
+__global__ void __launch_bounds__(256) k_scan_apply(MapView m) {
+    scan_apply_body(own_ctx(), m);
+}
+FB_FUSED_KERNEL(k_scan_apply, scan_apply_body, 256)
+
+__device__ __forceinline__ void alloc_place_body(const BlockCtx& ctx, MapView m) {
     const int M = m.ctr->snap_M;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
+    for (int i = ctx.bx * blockDim.x + threadIdx.x; i < M; i += ctx.gx * blockDim.x) {
         const NewBlock& nb = m.newblk[i];
         m.arrival[m.bucket_start[nb.bucket] + nb.j] = i;
     }
 }
+
+__global__ void __launch_bounds__(256) k_alloc_place(MapView m) {
+    alloc_place_body(own_ctx(), m);
+}
+FB_FUSED_KERNEL(k_alloc_place, alloc_place_body, 256)
 
 __device__ __forceinline__ bool coord_less(const NewBlock& a, const NewBlock& b) {
     if (a.x != b.x) return a.x < b.x;
@@ -296,9 +328,9 @@ __device__ __forceinline__ bool coord_less(const NewBlock& a, const NewBlock& b)
     return a.z < b.z;
 }
 
-__global__ void k_alloc_rank(MapView m) {
+__device__ __forceinline__ void alloc_rank_body(const BlockCtx& ctx, MapView m) {
     const int M = m.ctr->snap_M;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < M; p += gridDim.x * blockDim.x) {
+    for (int p = ctx.bx * blockDim.x + threadIdx.x; p < M; p += ctx.gx * blockDim.x) {
         const int i = m.arrival[p];
         const NewBlock me = m.newblk[i];
         const int s = m.bucket_start[me.bucket], n = m.bucket_cnt[me.bucket];
@@ -309,6 +341,11 @@ __global__ void k_alloc_rank(MapView m) {
         m.order[s + r] = i;
     }
 }
+
+__global__ void __launch_bounds__(256) k_alloc_rank(MapView m) {
+    alloc_rank_body(own_ctx(), m);
+}
+FB_FUSED_KERNEL(k_alloc_rank, alloc_rank_body, 256)
 
 // CreateBlock (DeviceMap.cu:23-62) without lock contention, one block at a
 // time, for the sequential path.  Returns the slot written or -1.
@@ -357,12 +394,12 @@ __device__ int create_block_seq(const MapView& m, int x, int y, int z, int& hc, 
     return -1;
 }
 
-__global__ void __launch_bounds__(256) k_alloc_insert(MapView m) {
+__device__ __forceinline__ void alloc_insert_body(const BlockCtx& ctx, MapView m) {
     MapCounters* c = m.ctr;
     const int M = c->snap_M;
     if (M == 0) return;
     const int hc0 = c->snap_hc, ep0 = c->snap_ep, na0 = c->snap_na;
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    const int gtid = ctx.bx * blockDim.x + threadIdx.x, gstride = ctx.gx * blockDim.x;
     if (!c->fast) {
         if (gtid == 0) {
             int hc = hc0, ep = ep0, holes = c->holes, na = na0;
@@ -421,12 +458,17 @@ __global__ void __launch_bounds__(256) k_alloc_insert(MapView m) {
     }
 }
 
-__global__ void k_alloc_finalize(MapView m) {
+__global__ void __launch_bounds__(256) k_alloc_insert(MapView m) {
+    alloc_insert_body(own_ctx(), m);
+}
+FB_FUSED_KERNEL(k_alloc_insert, alloc_insert_body, 256)
+
+__device__ __forceinline__ void alloc_finalize_body(const BlockCtx& ctx, MapView m) {
     MapCounters* c = m.ctr;
     const int M = c->snap_M;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x)
+    for (int i = ctx.bx * blockDim.x + threadIdx.x; i < M; i += ctx.gx * blockDim.x)
         m.bucket_cnt[m.newblk[i].bucket] = 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (ctx.bx == 0 && threadIdx.x == 0) {
         if (M > 0 && c->fast) {
             c->heap_counter = c->snap_hc - M;
             c->entry_ptr = c->snap_ep + c->excess_total;
@@ -439,6 +481,11 @@ __global__ void k_alloc_finalize(MapView m) {
         c->n_tiles = 0;
     }
 }
+
+__global__ void __launch_bounds__(256) k_alloc_finalize(MapView m) {
+    alloc_finalize_body(own_ctx(), m);
+}
+FB_FUSED_KERNEL(k_alloc_finalize, alloc_finalize_body, 256)
 
 // ---------------------------------------------------------------- visibility
 
@@ -477,20 +524,25 @@ __device__ bool block_visible(int bx, int by, int bz, const DevPose& P, const In
     return false;
 }
 
-__global__ void k_reset_visible(MapCounters* c) {
+__device__ __forceinline__ void reset_visible_body(const BlockCtx& ctx, MapCounters* c) {
     c->n_visible = 0;
     c->n_tiles = 0;
 }
 
-__global__ void __launch_bounds__(256) k_visibility(MapView m, int W, int H, Intr k, const DevPose* __restrict__ posep,
-                                                    const int* __restrict__ skip) {
+__global__ void __launch_bounds__(32) k_reset_visible(MapCounters* c) {
+    reset_visible_body(own_ctx(), c);
+}
+FB_FUSED_KERNEL(k_reset_visible, reset_visible_body, 32)
+
+__device__ __forceinline__ void visibility_body(const BlockCtx& ctx, MapView m, int W, int H, Intr k,
+                                                const DevPose* __restrict__ posep, const int* __restrict__ skip) {
     if (skip && *skip) return;
     const DevPose P = *posep;
     const int n = m.ctr->n_alloc;
     const int lane = threadIdx.x & 31;
-    const int nIter = (n + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x);
+    const int nIter = (n + ctx.gx * blockDim.x - 1) / (ctx.gx * blockDim.x);
     for (int it = 0; it < nIter; ++it) {
-        const int i = (it * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
+        const int i = (it * ctx.gx + ctx.bx) * blockDim.x + threadIdx.x;
         bool vis = false;
         int slot = -1;
         HEntry e;
@@ -517,6 +569,12 @@ __global__ void __launch_bounds__(256) k_visibility(MapView m, int W, int H, Int
         }
     }
 }
+
+__global__ void __launch_bounds__(256) k_visibility(MapView m, int W, int H, Intr k,
+                                  const DevPose* __restrict__ posep, const int* __restrict__ skip) {
+    visibility_body(own_ctx(), m, W, H, k, posep, skip);
+}
+FB_FUSED_KERNEL(k_visibility, visibility_body, 256)
 
 // --------------------------------------------------------------- integration
 
@@ -587,8 +645,8 @@ __device__ __forceinline__ bool integrate_voxel(Voxel& vox, int vx, int vy, int 
     return true;
 }
 
-__global__ void __launch_bounds__(256) k_integrate(MapView m, int W, int H, Intr k, const DevPose* __restrict__ posep,
-                                                   const int* __restrict__ skip) {
+__device__ __forceinline__ void integrate_body(const BlockCtx& ctx, MapView m, int W, int H, Intr k,
+                                               const DevPose* __restrict__ posep, const int* __restrict__ skip) {
     if (skip && *skip) return;
     __shared__ float s_div255[256];
     s_div255[threadIdx.x] = fd((float)threadIdx.x, 255.f);   // blockDim.x == 256
@@ -599,7 +657,7 @@ __global__ void __launch_bounds__(256) k_integrate(MapView m, int W, int H, Intr
     const int lx = (2 * t) & 7, ly = (t >> 2) & 7, lz = t >> 5;
     const float4* __restrict__ rec = m.frec;
     const uint32_t* __restrict__ col = m.fcol;
-    for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    for (int b = ctx.bx; b < n; b += ctx.gx) {
         const HEntry e = m.vis_blocks[b];
         const int vx = e.x * 8 + lx, vy = e.y * 8 + ly, vz = e.z * 8 + lz;
         uint4* base = (uint4*)(m.voxels + (size_t)e.ptr * 512) + t;
@@ -615,6 +673,12 @@ __global__ void __launch_bounds__(256) k_integrate(MapView m, int W, int H, Intr
         }
     }
 }
+
+__global__ void __launch_bounds__(256) k_integrate(MapView m, int W, int H, Intr k, const DevPose* __restrict__ posep,
+                                  const int* __restrict__ skip) {
+    integrate_body(own_ctx(), m, W, H, k, posep, skip);
+}
+FB_FUSED_KERNEL(k_integrate, integrate_body, 256)
 
 // Precision form of k_integrate: 6-byte voxels (FP16 TSDF and one r, g, b,
 // weight word), contracted FP32.  One wave of CTAs of 128 threads; each CTA
@@ -643,9 +707,9 @@ __device__ __forceinline__ float byte_as_magic(uint32_t word, uint32_t sel) {
     return __uint_as_float(__byte_perm(word, 0x4b400000u, sel | 0x7650u));
 }
 
-__global__ void __launch_bounds__(128, 7) k_integrate_compact(MapView m, int W, int H, Intr k,
-                                                           const DevPose* __restrict__ posep,
-                                                           const int* __restrict__ skip) {
+__device__ __forceinline__ void integrate_compact_body(const BlockCtx& ctx, MapView m, int W, int H, Intr k,
+                                                       const DevPose* __restrict__ posep,
+                                                       const int* __restrict__ skip) {
     if (skip && *skip) return;
     const DevPose P = *posep;
     const int n = min(m.ctr->n_visible, m.NS);
@@ -678,7 +742,7 @@ __global__ void __launch_bounds__(128, 7) k_integrate_compact(MapView m, int W, 
                       -(P.Rinv.r1.x * P.t.x + P.Rinv.r1.y * P.t.y + P.Rinv.r1.z * P.t.z),
                       -(P.Rinv.r2.x * P.t.x + P.Rinv.r2.y * P.t.y + P.Rinv.r2.z * P.t.z));
     const uint4* __restrict__ rec = (const uint4*)m.frec;   // packed records (fuse_record_packed)
-    for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    for (int b = ctx.bx; b < n; b += ctx.gx) {
         const HEntry e4 = m.vis_blocks[b];
         const int4 e = make_int4(e4.x, e4.y, e4.z, e4.ptr);
         uint8_t* blk = m.cvox + (size_t)e.w * kCBlockBytes;
@@ -746,6 +810,12 @@ __global__ void __launch_bounds__(128, 7) k_integrate_compact(MapView m, int W, 
         }
     }
 }
+
+__global__ void __launch_bounds__(128, 7) k_integrate_compact(MapView m, int W, int H, Intr k,
+                                  const DevPose* __restrict__ posep, const int* __restrict__ skip) {
+    integrate_compact_body(own_ctx(), m, W, H, k, posep, skip);
+}
+FB_FUSED_KERNEL(k_integrate_compact, integrate_compact_body, 128, 7)
 
 // ------------------------------------------------- the reference's layouts
 
@@ -866,23 +936,23 @@ int launch_map_reset(const MapView& m, cudaStream_t s) { k_map_reset<<<sm_count(
 int launch_allocate(const MapView& m, const float* raw, int rp, int W, int H, const Intr& k, const DevPose* pose,
                      const int* skip, cudaStream_t s) {
     dim3 b(32, 8), g((W + 31) / 32, (H + 7) / 8);
-    k_alloc_requests<<<g, b, 0, s>>>(m, raw, rp, W, H, k, pose, skip);
+    fb_launch(k_alloc_requests, (const void*)k_alloc_requests_fused, g, b, 0, s, m, raw, rp, W, H, k, pose, skip);
     const int gs = sm_count() * 4;
-    k_alloc_count<<<gs, 256, 0, s>>>(m);
-    k_scan_chunks<<<m.nchunks, 256, 0, s>>>(m);
-    k_scan_top<<<1, 1024, 0, s>>>(m);
-    k_scan_apply<<<m.nchunks, 256, 0, s>>>(m);
-    k_alloc_place<<<gs, 256, 0, s>>>(m);
-    k_alloc_rank<<<gs, 256, 0, s>>>(m);
-    k_alloc_insert<<<gs, 256, 0, s>>>(m);
-    k_alloc_finalize<<<gs, 256, 0, s>>>(m);
+    fb_launch(k_alloc_count, (const void*)k_alloc_count_fused, gs, 256, 0, s, m);
+    fb_launch(k_scan_chunks, (const void*)k_scan_chunks_fused, m.nchunks, 256, 0, s, m);
+    fb_launch(k_scan_top, (const void*)k_scan_top_fused, 1, 1024, 0, s, m);
+    fb_launch(k_scan_apply, (const void*)k_scan_apply_fused, m.nchunks, 256, 0, s, m);
+    fb_launch(k_alloc_place, (const void*)k_alloc_place_fused, gs, 256, 0, s, m);
+    fb_launch(k_alloc_rank, (const void*)k_alloc_rank_fused, gs, 256, 0, s, m);
+    fb_launch(k_alloc_insert, (const void*)k_alloc_insert_fused, gs, 256, 0, s, m);
+    fb_launch(k_alloc_finalize, (const void*)k_alloc_finalize_fused, gs, 256, 0, s, m);
     return 9;
 }
 
 int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
                        cudaStream_t s) {
-    k_reset_visible<<<1, 1, 0, s>>>(m.ctr);
-    k_visibility<<<sm_count() * 4, 256, 0, s>>>(m, W, H, k, pose, skip);
+    fb_launch(k_reset_visible, (const void*)k_reset_visible_fused, 1, 1, 0, s, m.ctr);
+    fb_launch(k_visibility, (const void*)k_visibility_fused, sm_count() * 4, 256, 0, s, m, W, H, k, pose, skip);
     return 2;
 }
 
@@ -910,9 +980,10 @@ int launch_fuse_records(const MapView& m, const float* raw, int rp, const uint8_
 int launch_integrate(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
                      cudaStream_t s) {
     if (m.cvox)
-        k_integrate_compact<<<sm_count() * 7, 128, 0, s>>>(m, W, H, k, pose, skip);
+        fb_launch(k_integrate_compact, (const void*)k_integrate_compact_fused, sm_count() * 7, 128, 0, s, m, W, H, k,
+                  pose, skip);
     else
-        k_integrate<<<sm_count() * 8, 256, 0, s>>>(m, W, H, k, pose, skip);
+        fb_launch(k_integrate, (const void*)k_integrate_fused, sm_count() * 8, 256, 0, s, m, W, H, k, pose, skip);
     return 1;
 }
 

@@ -8,6 +8,7 @@
 // (the neighbour vertices the normal needs are recomputed from depth instead
 // of being re-read from a separate vertex-map pass).  All kernels are
 // elementwise over pixels with small stencils served from L1.
+#include "fb_fused.cuh"
 #include "fb_internal.h"
 
 namespace fb {
@@ -17,12 +18,13 @@ __constant__ float c_gauss[25] = {1, 4, 6, 4, 1, 4, 16, 24, 16, 4, 6, 24, 36,
 
 // FilterDepthKernel (Tracking/Pyrdown.cu:3-41) + ImageToIntensityKernel
 // (Pyrdown.cu:183-193) for one level-0 pixel.
-__global__ void k_level0(const uint16_t* __restrict__ depth, int dpitch, const uint8_t* __restrict__ rgb,
-                         int rgbpitch, int W, int H, float inv, float cutoff, float* __restrict__ raw,
-                         int rawpitch, float* __restrict__ filt, int fpitch, uint8_t* __restrict__ gray,
-                         int gpitch) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void level0_body(const BlockCtx& ctx, const uint16_t* __restrict__ depth, int dpitch,
+                                            const uint8_t* __restrict__ rgb, int rgbpitch, int W, int H, float inv,
+                                            float cutoff, float* __restrict__ raw, int rawpitch,
+                                            float* __restrict__ filt, int fpitch, uint8_t* __restrict__ gray,
+                                            int gpitch) {
+    const int x = ctx.bx * blockDim.x + threadIdx.x;
+    const int y = ctx.by * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
     if (gray) {
         const uint8_t* px = rgb + (size_t)y * rgbpitch + 3 * x;
@@ -53,6 +55,14 @@ __global__ void k_level0(const uint16_t* __restrict__ depth, int dpitch, const u
     filt[(size_t)y * fpitch + x] = fin < cutoff ? fin : qnan();
 }
 
+__global__ void k_level0(const uint16_t* __restrict__ depth, int dpitch, const uint8_t* __restrict__ rgb,
+                         int rgbpitch, int W, int H, float inv, float cutoff, float* __restrict__ raw,
+                         int rawpitch, float* __restrict__ filt, int fpitch, uint8_t* __restrict__ gray,
+                         int gpitch) {
+    level0_body(own_ctx(), depth, dpitch, rgb, rgbpitch, W, H, inv, cutoff, raw, rawpitch, filt, fpitch, gray, gpitch);
+}
+FB_FUSED_KERNEL(k_level0, level0_body, 256)
+
 // PyrDownGaussKernel<float> and <uchar> (Tracking/Pyrdown.cu:134-158) for one
 // destination pixel: window clipped to [max(0, 2x-2), min(2x+3, cols-1)),
 // kernel indexed from the clipped end, NaN taps skipped, truncating cast.
@@ -73,15 +83,22 @@ __device__ __forceinline__ T pyr_pixel(const T* __restrict__ src, int spitch, in
     return (T)fd(sum, (float)count);
 }
 
-__global__ void k_pyrdown(const float* __restrict__ sd, int sdp, const uint8_t* __restrict__ sg, int sgp,
-                          int SW, int SH, float* __restrict__ dd, int ddp, uint8_t* __restrict__ dg,
-                          int dgp) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void pyrdown_body(const BlockCtx& ctx, const float* __restrict__ sd, int sdp,
+                                             const uint8_t* __restrict__ sg, int sgp, int SW, int SH,
+                                             float* __restrict__ dd, int ddp, uint8_t* __restrict__ dg, int dgp) {
+    const int x = ctx.bx * blockDim.x + threadIdx.x;
+    const int y = ctx.by * blockDim.y + threadIdx.y;
     if (x >= SW / 2 || y >= SH / 2) return;
     if (dd) dd[(size_t)y * ddp + x] = pyr_pixel<float>(sd, sdp, SW, SH, x, y);
     if (dg) dg[(size_t)y * dgp + x] = pyr_pixel<uint8_t>(sg, sgp, SW, SH, x, y);
 }
+
+__global__ void k_pyrdown(const float* __restrict__ sd, int sdp, const uint8_t* __restrict__ sg, int sgp,
+                          int SW, int SH, float* __restrict__ dd, int ddp, uint8_t* __restrict__ dg,
+                          int dgp) {
+    pyrdown_body(own_ctx(), sd, sdp, sg, sgp, SW, SH, dd, ddp, dg, dgp);
+}
+FB_FUSED_KERNEL(k_pyrdown, pyrdown_body, 256)
 
 // ComputeVMapKernel (Tracking/Pyrdown.cu:56-78) for one pixel; invalid
 // vertices get NaN in x (the reference leaves y and w unset; NaN here).
@@ -120,12 +137,13 @@ __global__ void k_nmap(const float4* __restrict__ vmap, int vp, int W, int H, fl
 
 // Vertex map, normal map (ComputeNMapKernel, Pyrdown.cu:93-114) and Sobel
 // derivatives (ComputeDerivativeImageKernel, Pyrdown.cu:207-237) of one level.
-__global__ void k_maps(const float* __restrict__ depth, int dp, const uint8_t* __restrict__ gray, int gp,
-                       int W, int H, Intr k, float cutoff, float4* __restrict__ vmap, int vp,
-                       float4* __restrict__ nmap, int np, int16_t* __restrict__ dxo, int16_t* __restrict__ dyo,
-                       int sp, uint8_t* __restrict__ rgbok, FuseRecDst fr) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void maps_body(const BlockCtx& ctx, const float* __restrict__ depth, int dp,
+                                          const uint8_t* __restrict__ gray, int gp, int W, int H, Intr k,
+                                          float cutoff, float4* __restrict__ vmap, int vp, float4* __restrict__ nmap,
+                                          int np, int16_t* __restrict__ dxo, int16_t* __restrict__ dyo, int sp,
+                                          uint8_t* __restrict__ rgbok, FuseRecDst fr) {
+    const int x = ctx.bx * blockDim.x + threadIdx.x;
+    const int y = ctx.by * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
     if (vmap) {
         float4 c = vertex(depth, dp, x, y, k, cutoff);
@@ -181,13 +199,22 @@ __global__ void k_maps(const float* __restrict__ depth, int dp, const uint8_t* _
     }
 }
 
+__global__ void k_maps(const float* __restrict__ depth, int dp, const uint8_t* __restrict__ gray, int gp,
+                       int W, int H, Intr k, float cutoff, float4* __restrict__ vmap, int vp,
+                       float4* __restrict__ nmap, int np, int16_t* __restrict__ dxo, int16_t* __restrict__ dyo,
+                       int sp, uint8_t* __restrict__ rgbok, FuseRecDst fr) {
+    maps_body(own_ctx(), depth, dp, gray, gp, W, H, k, cutoff, vmap, vp, nmap, np, dxo, dyo, sp, rgbok, fr);
+}
+FB_FUSED_KERNEL(k_maps, maps_body, 256)
+
 // ResizeMapKernel (Tracking/Pyrdown.cu:251-279): 2x2 means; the normal mean
 // is normalised over all four lanes.  Bounds are the destination size (the
 // reference checks the source size and writes past short destinations).
-__global__ void k_resize(const float4* __restrict__ vs, const float4* __restrict__ ns, int sp, int SW, int SH,
-                         float4* __restrict__ vd, float4* __restrict__ nd, int dp) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void resize_body(const BlockCtx& ctx, const float4* __restrict__ vs,
+                                            const float4* __restrict__ ns, int sp, int SW, int SH,
+                                            float4* __restrict__ vd, float4* __restrict__ nd, int dp) {
+    const int x = ctx.bx * blockDim.x + threadIdx.x;
+    const int y = ctx.by * blockDim.y + threadIdx.y;
     if (x >= SW / 2 || y >= SH / 2) return;
     const size_t i00 = (size_t)(2 * y) * sp + 2 * x, i10 = i00 + sp;
     float4 v00 = vs[i00], v01 = vs[i00 + 1], v10 = vs[i10], v11 = vs[i10 + 1];
@@ -215,6 +242,12 @@ __global__ void k_resize(const float4* __restrict__ vs, const float4* __restrict
     nd[(size_t)y * dp + x] = o;
 }
 
+__global__ void k_resize(const float4* __restrict__ vs, const float4* __restrict__ ns, int sp, int SW, int SH,
+                         float4* __restrict__ vd, float4* __restrict__ nd, int dp) {
+    resize_body(own_ctx(), vs, ns, sp, SW, SH, vd, nd, dp);
+}
+FB_FUSED_KERNEL(k_resize, resize_body, 256)
+
 static inline dim3 grid2d(int W, int H, dim3 b) { return dim3((W + b.x - 1) / b.x, (H + b.y - 1) / b.y); }
 
 // ---- launchers (pitches in elements) ----
@@ -225,15 +258,16 @@ int launch_level0(const uint16_t* depth, int dpitch, const uint8_t* rgb, int rgb
     dim3 b(32, 8);
     // FilterDepth passes 1.0 / depthScale computed in double (Pyrdown.cu:50)
     float inv = (float)(1.0 / (double)depth_scale);
-    k_level0<<<grid2d(W, H, b), b, 0, st>>>(depth, dpitch, rgb, rgbpitch, W, H, inv, cutoff, raw,
-                                             rawpitch, filt, fpitch, gray, gpitch);
+    fb_launch(k_level0, (const void*)k_level0_fused, grid2d(W, H, b), b, 0, st, depth, dpitch, rgb, rgbpitch, W, H,
+              inv, cutoff, raw, rawpitch, filt, fpitch, gray, gpitch);
     return 1;
 }
 
 int launch_pyrdown(const float* sd, int sdp, const uint8_t* sg, int sgp, int SW, int SH, float* dd,
                     int ddp, uint8_t* dg, int dgp, cudaStream_t st) {
     dim3 b(32, 8);
-    k_pyrdown<<<grid2d(SW / 2, SH / 2, b), b, 0, st>>>(sd, sdp, sg, sgp, SW, SH, dd, ddp, dg, dgp);
+    fb_launch(k_pyrdown, (const void*)k_pyrdown_fused, grid2d(SW / 2, SH / 2, b), b, 0, st, sd, sdp, sg, sgp, SW, SH,
+              dd, ddp, dg, dgp);
     return 1;
 }
 
@@ -242,8 +276,8 @@ int launch_maps(const float* depth, int dp, const uint8_t* gray, int gp, int W, 
                  int sp, cudaStream_t st, uint8_t* rgbok, const FuseRecDst* fr) {
     dim3 b(32, 8);
     const FuseRecDst none{};
-    k_maps<<<grid2d(W, H, b), b, 0, st>>>(depth, dp, gray, gp, W, H, k, cutoff, vmap, vp, nmap, np, dx,
-                                           dy, sp, rgbok, fr ? *fr : none);
+    fb_launch(k_maps, (const void*)k_maps_fused, grid2d(W, H, b), b, 0, st, depth, dp, gray, gp, W, H, k, cutoff, vmap,
+              vp, nmap, np, dx, dy, sp, rgbok, fr ? *fr : none);
     return 1;
 }
 
@@ -256,7 +290,8 @@ int launch_nmap(const float4* vmap, int vp, int W, int H, float4* nmap, int np, 
 int launch_resize(const float4* vs, const float4* ns, int sp, int SW, int SH, float4* vd, float4* nd,
                    int dp, cudaStream_t st) {
     dim3 b(32, 8);
-    k_resize<<<grid2d(SW / 2, SH / 2, b), b, 0, st>>>(vs, ns, sp, SW, SH, vd, nd, dp);
+    fb_launch(k_resize, (const void*)k_resize_fused, grid2d(SW / 2, SH / 2, b), b, 0, st, vs, ns, sp, SW, SH, vd, nd,
+              dp);
     return 1;
 }
 

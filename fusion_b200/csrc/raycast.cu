@@ -16,31 +16,37 @@
 
 #include <type_traits>
 
+#include "fb_fused.cuh"
 #include "fb_internal.h"
 
 namespace fb {
 
-__global__ void k_zrange_init(MapView m, const int* __restrict__ skip) {
+__device__ __forceinline__ void zrange_init_body(const BlockCtx& ctx, MapView m, const int* __restrict__ skip) {
     if (skip && *skip) return;
-    if (blockIdx.x == 0 && threadIdx.x < 3) {
+    if (ctx.bx == 0 && threadIdx.x < 3) {
         m.ctr->bmin[threadIdx.x] = 0x7fffffff;
         m.ctr->bmax[threadIdx.x] = -0x7fffffff;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (ctx.bx == 0 && threadIdx.x == 0) {
         m.ctr->ray_next = 0;
         m.ctr->n_tiles = 0;   // counted again by each z-range pass
     }
     const int n = m.zc * m.zr;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int i = ctx.bx * blockDim.x + threadIdx.x; i < n; i += ctx.gx * blockDim.x) {
         m.zmin[i] = 100.f;   // CreateRenderingBlocks uploads 100 (RenderScene.cu:245-251)
         m.zmax[i] = 0.f;     // and clears zRangeY (RenderScene.cu:244)
     }
 }
 
+__global__ void __launch_bounds__(256) k_zrange_init(MapView m, const int* __restrict__ skip) {
+    zrange_init_body(own_ctx(), m, skip);
+}
+FB_FUSED_KERNEL(k_zrange_init, zrange_init_body, 256)
+
 // Projection::projectBlock (RenderScene.cu:54-104) + the first tile's fill
 // (fillBlocks, RenderScene.cu:156-179).
-__global__ void __launch_bounds__(256) k_zrange(MapView m, Intr k, const DevPose* __restrict__ posep,
-                                                const int* __restrict__ skip) {
+__device__ __forceinline__ void zrange_body(const BlockCtx& ctx, MapView m, Intr k, const DevPose* __restrict__ posep,
+                                            const int* __restrict__ skip) {
     if (skip && *skip) return;
     const DevPose P = *posep;
     const int n = min(m.ctr->n_visible, m.NS);
@@ -48,7 +54,7 @@ __global__ void __launch_bounds__(256) k_zrange(MapView m, Intr k, const DevPose
     // box of the visible blocks (warp-reduced, then one atomic per warp)
     {
         int lo[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, hi[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
-        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        for (int i = ctx.bx * blockDim.x + threadIdx.x; i < n; i += ctx.gx * blockDim.x) {
             const HEntry e = m.vis_blocks[i];
             lo[0] = min(lo[0], (int)e.x);
             lo[1] = min(lo[1], (int)e.y);
@@ -70,7 +76,7 @@ __global__ void __launch_bounds__(256) k_zrange(MapView m, Intr k, const DevPose
             }
         }
     }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int i = ctx.bx * blockDim.x + threadIdx.x; i < n; i += ctx.gx * blockDim.x) {
         const HEntry e = m.vis_blocks[i];
         int ulx = zc, uly = zr, lrx = -1, lry = -1;
         float zx = m.g.depth_max, zy = m.g.depth_min;
@@ -108,6 +114,12 @@ __global__ void __launch_bounds__(256) k_zrange(MapView m, Intr k, const DevPose
     }
 }
 
+__global__ void __launch_bounds__(256) k_zrange(MapView m, Intr k, const DevPose* __restrict__ posep,
+                                  const int* __restrict__ skip) {
+    zrange_body(own_ctx(), m, k, posep, skip);
+}
+FB_FUSED_KERNEL(k_zrange, zrange_body, 256)
+
 // Dense block index for the raycast: every allocated block inside the box of
 // this frame's visible blocks (one block of margin) gets its pool index in
 // grid[], -1 elsewhere; outside the box, or when the box exceeds the grid,
@@ -115,7 +127,7 @@ __global__ void __launch_bounds__(256) k_zrange(MapView m, Intr k, const DevPose
 // hash table holds for those coordinates (one entry per block), so every
 // lookup returns the same block: a ray's samples turn one indexed load instead
 // of a bucket probe and chain walk, which also keeps a warp's lanes together.
-__global__ void k_grid_prepare(MapView m, const int* __restrict__ skip) {
+__device__ __forceinline__ void grid_prepare_body(const BlockCtx& ctx, MapView m, const int* __restrict__ skip) {
     if (skip && *skip) return;
     MapCounters* c = m.ctr;
     long long vol = 1;
@@ -134,15 +146,25 @@ __global__ void k_grid_prepare(MapView m, const int* __restrict__ skip) {
     c->g_on = on ? 1 : 0;
 }
 
-__global__ void k_grid_clear(MapView m, const int* __restrict__ skip) {
+__global__ void __launch_bounds__(32) k_grid_prepare(MapView m, const int* __restrict__ skip) {
+    grid_prepare_body(own_ctx(), m, skip);
+}
+FB_FUSED_KERNEL(k_grid_prepare, grid_prepare_body, 32)
+
+__device__ __forceinline__ void grid_clear_body(const BlockCtx& ctx, MapView m, const int* __restrict__ skip) {
     if (skip && *skip) return;
     const MapCounters* c = m.ctr;
     if (!c->g_on) return;
     const int vol = c->g_n[0] * c->g_n[1] * c->g_n[2];
     int4* g4 = (int4*)m.grid;
     const int4 none = make_int4(-1, -1, -1, -1);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (vol + 3) / 4; i += gridDim.x * blockDim.x) g4[i] = none;
+    for (int i = ctx.bx * blockDim.x + threadIdx.x; i < (vol + 3) / 4; i += ctx.gx * blockDim.x) g4[i] = none;
 }
+
+__global__ void __launch_bounds__(256) k_grid_clear(MapView m, const int* __restrict__ skip) {
+    grid_clear_body(own_ctx(), m, skip);
+}
+FB_FUSED_KERNEL(k_grid_clear, grid_clear_body, 256)
 
 // FindEntry's block (DeviceMap.cu:122-135): the first entry of the chain
 // holding block (x, y, z), or -1.
@@ -156,14 +178,14 @@ __device__ __forceinline__ int first_ptr(const MapView& m, int x, int y, int z) 
     return -1;
 }
 
-__global__ void k_grid_fill(MapView m, const int* __restrict__ skip) {
+__device__ __forceinline__ void grid_fill_body(const BlockCtx& ctx, MapView m, const int* __restrict__ skip) {
     if (skip && *skip) return;
     const MapCounters* c = m.ctr;
     if (!c->g_on) return;
     const int ox = c->g_o[0], oy = c->g_o[1], oz = c->g_o[2];
     const int nx = c->g_n[0], ny = c->g_n[1], nz = c->g_n[2];
     const int n = min(c->n_alloc, m.NS);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int i = ctx.bx * blockDim.x + threadIdx.x; i < n; i += ctx.gx * blockDim.x) {
         const HEntry e = m.entries[m.alloc_list[i]];
         const int gx = e.x - ox, gy = e.y - oy, gz = e.z - oz;
         // a map with two entries for one block (the reference's racy
@@ -172,6 +194,11 @@ __global__ void k_grid_fill(MapView m, const int* __restrict__ skip) {
             m.grid[(gz * ny + gy) * nx + gx] = first_ptr(m, e.x, e.y, e.z);
     }
 }
+
+__global__ void __launch_bounds__(256) k_grid_fill(MapView m, const int* __restrict__ skip) {
+    grid_fill_body(own_ctx(), m, skip);
+}
+FB_FUSED_KERNEL(k_grid_fill, grid_fill_body, 256)
 
 // The raycast's view of the dense index (registers).
 struct GridView {
@@ -346,13 +373,13 @@ __device__ bool read_normal(const MapView& m, const GridView& gv, f3 pt, EntryCa
 
 // Rendering::operator() (RenderScene.cu:354-440)
 template <class VR>
-__global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__ vmap, float4* __restrict__ nmap,
-                                                 int vp, int W, int H, Intr k, const DevPose* __restrict__ posep,
-                                                 const int* __restrict__ skip) {
+__device__ __forceinline__ void raycast_body(const BlockCtx& ctx, MapView m, float4* __restrict__ vmap,
+                                             float4* __restrict__ nmap, int vp, int W, int H, Intr k,
+                                             const DevPose* __restrict__ posep, const int* __restrict__ skip) {
     if (skip && *skip) return;
     if (m.ctr->n_tiles == 0) return;   // CreateRenderingBlocks returned false: maps untouched
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int x = ctx.bx * blockDim.x + threadIdx.x;
+    const int y = ctx.by * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
     const DevPose P = *posep;
     GridView gv;
@@ -417,6 +444,18 @@ __global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__
     nmap[o] = nout;
 }
 
+template <class VR>
+__global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__ vmap, float4* __restrict__ nmap,
+                                                 int vp, int W, int H, Intr k, const DevPose* __restrict__ posep,
+                                                 const int* __restrict__ skip) {
+    raycast_body<VR>(own_ctx(), m, vmap, nmap, vp, W, H, k, posep, skip);
+}
+template <class VR>
+__global__ void __launch_bounds__(128) k_raycast_fused(FusedArgs fa) {
+    run_part<ArgsOf<decltype(&k_raycast<VR>)>>(
+        fa, [](const BlockCtx& c, const auto&... a) { raycast_body<VR>(c, a...); });
+}
+
 // The same rays with lane refill: a persistent grid whose warps take pixels
 // from a work counter (8 x 4 pixel tiles in row-major order, 32 at a time),
 // and every lane whose ray has ended takes the next pixel at once, so the
@@ -427,10 +466,9 @@ __global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__
 // per warp and loop turn), faster only on 160x120 images, where the
 // batched form's autotuner may pick it.
 template <class VR>
-__global__ void __launch_bounds__(128, 8) k_raycast_pool(MapView m, float4* __restrict__ vmap,
-                                                         float4* __restrict__ nmap, int vp, int W, int H, Intr k,
-                                                         const DevPose* __restrict__ posep,
-                                                         const int* __restrict__ skip) {
+__device__ __forceinline__ void raycast_pool_body(const BlockCtx&, MapView m, float4* __restrict__ vmap,
+                                                  float4* __restrict__ nmap, int vp, int W, int H, Intr k,
+                                                  const DevPose* __restrict__ posep, const int* __restrict__ skip) {
     if (skip && *skip) return;
     if (m.ctr->n_tiles == 0) return;   // CreateRenderingBlocks returned false: maps untouched
     const DevPose P = *posep;
@@ -537,6 +575,19 @@ __global__ void __launch_bounds__(128, 8) k_raycast_pool(MapView m, float4* __re
     }
 }
 
+template <class VR>
+__global__ void __launch_bounds__(128, 8) k_raycast_pool(MapView m, float4* __restrict__ vmap,
+                                                         float4* __restrict__ nmap, int vp, int W, int H, Intr k,
+                                                         const DevPose* __restrict__ posep,
+                                                         const int* __restrict__ skip) {
+    raycast_pool_body<VR>(own_ctx(), m, vmap, nmap, vp, W, H, k, posep, skip);
+}
+template <class VR>
+__global__ void __launch_bounds__(128, 8) k_raycast_pool_fused(FusedArgs fa) {
+    run_part<ArgsOf<decltype(&k_raycast_pool<VR>)>>(
+        fa, [](const BlockCtx& c, const auto&... a) { raycast_pool_body<VR>(c, a...); });
+}
+
 static int sm_count_rc() {
     static int n = 0;
     if (!n) {
@@ -549,11 +600,11 @@ static int sm_count_rc() {
 }
 
 int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s) {
-    k_zrange_init<<<(m.zc * m.zr + 255) / 256, 256, 0, s>>>(m, skip);
-    k_zrange<<<sm_count_rc() * 2, 256, 0, s>>>(m, k, pose, skip);
-    k_grid_prepare<<<1, 1, 0, s>>>(m, skip);
-    k_grid_clear<<<sm_count_rc() * 4, 256, 0, s>>>(m, skip);
-    k_grid_fill<<<sm_count_rc() * 4, 256, 0, s>>>(m, skip);
+    fb_launch(k_zrange_init, (const void*)k_zrange_init_fused, (m.zc * m.zr + 255) / 256, 256, 0, s, m, skip);
+    fb_launch(k_zrange, (const void*)k_zrange_fused, sm_count_rc() * 2, 256, 0, s, m, k, pose, skip);
+    fb_launch(k_grid_prepare, (const void*)k_grid_prepare_fused, 1, 1, 0, s, m, skip);
+    fb_launch(k_grid_clear, (const void*)k_grid_clear_fused, sm_count_rc() * 4, 256, 0, s, m, skip);
+    fb_launch(k_grid_fill, (const void*)k_grid_fill_fused, sm_count_rc() * 4, 256, 0, s, m, skip);
     return 5;
 }
 
@@ -562,16 +613,20 @@ int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, i
     if (bx == 0 && by == 0) {
         const int blocks = sm_count_rc() * 8;
         if (m.cvox)
-            k_raycast_pool<CompactVox><<<blocks, 128, 0, s>>>(m, vmap, nmap, p, W, H, k, pose, skip);
+            fb_launch(k_raycast_pool<CompactVox>, (const void*)k_raycast_pool_fused<CompactVox>, blocks, 128, 0, s, m,
+                      vmap, nmap, p, W, H, k, pose, skip);
         else
-            k_raycast_pool<ExactVox><<<blocks, 128, 0, s>>>(m, vmap, nmap, p, W, H, k, pose, skip);
+            fb_launch(k_raycast_pool<ExactVox>, (const void*)k_raycast_pool_fused<ExactVox>, blocks, 128, 0, s, m, vmap,
+                      nmap, p, W, H, k, pose, skip);
         return 1;
     }
     dim3 b(bx, by), g((W + bx - 1) / bx, (H + by - 1) / by);
     if (m.cvox)
-        k_raycast<CompactVox><<<g, b, 0, s>>>(m, vmap, nmap, p, W, H, k, pose, skip);
+        fb_launch(k_raycast<CompactVox>, (const void*)k_raycast_fused<CompactVox>, g, b, 0, s, m, vmap, nmap, p, W, H,
+                  k, pose, skip);
     else
-        k_raycast<ExactVox><<<g, b, 0, s>>>(m, vmap, nmap, p, W, H, k, pose, skip);
+        fb_launch(k_raycast<ExactVox>, (const void*)k_raycast_fused<ExactVox>, g, b, 0, s, m, vmap, nmap, p, W, H, k,
+                  pose, skip);
     return 1;
 }
 

@@ -54,7 +54,7 @@ namespace {
 
 
 
-__global__ void k_init_poses(TrackState* st) {
+__device__ __forceinline__ void init_poses_body(const BlockCtx&, TrackState* st) {
     for (int i = 0; i < 16; ++i) st->pose[i] = st->last_pose[i] = st->init_pose[i] = (i % 5 == 0) ? 1.0 : 0.0;
     st->cur = make_dev_pose_d(st->pose);
     st->last = st->cur;
@@ -62,9 +62,12 @@ __global__ void k_init_poses(TrackState* st) {
     st->icp_error = st->rgb_error = qnan();
     st->icp_count = st->rgb_count = 0;
 }
+__global__ void k_init_poses(TrackState* st) { init_poses_body(own_ctx(), st); }
+FB_FUSED_KERNEL(k_init_poses, init_poses_body, 32)
 
 // After the frame: a tracked frame becomes the last frame (SwapFrame).
-__global__ void k_commit(TrackState* st, MapCounters* c, FrameOut* out, int tracked_path) {
+__device__ __forceinline__ void commit_body(const BlockCtx&, TrackState* st, MapCounters* c, FrameOut* out,
+                                            int tracked_path) {
     if (tracked_path && !st->failed) {
         for (int i = 0; i < 16; ++i) st->last_pose[i] = st->pose[i];
         st->last = st->cur;
@@ -84,6 +87,21 @@ __global__ void k_commit(TrackState* st, MapCounters* c, FrameOut* out, int trac
     out->entry_ptr = c->entry_ptr;
     out->seq_path = c->seq_path;
 }
+__global__ void k_commit(TrackState* st, MapCounters* c, FrameOut* out, int tracked_path) {
+    commit_body(own_ctx(), st, c, out, tracked_path);
+}
+FB_FUSED_KERNEL(k_commit, commit_body, 32)
+
+// The frame result into the caller's pinned host memory (device-accessible
+// through unified addressing): the fused batch step reads every session's
+// result this way instead of one copy per session.
+__device__ __forceinline__ void result_out_body(const BlockCtx&, const FrameOut* d, FrameOut* h) {
+    static_assert(sizeof(FrameOut) % 4 == 0, "FrameOut is copied in words");
+    const int n = (int)(sizeof(FrameOut) / 4);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) ((int*)h)[i] = ((const int*)d)[i];
+}
+__global__ void k_result_out(const FrameOut* d, FrameOut* h) { result_out_body(own_ctx(), d, h); }
+FB_FUSED_KERNEL(k_result_out, result_out_body, 64)
 
 
 // Export of the hash table in the reference's field order, ptr as voxel index.
@@ -99,10 +117,12 @@ __global__ void k_export_entries(const HEntry* e, int n, int* out) {
 }
 
 
-__global__ void k_track_start(TrackState* st, Pose16 T) {
+__device__ __forceinline__ void track_start_body(const BlockCtx&, TrackState* st, Pose16 T) {
     for (int i = 0; i < 16; ++i) st->pose[i] = st->init_pose[i] = T.m[i];
     st->cur = make_dev_pose_d(st->pose);
 }
+__global__ void k_track_start(TrackState* st, Pose16 T) { track_start_body(own_ctx(), st, T); }
+FB_FUSED_KERNEL(k_track_start, track_start_body, 32)
 
 // A relocalised frame: its pose is the solver's, and it becomes the last frame.
 __global__ void k_track_reloc(TrackState* st, Pose16 T) {
@@ -350,12 +370,14 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
     if (part != 2) {
         // Tracker::GrabFrame (Tracking.cc:236-243): LastFrame->ResizeImages ...
         mark(0);
+        launch_slot(kSlotResize);
         for (int l = 1; l < 3; ++l)
             n += launch_resize(L.vmap[l - 1], L.nmap[l - 1], s->W[l - 1], s->W[l - 1], s->H[l - 1], L.vmap[l], L.nmap[l],
                                s->W[l], st);
         *ran |= 1u << 0;
         // ... NextFrame->FillImages (Core/Frame.cc:59-78)
         mark(1);
+        launch_slot(kSlotPyramid);
         n += launch_level0(N.depth_in, s->W[0], N.rgb, 3 * s->W[0], s->W[0], s->H[0], c.depth_scale, c.depth_cutoff,
                            N.raw, s->W[0], N.depth[0], s->W[0], N.gray[0], s->W[0], st);
         for (int l = 1; l < 3; ++l)
@@ -374,8 +396,9 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
     }
     mark(2);
     const int* skip = nullptr;
+    launch_slot(kSlotTrackInit);
     if (init) {
-        k_init_poses<<<1, 1, 0, st>>>(s->st);
+        fb_launch(k_init_poses, (const void*)k_init_poses_fused, 1, 1, 0, st, s->st);
         n += 1;
     } else if (track) {
         // Tracker::ComputeSE3 (Tracking.cc:296-409)
@@ -384,7 +407,7 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
         if (start) {
             Pose16 T;
             std::memcpy(T.m, start, sizeof T.m);
-            k_track_start<<<1, 1, 0, st>>>(s->st, T);
+            fb_launch(k_track_start, (const void*)k_track_start_fused, 1, 1, 0, st, s->st, T);
             n += 1;
         }
         int last_level = -1;
@@ -392,10 +415,12 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
             if (c.iters[l] > 0) last_level = l;
         for (int l = 2; l >= 0; --l) {
             TrackLevel lv = level_view(s, l);
-            for (int it = 0; it < c.iters[l]; ++it)
+            for (int it = 0; it < c.iters[l]; ++it) {
+                launch_slot(kSlotTrack, 2 - l, it);
                 n += launch_track_iter(lv, s->st, s->tickets, s->residual, s->counts, min_count[l],
                                        l == last_level && it == c.iters[l] - 1, st, s->shared_gpu,
                                        c.form == FB_FORM_PRECISION);
+            }
         }
         skip = &s->st->failed;
         *ran |= 1u << 2;
@@ -405,10 +430,13 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
     if (fuse) {
         // Mapping::FuseColor(LastFrame) after the swap (Mapping.cc:76-90):
         // raw depth, colour and level-0 normals of the frame just tracked
+        launch_slot(kSlotAllocate);
         n += launch_allocate(s->map, N.raw, s->W[0], s->W[0], s->H[0], s->K[0], pose, skip, st);
         mark(4);
+        launch_slot(kSlotVisibility);
         n += launch_visibility(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st);
         mark(5);
+        launch_slot(kSlotIntegrate);
         n += launch_integrate(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st);
         *ran |= 7u << 3;
     } else {
@@ -419,10 +447,15 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
     if (render) {
         // with mapping disabled, System::GrabImage refreshes the visible
         // blocks first (Mapping::UpdateVisibility, System.cc:116-118)
-        if (!fuse && s->mapping_disabled) n += launch_visibility(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st);
+        if (!fuse && s->mapping_disabled) {
+            launch_slot(kSlotRenderVisibility);
+            n += launch_visibility(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st);
+        }
         // Mapping::RayTrace (Mapping.cc:92-109) into the frame's level-0 maps
+        launch_slot(kSlotZRange);
         n += launch_zrange(s->map, s->K[0], pose, skip, st);
         mark(7);
+        launch_slot(kSlotRaycast);
         n += launch_raycast(s->map, N.vmap[0], N.nmap[0], s->W[0], s->W[0], s->H[0], s->K[0], pose, skip, st,
                             s->rc_bx, s->rc_by);
         *ran |= 3u << 6;
@@ -430,6 +463,7 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
         mark(7);
     }
     mark(8);
+    launch_slot(kSlotCommit);
     launch_commit(s, track || init, st);
     return n + 1;
 }
@@ -494,8 +528,17 @@ void launch_track_reloc(fb_session* s, const double* T, cudaStream_t st) {
     k_track_reloc<<<1, 1, 0, st>>>(s->st, P);
 }
 
+LaunchRecorder*& launch_recorder() {
+    static thread_local LaunchRecorder* r = nullptr;
+    return r;
+}
+
+void launch_result_out(fb_session* s, cudaStream_t st) {
+    fb_launch(k_result_out, (const void*)k_result_out_fused, 1, 64, 0, st, s->d_out, s->h_out_dev);
+}
+
 void launch_commit(fb_session* s, int tracked_path, cudaStream_t st) {
-    k_commit<<<1, 1, 0, st>>>(s->st, s->ctr, s->d_out, tracked_path);
+    fb_launch(k_commit, (const void*)k_commit_fused, 1, 1, 0, st, s->st, s->ctr, s->d_out, tracked_path);
 }
 
 }  // namespace fb
@@ -773,6 +816,7 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
     if (!s) return FB_ENOMEM;
     s->cfg = *cfg;
     s->h_out = nullptr;
+    s->h_out_dev = nullptr;
     s->profile = false;
     for (int i = 0; i <= kStages; ++i) s->ev[i] = nullptr;
     for (int i = 0; i < kStages; ++i) {
@@ -817,6 +861,12 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
     if (ok) {
         s->h_out = (FrameOut*)take_out_slot(sizeof(FrameOut));
         ok = s->h_out != nullptr;
+        // the device address of the pinned result (fused batch steps write it
+        // from a kernel); without one the session cannot take fused steps
+        if (ok && cudaHostGetDevicePointer((void**)&s->h_out_dev, s->h_out, 0) != cudaSuccess) {
+            s->h_out_dev = nullptr;
+            cudaGetLastError();
+        }
     }
     for (int i = 0; i <= kStages && ok; ++i) ok = cuda_ok(cudaEventCreate(&s->ev[i]));
     if (!ok) {

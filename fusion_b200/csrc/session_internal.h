@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/fusion_b200.h"
+#include "fb_fused.cuh"
 #include "fb_internal.h"
 
 // Returns FB_ECUDA from the calling function when a CUDA call fails.
@@ -133,6 +134,7 @@ struct fb_session {
     DevPose* scratch_pose;
     FrameOut* d_out;
     FrameOut* h_out;           // pinned
+    FrameOut* h_out_dev;       // h_out's device address (cudaHostGetDevicePointer), null if none
     void* arena;               // one stream-ordered device allocation
     size_t arena_size, arena_used;
     bool sizing;               // dalloc only adds up sizes
@@ -199,6 +201,9 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
 // frame) and, after the caller's launches, the frame result.
 void launch_track_reloc(fb_session* s, const double* T, cudaStream_t st);
 void launch_commit(fb_session* s, int tracked_path, cudaStream_t st);
+// The frame result from the device into the session's pinned h_out by a
+// kernel (the fused batch step's replacement of the per-session copy).
+void launch_result_out(fb_session* s, cudaStream_t st);
 int image_ok(const fb_image* im, size_t elem);
 cudaStream_t as_stream(void* s);
 DevPose pose_from(const float R[9], const float Rinv[9], const float t[3]);

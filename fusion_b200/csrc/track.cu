@@ -24,6 +24,7 @@
 // adds into FMAs, so both instances compute the same bits.
 #include <cooperative_groups.h>
 
+#include "fb_fused.cuh"
 #include "fb_internal.h"
 
 namespace cg = cooperative_groups;
@@ -472,7 +473,7 @@ __device__ __forceinline__ void unpack29(const double* s, double* A, double* b) 
 
 // Frame start: the next pose starts from the last pose (TrackFrame's
 // bootstrap fallback, Tracking.cc:156-159) and delta is the identity.
-__global__ void k_track_begin(TrackState* st) {
+__device__ __forceinline__ void track_begin_body(const BlockCtx&, TrackState* st) {
     for (int i = 0; i < 16; ++i) {
         st->pose[i] = st->last_pose[i];
         st->init_pose[i] = st->last_pose[i];
@@ -484,6 +485,8 @@ __global__ void k_track_begin(TrackState* st) {
     st->icp_error = st->rgb_error = qnan();
     st->icp_count = st->rgb_count = 0;
 }
+__global__ void k_track_begin(TrackState* st) { track_begin_body(own_ctx(), st); }
+FB_FUSED_KERNEL(k_track_begin, track_begin_body, 32)
 
 // Fixed-order FP64 sum of nv values over nb block partials laid out as
 // partials[b * stride + v], computed by the whole block: thread t sums value
@@ -833,8 +836,8 @@ constexpr int kGrpMinBlocks = 4;
 // a quarter of the block slots for longer, and other sessions' passes run
 // beside it.
 template <int kMinBlocks, bool kComp>
-__global__ void __launch_bounds__(256, kMinBlocks)
-    k_track_a_grp(TrackLevel L, TrackState* st, int2* list, int* counts, int G, int gpc) {
+__device__ __forceinline__ void track_a_grp_body(const BlockCtx& ctx, TrackLevel L, TrackState* st, int2* list,
+                                                 int* counts, int G, int gpc) {
     const int N = L.W * L.H, NG = G / kTrackCluster;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (st->failed) return;   // uniform over the grid: written by an earlier kernel
@@ -847,7 +850,7 @@ __global__ void __launch_bounds__(256, kMinBlocks)
     const int iters = (N + G * 256 - 1) / (G * 256);
     const unsigned lt = (1u << lane) - 1u;
     for (int j = 0; j < gpc; ++j) {
-    const int g = blockIdx.x * gpc + j;
+    const int g = ctx.bx * gpc + j;
     if (g >= NG) break;
     for (int r = 0; r < kTrackCluster; ++r) {
         const int b = g * kTrackCluster + r;
@@ -927,9 +930,9 @@ __global__ void __launch_bounds__(256, kMinBlocks)
 }
 
 template <int kMinBlocks, bool kComp>
-__global__ void __launch_bounds__(256, kMinBlocks)
-    k_track_b_grp(TrackLevel L, TrackState* st, unsigned int* ticket, const int2* list, const int* counts,
-                  int seg_size, int min_count, int is_final, int NG, int gpc) {
+__device__ __forceinline__ void track_b_grp_body(const BlockCtx& ctx, TrackLevel L, TrackState* st,
+                                                 unsigned int* ticket, const int2* list, const int* counts,
+                                                 int seg_size, int min_count, int is_final, int NG, int gpc) {
     __shared__ float sm[32 * 29];
     __shared__ float s_rgb[kTrackCluster][32];
     __shared__ double s_part[4][64];
@@ -964,7 +967,7 @@ __global__ void __launch_bounds__(256, kMinBlocks)
     }
     const float sigma = sqrtf((float)q / (float)(c == 0 ? 1 : c));
     for (int j = 0; j < gpc; ++j) {
-    const int grp = blockIdx.x * gpc + j;
+    const int grp = ctx.bx * gpc + j;
     if (grp >= NG) break;
     for (int r = 0; r < kTrackCluster; ++r) {
         const int b = grp * kTrackCluster + r;
@@ -1004,10 +1007,34 @@ __global__ void __launch_bounds__(256, kMinBlocks)
     }
     // last block to finish
     __syncthreads();
-    if (threadIdx.x == 0) s_last = ticket_acq_rel(ticket) == gridDim.x - 1u;
+    if (threadIdx.x == 0) s_last = ticket_acq_rel(ticket) == (unsigned)ctx.gx - 1u;
     __syncthreads();
     if (!s_last) return;
     finish_iteration<kComp>(st, ticket, NG, c, q, sigma, min_count, is_final, io, s_part, s_partc, sums);
+}
+
+template <int kMinBlocks, bool kComp>
+__global__ void __launch_bounds__(256, kMinBlocks)
+    k_track_a_grp(TrackLevel L, TrackState* st, int2* list, int* counts, int G, int gpc) {
+    track_a_grp_body<kMinBlocks, kComp>(own_ctx(), L, st, list, counts, G, gpc);
+}
+template <int kMinBlocks, bool kComp>
+__global__ void __launch_bounds__(256, kMinBlocks) k_track_a_grp_fused(FusedArgs fa) {
+    run_part<ArgsOf<decltype(&k_track_a_grp<kMinBlocks, kComp>)>>(
+        fa, [](const BlockCtx& c, const auto&... a) { track_a_grp_body<kMinBlocks, kComp>(c, a...); });
+}
+
+template <int kMinBlocks, bool kComp>
+__global__ void __launch_bounds__(256, kMinBlocks)
+    k_track_b_grp(TrackLevel L, TrackState* st, unsigned int* ticket, const int2* list, const int* counts,
+                  int seg_size, int min_count, int is_final, int NG, int gpc) {
+    track_b_grp_body<kMinBlocks, kComp>(own_ctx(), L, st, ticket, list, counts, seg_size, min_count, is_final, NG,
+                                        gpc);
+}
+template <int kMinBlocks, bool kComp>
+__global__ void __launch_bounds__(256, kMinBlocks) k_track_b_grp_fused(FusedArgs fa) {
+    run_part<ArgsOf<decltype(&k_track_b_grp<kMinBlocks, kComp>)>>(
+        fa, [](const BlockCtx& c, const auto&... a) { track_b_grp_body<kMinBlocks, kComp>(c, a...); });
 }
 
 // The Gauss-Newton update of one iteration (Tracking.cc:319-394) and, after
@@ -1252,7 +1279,8 @@ int track_grid(int n) {
     return g < cap ? g : cap;
 }
 
-int launch_track_begin(TrackState* st, cudaStream_t s) { k_track_begin<<<1, 1, 0, s>>>(st);
+int launch_track_begin(TrackState* st, cudaStream_t s) {
+    fb_launch(k_track_begin, (const void*)k_track_begin_fused, 1, 1, 0, s, st);
     return 1;
 }
 
@@ -1292,21 +1320,25 @@ int launch_track_iter(const TrackLevel& L, TrackState* st, unsigned int* tickets
     const int seg = (n + g * 256 - 1) / (g * 256) * 32;
     const int fin = is_final ? 1 : 0;
     // sessions sharing the GPU: the group forms, kGroupsPerBlock groups per
-    // block, the same results
+    // block, the same results; fused launches (a recorder) take the group
+    // forms too, since clusters do not span the parts of a fused grid
+    if (launch_recorder()) shared_gpu = true;
     const int ng = g / kTrackCluster, gpc = kGroupsPerBlock, gb = (ng + gpc - 1) / gpc;
     if (compensated) {
         if (shared_gpu) {
-            k_track_a_grp<kGrpMinBlocks, true><<<gb, 256, 0, s>>>(L, st, residual, counts, g, gpc);
-            k_track_b_grp<kGrpMinBlocks, true><<<gb, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg,
-                                                                  min_count, fin, ng, gpc);
+            fb_launch(k_track_a_grp<kGrpMinBlocks, true>, (const void*)k_track_a_grp_fused<kGrpMinBlocks, true>, gb,
+                      256, 0, s, L, st, residual, counts, g, gpc);
+            fb_launch(k_track_b_grp<kGrpMinBlocks, true>, (const void*)k_track_b_grp_fused<kGrpMinBlocks, true>, gb,
+                      256, 0, s, L, st, tickets + 1, residual, counts, seg, min_count, fin, ng, gpc);
         } else {
             k_track_a<2, true><<<g, 256, 0, s>>>(L, st, residual, counts);
             k_track_b<2, true><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, fin);
         }
     } else if (shared_gpu) {
-        k_track_a_grp<kGrpMinBlocks, false><<<gb, 256, 0, s>>>(L, st, residual, counts, g, gpc);
-        k_track_b_grp<kGrpMinBlocks, false><<<gb, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count,
-                                                               fin, ng, gpc);
+        fb_launch(k_track_a_grp<kGrpMinBlocks, false>, (const void*)k_track_a_grp_fused<kGrpMinBlocks, false>, gb, 256,
+                  0, s, L, st, residual, counts, g, gpc);
+        fb_launch(k_track_b_grp<kGrpMinBlocks, false>, (const void*)k_track_b_grp_fused<kGrpMinBlocks, false>, gb, 256,
+                  0, s, L, st, tickets + 1, residual, counts, seg, min_count, fin, ng, gpc);
     } else {
         k_track_a<2, false><<<g, 256, 0, s>>>(L, st, residual, counts);
         k_track_b<2, false><<<g, 256, 0, s>>>(L, st, tickets + 1, residual, counts, seg, min_count, fin);

@@ -232,7 +232,12 @@ FB_API int fb_batch_reserve(fb_batch* b, size_t bytes);
  * sessions changes).  1: one graph per step holding every session's frame,
  * captured once per composition (sessions, their tracker modes and frame
  * parities) and launched as a single graph; best for a fixed set of sessions
- * stepped together. */
+ * stepped together.  2: fused launches -- each stage kernel of the frame runs
+ * ONCE for all sessions of the step, its grid the concatenation of the
+ * sessions' grids (ragged resolutions, cameras and voxel sizes in one
+ * launch), so a step makes about as many launches as one frame instead of
+ * one frame's launches per session; a composition seen before runs as one
+ * captured graph.  Results are the same in every mode. */
 FB_API int fb_batch_set_mode(fb_batch* b, int mode);
 /* One frame for each of n distinct sessions; out[i] as fb_grab_frame's.
  * Synchronous.  A session must not be used elsewhere during the call. */
@@ -240,6 +245,9 @@ FB_API int fb_batch_step(fb_batch* b, fb_session* const* sessions, int n, const 
                          fb_frame_result* out);
 /* Graph launches and captures so far (mode 1 captures once per composition). */
 FB_API int fb_batch_stats(fb_batch* b, uint64_t* steps, uint64_t* captures);
+/* Mode 2: kernel launches of the last step, and the per-session kernel
+ * launches they carried (the launches modes 0 and 1 make for that step). */
+FB_API int fb_batch_launch_stats(fb_batch* b, int* launches, int* kernels);
 
 /* Pose of the last tracked frame (LastFrame->pose). */
 FB_API int fb_get_pose(fb_session* s, double pose[16]);

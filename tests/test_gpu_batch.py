@@ -3,11 +3,14 @@
 Each session's result in a batch must be the one the same session gives
 alone: the test runs ragged sessions (three resolutions, five voxel sizes,
 independent seeded sequences) once alone through fb_grab_frame and once
-together through fb_batch_step, in both batch modes, with sessions joining
-and skipping steps the way a server admits them -- so that steps of more
-than three sessions (the group forms of the tracking kernels) and of three
-(the forms of a session alone) alternate -- and compares every frame's
-pose and counts and the final hash table and voxels bit for bit.
+together through fb_batch_step, in all three batch modes, with sessions
+joining and skipping steps the way a server admits them -- so that steps of
+more than three sessions (the group forms of the tracking kernels) and of
+three (the forms of a session alone) alternate -- and compares every frame's
+pose and counts and the final hash table and voxels bit for bit.  Mode 2
+runs every stage kernel once for all sessions of a step (fused launches over
+the concatenated grids); its sessions must still equal themselves alone, in
+both map forms mixed in one step and with different raycast tiles.
 """
 import hashlib
 
@@ -48,11 +51,20 @@ def _row(r):
             tuple(r.pose[:]), r.icp_count, r.rgb_count)
 
 
-def _alone(frames, schedule):
-    from fusion_b200 import Session, mixed_config
+def _config(i, forms=None):
+    from fusion_b200 import mixed_config
+    w, h, v, _ = SPECS[i]
+    c = mixed_config(w, h, v)
+    if forms:
+        c.form = forms[i]
+    return c
+
+
+def _alone(frames, schedule, forms=None):
+    from fusion_b200 import Session
     out = []
-    for i, (w, h, v, _) in enumerate(SPECS):
-        s = Session(mixed_config(w, h, v))
+    for i in range(len(SPECS)):
+        s = Session(_config(i, forms))
         d, c = frames[i]
         rows = [_row(s.grab(d[k], c[k])) for k in range(len(schedule[i]))]
         out.append((rows, _map_digest(s)))
@@ -61,11 +73,11 @@ def _alone(frames, schedule):
     return out
 
 
-def _batched(frames, schedule, mode, tiles=None):
+def _batched(frames, schedule, mode, tiles=None, forms=None, launch_stats=None):
     """schedule[i] = the steps at which session i has a frame."""
-    from fusion_b200 import Batch, Session, mixed_config
+    from fusion_b200 import Batch, Session
     from fusion_b200.batch import set_raycast_tile
-    sess = [Session(mixed_config(w, h, v)) for (w, h, v, _) in SPECS]
+    sess = [Session(_config(i, forms)) for i in range(len(SPECS))]
     if tiles:
         for s, t in zip(sess, tiles):
             set_raycast_tile(s, *t)
@@ -83,6 +95,8 @@ def _batched(frames, schedule, mode, tiles=None):
             res = b.step([sess[i] for i in idx], fr)
             for i, r in zip(idx, res):
                 rows[i].append(_row(r))
+            if launch_stats is not None:
+                launch_stats.append((len(idx), *b.launch_stats()))
         stats = b.stats()
     out = [(rows[i], _map_digest(s)) for i, s in enumerate(sess)]
     for s in sess:
@@ -103,7 +117,7 @@ STAGGERED = [[0, 1, 2, 5, 6, 7], [2, 3, 4, 5, 6, 7], [0, 1, 2, 3, 4, 5], [0, 1, 
              [1, 2, 3, 5, 6, 7]]
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2])
 @pytest.mark.parametrize("schedule", ["lockstep", "staggered"])
 def test_each_session_in_the_batch_equals_it_alone(frames, mode, schedule):
     sch = LOCKSTEP if schedule == "lockstep" else STAGGERED
@@ -122,6 +136,41 @@ def test_raycast_tile_does_not_change_results(frames):
     base, _ = _batched(frames, LOCKSTEP, 0)
     tiled, _ = _batched(frames, LOCKSTEP, 0, tiles=[(0, 0), (32, 4), (8, 8)])
     assert tiled == base
+    # fused steps: sessions with different tiles (and the lane-refill
+    # raycast) run as separate fused raycast launches
+    fused, _ = _batched(frames, LOCKSTEP, 2, tiles=[(0, 0), (32, 4), (8, 8)])
+    assert fused == base
+
+
+FORMS = [1, 0, 1, 0, 0]   # precision and reference forms mixed in one step
+
+
+def test_fused_step_mixes_map_forms(frames):
+    """A fused step holding precision-form and reference-form sessions
+    (different integration and raycast kernels, tracking sums compensated or
+    not) gives every session its results alone."""
+    alone = _alone(frames, STAGGERED, forms=FORMS)
+    stats = []
+    fused, _ = _batched(frames, STAGGERED, 2, forms=FORMS, launch_stats=stats)
+    for i in range(len(SPECS)):
+        assert fused[i][0] == alone[i][0], f"session {i}: per-frame results differ"
+        assert fused[i][1] == alone[i][1], f"session {i}: final map differs"
+
+
+def test_fused_step_launch_count(frames):
+    """A fused step makes about one frame's worth of launches whatever the
+    number of sessions: each merged launch carries every session's kernel of
+    that stage (a few more where sessions run different kernels -- two map
+    forms, different tracker modes)."""
+    stats = []
+    _batched(frames, LOCKSTEP, 2, launch_stats=stats)
+    print("(sessions, launches, per-session kernels) per step:", stats)
+    for n, launches, kernels in stats:
+        assert 0 < launches <= kernels
+    # steady tracking steps: one frame's launches carry all five sessions'
+    n, launches, kernels = stats[-1]
+    assert n == len(SPECS)
+    assert launches * (n - 1) < kernels, (launches, kernels)
 
 
 def test_batch_rejects_a_session_twice(frames):
