@@ -114,6 +114,10 @@ class Batch:
         check("fb_batch_stats", self.lib.fb_batch_stats(self.h, ctypes.byref(steps), ctypes.byref(caps)))
         return steps.value, caps.value
 
+    def set_lanes(self, lanes):
+        """Mode 2: number of session groups whose fused launches overlap."""
+        check("fb_batch_set_lanes", self.lib.fb_batch_set_lanes(self.h, int(lanes)))
+
     def launch_stats(self):
         """Mode 2: (kernel launches of the last step, per-session kernels they carried)."""
         launches, kernels = ctypes.c_int(), ctypes.c_int()

@@ -54,6 +54,7 @@ def _compile(src, verbose):
 def build_cuda(force=False, verbose=False):
     srcs = [os.path.join(CSRC, s) for s in CU_SOURCES]
     deps = srcs + [os.path.join(CSRC, "fb_common.cuh"), os.path.join(CSRC, "fb_internal.h"),
+                   os.path.join(CSRC, "fb_fused.cuh"), os.path.join(CSRC, "fb_async.cuh"),
                    os.path.join(CSRC, "session_internal.h"),
                    os.path.join(ROOT, "include", "fusion_b200.h"), os.path.abspath(__file__)]
     if not force and _newer(LIB, deps):

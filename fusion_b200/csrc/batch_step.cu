@@ -16,20 +16,23 @@
 // ------------------------------------------------------------------ batches
 
 // One merged launch of a fused step: the fused kernel over n parts (one per
-// session that issued this launch), its parts and argument tuples at byte
-// offsets of the plan's device buffer.
+// session that issued this launch, at most kFusedMaxParts), with its
+// parameter (FusedParams: parts and argument tuples) at a byte offset of the
+// plan's parameter bytes.
 struct FusedLaunch {
     const void* fused;
     dim3 block;
     size_t smem;
     int n, blocks;
-    size_t parts_off, args_off;
+    int lane;               // the stream (lane) it runs on
+    size_t param_off;
 };
 
-// The fused launches of one composition, their device-side arguments and,
-// once the composition repeats, their graph.
+// The fused launches of one composition, their parameters and, once the
+// composition repeats, their graph.
 struct FusedPlan {
-    void* dev = nullptr;
+    std::vector<unsigned char> params;
+    int lanes = 1;
     std::vector<FusedLaunch> launches;
     cudaGraphExec_t exec = nullptr;
     int kernels = 0;      // per-session kernel launches the merged ones replace
@@ -49,7 +52,7 @@ struct fb_batch {
     // mode 2: fused plans by composition, the recorders of a step's frames
     std::map<std::vector<uint64_t>, FusedPlan> fused;
     std::vector<LaunchRecorder> recs;
-    std::vector<unsigned char> blob;
+    int lanes = 4;                             // fb_batch_set_lanes
     int last_launches = 0, last_kernels = 0;   // of the last fused step
 };
 
@@ -64,13 +67,19 @@ void clear_cache(fb_batch* b) {
 
 constexpr size_t kFusedCacheMax = 64;
 
+// Slot streams of a batch: a fixed set, created with the batch.  Creating a
+// stream while frames run can take tens of milliseconds (the driver
+// serialises it with the device's work), so a step never creates one; beyond
+// kBatchSlots sessions, sessions share slots round-robin (their frames then
+// run one after the other on that slot, with the same results).  Fused steps
+// use the first slots as their lanes.
+constexpr int kBatchSlots = 32;
+
 void clear_fused(fb_batch* b) {
     if (b->fused.empty()) return;
     cudaStreamSynchronize(b->origin);
-    for (auto& kv : b->fused) {
+    for (auto& kv : b->fused)
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-        if (kv.second.dev) cudaFreeAsync(kv.second.dev, b->origin);
-    }
     b->fused.clear();
 }
 
@@ -89,9 +98,30 @@ std::vector<uint64_t> composition(fb_session* const* ss, int n, const FramePlan*
     return key;
 }
 
+// Lanes of a fused step: the sessions split into `lanes` groups of about
+// equal pixel counts (largest first into the lightest lane).  Each lane's
+// fused launches run on a stream of their own, so one lane's latency-bound
+// tracking overlaps another lane's raycast or integration.
+std::vector<int> assign_lanes(fb_session* const* ss, int n, int lanes) {
+    std::vector<int> order(n), lane(n, 0);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int c) { return ss[a]->W[0] * ss[a]->H[0] > ss[c]->W[0] * ss[c]->H[0]; });
+    std::vector<long long> load(lanes, 0);
+    for (int i : order) {
+        int best = 0;
+        for (int l = 1; l < lanes; ++l)
+            if (load[l] < load[best]) best = l;
+        lane[i] = best;
+        load[best] += (long long)ss[i]->W[0] * ss[i]->H[0];
+    }
+    return lane;
+}
+
 // Records every session's frame (and its result read-back), merges the
-// launches of the same slot and kernel across sessions, and uploads the
-// merged launches' parts and argument tuples.
+// launches of the same lane, slot and kernel across sessions (up to
+// kFusedMaxParts sessions per launch), and lays out each merged launch's
+// parameter.
 int build_fused(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plans, FusedPlan& out) {
     if ((int)b->recs.size() < n) b->recs.resize(n);
     int kernels = 0;
@@ -125,9 +155,10 @@ int build_fused(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plan
             }
         kernels += (int)r.recs.size();
     }
-    // (slot, kernel, block shape, shared memory, session): launches of one
-    // slot and kernel merge; the sessions' parts keep session order
-    using Ent = std::tuple<uint64_t, uintptr_t, unsigned, unsigned, unsigned, size_t, int, int>;
+    // (lane, slot, kernel, block shape, shared memory, session): launches of
+    // one lane, slot and kernel merge; the sessions' parts keep session order
+    const std::vector<int> lane = assign_lanes(ss, n, out.lanes);
+    using Ent = std::tuple<int, uint64_t, uintptr_t, unsigned, unsigned, size_t, int, int>;
     std::vector<Ent> ents;
     ents.reserve((size_t)kernels);
     for (int i = 0; i < n; ++i)
@@ -137,7 +168,7 @@ int build_fused(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plan
                 fb_set_error_text("fused batch step: 3-D grid");
                 return FB_ECUDA;
             }
-            ents.emplace_back(r.slot, (uintptr_t)r.fused, r.block.x, r.block.y, r.block.z, r.smem, i, k);
+            ents.emplace_back(lane[i], r.slot, (uintptr_t)r.fused, r.block.x, r.block.y, r.smem, i, k);
         }
     std::sort(ents.begin(), ents.end());
     std::vector<FusedLaunch> launches;
@@ -145,9 +176,10 @@ int build_fused(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plan
     size_t bytes = 0;
     for (size_t e = 0; e < ents.size();) {
         size_t f = e + 1;
-        while (f < ents.size() && std::get<0>(ents[f]) == std::get<0>(ents[e]) &&
+        while (f < ents.size() && f - e < (size_t)kFusedMaxParts && std::get<0>(ents[f]) == std::get<0>(ents[e]) &&
                std::get<1>(ents[f]) == std::get<1>(ents[e]) && std::get<2>(ents[f]) == std::get<2>(ents[e]) &&
-               std::get<3>(ents[f]) == std::get<3>(ents[e]) && std::get<5>(ents[f]) == std::get<5>(ents[e]))
+               std::get<3>(ents[f]) == std::get<3>(ents[e]) && std::get<4>(ents[f]) == std::get<4>(ents[e]) &&
+               std::get<5>(ents[f]) == std::get<5>(ents[e]))
             ++f;
         const LaunchRec& r0 = b->recs[std::get<6>(ents[e])].recs[std::get<7>(ents[e])];
         FusedLaunch L;
@@ -155,19 +187,19 @@ int build_fused(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plan
         L.block = r0.block;
         L.smem = r0.smem;
         L.n = (int)(f - e);
+        L.lane = std::get<0>(ents[e]);
         L.blocks = 0;
-        L.parts_off = (bytes + 15) & ~(size_t)15;
-        bytes = L.parts_off + sizeof(FusedPart) * L.n;
-        L.args_off = (bytes + 15) & ~(size_t)15;
-        bytes = L.args_off + r0.size * L.n;
+        L.param_off = bytes;
+        bytes += fused_param_bytes(r0.size);
         launches.push_back(L);
         groups.emplace_back(e, f);
         e = f;
     }
-    b->blob.assign(bytes, 0);
+    out.params.assign(bytes, 0);
     for (size_t g = 0; g < launches.size(); ++g) {
         FusedLaunch& L = launches[g];
-        FusedPart* parts = (FusedPart*)(b->blob.data() + L.parts_off);
+        unsigned char* prm = out.params.data() + L.param_off;
+        FusedPart* parts = (FusedPart*)prm;
         size_t size0 = 0;
         for (size_t e = groups[g].first; e < groups[g].second; ++e) {
             const LaunchRec& r = b->recs[std::get<6>(ents[e])].recs[std::get<7>(ents[e])];
@@ -185,25 +217,33 @@ int build_fused(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plan
             parts[j] = FusedPart{L.blocks, (int)r.grid.x, (int)r.grid.y, 0};
             L.blocks += (int)nb;
             const unsigned char* src = b->recs[std::get<6>(ents[e])].bytes.data() + r.off;
-            std::memcpy(b->blob.data() + L.args_off + (size_t)j * r.size, src, r.size);
+            std::memcpy(prm + kFusedArgsOffset + (size_t)j * r.size, src, r.size);
         }
+        std::memcpy(prm + kFusedNOffset, &L.n, sizeof(int));
     }
-    FB_CUDA(cudaMallocAsync(&out.dev, bytes ? bytes : 16, b->origin));
-    if (bytes) FB_CUDA(cudaMemcpyAsync(out.dev, b->blob.data(), bytes, cudaMemcpyHostToDevice, b->origin));
     out.launches = std::move(launches);
     out.kernels = kernels;
     return FB_OK;
 }
 
+// The plan's launches: lane l on slot stream l, forked from and joined back
+// into the origin stream (one lane: on the origin stream itself).
 int launch_fused(fb_batch* b, const FusedPlan& p) {
-    for (const FusedLaunch& L : p.launches) {
-        FusedArgs fa;
-        fa.parts = (const FusedPart*)((const char*)p.dev + L.parts_off);
-        fa.args = (const char*)p.dev + L.args_off;
-        fa.n = L.n;
-        void* kargs[] = {&fa};
-        FB_CUDA(cudaLaunchKernel(L.fused, dim3((unsigned)L.blocks), L.block, kargs, L.smem, b->origin));
+    const bool fork = p.lanes > 1;
+    if (fork) {
+        FB_CUDA(cudaEventRecord(b->fork, b->origin));
+        for (int l = 0; l < p.lanes; ++l) FB_CUDA(cudaStreamWaitEvent(b->slots[l], b->fork, 0));
     }
+    for (const FusedLaunch& L : p.launches) {
+        void* kargs[] = {(void*)(p.params.data() + L.param_off)};
+        cudaStream_t st = fork ? b->slots[L.lane] : b->origin;
+        FB_CUDA(cudaLaunchKernel(L.fused, dim3((unsigned)L.blocks), L.block, kargs, L.smem, st));
+    }
+    if (fork)
+        for (int l = 0; l < p.lanes; ++l) {
+            FB_CUDA(cudaEventRecord(b->done[l], b->slots[l]));
+            FB_CUDA(cudaStreamWaitEvent(b->origin, b->done[l], 0));
+        }
     return FB_OK;
 }
 
@@ -212,15 +252,14 @@ int launch_fused(fb_batch* b, const FusedPlan& p) {
 // directly: no instantiation for one-off mixes of the served form).
 int fused_step(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plans) {
     std::vector<uint64_t> key = composition(ss, n, plans);
+    const int lanes = std::max(1, std::min(std::min(b->lanes, n), kBatchSlots));
+    key.push_back((uint64_t)lanes);
     auto it = b->fused.find(key);
     if (it == b->fused.end()) {
         if (b->fused.size() >= kFusedCacheMax) clear_fused(b);
         FusedPlan p;
-        int rc = build_fused(b, ss, n, plans, p);
-        if (rc) {
-            if (p.dev) cudaFreeAsync(p.dev, b->origin);
-            return rc;
-        }
+        p.lanes = lanes;
+        if (int rc = build_fused(b, ss, n, plans, p)) return rc;
         it = b->fused.emplace(std::move(key), std::move(p)).first;
     }
     FusedPlan& p = it->second;
@@ -246,12 +285,7 @@ int fused_step(fb_batch* b, fb_session* const* ss, int n, const FramePlan* plans
     return check_launch();
 }
 
-// Slot streams of a batch: a fixed set, created with the batch.  Creating a
-// stream while frames run can take tens of milliseconds (the driver
-// serialises it with the device's work), so a step never creates one; beyond
-// kBatchSlots sessions, sessions share slots round-robin (their frames then
-// run one after the other on that slot, with the same results).
-constexpr int kBatchSlots = 32;
+
 // Steps of at most this many sessions run each frame as a session alone
 // (served p50 at 64 clients on B200: 2.50 ms with 1, 2.25 with 2, 1.67 with 3).
 constexpr int kBatchSharedMin = 3;
@@ -371,6 +405,12 @@ int fb_batch_reserve(fb_batch* b, size_t bytes) {
 int fb_batch_set_mode(fb_batch* b, int mode) {
     if (!b || mode < 0 || mode > 2) return FB_EINVAL;
     b->mode = mode;
+    return FB_OK;
+}
+
+int fb_batch_set_lanes(fb_batch* b, int lanes) {
+    if (!b || lanes < 1 || lanes > kBatchSlots) return FB_EINVAL;
+    b->lanes = lanes;
     return FB_OK;
 }
 

@@ -5,10 +5,14 @@
 // coordinates as an argument (BlockCtx) instead of reading blockIdx and
 // gridDim.  Two kernels wrap each body:
 //   - the ordinary kernel (one session), which passes its own coordinates;
-//   - the fused kernel, whose 1-D grid is the concatenation of several
-//     sessions' grids ("parts"): each block finds its part, takes that
-//     part's argument tuple and runs the body with the coordinates it has in
-//     that part's own grid.
+//   - the fused kernel, whose 1-D grid is the concatenation of up to
+//     kFusedMaxParts sessions' grids ("parts"): each block finds its part,
+//     takes that part's argument tuple and runs the body with the
+//     coordinates it has in that part's own grid.
+// The parts and their argument tuples are the fused kernel's parameter (a
+// __grid_constant__ block of at most a few KB), so a body reads its
+// arguments from the constant bank as the ordinary kernel does, instead of
+// holding them in registers.
 // A body therefore sees exactly what it sees in a launch of its own -- the
 // same arguments, blocks and grid size -- and computes the same bits.
 //
@@ -46,13 +50,25 @@ struct FusedPart {
     int start, gx, gy, pad;
 };
 
-// Arguments of a fused kernel: n parts (ascending start) and n argument
-// tuples of the kernel's type, both in device memory.
-struct FusedArgs {
-    const FusedPart* __restrict__ parts;
-    const void* __restrict__ args;
-    int n;
+constexpr int kFusedMaxParts = 32;
+
+// Parameter of a fused kernel: n parts (ascending start) and their argument
+// tuples (type Tup, stored as bytes: kFusedMaxParts slots of sizeof(Tup)).
+// Layout (host and device): parts at 0, n at 16 * kFusedMaxParts, the
+// tuples from 16 * kFusedMaxParts + 16.
+template <class Tup>
+struct alignas(16) FusedParams {
+    FusedPart parts[kFusedMaxParts];
+    int n, pad[3];
+    alignas(16) unsigned char args[kFusedMaxParts * sizeof(Tup)];
 };
+
+// The byte layout of FusedParams for a tuple of `tup_size` bytes.
+constexpr size_t kFusedNOffset = sizeof(FusedPart) * kFusedMaxParts;
+constexpr size_t kFusedArgsOffset = kFusedNOffset + 16;
+constexpr size_t fused_param_bytes(size_t tup_size) {
+    return (kFusedArgsOffset + kFusedMaxParts * tup_size + 15) & ~(size_t)15;
+}
 
 // The argument tuple of a kernel: its parameter types, in order.
 template <class F>
@@ -64,38 +80,33 @@ struct KernelArgs<void (*)(P...)> {
 template <class F>
 using ArgsOf = typename KernelArgs<F>::type;
 
-// The part of block b: the last part whose start is <= b.
-__device__ __forceinline__ int find_part(const FusedPart* __restrict__ parts, int n, int b) {
-    int lo = 0, hi = n - 1;
+// Runs body(ctx, args...) for this block's part of a fused launch: the
+// last part whose start is <= blockIdx.x.
+template <class Tup, class Body>
+__device__ __forceinline__ void run_part(const FusedParams<Tup>& fp, Body body) {
+    static_assert(alignof(Tup) <= 16 && sizeof(FusedParams<Tup>) <= 32764, "fused kernel parameter");
+    const int b = (int)blockIdx.x;
+    int lo = 0, hi = fp.n - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(&parts[mid].start) <= b)
+        if (fp.parts[mid].start <= b)
             lo = mid;
         else
             hi = mid - 1;
     }
-    return lo;
-}
-
-// Runs body(ctx, args...) for this block's part of a fused launch.
-template <class Tup, class Body>
-__device__ __forceinline__ void run_part(const FusedArgs& fa, Body body) {
-    const int b = (int)blockIdx.x;
-    const int i = find_part(fa.parts, fa.n, b);
-    const FusedPart p = fa.parts[i];
+    const FusedPart& p = fp.parts[lo];
     const int local = b - p.start;
     const BlockCtx c{local % p.gx, local / p.gx, p.gx, p.gy};
-    const Tup& t = static_cast<const Tup*>(fa.args)[i];
+    const Tup& t = reinterpret_cast<const Tup*>(fp.args)[lo];
     cuda::std::apply([&](const auto&... a) { body(c, a...); }, t);
 }
 
 // The fused form of kernel `single` (whose body is `body`), with the given
 // launch bounds: named single##_fused.
-#define FB_FUSED_KERNEL(single, body, ...)                                                              \
-    __global__ void __launch_bounds__(__VA_ARGS__) single##_fused(fb::FusedArgs fa) {                  \
-        fb::run_part<fb::ArgsOf<decltype(&single)>>(fa, [](const fb::BlockCtx& c, const auto&... a) {  \
-            body(c, a...);                                                                              \
-        });                                                                                             \
+#define FB_FUSED_KERNEL(single, body, ...)                                                                     \
+    __global__ void __launch_bounds__(__VA_ARGS__)                                                             \
+        single##_fused(const __grid_constant__ fb::FusedParams<fb::ArgsOf<decltype(&single)>> fp) {           \
+        fb::run_part(fp, [](const fb::BlockCtx& c, const auto&... a) { body(c, a...); });                      \
     }
 
 // ------------------------------------------------------------------ host side

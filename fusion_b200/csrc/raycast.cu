@@ -451,9 +451,9 @@ __global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__
     raycast_body<VR>(own_ctx(), m, vmap, nmap, vp, W, H, k, posep, skip);
 }
 template <class VR>
-__global__ void __launch_bounds__(128) k_raycast_fused(FusedArgs fa) {
-    run_part<ArgsOf<decltype(&k_raycast<VR>)>>(
-        fa, [](const BlockCtx& c, const auto&... a) { raycast_body<VR>(c, a...); });
+__global__ void __launch_bounds__(128)
+    k_raycast_fused(const __grid_constant__ FusedParams<ArgsOf<decltype(&k_raycast<VR>)>> fp) {
+    run_part(fp, [](const BlockCtx& c, const auto&... a) { raycast_body<VR>(c, a...); });
 }
 
 // The same rays with lane refill: a persistent grid whose warps take pixels
@@ -583,9 +583,9 @@ __global__ void __launch_bounds__(128, 8) k_raycast_pool(MapView m, float4* __re
     raycast_pool_body<VR>(own_ctx(), m, vmap, nmap, vp, W, H, k, posep, skip);
 }
 template <class VR>
-__global__ void __launch_bounds__(128, 8) k_raycast_pool_fused(FusedArgs fa) {
-    run_part<ArgsOf<decltype(&k_raycast_pool<VR>)>>(
-        fa, [](const BlockCtx& c, const auto&... a) { raycast_pool_body<VR>(c, a...); });
+__global__ void __launch_bounds__(128, 8)
+    k_raycast_pool_fused(const __grid_constant__ FusedParams<ArgsOf<decltype(&k_raycast_pool<VR>)>> fp) {
+    run_part(fp, [](const BlockCtx& c, const auto&... a) { raycast_pool_body<VR>(c, a...); });
 }
 
 static int sm_count_rc() {

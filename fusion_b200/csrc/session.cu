@@ -200,7 +200,6 @@ float half_bits_to_float(uint16_t h) {
 
 bool valid_config(const fb_config* c) {
     if (!c || c->width < 16 || c->height < 16 || c->width > 4096 || c->height > 2048) return false;
-    if ((size_t)c->width * c->height >= (1u << 22)) return false;  // packed RGB correspondences
     if (!(c->fx > 0) || !(c->fy > 0) || !(c->depth_scale > 0) || !(c->voxel_size > 0) || !(c->trunc_dist > 0))
         return false;
     if (c->num_buckets <= 0 || c->num_excess < 0 || c->num_blocks <= 0) return false;

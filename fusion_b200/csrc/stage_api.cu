@@ -139,6 +139,7 @@ int rgb_step_check(const fb_image* gcurr, const fb_image* glast, const fb_image*
     if (!Rcurr || !RcurrInv || !Rlast || !RlastInv || !tcurr || !tlast || !K || !residual || !A || !b)
         return FB_EINVAL;
     const int W = gcurr->cols, H = gcurr->rows;
+    if (W > 4096 || H > 2048) return FB_EINVAL;   // packed correspondences: 12-bit column, 11-bit row
     if (glast->cols != W || glast->rows != H || vcurr->cols != W || vcurr->rows != H || vlast->cols != W ||
         vlast->rows != H || dx->cols != W || dy->cols != W || dx->rows != H || dy->rows != H ||
         gcurr->pitch != glast->pitch || vcurr->pitch != vlast->pitch || dx->pitch != dy->pitch)

@@ -32,6 +32,36 @@ namespace cg = cooperative_groups;
 namespace fb {
 
 // ------------------------------------------------------------ row builders
+//
+// The reference evaluates a few float expressions in double (Reduction.cu:
+// (float)(1.0 / (double)z), (int)((double)f + 0.5), (float)((double)f + 0.5),
+// (double)dx / 9.0, (double)x < c).  Their float equivalents below give the
+// same bits for every float input:
+//   - a quotient or sum of floats computed in double and rounded to float is
+//     the IEEE float quotient or sum (double rounding is innocuous when the
+//     wide format has at least 2p + 2 bits: 53 >= 50; f + 0.5 is exact in
+//     double where it matters), hence __frcp_rn, __fdiv_rn, __fadd_rn;
+//   - (int)((double)f + 0.5) truncates f + 0.5; the float sum rounded toward
+//     zero lies between that integer and the exact sum, so it truncates to
+//     the same integer (saturation and NaN -> 0 as the double conversion);
+//   - (double)x < c for a double c that is not a float holds exactly when x
+//     is below the smallest float above c.
+__device__ __forceinline__ int trunc_half_up(float f) { return __float2int_rz(__fadd_rz(f, 0.5f)); }
+constexpr float kBelow1em3 = 0.001f;   // (double)x < 1e-3  <=>  x < 0.001f
+constexpr float kBelow0p1 = 0.1f;      // (double)x < 0.1   <=>  x < 0.1f
+__device__ __forceinline__ float below_1em6() { return __int_as_float(0x358637be); }   // (double)x < 1e-6
+
+// Photometric correspondences are packed in 32 bits: last-frame pixel
+// (u, v) and the gray difference d (-254..255, as d + 255 in 1..510):
+// v << 21 | u << 9 | (d + 255).  Images are at most 4096 x 2048; the low 9
+// bits are never all ones, so -1 (all ones) marks "no correspondence".
+// Pixels of the correspondence lists are packed as y << 12 | x.
+__device__ __forceinline__ int pack_corr(int u, int v, int d255) {
+    return (int)(((unsigned)v << 21) | ((unsigned)u << 9) | (unsigned)d255);
+}
+__device__ __forceinline__ int corr_u(int c) { return (int)(((unsigned)c >> 9) & 4095u); }
+__device__ __forceinline__ int corr_v(int c) { return (int)((unsigned)c >> 21); }
+__device__ __forceinline__ int pack_xy(int x, int y) { return (y << 12) | x; }
 
 // ICPReduce::searchPoint + getRow (Reduction.cu:227-286).  Returns false when
 // the pixel has no correspondence.  Decisions use the order-exact float ops.
@@ -40,12 +70,12 @@ __device__ __forceinline__ bool icp_row(const TrackLevel& L, const DevPose& cur,
     const size_t i = (size_t)y * L.vp + x;
     float4 vc4 = L.vcurr[i];
     f3 vcurr_c = xyz(vc4);
-    if (isnan(vcurr_c.x) || (double)vcurr_c.z < 1e-3) return false;
+    if (isnan(vcurr_c.x) || vcurr_c.z < kBelow1em3) return false;
     f3 vcurr_g = add3(mv(cur.R, vcurr_c), cur.t);
     f3 vcurr_p = mv(last.Rinv, sub3(vcurr_g, last.t));
-    float invz = (float)(1.0 / (double)vcurr_p.z);
-    int u = (int)((double)fa(fm(fm(vcurr_p.x, invz), L.k.fx), L.k.cx) + 0.5);
-    int v = (int)((double)fa(fm(fm(vcurr_p.y, invz), L.k.fy), L.k.cy) + 0.5);
+    float invz = __frcp_rn(vcurr_p.z);
+    int u = trunc_half_up(fa(fm(fm(vcurr_p.x, invz), L.k.fx), L.k.cx));
+    int v = trunc_half_up(fa(fm(fm(vcurr_p.y, invz), L.k.fy), L.k.cy));
     if (u < 0 || v < 0 || u >= L.W || v >= L.H) return false;
     const size_t j = (size_t)v * L.vp + u;
     f3 vlast_c = xyz(L.vlast[j]);
@@ -72,8 +102,7 @@ __device__ __forceinline__ bool icp_row(const TrackLevel& L, const DevPose& cur,
 }
 
 // RGBReduction::FindCorresp (Reduction.cu:404-451).  Returns the packed
-// correspondence ((v * W + u) << 9 | (diff + 255)) of last-frame pixel (u, v),
-// or -1.
+// correspondence (pack_corr) of last-frame pixel (u, v), or -1.
 __device__ __forceinline__ int rgb_corresp(const TrackLevel& L, const DevPose& cur, const DevPose& last, int x,
                                            int y) {
     const int W = L.W, H = L.H;
@@ -95,36 +124,35 @@ __device__ __forceinline__ int rgb_corresp(const TrackLevel& L, const DevPose& c
     f3 vcl = mv(last.Rinv, sub3(vcurr_g, last.t));
     float pu = fa(fd(fm(L.k.fx, vcl.x), vcl.z), L.k.cx);
     float pv = fa(fd(fm(L.k.fy, vcl.y), vcl.z), L.k.cy);
-    int u = (int)floorf((float)((double)pu + 0.5));
-    int v = (int)floorf((float)((double)pv + 0.5));
+    int u = (int)floorf(__fadd_rn(pu, 0.5f));
+    int v = (int)floorf(__fadd_rn(pv, 0.5f));
     if (!(u >= 0 && v >= 0 && u < W && v < H)) return -1;
     float4 vlast = L.vlast[(size_t)v * L.vp + u];
     if (isnan(vlast.x)) return -1;
     float ddx = fs(vlast.x, vcurr.x), ddy = fs(vlast.y, vcurr.y), ddz = fs(vlast.z, vcurr.z),
           ddw = fs(vlast.w, vcurr.w);
     float nd = fsq(fa(fa(fa(fm(ddx, ddx), fm(ddy, ddy)), fm(ddz, ddz)), fm(ddw, ddw)));
-    if (!((double)nd < 0.1)) return -1;
+    if (!(nd < kBelow0p1)) return -1;
     int gl = L.glast[(size_t)v * L.gp + u];
     if (gl == 0) return -1;
     int diff = (int)L.gcurr[(size_t)y * L.gp + x] - gl;
-    return ((v * W + u) << 9) | (diff + 255);
+    return pack_corr(u, v, diff + 255);
 }
 
 // RGBReduction::GetRow (Reduction.cu:471-508)
 __device__ __forceinline__ void rgb_row(const TrackLevel& L, const DevPose& cur, const DevPose& last, int x, int y,
                                         int packed, float sigma, float row[7]) {
-    const int j = packed >> 9;
-    const int v = j / L.W, u = j - v * L.W;
+    const int v = corr_v(packed), u = corr_u(packed);
     const int diff = (packed & 511) - 255;
     float w = sigma + (float)abs(diff);
-    w = (double)w < 1e-3 ? 1.0f : 1.0f / w;
-    if ((double)sigma < 1e-6) w = 1.0f;
-    f3 vlast = xyz(L.vlast[(size_t)v * L.vp + u]);
+    w = w < kBelow1em3 ? 1.0f : __frcp_rn(w);
+    if (sigma < below_1em6()) w = 1.0f;
+    f3 vlast = xyz(L.vlast[v * L.vp + u]);
     f3 point = mv(cur.Rinv, sub3(add3(mv(last.R, vlast), last.t), cur.t));
-    const size_t k = (size_t)y * L.sp + x;
-    float gx = (float)((double)(float)L.dx[k] / 9.0);
-    float gy = (float)((double)(float)L.dy[k] / 9.0);
-    float invz = 1.0f / point.z;
+    const int k = y * L.sp + x;
+    float gx = __fdiv_rn((float)L.dx[k], 9.0f);
+    float gy = __fdiv_rn((float)L.dy[k], 9.0f);
+    float invz = __frcp_rn(point.z);
     f3 left;
     left.x = gx * L.k.fx * invz;
     left.y = gy * L.k.fy * invz;
@@ -147,17 +175,37 @@ struct PixelIn {
     int gc;         // current gray value
 };
 
-__device__ __forceinline__ PixelIn load_pixel(const TrackLevel& L, int p) {
+__device__ __forceinline__ PixelIn load_pixel(const TrackLevel& L, int x, int y) {
     PixelIn in;
-    const int y = p / L.W, x = p - y * L.W;
-    const size_t i = (size_t)y * L.vp + x, k = (size_t)y * L.sp + x;
+    const int i = y * L.vp + x;
     in.vc = L.vcurr[i];
     const float4 n = L.ncurr[i];
     in.nc = make_float3(n.x, n.y, n.z);
-    in.ok = L.rgbok[k];
-    in.gc = L.gcurr[(size_t)y * L.gp + x];
+    in.ok = L.rgbok[y * L.sp + x];
+    in.gc = L.gcurr[y * L.gp + x];
     return in;
 }
+
+// Pixel coordinates of a strided pixel walk without divisions: the walk
+// starts at linear pixel p and steps by S pixels (S = SY rows + SX columns).
+struct PixelWalk {
+    int x, y, sx, sy, W;
+    __device__ __forceinline__ PixelWalk(int p, int S, int W_) : W(W_) {
+        y = p / W;
+        x = p - y * W;
+        sy = S / W;
+        sx = S - sy * W;
+    }
+    __device__ __forceinline__ void next(int& nx, int& ny) const {
+        nx = x + sx;
+        ny = y + sy;
+        if (nx >= W) {
+            nx -= W;
+            ++ny;
+        }
+    }
+    __device__ __forceinline__ void step() { next(x, y); }
+};
 
 // icp_row and rgb_corresp of one pixel together (same arithmetic, same
 // decisions), with the pose-independent loads done by the caller and the four
@@ -172,11 +220,11 @@ __device__ __forceinline__ bool pixel_pass_a(const TrackLevel& L, const DevPose&
     const f3 vcurr_g = add3(mv(cur.R, vcurr_c), cur.t);
     // ICP projection (ICPReduce::searchPoint, Reduction.cu:227-250)
     int ju = -1;
-    if (!vnan && !((double)vcurr_c.z < 1e-3)) {
+    if (!vnan && !(vcurr_c.z < kBelow1em3)) {
         const f3 vcurr_p = mv(last.Rinv, sub3(vcurr_g, last.t));
-        const float invz = (float)(1.0 / (double)vcurr_p.z);
-        const int u = (int)((double)fa(fm(fm(vcurr_p.x, invz), L.k.fx), L.k.cx) + 0.5);
-        const int v = (int)((double)fa(fm(fm(vcurr_p.y, invz), L.k.fy), L.k.cy) + 0.5);
+        const float invz = __frcp_rn(vcurr_p.z);
+        const int u = trunc_half_up(fa(fm(fm(vcurr_p.x, invz), L.k.fx), L.k.cx));
+        const int v = trunc_half_up(fa(fm(fm(vcurr_p.y, invz), L.k.fy), L.k.cy));
         if (!(u < 0 || v < 0 || u >= L.W || v >= L.H)) ju = v * L.vp + u;
     }
     // photometric projection (RGBReduction::FindCorresp, Reduction.cu:404-451)
@@ -185,22 +233,22 @@ __device__ __forceinline__ bool pixel_pass_a(const TrackLevel& L, const DevPose&
         const f3 vcl = mv(last.Rinv, sub3(vcurr_g, last.t));
         const float pu = fa(fd(fm(L.k.fx, vcl.x), vcl.z), L.k.cx);
         const float pv = fa(fd(fm(L.k.fy, vcl.y), vcl.z), L.k.cy);
-        ur = (int)floorf((float)((double)pu + 0.5));
-        vr = (int)floorf((float)((double)pv + 0.5));
+        ur = (int)floorf(__fadd_rn(pu, 0.5f));
+        vr = (int)floorf(__fadd_rn(pv, 0.5f));
         if (ur >= 0 && vr >= 0 && ur < L.W && vr < L.H) jr = vr * L.vp + ur;
     }
     const float nanf_ = qnan();
     const float4 vl4 = ju >= 0 ? L.vlast[ju] : make_float4(nanf_, nanf_, nanf_, nanf_);
     const float4 nl4 = ju >= 0 ? L.nlast[ju] : make_float4(nanf_, nanf_, nanf_, nanf_);
     const float4 vr4 = jr >= 0 ? L.vlast[jr] : make_float4(nanf_, nanf_, nanf_, nanf_);
-    const int gl = jr >= 0 ? (int)L.glast[(size_t)vr * L.gp + ur] : 0;
+    const int gl = jr >= 0 ? (int)L.glast[vr * L.gp + ur] : 0;
     // photometric residual
     *rgb = -1;
     if (jr >= 0 && !isnan(vr4.x)) {
         const float ddx = fs(vr4.x, in.vc.x), ddy = fs(vr4.y, in.vc.y), ddz = fs(vr4.z, in.vc.z),
                     ddw = fs(vr4.w, in.vc.w);
         const float nd = fsq(fa(fa(fa(fm(ddx, ddx), fm(ddy, ddy)), fm(ddz, ddz)), fm(ddw, ddw)));
-        if ((double)nd < 0.1 && gl != 0) *rgb = ((vr * L.W + ur) << 9) | (in.gc - gl + 255);
+        if (nd < kBelow0p1 && gl != 0) *rgb = pack_corr(ur, vr, in.gc - gl + 255);
     }
     // ICP row (ICPReduce::getRow, Reduction.cu:252-286)
     if (ju < 0) return false;
@@ -570,8 +618,9 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     const int N = L.W * L.H;
     const int G = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int p = blockIdx.x * 256 + threadIdx.x;
+    PixelWalk pw(p, G * 256, L.W);
     PixelIn nxt;
-    if (p < N) nxt = load_pixel(L, p);
+    if (p < N) nxt = load_pixel(L, pw.x, pw.y);
     if (st->failed) return;   // uniform over the grid: written by an earlier kernel
     cg::cluster_group cl = cg::this_cluster();
     __shared__ float sm[8 * 32];
@@ -589,19 +638,21 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     int run = 0;
     for (int k = 0; k < iters; ++k, p += G * 256) {
         const PixelIn in = nxt;
-        if (k + 1 < iters && p + G * 256 < N) nxt = load_pixel(L, p + G * 256);   // one pixel ahead
+        const int px = pw.x, py = pw.y;
+        pw.step();
+        if (k + 1 < iters && p + G * 256 < N) nxt = load_pixel(L, pw.x, pw.y);   // one pixel ahead
         int r = -1;
         if (p < N) {
             float row[7];
             if (pixel_pass_a(L, cur, last, in, row, &r)) add_products(row, acc);
-            if (r >= 0) {
+            if (r != -1) {
                 int d = (r & 511) - 255;
                 rc += 1;
                 rsq += d * d;
             }
         }
-        const unsigned m = __ballot_sync(0xffffffffu, r >= 0);
-        if (r >= 0) seg[run + __popc(m & lt)] = make_int2(p, r);
+        const unsigned m = __ballot_sync(0xffffffffu, r != -1);
+        if (r != -1) seg[run + __popc(m & lt)] = make_int2(pack_xy(px, py), r);
         run += __popc(m);
     }
     if (lane == 0) counts[gw] = run;
@@ -789,7 +840,7 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     const int2* seg = list + (size_t)gw * seg_size;
     for (int i = lane; i < n; i += 32) {
         const int2 e = seg[i];
-        const int y = e.x / L.W, x = e.x - y * L.W;
+        const int y = e.x >> 12, x = e.x & 4095;
         float row[7];
         rgb_row(L, cur, last, x, y, e.y, sigma, row);
         add_products(row, acc);
@@ -855,8 +906,9 @@ __device__ __forceinline__ void track_a_grp_body(const BlockCtx& ctx, TrackLevel
     for (int r = 0; r < kTrackCluster; ++r) {
         const int b = g * kTrackCluster + r;
         int p = b * 256 + threadIdx.x;
+        PixelWalk pw(p, G * 256, L.W);
         PixelIn nxt;
-        if (p < N) nxt = load_pixel(L, p);
+        if (p < N) nxt = load_pixel(L, pw.x, pw.y);
         float acc[29];
 #pragma unroll
         for (int k = 0; k < 29; ++k) acc[k] = 0.f;
@@ -866,19 +918,21 @@ __device__ __forceinline__ void track_a_grp_body(const BlockCtx& ctx, TrackLevel
         int run = 0;
         for (int k = 0; k < iters; ++k, p += G * 256) {
             const PixelIn in = nxt;
-            if (k + 1 < iters && p + G * 256 < N) nxt = load_pixel(L, p + G * 256);   // one pixel ahead
+            const int px = pw.x, py = pw.y;
+            pw.step();
+            if (k + 1 < iters && p + G * 256 < N) nxt = load_pixel(L, pw.x, pw.y);   // one pixel ahead
             int rr = -1;
             if (p < N) {
                 float row[7];
                 if (pixel_pass_a(L, cur, last, in, row, &rr)) add_products(row, acc);
-                if (rr >= 0) {
+                if (rr != -1) {
                     int d = (rr & 511) - 255;
                     rc += 1;
                     rsq += d * d;
                 }
             }
-            const unsigned m = __ballot_sync(0xffffffffu, rr >= 0);
-            if (rr >= 0) seg[run + __popc(m & lt)] = make_int2(p, rr);
+            const unsigned m = __ballot_sync(0xffffffffu, rr != -1);
+            if (rr != -1) seg[run + __popc(m & lt)] = make_int2(pack_xy(px, py), rr);
             run += __popc(m);
         }
         if (lane == 0) counts[gw] = run;
@@ -979,7 +1033,7 @@ __device__ __forceinline__ void track_b_grp_body(const BlockCtx& ctx, TrackLevel
         const int2* seg = list + (size_t)gw * seg_size;
         for (int i = lane; i < n; i += 32) {
             const int2 e = seg[i];
-            const int y = e.x / L.W, x = e.x - y * L.W;
+            const int y = e.x >> 12, x = e.x & 4095;
             float row[7];
             rgb_row(L, cur, last, x, y, e.y, sigma, row);
             add_products(row, acc);
@@ -1019,9 +1073,9 @@ __global__ void __launch_bounds__(256, kMinBlocks)
     track_a_grp_body<kMinBlocks, kComp>(own_ctx(), L, st, list, counts, G, gpc);
 }
 template <int kMinBlocks, bool kComp>
-__global__ void __launch_bounds__(256, kMinBlocks) k_track_a_grp_fused(FusedArgs fa) {
-    run_part<ArgsOf<decltype(&k_track_a_grp<kMinBlocks, kComp>)>>(
-        fa, [](const BlockCtx& c, const auto&... a) { track_a_grp_body<kMinBlocks, kComp>(c, a...); });
+__global__ void __launch_bounds__(256, kMinBlocks)
+    k_track_a_grp_fused(const __grid_constant__ FusedParams<ArgsOf<decltype(&k_track_a_grp<kMinBlocks, kComp>)>> fp) {
+    run_part(fp, [](const BlockCtx& c, const auto&... a) { track_a_grp_body<kMinBlocks, kComp>(c, a...); });
 }
 
 template <int kMinBlocks, bool kComp>
@@ -1032,9 +1086,9 @@ __global__ void __launch_bounds__(256, kMinBlocks)
                                         gpc);
 }
 template <int kMinBlocks, bool kComp>
-__global__ void __launch_bounds__(256, kMinBlocks) k_track_b_grp_fused(FusedArgs fa) {
-    run_part<ArgsOf<decltype(&k_track_b_grp<kMinBlocks, kComp>)>>(
-        fa, [](const BlockCtx& c, const auto&... a) { track_b_grp_body<kMinBlocks, kComp>(c, a...); });
+__global__ void __launch_bounds__(256, kMinBlocks)
+    k_track_b_grp_fused(const __grid_constant__ FusedParams<ArgsOf<decltype(&k_track_b_grp<kMinBlocks, kComp>)>> fp) {
+    run_part(fp, [](const BlockCtx& c, const auto&... a) { track_b_grp_body<kMinBlocks, kComp>(c, a...); });
 }
 
 // The Gauss-Newton update of one iteration (Tracking.cc:319-394) and, after
@@ -1211,7 +1265,7 @@ __global__ void __launch_bounds__(256) k_step_rgb_a(TrackLevel L, DevPose cur, D
         const int y = p / L.W, x = p - y * L.W;
         int r = rgb_corresp(L, cur, last, x, y);
         residual[p] = r;
-        if (r >= 0) {
+        if (r != -1) {
             int d = (r & 511) - 255;
             rc += 1;
             rsq += d * d;
@@ -1244,7 +1298,7 @@ __global__ void __launch_bounds__(256) k_step_rgb_b(TrackLevel L, DevPose cur, D
     const int N = L.W * L.H;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
         int r = residual[p];
-        if (r < 0) continue;
+        if (r == -1) continue;
         const int y = p / L.W, x = p - y * L.W;
         float row[7];
         rgb_row(L, cur, last, x, y, r, sigma, row);

@@ -119,9 +119,8 @@ FB_API void fb_graph_exec_stats(long long* pooled, long long* updated, long long
 
 /* Replaces: System::System (Core/System.cc:16-73) -- Mapping::Create,
  * Tracker::Tracker, Frame::Create. stream: cudaStream_t or NULL (a stream is
- * created).  FB_EINVAL for images outside width 16-4096, height 16-2048 or
- * of 2^22 pixels or more (the photometric correspondences pack a 22-bit
- * pixel index). */
+ * created).  FB_EINVAL for images outside width 16-4096, height 16-2048
+ * (the photometric correspondences pack a 12-bit column and an 11-bit row). */
 FB_API int fb_session_create(const fb_config* cfg, void* stream, fb_session** out);
 FB_API int fb_session_destroy(fb_session* s);
 /* Replaces: System::RebootSystem / Mapping::Reset + Tracker::ResetTracking. */
@@ -245,6 +244,12 @@ FB_API int fb_batch_step(fb_batch* b, fb_session* const* sessions, int n, const 
                          fb_frame_result* out);
 /* Graph launches and captures so far (mode 1 captures once per composition). */
 FB_API int fb_batch_stats(fb_batch* b, uint64_t* steps, uint64_t* captures);
+/* Mode 2: the step's sessions are split into `lanes` groups of about equal
+ * pixel counts (1..32, default 4); each group's fused launches run on a
+ * stream of their own, so one group's latency-bound tracking overlaps
+ * another's throughput-bound raycast and integration.  Results do not depend
+ * on it. */
+FB_API int fb_batch_set_lanes(fb_batch* b, int lanes);
 /* Mode 2: kernel launches of the last step, and the per-session kernel
  * launches they carried (the launches modes 0 and 1 make for that step). */
 FB_API int fb_batch_launch_stats(fb_batch* b, int* launches, int* kernels);

@@ -73,7 +73,7 @@ def _alone(frames, schedule, forms=None):
     return out
 
 
-def _batched(frames, schedule, mode, tiles=None, forms=None, launch_stats=None):
+def _batched(frames, schedule, mode, tiles=None, forms=None, launch_stats=None, lanes=None):
     """schedule[i] = the steps at which session i has a frame."""
     from fusion_b200 import Batch, Session
     from fusion_b200.batch import set_raycast_tile
@@ -84,6 +84,8 @@ def _batched(frames, schedule, mode, tiles=None, forms=None, launch_stats=None):
     rows = [[] for _ in sess]
     nxt = [0] * len(sess)
     with Batch(mode=mode) as b:
+        if lanes:
+            b.set_lanes(lanes)
         n_steps = max(max(sch) for sch in schedule) + 1
         for step in range(n_steps):
             idx = [i for i in range(len(sess)) if step in schedule[i]]
@@ -150,8 +152,7 @@ def test_fused_step_mixes_map_forms(frames):
     (different integration and raycast kernels, tracking sums compensated or
     not) gives every session its results alone."""
     alone = _alone(frames, STAGGERED, forms=FORMS)
-    stats = []
-    fused, _ = _batched(frames, STAGGERED, 2, forms=FORMS, launch_stats=stats)
+    fused, _ = _batched(frames, STAGGERED, 2, forms=FORMS, lanes=2)
     for i in range(len(SPECS)):
         assert fused[i][0] == alone[i][0], f"session {i}: per-frame results differ"
         assert fused[i][1] == alone[i][1], f"session {i}: final map differs"
@@ -163,7 +164,9 @@ def test_fused_step_launch_count(frames):
     that stage (a few more where sessions run different kernels -- two map
     forms, different tracker modes)."""
     stats = []
-    _batched(frames, LOCKSTEP, 2, launch_stats=stats)
+    one_lane, _ = _batched(frames, LOCKSTEP, 2, launch_stats=stats, lanes=1)
+    alone = _alone(frames, LOCKSTEP)
+    assert one_lane == alone
     print("(sessions, launches, per-session kernels) per step:", stats)
     for n, launches, kernels in stats:
         assert 0 < launches <= kernels

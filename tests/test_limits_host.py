@@ -11,11 +11,12 @@ def _bytes(cfg):
 
 
 def test_image_size_limits():
-    # below 2^22 pixels (the packed photometric correspondence's pixel index)
+    # width <= 4096 and height <= 2048 (the packed photometric correspondence
+    # holds a 12-bit column and an 11-bit row)
     assert _bytes(make_config(2048, 2047, 0.01, 4, 1 << 16, 1 << 14, 1 << 14)) > 0
-    assert _bytes(make_config(4096, 1023, 0.01, 4, 1 << 16, 1 << 14, 1 << 14)) > 0
-    assert _bytes(make_config(4096, 1024, 0.01, 4, 1 << 16, 1 << 14, 1 << 14)) == 0   # exactly 2^22
-    assert _bytes(make_config(4096, 2048, 0.01, 4, 1 << 16, 1 << 14, 1 << 14)) == 0
+    assert _bytes(make_config(4096, 1024, 0.01, 4, 1 << 16, 1 << 14, 1 << 14)) > 0
+    assert _bytes(make_config(4096, 2048, 0.01, 4, 1 << 16, 1 << 14, 1 << 14)) > 0
+    assert _bytes(make_config(4096, 2049, 0.01, 4, 1 << 16, 1 << 14, 1 << 14)) == 0
     assert _bytes(make_config(4097, 16, 0.01, 4, 1 << 16, 1 << 14, 1 << 14)) == 0
     assert _bytes(make_config(16, 16, 0.01, 4, 1 << 16, 1 << 14, 1 << 14)) > 0
     assert _bytes(make_config(15, 16, 0.01, 4, 1 << 16, 1 << 14, 1 << 14)) == 0
