@@ -139,19 +139,39 @@ __device__ __forceinline__ int rgb_corresp(const TrackLevel& L, const DevPose& c
     return pack_corr(u, v, diff + 255);
 }
 
-// RGBReduction::GetRow (Reduction.cu:471-508)
-__device__ __forceinline__ void rgb_row(const TrackLevel& L, const DevPose& cur, const DevPose& last, int x, int y,
-                                        int packed, float sigma, float row[7]) {
-    const int v = corr_v(packed), u = corr_u(packed);
-    const int diff = (packed & 511) - 255;
+// The memory inputs of one photometric row: the last frame's vertex at the
+// correspondence, the current pixel's derivatives and the packed value.
+struct RgbIn {
+    float4 vlast;
+    int dx, dy, packed;
+};
+
+__device__ __forceinline__ RgbIn rgb_fetch(const TrackLevel& L, int x, int y, int packed) {
+    RgbIn in;
+    in.vlast = L.vlast[corr_v(packed) * L.vp + corr_u(packed)];
+    const int k = y * L.sp + x;
+    in.dx = L.dx[k];
+    in.dy = L.dy[k];
+    in.packed = packed;
+    return in;
+}
+
+// The fetch of correspondence list entry e (pixel y << 12 | x, packed value).
+__device__ __forceinline__ RgbIn rgb_fetch_entry(const TrackLevel& L, int2 e) {
+    return rgb_fetch(L, e.x & 4095, e.x >> 12, e.y);
+}
+
+// RGBReduction::GetRow (Reduction.cu:471-508) from fetched inputs.
+__device__ __forceinline__ void rgb_row_of(const RgbIn& in, const TrackLevel& L, const DevPose& cur,
+                                           const DevPose& last, float sigma, float row[7]) {
+    const int diff = (in.packed & 511) - 255;
     float w = sigma + (float)abs(diff);
     w = w < kBelow1em3 ? 1.0f : __frcp_rn(w);
     if (sigma < below_1em6()) w = 1.0f;
-    f3 vlast = xyz(L.vlast[v * L.vp + u]);
+    f3 vlast = xyz(in.vlast);
     f3 point = mv(cur.Rinv, sub3(add3(mv(last.R, vlast), last.t), cur.t));
-    const int k = y * L.sp + x;
-    float gx = __fdiv_rn((float)L.dx[k], 9.0f);
-    float gy = __fdiv_rn((float)L.dy[k], 9.0f);
+    float gx = __fdiv_rn((float)in.dx, 9.0f);
+    float gy = __fdiv_rn((float)in.dy, 9.0f);
     float invz = __frcp_rn(point.z);
     f3 left;
     left.x = gx * L.k.fx * invz;
@@ -165,6 +185,12 @@ __device__ __forceinline__ void rgb_row(const TrackLevel& L, const DevPose& cur,
     row[4] = w * c.y;
     row[5] = w * c.z;
     row[6] = -w * (float)diff;
+}
+
+// RGBReduction::GetRow of the correspondence `packed` of pixel (x, y).
+__device__ __forceinline__ void rgb_row(const TrackLevel& L, const DevPose& cur, const DevPose& last, int x, int y,
+                                        int packed, float sigma, float row[7]) {
+    rgb_row_of(rgb_fetch(L, x, y, packed), L, cur, last, sigma, row);
 }
 
 // Pose-independent inputs of one pixel for pass A (loaded one pixel ahead).
@@ -282,6 +308,25 @@ __device__ __forceinline__ void add_products(const float row[7], float acc[29]) 
 #pragma unroll
         for (int j = i; j < 7; ++j) acc[n++] += row[i] * row[j];
     acc[28] += 1.0f;
+}
+
+// Pass B's rows of one warp segment (n entries): lane l adds the rows of
+// entries l, l + 32, ... in that order.  The next entry's loads are issued
+// before the current row is computed, so the list read and the dependent
+// gathers of two entries overlap.
+__device__ __forceinline__ void add_segment_rows(const TrackLevel& L, const DevPose& cur, const DevPose& last,
+                                                 float sigma, const int2* seg, int n, int lane, float acc[29]) {
+    int i = lane;
+    if (i >= n) return;
+    RgbIn a = rgb_fetch_entry(L, seg[i]);
+    for (; i < n; i += 32) {
+        RgbIn b = a;
+        if (i + 32 < n) b = rgb_fetch_entry(L, seg[i + 32]);
+        float row[7];
+        rgb_row_of(a, L, cur, last, sigma, row);
+        add_products(row, acc);
+        a = b;
+    }
 }
 
 // ------------------------------------------------------------- reductions
@@ -836,15 +881,7 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
 #pragma unroll
     for (int k = 0; k < 29; ++k) acc[k] = 0.f;
     const int gw = blockIdx.x * kTrackWarps + wid;
-    const int n = counts[gw];
-    const int2* seg = list + (size_t)gw * seg_size;
-    for (int i = lane; i < n; i += 32) {
-        const int2 e = seg[i];
-        const int y = e.x >> 12, x = e.x & 4095;
-        float row[7];
-        rgb_row(L, cur, last, x, y, e.y, sigma, row);
-        add_products(row, acc);
-    }
+    add_segment_rows(L, cur, last, sigma, list + (size_t)gw * seg_size, counts[gw], lane, acc);
     const float bsum = block_sum29(acc, sm);
     if (wid == 0) s_rgb[lane] = lane < 29 ? bsum : 0.f;
     const int grp = blockIdx.x / kTrackCluster;
@@ -1029,15 +1066,7 @@ __device__ __forceinline__ void track_b_grp_body(const BlockCtx& ctx, TrackLevel
 #pragma unroll
         for (int k = 0; k < 29; ++k) acc[k] = 0.f;
         const int gw = b * kTrackWarps + wid;
-        const int n = counts[gw];
-        const int2* seg = list + (size_t)gw * seg_size;
-        for (int i = lane; i < n; i += 32) {
-            const int2 e = seg[i];
-            const int y = e.x >> 12, x = e.x & 4095;
-            float row[7];
-            rgb_row(L, cur, last, x, y, e.y, sigma, row);
-            add_products(row, acc);
-        }
+        add_segment_rows(L, cur, last, sigma, list + (size_t)gw * seg_size, counts[gw], lane, acc);
         const float bsum = block_sum29(acc, sm);
         if (wid == 0) s_rgb[r][lane] = lane < 29 ? bsum : 0.f;
         __syncthreads();   // sm is reused by the next logical block
