@@ -24,6 +24,17 @@ __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); 
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+// a / b given y, the correctly rounded reciprocal of b (__frcp_rn(b)), by
+// Markstein's correction step (Markstein 1990): q = a y, r = a - q b (exact
+// by FMA), q + r y rounded once.  This is the IEEE quotient fd(a, b) when a,
+// b and a / b are normal floats or a is zero (the case r == 0 keeps q and its
+// sign); b must not be zero.  Several quotients by one divisor then share
+// one reciprocal.
+__device__ __forceinline__ float fd_rcp(float a, float b, float y) {
+    const float q = __fmul_rn(a, y);
+    const float r = __fmaf_rn(-q, b, a);
+    return r == 0.0f ? q : __fmaf_rn(r, y, q);
+}
 __device__ __forceinline__ float fsq(float a) { return __fsqrt_rn(a); }
 __device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }

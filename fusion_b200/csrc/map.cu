@@ -606,7 +606,17 @@ __device__ __forceinline__ bool integrate_voxel(Voxel& vox, int vx, int vy, int 
                                                 const float* __restrict__ div255) {
     f3 pos = mk3(fm((float)vx, g.voxel_size), fm((float)vy, g.voxel_size), fm((float)vz, g.voxel_size));
     pos = mv(P.Rinv, sub3(pos, P.t));
-    const float pu = fa(fd(fm(k.fx, pos.x), pos.z), k.cx), pv = fa(fd(fm(k.fy, pos.y), pos.z), k.cy);
+    // the two quotients by pos.z share one reciprocal (fd_rcp); positions are
+    // sums of products of voxel-scale values, normal floats or exactly zero
+    float pu, pv;
+    if (pos.z != 0.0f) {
+        const float rz = __frcp_rn(pos.z);
+        pu = fa(fd_rcp(fm(k.fx, pos.x), pos.z, rz), k.cx);
+        pv = fa(fd_rcp(fm(k.fy, pos.y), pos.z, rz), k.cy);
+    } else {
+        pu = fa(fd(fm(k.fx, pos.x), pos.z), k.cx);
+        pv = fa(fd(fm(k.fy, pos.y), pos.z), k.cy);
+    }
     const int u = __float2int_rz(pu), v = __float2int_rz(pv);  // make_int2(float2)
     if (u < 0 || v < 0 || u >= W || v >= H) return false;
     const int pix = v * W + u;
@@ -614,12 +624,16 @@ __device__ __forceinline__ bool integrate_voxel(Voxel& vox, int vx, int vy, int 
     const float thresh = g.trunc_dist;
     float sdf = fs(r.x, pos.z);
     if (!(sdf >= -thresh)) return false;
-    sdf = fminf(1.0f, fd(sdf, thresh));
+    sdf = fminf(1.0f, fd_rcp(sdf, thresh, __frcp_rn(thresh)));
     // w = nl * normalised(float4(pos, 1)): the dot runs over all four lanes
     // (the normal's w lane is 1, so its term is 1 / nrm)
     const float nrm = fsq(fa(fa(fa(fm(pos.x, pos.x), fm(pos.y, pos.y)), fm(pos.z, pos.z)), 1.0f));
-    const float w = fa(fa(fa(fm(r.y, fd(pos.x, nrm)), fm(r.z, fd(pos.y, nrm))), fm(r.w, fd(pos.z, nrm))),
-                       fd(1.0f, nrm));
+    // nrm >= 1: the four quotients share its reciprocal (1 / nrm is that
+    // reciprocal itself)
+    const float rn = __frcp_rn(nrm);
+    const float w = fa(fa(fa(fm(r.y, fd_rcp(pos.x, nrm, rn)), fm(r.z, fd_rcp(pos.y, nrm, rn))),
+                          fm(r.w, fd_rcp(pos.z, nrm, rn))),
+                       rn);
     const uint32_t c = __ldg(col + pix);
     const uint32_t cr = c & 255u, cg = (c >> 8) & 255u, cb = c >> 16;
     if (vox.weight == 0) {
