@@ -23,12 +23,16 @@ Our arm prints one JSON line with
   batched the batched form (N=1): many sessions stepped together by
           fb_batch_step -- sessions of the same full-size configuration (like
           for like with `value`) and the ragged mix (three resolutions, voxels
-          4-20 mm) with autotuned raycast tiles; aggregate frames/s;
+          4-20 mm) with autotuned raycast tiles; aggregate frames/s; each also
+          with fused launches (batch mode 2: one launch per stage kernel for
+          all sessions) and with four batches in flight (fb_batch_submit /
+          fb_batch_collect);
   served  the served form (N=1): clients arriving and leaving, 30 Hz Poisson
           frames, admission by HBM budget and calibrated GPU load,
-          continuous batching; aggregate frames/s and p50/p99 latency from
-          frame arrival to fusion, at 64 clients and (more_clients) at 256
-          clients plus arrivals, more than one GPU serves;
+          continuous batching with two steps in flight; aggregate frames/s
+          and p50/p99 latency from frame arrival to fusion, at 64 clients and
+          (more_clients) at 256 clients plus arrivals, more than one GPU
+          serves;
   precision, mesh, keypoints, widened, reference_constants
           the precision form, mesh extraction, frames with key points, the
           top-down view / shading / snapshot / map-file timings, and this
@@ -465,6 +469,69 @@ def ours_at_reference_constants(depth, rgb, frames=80, warmup=5):
             "mesh": mesh}
 
 
+def _pipelined_run(specs, seeds, warmup, steps, mode=0, parts=2, lanes=None):
+    """The sessions split into `parts` groups of equal pixel counts, each
+    group a batch with one step in flight (fb_batch_submit / fb_batch_collect
+    in turn), frames resident in HBM.  Aggregate frames/s over all groups."""
+    import torch
+    import rgbd_synth as synth
+    from fusion_b200 import Batch, Session
+    n_fr = 24
+    seqs = {}
+    for k, (w, h, _, _) in enumerate(specs):
+        key = (w, h, k % len(seeds))
+        if key not in seqs:
+            p = synth.params(w, h, seeds[key[2]], fx=525.0 * w / 640.0, fy=525.0 * w / 640.0, cx=w / 2.0,
+                             cy=h / 2.0, depth_scale=5000.0)
+            d, c, _ = synth.render(p, 0, n_fr)
+            seqs[key] = (torch.from_numpy(d).cuda(), torch.from_numpy(c).cuda())
+    keys = [(w, h, k % len(seeds)) for k, (w, h, _, _) in enumerate(specs)]
+    sess = [Session(cfg) for (_, _, _, cfg) in specs]
+    order = sorted(range(len(specs)), key=lambda i: -specs[i][0] * specs[i][1])
+    halves, load = [[] for _ in range(parts)], [0] * parts
+    for i in order:
+        j = min(range(parts), key=lambda q: load[q])
+        halves[j].append(i)
+        load[j] += specs[i][0] * specs[i][1]
+    batches = [Batch(mode=mode) for _ in range(parts)]
+    if lanes:
+        for b in batches:
+            b.set_lanes(lanes)
+    step_no = [0] * parts
+
+    def frames(hh):
+        i = step_no[hh]
+        step_no[hh] += 1
+        j = i % (2 * n_fr - 2)
+        j = j if j < n_fr else 2 * n_fr - 2 - j
+        return [(seqs[keys[k]][0][j], seqs[keys[k]][1][j]) for k in halves[hh]]
+
+    for hh in range(parts):
+        batches[hh].submit([sess[k] for k in halves[hh]], frames(hh), on_device=True)
+    tracked = 0
+    t0 = None
+    for it in range(warmup + steps):
+        if it == warmup:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+        for hh in range(parts):
+            res = batches[hh].collect()
+            if it >= warmup:
+                tracked += sum(r.tracked for r in res)
+            if it + 1 < warmup + steps:
+                batches[hh].submit([sess[k] for k in halves[hh]], frames(hh), on_device=True)
+    dt = time.perf_counter() - t0
+    for b in batches:
+        b.close()
+    for s in sess:
+        s.close()
+    n = len(specs)
+    return {"value": n * steps / dt, "unit": "frames/s", "ms_per_step": dt / steps * 1e3, "sessions": n,
+            "steps": steps, "warmup": warmup, "tracked_fraction": tracked / (n * steps), "batch_mode": mode,
+            "pipelined": f"{parts} batches of 1/{parts} of the sessions, one step each in flight",
+            "lanes": lanes if mode == 2 else None}
+
+
 def _batched_run(specs, seeds, warmup, steps, tune=False, mode=0):
     """Sessions `specs` [(w, h, voxel, config)] stepped together through
     fb_batch_step in batch mode `mode`, frames resident in HBM (each session
@@ -608,14 +675,28 @@ def batched_forms(args, rank, plain_value):
                        "uniform 4-20 mm, truncation 4 voxels, maps sized per voxel size")
     mix["vs_plain"] = mix["value"] / plain_value
     # fused launches (batch mode 2): one launch per stage kernel for all sessions
-    c2f = _batched_run([(640, 480, 0.005, S.config_c2())] * n, seeds, 3, 8, mode=2)
+    # (warm-up long enough for every composition of the timed steps -- the
+    # fusion switch at frame 10, both frame parities -- to have its graph)
+    c2f = _batched_run([(640, 480, 0.005, S.config_c2())] * n, seeds, 14, 8, mode=2)
     c2f["workload"] = c2["workload"] + "; fused launches"
     c2f["vs_plain"] = c2f["value"] / plain_value
     mixf = _batched_run([(w, h, v, mixed_config(w, h, v)) for (w, h, v) in mixed_population(n, 1234 + rank)],
-                        seeds, 3, 10, mode=2)
+                        seeds, 14, 10, mode=2)
     mixf["workload"] = mix["workload"] + "; fused launches"
     mixf["vs_plain"] = mixf["value"] / plain_value
-    return {"same_config": c2, "mixed": mix, "same_config_fused": c2f, "mixed_fused": mixf}
+    # several steps in flight: the sessions in four groups of equal pixel
+    # counts, one batch each, stepped in turn with fb_batch_submit / collect
+    out = {"same_config": c2, "mixed": mix, "same_config_fused": c2f, "mixed_fused": mixf}
+    mix_specs = [(w, h, v, mixed_config(w, h, v)) for (w, h, v) in mixed_population(n, 1234 + rank)]
+    for key, specs, mode, lanes, steps, wl in (
+            ("same_config_pipelined", [(640, 480, 0.005, S.config_c2())] * n, 0, None, 8, c2["workload"]),
+            ("mixed_pipelined", mix_specs, 0, None, 10, mix["workload"]),
+            ("mixed_fused_pipelined", mix_specs, 2, 2, 10, mixf["workload"])):
+        r = _pipelined_run(specs, seeds, 14, steps, mode=mode, parts=4, lanes=lanes)
+        r["workload"] = wl + "; four batches in flight"
+        r["vs_plain"] = r["value"] / plain_value
+        out[key] = r
+    return out
 
 
 def served_form(args, rank, plain_value):
@@ -629,7 +710,7 @@ def served_form(args, rank, plain_value):
     admission holding the latency of the admitted clients."""
     from fusion_b200.serve import FramePool, Server, make_clients, sequence_seeds
     pool = FramePool(sequence_seeds(7 + rank, 4), 30)
-    srv = Server(pool, budget_bytes=120e9, mode=0, max_batch=256)
+    srv = Server(pool, budget_bytes=120e9, mode=0, max_batch=256, pipeline=2)
     cost = srv.calibrate()
     runs = []
     for n in [int(x) for x in str(args.served_clients).split(",")]:

@@ -84,10 +84,7 @@ class Batch:
     def __exit__(self, *a):
         self.close()
 
-    def step(self, sessions, frames, on_device=False):
-        """One frame per session.  frames[i] = (depth u16 [H, W], rgb u8
-        [H, W, 3]): numpy arrays, or with on_device objects with data_ptr()
-        (contiguous device memory).  Returns one FrameResult per session."""
+    def _inputs(self, sessions, frames, on_device):
         n = len(sessions)
         hs = (ctypes.c_void_p * n)(*[s.h.value for s in sessions])
         ins = (FrameInput * n)()
@@ -101,8 +98,31 @@ class Batch:
                 c = np.ascontiguousarray(c, np.uint8)
                 keep.append((d, c))
                 ins[i] = FrameInput(d.ctypes.data, d.strides[0], c.ctypes.data, c.strides[0], 0)
+        return hs, ins, keep
+
+    def step(self, sessions, frames, on_device=False):
+        """One frame per session.  frames[i] = (depth u16 [H, W], rgb u8
+        [H, W, 3]): numpy arrays, or with on_device objects with data_ptr()
+        (contiguous device memory).  Returns one FrameResult per session."""
+        n = len(sessions)
+        hs, ins, keep = self._inputs(sessions, frames, on_device)
         out = (FrameResult * n)()
         check("fb_batch_step", self.lib.fb_batch_step(self.h, hs, n, ins, out))
+        return list(out)
+
+    def submit(self, sessions, frames, on_device=False):
+        """The first half of step(): starts the step and returns at once.
+        The frames (kept alive here) are read until collect()."""
+        hs, ins, keep = self._inputs(sessions, frames, on_device)
+        check("fb_batch_submit", self.lib.fb_batch_submit(self.h, hs, len(sessions), ins))
+        self._pending = (len(sessions), hs, ins, keep)
+
+    def collect(self):
+        """Waits for the submitted step; one FrameResult per session."""
+        n = self._pending[0]
+        out = (FrameResult * n)()
+        check("fb_batch_collect", self.lib.fb_batch_collect(self.h, out))
+        self._pending = None
         return list(out)
 
     def reserve(self, nbytes):

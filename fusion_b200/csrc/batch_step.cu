@@ -52,7 +52,12 @@ struct fb_batch {
     // mode 2: fused plans by composition, the recorders of a step's frames
     std::map<std::vector<uint64_t>, FusedPlan> fused;
     std::vector<LaunchRecorder> recs;
-    int lanes = 4;                             // fb_batch_set_lanes
+    int lanes = 4;
+    // the step in flight between fb_batch_submit and fb_batch_collect
+    bool pending = false;
+    std::vector<fb_session*> pend_ss;
+    std::vector<FramePlan> pend_plans;
+    cudaEvent_t pend_done = nullptr;                             // fb_batch_set_lanes
     int last_launches = 0, last_kernels = 0;   // of the last fused step
 };
 
@@ -379,6 +384,7 @@ int fb_batch_create(void* stream, fb_batch** out) {
 int fb_batch_destroy(fb_batch* b) {
     if (!b) return FB_EINVAL;
     cudaStreamSynchronize(b->origin);
+    if (b->pend_done) cudaEventDestroy(b->pend_done);
     clear_cache(b);
     clear_fused(b);
     for (size_t i = 0; i < b->slots.size(); ++i) {
@@ -429,7 +435,13 @@ int fb_batch_stats(fb_batch* b, uint64_t* steps, uint64_t* captures) {
 }
 
 int fb_batch_step(fb_batch* b, fb_session* const* ss, int n, const fb_frame_input* in, fb_frame_result* out) {
-    if (!b || !ss || !in || n <= 0) return FB_EINVAL;
+    int rc = fb_batch_submit(b, ss, n, in);
+    if (rc) return rc;
+    return fb_batch_collect(b, out);
+}
+
+int fb_batch_submit(fb_batch* b, fb_session* const* ss, int n, const fb_frame_input* in) {
+    if (!b || !ss || !in || n <= 0 || b->pending) return FB_EINVAL;
     for (int i = 0; i < n; ++i) {
         if (!ss[i] || !in[i].depth || !in[i].rgb || ss[i]->keys) return FB_EINVAL;
         if (in[i].depth_pitch < (size_t)ss[i]->W[0] * 2 || in[i].rgb_pitch < (size_t)ss[i]->W[0] * 3)
@@ -488,10 +500,22 @@ int fb_batch_step(fb_batch* b, fb_session* const* ss, int n, const fb_frame_inpu
         rc = issue_step(b, ss, n, plans.data(), true, &kernels);
         if (rc) return rc;
     }
-    FB_CUDA(cudaStreamSynchronize(b->origin));
+    if (!b->pend_done) FB_CUDA(cudaEventCreateWithFlags(&b->pend_done, cudaEventDisableTiming));
+    FB_CUDA(cudaEventRecord(b->pend_done, b->origin));
+    b->pend_ss.assign(ss, ss + n);
+    b->pend_plans = std::move(plans);
+    b->pending = true;
+    return FB_OK;
+}
+
+int fb_batch_collect(fb_batch* b, fb_frame_result* out) {
+    if (!b || !b->pending) return FB_EINVAL;
+    b->pending = false;
+    FB_CUDA(cudaEventSynchronize(b->pend_done));
+    const int n = (int)b->pend_ss.size();
     for (int i = 0; i < n; ++i) {
-        finish_frame(ss[i], plans[i], out ? &out[i] : nullptr);
-        ss[i]->shared_gpu = false;
+        finish_frame(b->pend_ss[i], b->pend_plans[i], out ? &out[i] : nullptr);
+        b->pend_ss[i]->shared_gpu = false;
     }
     b->steps++;
     return FB_OK;

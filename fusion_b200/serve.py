@@ -181,14 +181,23 @@ class Server:
     becomes active, and its frames start arriving, once its session is ready.
     Clients present at the start are admitted before the clock starts.
     Admission (class Admission) is by the HBM budget and, once calibrate()
-    has measured the per-resolution frame costs, by GPU load."""
+    has measured the per-resolution frame costs, by GPU load.
 
-    def __init__(self, pool, budget_bytes=120e9, mode=0, max_batch=256, frame_cost_ms=None, load_max=1.15):
+    pipeline: how many batch steps may be in flight at once (fb_batch_submit
+    / fb_batch_collect on that many batches).  With two, the loop submits
+    the ready clients' frames while another step runs, and collects the
+    oldest step when no further step can start (every batch busy, or every
+    ready client already in flight): one step's last kernels overlap the
+    next one's first.  A client has at most one frame in flight."""
+
+    def __init__(self, pool, budget_bytes=120e9, mode=0, max_batch=256, frame_cost_ms=None, load_max=1.15,
+                 pipeline=1):
         import torch
         self.lib = _lib.load()
         self.pool = pool
         self.budget = float(budget_bytes)
         self.batch = Batch(mode=mode)
+        self.batches = [self.batch] + [Batch(mode=mode) for _ in range(max(1, int(pipeline)) - 1)]
         self.max_batch = max_batch
         self.frame_cost_ms = dict(frame_cost_ms) if frame_cost_ms else None
         self.load_max = float(load_max)
@@ -199,7 +208,8 @@ class Server:
         self.stream = self._stream.cuda_stream
 
     def close(self):
-        self.batch.close()
+        for b in self.batches:
+            b.close()
 
     def _need(self, c):
         return float(self.lib.fb_session_bytes(mixed_config(c.width, c.height, c.voxel)))
@@ -330,6 +340,35 @@ class Server:
                 return
             worst[key] = max(worst[key], (time.perf_counter() - t_s) * 1e3)
 
+        free = list(range(len(self.batches)))
+        inflight = []    # (batch, clients, frames, submit time), oldest first
+        for c in clients:
+            c.in_flight = c.leaving = False
+
+        def close_client(c):
+            t_c = time.perf_counter()
+            c.session.close()
+            worst["close_ms"] = max(worst["close_ms"], (time.perf_counter() - t_c) * 1e3)
+            c.session = None
+            adm.release(c)
+            admit_waiting()
+
+        def collect_oldest():
+            b, ready, _, t_s = inflight.pop(0)
+            self.batches[b].collect()
+            t_done = now()
+            key = "step_with_new_session_ms" if any(c.sent < 2 for c in ready) else "step_ms"
+            worst[key] = max(worst[key], (t_done - t_s) * 1e3)
+            for c in ready:
+                lat.append(t_done - c.pending.pop(0))
+                c.sent += 1
+                c.in_flight = False
+                if c.leaving:
+                    c.leaving = False
+                    close_client(c)
+            batch_sizes.append(len(ready))
+            free.append(b)
+
         for c in warm:
             activate(c, 0.0)
         try:
@@ -348,38 +387,45 @@ class Server:
                             queued += 1
                     elif cid in active:
                         del active[cid]
-                        t_c = time.perf_counter()
-                        c.session.close()
-                        worst["close_ms"] = max(worst["close_ms"], (time.perf_counter() - t_c) * 1e3)
-                        c.session = None
-                        adm.release(c)
-                        admit_waiting()
+                        if c.in_flight:
+                            c.leaving = True    # closed when its step is collected
+                        else:
+                            close_client(c)
                 if preparing or to_open:
                     admission_slice()
                 for c in active.values():
                     while c.next_arrival is not None and c.next_arrival <= t and c.next_arrival < c.t_end:
                         c.pending.append(c.next_arrival)
                         c.next_arrival += c.rng.exponential(1.0 / c.rate)
-                ready = sorted((c for c in active.values() if c.pending), key=lambda c: c.pending[0])
-                if not ready:
-                    if not (preparing or to_open):
-                        nxt = min([c.next_arrival for c in active.values() if c.next_arrival is not None] +
-                                  ([events[0][0]] if events else []) + [duration])
-                        time.sleep(max(0.0, min(nxt - now(), 0.001)))
+                ready = sorted((c for c in active.values() if c.pending and not c.in_flight),
+                               key=lambda c: c.pending[0])
+                if ready and free:
+                    ready = ready[:self.max_batch]
+                    frames = [self.pool.frame(c.width, c.height, c.seq, c.sent) for c in ready]
+                    b = free.pop(0)
+                    t_s = now()
+                    self.batches[b].submit([c.session for c in ready], frames)
+                    for c in ready:
+                        c.in_flight = True
+                    inflight.append((b, ready, frames, t_s))
                     continue
-                ready = ready[:self.max_batch]
-                frames = [self.pool.frame(c.width, c.height, c.seq, c.sent) for c in ready]
-                t_s = now()
-                self.batch.step([c.session for c in ready], frames)
-                t_done = now()
-                key = "step_with_new_session_ms" if any(c.sent < 2 for c in ready) else "step_ms"
-                worst[key] = max(worst[key], (t_done - t_s) * 1e3)
-                for c in ready:
-                    lat.append(t_done - c.pending.pop(0))
-                    c.sent += 1
-                batch_sizes.append(len(ready))
+                if inflight:
+                    collect_oldest()
+                    continue
+                if not (preparing or to_open):
+                    nxt = min([c.next_arrival for c in active.values() if c.next_arrival is not None] +
+                              ([events[0][0]] if events else []) + [duration])
+                    time.sleep(max(0.0, min(nxt - now(), 0.001)))
+            while inflight:
+                collect_oldest()
             wall = now()
         finally:
+            # no session is closed while a step holding it may still run
+            for b, _, _, _ in inflight:
+                try:
+                    self.batches[b].collect()
+                except Exception:
+                    pass
             for c in clients:
                 if c.session is not None:
                     c.session.close()

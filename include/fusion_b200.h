@@ -242,6 +242,16 @@ FB_API int fb_batch_set_mode(fb_batch* b, int mode);
  * Synchronous.  A session must not be used elsewhere during the call. */
 FB_API int fb_batch_step(fb_batch* b, fb_session* const* sessions, int n, const fb_frame_input* in,
                          fb_frame_result* out);
+/* fb_batch_step in two halves: submit starts the step and collect waits for
+ * it and writes out[i] for the sessions in submission order.  The inputs are
+ * read by the device after submit returns: they must stay unchanged until
+ * collect.  One step per batch is in flight at a time
+ * (FB_EINVAL otherwise); until collect, its sessions must not be used
+ * elsewhere, in particular not in another batch.  Two batches over disjoint
+ * sessions, stepped alternately, keep two steps in flight: one step's last
+ * kernels overlap the other's first. */
+FB_API int fb_batch_submit(fb_batch* b, fb_session* const* sessions, int n, const fb_frame_input* in);
+FB_API int fb_batch_collect(fb_batch* b, fb_frame_result* out);
 /* Graph launches and captures so far (mode 1 captures once per composition). */
 FB_API int fb_batch_stats(fb_batch* b, uint64_t* steps, uint64_t* captures);
 /* Mode 2: the step's sessions are split into `lanes` groups of about equal

@@ -147,6 +147,34 @@ def test_raycast_tile_does_not_change_results(frames):
 FORMS = [1, 0, 1, 0, 0]   # precision and reference forms mixed in one step
 
 
+@pytest.mark.parametrize("mode", [0, 2])
+def test_two_batches_in_flight_equal_alone(frames, mode):
+    """Two batches over disjoint sessions, each with one step in flight
+    (fb_batch_submit / fb_batch_collect alternating), give every session its
+    results alone."""
+    from fusion_b200 import Batch, Session
+    alone = _alone(frames, LOCKSTEP)
+    sess = [Session(_config(i)) for i in range(len(SPECS))]
+    halves = [[0, 2, 4], [1, 3]]
+    rows = [[] for _ in sess]
+    batches = [Batch(mode=mode), Batch(mode=mode)]
+    for h, b in zip(halves, batches):
+        b.submit([sess[i] for i in h], [(frames[i][0][0], frames[i][1][0]) for i in h])
+    for k in range(N_FRAMES):
+        for h, b in zip(halves, batches):
+            res = b.collect()
+            for i, r in zip(h, res):
+                rows[i].append(_row(r))
+            if k + 1 < N_FRAMES:
+                b.submit([sess[i] for i in h], [(frames[i][0][k + 1], frames[i][1][k + 1]) for i in h])
+    for b in batches:
+        b.close()
+    out = [(rows[i], _map_digest(s)) for i, s in enumerate(sess)]
+    for s in sess:
+        s.close()
+    assert out == alone
+
+
 def test_fused_step_mixes_map_forms(frames):
     """A fused step holding precision-form and reference-form sessions
     (different integration and raycast kernels, tracking sums compensated or
