@@ -27,9 +27,9 @@
 // Visibility walks the list of allocated entries rather than every slot of
 // the table (CheckVisibleBlockKernel, FuseMap.cu:113-138, scans all of them).
 // Integration processes one visible block per CTA iteration: 256 threads, two
-// voxels each, one 16-byte load and at most one 16-byte store per thread; the
-// per-pixel inputs come from the frame's fusion records (one 16-byte gather
-// of depth and normal, one word of colour).
+// voxels each, one 16-byte load (issued one block ahead) and at most one
+// 16-byte store per thread; the per-pixel inputs come from the frame's fusion
+// records (one 16-byte gather of depth and normal, one word of colour).
 #include <cuda_fp16.h>
 
 #include "fb_fused.cuh"
@@ -671,11 +671,23 @@ __device__ __forceinline__ void integrate_body(const BlockCtx& ctx, MapView m, i
     const int lx = (2 * t) & 7, ly = (t >> 2) & 7, lz = t >> 5;
     const float4* __restrict__ rec = m.frec;
     const uint32_t* __restrict__ col = m.fcol;
+    // the next block's entry and voxels are loaded while this block's voxels
+    // are integrated (the blocks of one CTA are distinct)
+    HEntry e_nx;
+    uint4 raw_nx;
+    if (ctx.bx < n) {
+        e_nx = m.vis_blocks[ctx.bx];
+        raw_nx = *((const uint4*)(m.voxels + (size_t)e_nx.ptr * 512) + t);
+    }
     for (int b = ctx.bx; b < n; b += ctx.gx) {
-        const HEntry e = m.vis_blocks[b];
+        const HEntry e = e_nx;
         const int vx = e.x * 8 + lx, vy = e.y * 8 + ly, vz = e.z * 8 + lz;
         uint4* base = (uint4*)(m.voxels + (size_t)e.ptr * 512) + t;
-        const uint4 raw2 = *base;
+        const uint4 raw2 = raw_nx;
+        if (b + ctx.gx < n) {
+            e_nx = m.vis_blocks[b + ctx.gx];
+            raw_nx = *((const uint4*)(m.voxels + (size_t)e_nx.ptr * 512) + t);
+        }
         Voxel v0 = *(const Voxel*)&raw2.x, v1 = *(const Voxel*)&raw2.z;
         bool c0 = integrate_voxel(v0, vx, vy, vz, rec, col, W, H, k, P, m.g, s_div255);
         bool c1 = integrate_voxel(v1, vx + 1, vy, vz, rec, col, W, H, k, P, m.g, s_div255);
