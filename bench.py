@@ -77,6 +77,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurements")
     ap.add_argument("--no-served", action="store_true", help="skip the served-form measurement")
     ap.add_argument("--batch-sessions", type=int, default=32)
+    ap.add_argument("--batched-forms", default="",
+                    help="comma-separated subset of the batched measurements (default: all of BATCHED_FORMS)")
     ap.add_argument("--served-clients", default="64,256",
                     help="client counts of the served runs (comma-separated; the first is the headline)")
     ap.add_argument("--served-seconds", type=float, default=10.0)
@@ -654,46 +656,51 @@ def precision_form(depth, rgb, W, K, plain_value, peak, peak_kind):
     return out
 
 
+BATCHED_FORMS = ("same_config", "mixed", "same_config_fused", "mixed_fused", "same_config_pipelined",
+                 "mixed_pipelined", "mixed_fused_pipelined")
+
+
 def batched_forms(args, rank, plain_value):
-    """The batched form on this GPU: (a) sessions of the plain full-size
+    """The batched form on this GPU, frames resident in HBM, wall-clock timed
+    (fb_batch_step is synchronous): (a) sessions of the plain full-size
     configuration (640x480, 5 mm) stepped together -- the same per-frame work
     as the plain line, so the ratio is like for like; (b) the ragged mix
     (resolutions 160x120 / 320x240 / 640x480, voxels 4-20 mm) with the
-    raycast tiles picked by the autotuner.  Wall-clock timed (fb_batch_step
-    is synchronous), frames resident in HBM."""
+    raycast tiles picked by the autotuner; each (c) with fused launches
+    (batch mode 2: one launch per stage kernel for all sessions of a step)
+    and (d) with four batches in flight (fb_batch_submit / fb_batch_collect).
+    args.batched_forms selects the measurements (names in BATCHED_FORMS)."""
     from fusion_b200 import mixed_config, mixed_population
     from fusion_b200 import system as S
     from fusion_b200.serve import sequence_seeds
     n = args.batch_sessions
+    want = set(args.batched_forms.split(",")) if args.batched_forms else set(BATCHED_FORMS)
     seeds = sequence_seeds(3 + rank, 8)
-    c2 = _batched_run([(640, 480, 0.005, S.config_c2())] * n, seeds, 3, 8)
-    c2["workload"] = f"{n} sessions x plain full-size configuration (640x480, 5 mm, 2^20 buckets, 2^18 blocks)"
-    c2["vs_plain"] = c2["value"] / plain_value
-    mix = _batched_run([(w, h, v, mixed_config(w, h, v)) for (w, h, v) in mixed_population(n, 1234 + rank)],
-                       seeds, 3, 10, tune=True)
-    mix["workload"] = (f"{n} ragged sessions: resolution uniform over 160x120/320x240/640x480, voxel "
-                       "uniform 4-20 mm, truncation 4 voxels, maps sized per voxel size")
-    mix["vs_plain"] = mix["value"] / plain_value
-    # fused launches (batch mode 2): one launch per stage kernel for all sessions
-    # (warm-up long enough for every composition of the timed steps -- the
-    # fusion switch at frame 10, both frame parities -- to have its graph)
-    c2f = _batched_run([(640, 480, 0.005, S.config_c2())] * n, seeds, 14, 8, mode=2)
-    c2f["workload"] = c2["workload"] + "; fused launches"
-    c2f["vs_plain"] = c2f["value"] / plain_value
-    mixf = _batched_run([(w, h, v, mixed_config(w, h, v)) for (w, h, v) in mixed_population(n, 1234 + rank)],
-                        seeds, 14, 10, mode=2)
-    mixf["workload"] = mix["workload"] + "; fused launches"
-    mixf["vs_plain"] = mixf["value"] / plain_value
-    # several steps in flight: the sessions in four groups of equal pixel
-    # counts, one batch each, stepped in turn with fb_batch_submit / collect
-    out = {"same_config": c2, "mixed": mix, "same_config_fused": c2f, "mixed_fused": mixf}
+    c2_specs = [(640, 480, 0.005, S.config_c2())] * n
     mix_specs = [(w, h, v, mixed_config(w, h, v)) for (w, h, v) in mixed_population(n, 1234 + rank)]
-    for key, specs, mode, lanes, steps, wl in (
-            ("same_config_pipelined", [(640, 480, 0.005, S.config_c2())] * n, 0, None, 8, c2["workload"]),
-            ("mixed_pipelined", mix_specs, 0, None, 10, mix["workload"]),
-            ("mixed_fused_pipelined", mix_specs, 2, 2, 10, mixf["workload"])):
-        r = _pipelined_run(specs, seeds, 14, steps, mode=mode, parts=4, lanes=lanes)
-        r["workload"] = wl + "; four batches in flight"
+    c2_wl = f"{n} sessions x plain full-size configuration (640x480, 5 mm, 2^20 buckets, 2^18 blocks)"
+    mix_wl = (f"{n} ragged sessions: resolution uniform over 160x120/320x240/640x480, voxel "
+              "uniform 4-20 mm, truncation 4 voxels, maps sized per voxel size")
+    # fused steps warm up long enough for every composition of the timed
+    # steps -- the fusion switch at frame 10, both frame parities -- to have
+    # its graph; pipelined runs split the sessions into four groups of equal
+    # pixel counts, one batch each, stepped in turn
+    runs = {
+        "same_config": lambda: _batched_run(c2_specs, seeds, 3, 8),
+        "mixed": lambda: _batched_run(mix_specs, seeds, 3, 10, tune=True),
+        "same_config_fused": lambda: _batched_run(c2_specs, seeds, 14, 8, mode=2),
+        "mixed_fused": lambda: _batched_run(mix_specs, seeds, 14, 10, mode=2),
+        "same_config_pipelined": lambda: _pipelined_run(c2_specs, seeds, 14, 8, mode=0, parts=4),
+        "mixed_pipelined": lambda: _pipelined_run(mix_specs, seeds, 14, 10, mode=0, parts=4),
+        "mixed_fused_pipelined": lambda: _pipelined_run(mix_specs, seeds, 14, 10, mode=2, parts=4, lanes=2),
+    }
+    out = {}
+    for key in BATCHED_FORMS:
+        if key not in want:
+            continue
+        r = runs[key]()
+        r["workload"] = (c2_wl if key.startswith("same_config") else mix_wl) + \
+            ("; fused launches" if "fused" in key else "") + ("; four batches in flight" if "pipelined" in key else "")
         r["vs_plain"] = r["value"] / plain_value
         out[key] = r
     return out
