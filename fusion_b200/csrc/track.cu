@@ -8,6 +8,8 @@
 //           correspondence search; ICP products and the RGB count / sum of
 //           squared differences are reduced.  The RGB correspondence of each
 //           pixel is kept as one packed int (last-frame pixel + difference).
+//           The current frame's per-pixel inputs are staged in shared memory
+//           by bulk copies (PixelStage), two 256-pixel chunks ahead.
 //   pass B: per pixel with a correspondence, the photometric row weighted by
 //           the robust scale sigma from pass A; products reduced.  The last
 //           block to finish also solves A x = b in FP64 (LDL^T), applies the
@@ -24,6 +26,7 @@
 // adds into FMAs, so both instances compute the same bits.
 #include <cooperative_groups.h>
 
+#include "fb_async.cuh"
 #include "fb_fused.cuh"
 #include "fb_internal.h"
 
@@ -232,6 +235,85 @@ struct PixelWalk {
     }
     __device__ __forceinline__ void step() { next(x, y); }
 };
+
+// Pass A's current-frame inputs staged in shared memory by bulk copies
+// (cp.async.bulk, this GPU's own memory, no multicast).  A chunk is one
+// logical block's 256 consecutive pixels of one pass over the image (the
+// frame buffers have pitch == width, so a chunk is one contiguous range of
+// each map): vertices and normals (4 KB each), photometric eligibility and
+// gray (256 B each, rounded up to 16 B at the image's end, inside the
+// allocations, which are 256-byte multiples).  Two buffers: chunk c + 2 is
+// copied while chunk c + 1 is processed.
+struct PixelStage {
+    float4 v[2][256];
+    float4 n[2][256];
+    uint8_t ok[2][256];
+    uint8_t g[2][256];
+    uint64_t bar[2];
+};
+
+// Thread 0: copy the chunk of pixels [start, min(start + 256, N)) into
+// buffer `buf`, completing on its barrier.
+__device__ __forceinline__ void stage_chunk(PixelStage& S, int buf, const TrackLevel& L, int start, int N) {
+    const int cnt = min(256, N - start);
+    const uint32_t b16 = (uint32_t)cnt * 16u, b1 = ((uint32_t)cnt + 15u) & ~15u;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&S.bar[buf], 2u * b16 + 2u * b1);
+    bulk_copy_g2s(S.v[buf], L.vcurr + start, b16, &S.bar[buf]);
+    bulk_copy_g2s(S.n[buf], L.ncurr + start, b16, &S.bar[buf]);
+    bulk_copy_g2s(S.ok[buf], L.rgbok + start, b1, &S.bar[buf]);
+    bulk_copy_g2s(S.g[buf], L.gcurr + start, b1, &S.bar[buf]);
+}
+
+// Every thread: wait for buffer `buf`'s fill number `use` (bounded); then
+// read pixel t of the chunk.  Returns false in every thread of the block
+// when any thread's wait gave up.
+__device__ __forceinline__ bool take_chunk(PixelStage& S, int buf, uint32_t use) {
+    const bool ok = mbar_wait(&S.bar[buf], use & 1u);
+    return !__syncthreads_or(!ok);
+}
+
+// The chunks of a group-form block in processing order: groups j of the
+// block, the group's kTrackCluster logical blocks r, their passes k over the
+// image while the chunk starts inside it.  start < 0: no chunk left.
+struct ChunkCursor {
+    int j, r, k, start;
+    __device__ __forceinline__ int start_of(int bx, int gpc, int S) const {
+        return ((bx * gpc + j) * kTrackCluster + r) * 256 + k * S;
+    }
+    // the first chunk at or after (j, r, k)
+    __device__ __forceinline__ void settle(int bx, int gpc, int NG, int iters, int S, int N) {
+        for (;;) {
+            if (j >= gpc || bx * gpc + j >= NG) {
+                start = -1;
+                return;
+            }
+            if (k < iters) {
+                start = start_of(bx, gpc, S);
+                if (start < N) return;
+            }
+            k = 0;
+            if (++r == kTrackCluster) {
+                r = 0;
+                ++j;
+            }
+            if (start_of(bx, gpc, S) >= N) {   // later logical blocks start later still
+                start = -1;
+                return;
+            }
+        }
+    }
+};
+
+__device__ __forceinline__ PixelIn staged_pixel(const PixelStage& S, int buf, int t) {
+    PixelIn in;
+    in.vc = S.v[buf][t];
+    const float4 n = S.n[buf][t];
+    in.nc = make_float3(n.x, n.y, n.z);
+    in.ok = S.ok[buf][t];
+    in.gc = S.g[buf][t];
+    return in;
+}
 
 // icp_row and rgb_corresp of one pixel together (same arithmetic, same
 // decisions), with the pose-independent loads done by the caller and the four
@@ -664,28 +746,43 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     const int G = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int p = blockIdx.x * 256 + threadIdx.x;
     PixelWalk pw(p, G * 256, L.W);
-    PixelIn nxt;
-    if (p < N) nxt = load_pixel(L, pw.x, pw.y);
     if (st->failed) return;   // uniform over the grid: written by an earlier kernel
     cg::cluster_group cl = cg::this_cluster();
     __shared__ float sm[8 * 32];
     __shared__ long long smll[32];
     __shared__ double s_vals[32];
+    __shared__ PixelStage stg;
+    const int iters = (N + G * 256 - 1) / (G * 256);
+    const int base = blockIdx.x * 256;
+    if (threadIdx.x == 0) {
+        mbar_init(&stg.bar[0], 1);
+        mbar_init(&stg.bar[1], 1);
+        for (int c = 0; c < 2 && c < iters && base + c * G * 256 < N; ++c) stage_chunk(stg, c, L, base + c * G * 256, N);
+    }
+    __syncthreads();
     const DevPose cur = st->cur, last = st->last;
     float acc[29];
 #pragma unroll
     for (int k = 0; k < 29; ++k) acc[k] = 0.f;
     long long rc = 0, rsq = 0;
-    const int iters = (N + G * 256 - 1) / (G * 256);
     const int gw = blockIdx.x * kTrackWarps + wid;
     int2* seg = list + (size_t)gw * iters * 32;
     const unsigned lt = (1u << lane) - 1u;
     int run = 0;
     for (int k = 0; k < iters; ++k, p += G * 256) {
-        const PixelIn in = nxt;
+        if (base + k * G * 256 >= N) break;   // uniform: no pixel of this block's chunk k
+        const int buf = k & 1;
+        if (!take_chunk(stg, buf, (uint32_t)(k >> 1))) {
+            if (threadIdx.x == 0) atomicOr((unsigned*)&st->failed, 2u);
+            return;
+        }
+        PixelIn in;
+        if (p < N) in = staged_pixel(stg, buf, threadIdx.x);
+        __syncthreads();   // buffer `buf` is read: chunk k + 2 may overwrite it
+        if (threadIdx.x == 0 && k + 2 < iters && base + (k + 2) * G * 256 < N)
+            stage_chunk(stg, buf, L, base + (k + 2) * G * 256, N);
         const int px = pw.x, py = pw.y;
         pw.step();
-        if (k + 1 < iters && p + G * 256 < N) nxt = load_pixel(L, pw.x, pw.y);   // one pixel ahead
         int r = -1;
         if (p < N) {
             float row[7];
@@ -934,9 +1031,24 @@ __device__ __forceinline__ void track_a_grp_body(const BlockCtx& ctx, TrackLevel
     __shared__ double s_vals[kTrackCluster][32];
     __shared__ float s_f[kTrackCluster][32];
     __shared__ long long s_c[kTrackCluster][2];
+    __shared__ PixelStage stg;
     const DevPose cur = st->cur, last = st->last;
     const int iters = (N + G * 256 - 1) / (G * 256);
     const unsigned lt = (1u << lane) - 1u;
+    // thread 0 keeps the copies two chunks ahead of the block
+    ChunkCursor prod{0, 0, 0, 0};
+    uint32_t used = 0;
+    if (threadIdx.x == 0) {
+        mbar_init(&stg.bar[0], 1);
+        mbar_init(&stg.bar[1], 1);
+        prod.settle(ctx.bx, gpc, NG, iters, G * 256, N);
+        for (int c = 0; c < 2 && prod.start >= 0; ++c) {
+            stage_chunk(stg, c, L, prod.start, N);
+            ++prod.k;
+            prod.settle(ctx.bx, gpc, NG, iters, G * 256, N);
+        }
+    }
+    __syncthreads();
     for (int j = 0; j < gpc; ++j) {
     const int g = ctx.bx * gpc + j;
     if (g >= NG) break;
@@ -944,8 +1056,6 @@ __device__ __forceinline__ void track_a_grp_body(const BlockCtx& ctx, TrackLevel
         const int b = g * kTrackCluster + r;
         int p = b * 256 + threadIdx.x;
         PixelWalk pw(p, G * 256, L.W);
-        PixelIn nxt;
-        if (p < N) nxt = load_pixel(L, pw.x, pw.y);
         float acc[29];
 #pragma unroll
         for (int k = 0; k < 29; ++k) acc[k] = 0.f;
@@ -954,10 +1064,23 @@ __device__ __forceinline__ void track_a_grp_body(const BlockCtx& ctx, TrackLevel
         int2* seg = list + (size_t)gw * iters * 32;
         int run = 0;
         for (int k = 0; k < iters; ++k, p += G * 256) {
-            const PixelIn in = nxt;
+            if (b * 256 + k * G * 256 >= N) break;   // uniform: no pixel of this chunk
+            const int buf = (int)(used & 1u);
+            if (!take_chunk(stg, buf, used >> 1)) {
+                if (threadIdx.x == 0) atomicOr((unsigned*)&st->failed, 2u);
+                return;
+            }
+            ++used;
+            PixelIn in;
+            if (p < N) in = staged_pixel(stg, buf, threadIdx.x);
+            __syncthreads();   // buffer `buf` is read: the chunk two ahead may overwrite it
+            if (threadIdx.x == 0 && prod.start >= 0) {
+                stage_chunk(stg, buf, L, prod.start, N);
+                ++prod.k;
+                prod.settle(ctx.bx, gpc, NG, iters, G * 256, N);
+            }
             const int px = pw.x, py = pw.y;
             pw.step();
-            if (k + 1 < iters && p + G * 256 < N) nxt = load_pixel(L, pw.x, pw.y);   // one pixel ahead
             int rr = -1;
             if (p < N) {
                 float row[7];
