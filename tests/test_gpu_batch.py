@@ -249,3 +249,54 @@ def test_recycled_frame_graphs_give_the_same_results():
     assert st3["instantiated"] == st2["instantiated"]
     assert rows_c == rows_a
     assert dig_c == dig_a
+
+
+def test_fused_step_of_more_sessions_than_one_launch_holds(frames):
+    """A fused launch carries at most 32 sessions; a step of 34 sessions in
+    one lane splits each stage into two launches, and every session still
+    equals itself alone."""
+    from fusion_b200 import Batch, Session, mixed_config
+    w, h, v, _ = SPECS[0]
+    d, c = frames[0]
+    n, n_frames = 34, 3
+    alone = []
+    for _ in range(2):   # two sessions alone cover both halves of the check
+        s = Session(mixed_config(w, h, v))
+        alone.append([_row(s.grab(d[k], c[k])) for k in range(n_frames)])
+        s.close()
+    assert alone[0] == alone[1]
+    sess = [Session(mixed_config(w, h, v)) for _ in range(n)]
+    rows = [[] for _ in sess]
+    with Batch(mode=2) as b:
+        b.set_lanes(1)
+        for k in range(n_frames):
+            for i, r in enumerate(b.step(sess, [(d[k], c[k])] * n)):
+                rows[i].append(_row(r))
+            launches, kernels = b.launch_stats()
+            assert launches < kernels
+    for s in sess:
+        s.close()
+    assert all(r == alone[0] for r in rows)
+
+
+def test_batch_call_errors(frames):
+    from fusion_b200 import Batch, FusionError, Session, mixed_config
+    w, h, v, _ = SPECS[0]
+    d, c = frames[0]
+    s = Session(mixed_config(w, h, v))
+    with Batch() as b:
+        with pytest.raises(FusionError):
+            b.set_mode(3)
+        with pytest.raises(FusionError):
+            b.set_lanes(0)
+        with pytest.raises(FusionError):
+            b.set_lanes(33)
+        with pytest.raises(FusionError):
+            b._pending = (1, None, None, None)
+            b.collect()                        # nothing submitted
+        b.submit([s], [(d[0], c[0])])
+        with pytest.raises(FusionError):
+            b.submit([s], [(d[1], c[1])])      # one step in flight per batch
+        r = b.collect()
+        assert len(r) == 1 and r[0].tracked
+    s.close()
