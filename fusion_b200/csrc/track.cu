@@ -395,7 +395,9 @@ __device__ __forceinline__ void add_products(const float row[7], float acc[29]) 
 // Pass B's rows of one warp segment (n entries): lane l adds the rows of
 // entries l, l + 32, ... in that order.  The next entry's loads are issued
 // before the current row is computed, so the list read and the dependent
-// gathers of two entries overlap.
+// gathers of two entries overlap (the clustered forms, with registers to
+// spare; the 64-register group forms add the rows one at a time,
+// add_segment_rows_seq: 2 % faster there, the same sums).
 __device__ __forceinline__ void add_segment_rows(const TrackLevel& L, const DevPose& cur, const DevPose& last,
                                                  float sigma, const int2* seg, int n, int lane, float acc[29]) {
     int i = lane;
@@ -408,6 +410,15 @@ __device__ __forceinline__ void add_segment_rows(const TrackLevel& L, const DevP
         rgb_row_of(a, L, cur, last, sigma, row);
         add_products(row, acc);
         a = b;
+    }
+}
+
+__device__ __forceinline__ void add_segment_rows_seq(const TrackLevel& L, const DevPose& cur, const DevPose& last,
+                                                     float sigma, const int2* seg, int n, int lane, float acc[29]) {
+    for (int i = lane; i < n; i += 32) {
+        float row[7];
+        rgb_row_of(rgb_fetch_entry(L, seg[i]), L, cur, last, sigma, row);
+        add_products(row, acc);
     }
 }
 
@@ -1189,7 +1200,7 @@ __device__ __forceinline__ void track_b_grp_body(const BlockCtx& ctx, TrackLevel
 #pragma unroll
         for (int k = 0; k < 29; ++k) acc[k] = 0.f;
         const int gw = b * kTrackWarps + wid;
-        add_segment_rows(L, cur, last, sigma, list + (size_t)gw * seg_size, counts[gw], lane, acc);
+        add_segment_rows_seq(L, cur, last, sigma, list + (size_t)gw * seg_size, counts[gw], lane, acc);
         const float bsum = block_sum29(acc, sm);
         if (wid == 0) s_rgb[r][lane] = lane < 29 ? bsum : 0.f;
         __syncthreads();   // sm is reused by the next logical block
