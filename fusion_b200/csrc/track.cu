@@ -196,24 +196,14 @@ __device__ __forceinline__ void rgb_row(const TrackLevel& L, const DevPose& cur,
     rgb_row_of(rgb_fetch(L, x, y, packed), L, cur, last, sigma, row);
 }
 
-// Pose-independent inputs of one pixel for pass A (loaded one pixel ahead).
+// Pose-independent inputs of one pixel for pass A (staged in shared memory
+// by PixelStage).
 struct PixelIn {
     float4 vc;      // current vertex
     float3 nc;      // current normal (xyz)
     int ok;         // photometric eligibility (border, window, gradient)
     int gc;         // current gray value
 };
-
-__device__ __forceinline__ PixelIn load_pixel(const TrackLevel& L, int x, int y) {
-    PixelIn in;
-    const int i = y * L.vp + x;
-    in.vc = L.vcurr[i];
-    const float4 n = L.ncurr[i];
-    in.nc = make_float3(n.x, n.y, n.z);
-    in.ok = L.rgbok[y * L.sp + x];
-    in.gc = L.gcurr[y * L.gp + x];
-    return in;
-}
 
 // Pixel coordinates of a strided pixel walk without divisions: the walk
 // starts at linear pixel p and steps by S pixels (S = SY rows + SX columns).
