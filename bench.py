@@ -543,7 +543,7 @@ def _batched_run(specs, seeds, warmup, steps, tune=False, mode=0):
     import torch
     import rgbd_synth as synth
     from fusion_b200 import Batch, Session
-    from fusion_b200.batch import autotune_raycast_tiles
+    from fusion_b200.batch import autotune_batch
     n_fr = 24
     seqs = {}
     for k, (w, h, _, _) in enumerate(specs):
@@ -567,10 +567,13 @@ def _batched_run(specs, seeds, warmup, steps, tune=False, mode=0):
     b = Batch(mode=mode)
     for _ in range(warmup):
         b.step(sess, frames(), on_device=True)
-    tiles = None
+    tuned = None
     if tune:
-        tiles, _ = autotune_raycast_tiles(b, sess, frames, candidates=((0, 0), (16, 8), (8, 8), (32, 4), (16, 4)),
-                                          steps_per=1, on_device=True)
+        tuned = autotune_batch(b, sess, frames, steps_per=2, on_device=True)
+        # the chosen shapes' frame graphs (and fused plans) are built before
+        # the clock starts
+        for _ in range(4):
+            b.step(sess, frames(), on_device=True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     tracked = 0
@@ -584,7 +587,11 @@ def _batched_run(specs, seeds, warmup, steps, tune=False, mode=0):
     n = len(specs)
     out = {"value": n * steps / dt, "unit": "frames/s", "ms_per_step": dt / steps * 1e3, "sessions": n,
            "steps": steps, "warmup": warmup, "tracked_fraction": tracked / (n * steps), "batch_mode": mode,
-           "raycast_tiles": {f"{w}x{h}": list(t) for (w, h), t in tiles.items()} if tiles else None}
+           "autotuned": None if not tuned else {
+               "raycast_tiles": {f"{w}x{h}": list(t) for (w, h), t in tuned["raycast_tiles"].items()},
+               "integration_ctas_per_sm": {f"{w}x{h}/voxel class {c}": g
+                                           for (w, h, c), g in tuned["integration_grids"].items()},
+               "lanes": tuned["lanes"], "steps": tuned["steps"]}}
     if launches:
         out["launches_per_step"] = launches[0]
         out["per_session_kernels_per_step"] = launches[1]
@@ -689,7 +696,7 @@ def batched_forms(args, rank, plain_value):
         "same_config": lambda: _batched_run(c2_specs, seeds, 3, 8),
         "mixed": lambda: _batched_run(mix_specs, seeds, 3, 10, tune=True),
         "same_config_fused": lambda: _batched_run(c2_specs, seeds, 14, 8, mode=2),
-        "mixed_fused": lambda: _batched_run(mix_specs, seeds, 14, 10, mode=2),
+        "mixed_fused": lambda: _batched_run(mix_specs, seeds, 14, 10, mode=2, tune=True),
         "same_config_pipelined": lambda: _pipelined_run(c2_specs, seeds, 14, 8, mode=0, parts=4),
         "mixed_pipelined": lambda: _pipelined_run(mix_specs, seeds, 14, 10, mode=0, parts=4),
         "mixed_fused_pipelined": lambda: _pipelined_run(mix_specs, seeds, 14, 10, mode=2, parts=4, lanes=2),

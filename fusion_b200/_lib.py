@@ -119,6 +119,7 @@ SIGNATURES = {
     "fb_batch_stats": (_i, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "fb_batch_launch_stats": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "fb_batch_set_lanes": (_i, [_vp, _i]),
+    "fb_session_set_integration_grid": (_i, [_vp, _i]),
     "fb_batch_submit": (_i, [_vp, _vp, _i, _vp]),
     "fb_batch_collect": (_i, [_vp, _vp]),
     "fb_session_launch_count": (_i, [_vp, ctypes.POINTER(ctypes.c_uint64)]),

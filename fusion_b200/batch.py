@@ -3,15 +3,17 @@
 `Batch` steps a set of sessions -- any resolutions, cameras and voxel sizes --
 by one frame each through fb_batch_step, with all of their frames in flight on
 the device together.  Each session's result is exactly what `Session.grab`
-gives for the same input on that session alone: the same per-session kernels
-run on the same data, only concurrently.
+gives for the same input on that session alone: the same kernel bodies run on
+the same data -- in per-session launches, or in fused launches that carry
+every session's part (mode 2) -- only concurrently.
 
 `mixed_population` draws the ragged session mix of the batched and served
 configurations (resolution from {160x120, 320x240, 640x480}, voxel size
 uniform in 4-20 mm) and `mixed_config` sizes each session's map for its voxel
-size.  `autotune_raycast_tiles` picks each resolution's raycast tile (the
-CUDA block shape of the model raycast, which does not change any result) by
-timing real steps of the batch.
+size.  `autotune_batch` picks, by timing real steps of the batch, each
+resolution's raycast tile (the CUDA block shape of the model raycast), each
+(resolution, voxel-size class)'s integration grid and, for fused steps, the
+number of lanes -- shapes that change no result.
 """
 import ctypes
 import math
@@ -150,23 +152,33 @@ def set_raycast_tile(session, bx, by):
     check("fb_session_set_raycast_tile", session.lib.fb_session_set_raycast_tile(session.h, bx, by))
 
 
-def autotune_raycast_tiles(batch, sessions, next_frames, candidates=TILE_CANDIDATES, steps_per=2,
-                           on_device=False):
-    """Pick the raycast tile of every resolution group of `sessions` by
-    timing batch steps: groups one after another, each candidate applied to
-    the whole group for `steps_per` steps (after one step that rebuilds the
-    frame graphs), the fastest kept.  next_frames() returns the next frame of
-    every session (the steps are real frames of the workload).  Returns
-    {(width, height): (bx, by)} and the number of steps taken."""
+def set_integration_grid(session, ctas_per_sm):
+    check("fb_session_set_integration_grid",
+          session.lib.fb_session_set_integration_grid(session.h, int(ctas_per_sm)))
+
+
+def voxel_bucket(voxel_size):
+    """Coarse voxel-size class of a session for the integration autotuner:
+    the visible-block count, and so the integration's work, scales with
+    1 / voxel_size^2."""
+    return 0 if voxel_size < 0.008 else 1 if voxel_size < 0.014 else 2
+
+
+def _tune_groups(batch, sessions, next_frames, key, candidates, apply, steps_per, on_device):
+    """For each group of sessions (by key(session)), one after another with
+    the other groups left as they are: every candidate applied to the whole
+    group, one step that rebuilds the frame graphs, `steps_per` timed steps
+    of the real workload; the fastest candidate is kept.  Returns
+    {group: candidate} and the number of steps taken."""
     groups = {}
     for s in sessions:
-        groups.setdefault((s.cfg.width, s.cfg.height), []).append(s)
+        groups.setdefault(key(s), []).append(s)
     chosen, taken = {}, 0
-    for res, members in sorted(groups.items()):
+    for g, members in sorted(groups.items()):
         best, best_t = None, float("inf")
-        for bx, by in candidates:
+        for cand in candidates:
             for s in members:
-                set_raycast_tile(s, bx, by)
+                apply(s, cand)
             batch.step(sessions, next_frames(), on_device=on_device)   # graphs rebuilt here
             taken += 1
             t0 = time.perf_counter()
@@ -175,8 +187,71 @@ def autotune_raycast_tiles(batch, sessions, next_frames, candidates=TILE_CANDIDA
             t = (time.perf_counter() - t0) / steps_per
             taken += steps_per
             if t < best_t:
-                best, best_t = (bx, by), t
+                best, best_t = cand, t
         for s in members:
-            set_raycast_tile(s, *best)
-        chosen[res] = best
+            apply(s, best)
+        chosen[g] = best
     return chosen, taken
+
+
+def autotune_raycast_tiles(batch, sessions, next_frames, candidates=TILE_CANDIDATES, steps_per=2,
+                           on_device=False):
+    """Pick the raycast tile of every resolution group of `sessions` by
+    timing batch steps: groups one after another, each candidate applied to
+    the whole group for `steps_per` steps (after one step that rebuilds the
+    frame graphs), the fastest kept.  next_frames() returns the next frame of
+    every session (the steps are real frames of the workload).  Returns
+    {(width, height): (bx, by)} and the number of steps taken."""
+    return _tune_groups(batch, sessions, next_frames, lambda s: (s.cfg.width, s.cfg.height), candidates,
+                        lambda s, t: set_raycast_tile(s, *t), steps_per, on_device)
+
+
+GRID_CANDIDATES = (0, 2, 4, 16)
+
+
+def autotune_integration_grids(batch, sessions, next_frames, candidates=GRID_CANDIDATES, steps_per=2,
+                               on_device=False):
+    """Pick the integration grid (CTAs per SM, 0 = the form's default) of
+    every (resolution, voxel-size class) group the same way.  Returns
+    {(width, height, class): ctas_per_sm} and the number of steps taken."""
+    return _tune_groups(batch, sessions, next_frames,
+                        lambda s: (s.cfg.width, s.cfg.height, voxel_bucket(s.cfg.voxel_size)), candidates,
+                        set_integration_grid, steps_per, on_device)
+
+
+LANE_CANDIDATES = (1, 2, 4, 8)
+
+
+def autotune_lanes(batch, sessions, next_frames, candidates=LANE_CANDIDATES, steps_per=2, on_device=False):
+    """Fused steps (batch mode 2): the number of lanes, timed the same way
+    (one step to build the new plans and graphs, then `steps_per` steps).
+    Returns (lanes, steps taken)."""
+    best, best_t, taken = None, float("inf"), 0
+    for lanes in candidates:
+        batch.set_lanes(lanes)
+        for _ in range(2):   # a composition runs as a graph from its second use
+            batch.step(sessions, next_frames(), on_device=on_device)
+        taken += 2
+        t0 = time.perf_counter()
+        for _ in range(steps_per):
+            batch.step(sessions, next_frames(), on_device=on_device)
+        t = (time.perf_counter() - t0) / steps_per
+        taken += steps_per
+        if t < best_t:
+            best, best_t = lanes, t
+    batch.set_lanes(best)
+    return best, taken
+
+
+def autotune_batch(batch, sessions, next_frames, steps_per=2, on_device=False):
+    """The batched form's block and tile shapes, picked on the real workload:
+    the raycast tile per resolution, the integration grid per resolution and
+    voxel-size class, and (fused steps) the number of lanes.  Results do not
+    depend on any of them.  Returns {"raycast_tiles", "integration_grids",
+    "lanes", "steps"}."""
+    tiles, n1 = autotune_raycast_tiles(batch, sessions, next_frames, steps_per=steps_per, on_device=on_device)
+    grids, n2 = autotune_integration_grids(batch, sessions, next_frames, steps_per=steps_per, on_device=on_device)
+    lanes, n3 = None, 0
+    if getattr(batch, "mode", 0) == 2:
+        lanes, n3 = autotune_lanes(batch, sessions, next_frames, steps_per=steps_per, on_device=on_device)
+    return {"raycast_tiles": tiles, "integration_grids": grids, "lanes": lanes, "steps": n1 + n2 + n3}

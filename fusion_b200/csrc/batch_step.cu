@@ -98,7 +98,7 @@ std::vector<uint64_t> composition(fb_session* const* ss, int n, const FramePlan*
         key.push_back((uint64_t)(uintptr_t)s);
         key.push_back((uint64_t)plans[i].mode | (uint64_t)plans[i].fuse << 2 | (uint64_t)s->next << 3 |
                       (uint64_t)s->shared_gpu << 5 | (uint64_t)s->mapping_disabled << 6 |
-                      (uint64_t)s->rc_bx << 8 | (uint64_t)s->rc_by << 20);
+                      (uint64_t)s->rc_bx << 8 | (uint64_t)s->rc_by << 20 | (uint64_t)s->integ_cps << 32);
     }
     return key;
 }

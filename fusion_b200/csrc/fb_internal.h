@@ -199,8 +199,10 @@ int launch_export_reference(const MapView& m, void* entries, void* voxels, int* 
 int launch_fuse_records(const MapView& m, const float* raw, int rp, const uint8_t* rgb, int cp, const float4* nmap,
                         int np, int W, int H, cudaStream_t s);
 // Integration of the visible blocks from the fusion records of a W x H frame.
+// ctas_per_sm: the grid (CTAs per SM, each taking every grid-th visible
+// block); 0: the form's default.  Results do not depend on it.
 int launch_integrate(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
-                     cudaStream_t s);
+                     cudaStream_t s, int ctas_per_sm = 0);
 int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s);
 // tile bx x by threads: bx * by <= 128 (the kernel's launch bound), a multiple
 // of 32; bx = by = 0: the pooled raycast (lane refill)

@@ -1004,12 +1004,12 @@ int launch_fuse_records(const MapView& m, const float* raw, int rp, const uint8_
 }
 
 int launch_integrate(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
-                     cudaStream_t s) {
+                     cudaStream_t s, int ctas_per_sm) {
+    const int ctas = sm_count() * (ctas_per_sm ? ctas_per_sm : m.cvox ? 7 : 8);
     if (m.cvox)
-        fb_launch(k_integrate_compact, (const void*)k_integrate_compact_fused, sm_count() * 7, 128, 0, s, m, W, H, k,
-                  pose, skip);
+        fb_launch(k_integrate_compact, (const void*)k_integrate_compact_fused, ctas, 128, 0, s, m, W, H, k, pose, skip);
     else
-        fb_launch(k_integrate, (const void*)k_integrate_fused, sm_count() * 8, 256, 0, s, m, W, H, k, pose, skip);
+        fb_launch(k_integrate, (const void*)k_integrate_fused, ctas, 256, 0, s, m, W, H, k, pose, skip);
     return 1;
 }
 

@@ -436,7 +436,7 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
         n += launch_visibility(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st);
         mark(5);
         launch_slot(kSlotIntegrate);
-        n += launch_integrate(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st);
+        n += launch_integrate(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st, s->integ_cps);
         *ran |= 7u << 3;
     } else {
         mark(4);
@@ -560,7 +560,7 @@ std::atomic<long long> g_exec_updated{0}, g_exec_instantiated{0};
 ExecKey exec_key(const fb_session* s, int mode, int fuse, int shared) {
     int dev = 0;
     cudaGetDevice(&dev);
-    return ExecKey(dev, s->W[0], s->H[0], s->cfg.form, mode, fuse, shared, 0, s->rc_bx, s->rc_by,
+    return ExecKey(dev, s->W[0], s->H[0], s->cfg.form, mode, fuse, shared, s->integ_cps, s->rc_bx, s->rc_by,
                    s->mapping_disabled ? 1 : 0);
 }
 
@@ -826,6 +826,7 @@ int fb_session_create(const fb_config* cfg, void* stream, fb_session** out) {
     s->use_graphs = true;
     s->rc_bx = 16;
     s->rc_by = 8;
+    s->integ_cps = 0;
     s->shared_gpu = false;
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 2; ++b)
@@ -1011,6 +1012,14 @@ int fb_session_set_raycast_tile(fb_session* s, int bx, int by) {
     drop_graphs(s);
     s->rc_bx = bx;
     s->rc_by = by;
+    return FB_OK;
+}
+
+int fb_session_set_integration_grid(fb_session* s, int ctas_per_sm) {
+    if (!s || ctas_per_sm < 0 || ctas_per_sm > 32) return FB_EINVAL;
+    if (ctas_per_sm == s->integ_cps) return FB_OK;
+    drop_graphs(s);
+    s->integ_cps = ctas_per_sm;
     return FB_OK;
 }
 

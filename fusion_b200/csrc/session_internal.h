@@ -155,6 +155,7 @@ struct fb_session {
     cudaGraphExec_t graph[3][2][2][2];
     int graph_kernels[3][2][2][2];
     int rc_bx, rc_by;          // raycast tile
+    int integ_cps;             // integration CTAs per SM (0: the form's default)
     bool shared_gpu;           // frames run beside other sessions (batch steps of more than three)
     // Tracker::mappingDisabled (set by System::ReadMapFromDisk): frames track
     // and render against the map without fusing into it

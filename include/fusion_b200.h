@@ -184,6 +184,12 @@ FB_API int fb_session_prepare_some(fb_session* s, int shared, int max_graphs, in
  * graphs are rebuilt on the next frame.  No reference counterpart: a tuning
  * knob for the batched form's autotuner. */
 FB_API int fb_session_set_raycast_tile(fb_session* s, int bx, int by);
+/* The integration kernel's grid: ctas_per_sm CTAs per SM (1..32), each
+ * taking every grid-th visible block; 0 (default) is the form's own (8 CTAs
+ * of 256 threads, or 7 of 128 in the precision form).  Results do not depend
+ * on it.  Cached frame graphs are rebuilt on the next frame.  No reference
+ * counterpart: a tuning knob for the batched form's autotuner. */
+FB_API int fb_session_set_integration_grid(fb_session* s, int ctas_per_sm);
 
 /* Snapshots (System::WriteMapToDisk / ReadMapFromDisk, Core/System.cc:195-271,
  * in memory and with the tracker included): everything a session needs to

@@ -300,3 +300,22 @@ def test_batch_call_errors(frames):
         r = b.collect()
         assert len(r) == 1 and r[0].tracked
     s.close()
+
+
+def test_integration_grid_does_not_change_results(frames):
+    from fusion_b200.batch import set_integration_grid
+    base, _ = _batched(frames, LOCKSTEP, 0)
+    from fusion_b200 import Batch, Session
+    sess = [Session(_config(i)) for i in range(len(SPECS))]
+    for s, g in zip(sess, [1, 2, 16, 0, 4]):
+        set_integration_grid(s, g)
+    rows = [[] for _ in sess]
+    with Batch(mode=2) as b:
+        for k in range(N_FRAMES):
+            res = b.step(sess, [(frames[i][0][k], frames[i][1][k]) for i in range(len(sess))])
+            for i, r in enumerate(res):
+                rows[i].append(_row(r))
+    out = [(rows[i], _map_digest(s)) for i, s in enumerate(sess)]
+    for s in sess:
+        s.close()
+    assert out == base
