@@ -14,8 +14,6 @@
 // pixels: [ul, min(ul + 15, lr)].  That is the rectangle filled here.
 #include <cuda_fp16.h>
 
-#include <type_traits>
-
 #include "fb_fused.cuh"
 #include "fb_internal.h"
 
@@ -241,30 +239,33 @@ struct CompactVox {
     static __device__ __forceinline__ int weight(ref v) { return v.blk[c_weight(v.idx)]; }
 };
 
+// FindEntry's block (DeviceMap.cu:122-135) through the dense index where it
+// covers (bx, by, bz), else the hash table: the pool index, or -1.
+__device__ __forceinline__ int lookup_block(const MapView& m, const GridView& gv, int bx, int by, int bz) {
+    const int gx = bx - gv.ox, gy = by - gv.oy, gz = bz - gv.oz;
+    if ((unsigned)gx < (unsigned)gv.nx && (unsigned)gy < (unsigned)gv.ny && (unsigned)gz < (unsigned)gv.nz)
+        return max(__ldg(m.grid + (gz * gv.ny + gy) * gv.nx + gx), -1);
+    int b = (int)bucket_of_m(bx, by, bz, (uint32_t)m.NB, m.nb_mask);
+    HEntry e = m.entries[b];
+    bool found = e.ptr != -1 && e.x == bx && e.y == by && e.z == bz;
+    for (int guard = 0; !found && e.offset > 0 && e.offset <= m.NE && guard <= m.NE; ++guard) {
+        e = m.entries[m.NB + e.offset - 1];
+        found = e.x == bx && e.y == by && e.z == bz && e.ptr != -1;
+    }
+    return found ? e.ptr : -1;
+}
+
 // FindEntry with the cache of FindVoxel(float3, cache, valid)
 // (DeviceMap.cu:97-114): the pool index of block (bx, by, bz), or -1.  The
 // reference's cache starts as HashEntry() -- position (0,0,0), ptr -1 -- and
 // a first probe inside block (0,0,0) then reads voxel index -1 + local
-// index; here the cache starts empty.
+// index; here the cache starts empty.  The cache holds what the lookup
+// returns, so it changes no result.
 __device__ __forceinline__ int find_block(const MapView& m, const GridView& gv, int bx, int by, int bz,
                                           EntryCache& c) {
     if (c.set && bx == c.x && by == c.y && bz == c.z) return c.ptr;
-    int ptr;
-    const int gx = bx - gv.ox, gy = by - gv.oy, gz = bz - gv.oz;
-    if ((unsigned)gx < (unsigned)gv.nx && (unsigned)gy < (unsigned)gv.ny && (unsigned)gz < (unsigned)gv.nz) {
-        ptr = __ldg(m.grid + (gz * gv.ny + gy) * gv.nx + gx);
-        if (ptr < 0) return -1;
-    } else {
-        int b = (int)bucket_of_m(bx, by, bz, (uint32_t)m.NB, m.nb_mask);
-        HEntry e = m.entries[b];
-        bool found = e.ptr != -1 && e.x == bx && e.y == by && e.z == bz;
-        for (int guard = 0; !found && e.offset > 0 && e.offset <= m.NE && guard <= m.NE; ++guard) {
-            e = m.entries[m.NB + e.offset - 1];
-            found = e.x == bx && e.y == by && e.z == bz && e.ptr != -1;
-        }
-        if (!found) return -1;
-        ptr = e.ptr;
-    }
+    const int ptr = lookup_block(m, gv, bx, by, bz);
+    if (ptr < 0) return -1;
     c.x = bx;
     c.y = by;
     c.z = bz;
@@ -292,9 +293,6 @@ __device__ __forceinline__ typename VR::ref find_voxel(const MapView& m, const G
     return find_voxel_i<VR>(m, gv, __float2int_rz(p.x), __float2int_rz(p.y), __float2int_rz(p.z), c, valid);
 }
 
-template <class VR>
-__device__ __forceinline__ float vsdf(typename VR::ref v) { return VR::null(v) ? qnan() : VR::sdf(v); }
-
 // Rendering::readSdf (RenderScene.cu:290-295)
 template <class VR>
 __device__ __forceinline__ float read_sdf(const MapView& m, const GridView& gv, f3 p, EntryCache& c, bool& valid) {
@@ -304,13 +302,26 @@ __device__ __forceinline__ float read_sdf(const MapView& m, const GridView& gv, 
     return VR::sdf(v);
 }
 
+// One corner of a trilinear read: the voxel's TSDF in block q, NaN for a
+// missing block (q < 0).  The load always reads a voxel of the pool (block
+// 0 for a missing block) so that the eight loads issue without branches.
+template <class VR>
+__device__ __forceinline__ float corner_sdf(const MapView& m, int q, int idx) {
+    const float v = VR::sdf(VR::at(m, max(q, 0), idx));
+    return q < 0 ? qnan() : v;
+}
+
 // Rendering::readSdfInterped (RenderScene.cu:297-319).  The eight corners are
 // the voxels at the truncated coordinates of pt and of pt + 1 per axis (each
 // sum rounded as the reference rounds it), read in the reference's order and
 // blended by its lerp sequence; `valid` ends as the last corner's (x+1, y+1,
-// z+1) lookup leaves it.  When the eight corners lie in one block (seven
-// times in eight per axis), that block is looked up once (11 % off the
-// raycast at 640x480, the same bits).
+// z+1) lookup leaves it.  The corners lie in at most eight blocks, one per
+// axis combination whose coordinates cross a block boundary: each distinct
+// block is looked up once (the first through the entry cache), then the
+// eight TSDF loads issue together.  Every lane of a warp runs the same code
+// whether or not its corners straddle blocks (only the extra lookups are
+// conditional), where a per-corner lookup through the one-entry cache made
+// straddling lanes run a second, eight-lookup path.
 template <class VR>
 __device__ float read_sdf_interp(const MapView& m, const GridView& gv, f3 pt, EntryCache& c, bool& valid) {
     const f3 f = mk3(fs(pt.x, floorf(pt.x)), fs(pt.y, floorf(pt.y)), fs(pt.z, floorf(pt.z)));
@@ -318,38 +329,33 @@ __device__ float read_sdf_interp(const MapView& m, const GridView& gv, f3 pt, En
     const int x0 = __float2int_rz(pt.x), x1 = __float2int_rz(fa(pt.x, 1.f));
     const int y0 = __float2int_rz(pt.y), y1 = __float2int_rz(fa(pt.y, 1.f));
     const int z0 = __float2int_rz(pt.z), z1 = __float2int_rz(fa(pt.z, 1.f));
-    float s000, s100, s010, s110, s001, s101, s011, s111;
-    const int bx = block_of(x0), by = block_of(y0), bz = block_of(z0);
-    // (the precision form measured no gain from the shared lookup on B200 and
-    // keeps one lookup per corner)
-    if (std::is_same<VR, ExactVox>::value && bx == block_of(x1) && by == block_of(y1) && bz == block_of(z1)) {
-        const int ptr = find_block(m, gv, bx, by, bz, c);
-        valid = ptr >= 0;
-        if (ptr < 0) {
-            s000 = s100 = s010 = s110 = s001 = s101 = s011 = s111 = qnan();
-        } else {
-            const int ax = local_of(x0), bxl = local_of(x1);
-            const int ay = local_of(y0) * 8, byl = local_of(y1) * 8;
-            const int az = local_of(z0) * 64, bzl = local_of(z1) * 64;
-            s000 = VR::sdf(VR::at(m, ptr, az + ay + ax));
-            s100 = VR::sdf(VR::at(m, ptr, az + ay + bxl));
-            s010 = VR::sdf(VR::at(m, ptr, az + byl + ax));
-            s110 = VR::sdf(VR::at(m, ptr, az + byl + bxl));
-            s001 = VR::sdf(VR::at(m, ptr, bzl + ay + ax));
-            s101 = VR::sdf(VR::at(m, ptr, bzl + ay + bxl));
-            s011 = VR::sdf(VR::at(m, ptr, bzl + byl + ax));
-            s111 = VR::sdf(VR::at(m, ptr, bzl + byl + bxl));
-        }
-    } else {
-        s000 = vsdf<VR>(find_voxel_i<VR>(m, gv, x0, y0, z0, c, valid));
-        s100 = vsdf<VR>(find_voxel_i<VR>(m, gv, x1, y0, z0, c, valid));
-        s010 = vsdf<VR>(find_voxel_i<VR>(m, gv, x0, y1, z0, c, valid));
-        s110 = vsdf<VR>(find_voxel_i<VR>(m, gv, x1, y1, z0, c, valid));
-        s001 = vsdf<VR>(find_voxel_i<VR>(m, gv, x0, y0, z1, c, valid));
-        s101 = vsdf<VR>(find_voxel_i<VR>(m, gv, x1, y0, z1, c, valid));
-        s011 = vsdf<VR>(find_voxel_i<VR>(m, gv, x0, y1, z1, c, valid));
-        s111 = vsdf<VR>(find_voxel_i<VR>(m, gv, x1, y1, z1, c, valid));
+    const int bx0 = block_of(x0), bx1 = block_of(x1);
+    const int by0 = block_of(y0), by1 = block_of(y1);
+    const int bz0 = block_of(z0), bz1 = block_of(z1);
+    const bool sx = bx1 != bx0, sy = by1 != by0, sz = bz1 != bz0;
+    const int q000 = find_block(m, gv, bx0, by0, bz0, c);
+    const int q100 = sx ? lookup_block(m, gv, bx1, by0, bz0) : q000;
+    const int q010 = sy ? lookup_block(m, gv, bx0, by1, bz0) : q000;
+    const int q110 = sy ? (sx ? lookup_block(m, gv, bx1, by1, bz0) : q010) : q100;
+    int q001 = q000, q101 = q100, q011 = q010, q111 = q110;
+    if (sz) {
+        q001 = lookup_block(m, gv, bx0, by0, bz1);
+        q101 = sx ? lookup_block(m, gv, bx1, by0, bz1) : q001;
+        q011 = sy ? lookup_block(m, gv, bx0, by1, bz1) : q001;
+        q111 = sy ? (sx ? lookup_block(m, gv, bx1, by1, bz1) : q011) : q101;
     }
+    valid = q111 >= 0;
+    const int ax = local_of(x0), bxl = local_of(x1);
+    const int ay = local_of(y0) * 8, byl = local_of(y1) * 8;
+    const int az = local_of(z0) * 64, bzl = local_of(z1) * 64;
+    const float s000 = corner_sdf<VR>(m, q000, az + ay + ax);
+    const float s100 = corner_sdf<VR>(m, q100, az + ay + bxl);
+    const float s010 = corner_sdf<VR>(m, q010, az + byl + ax);
+    const float s110 = corner_sdf<VR>(m, q110, az + byl + bxl);
+    const float s001 = corner_sdf<VR>(m, q001, bzl + ay + ax);
+    const float s101 = corner_sdf<VR>(m, q101, bzl + ay + bxl);
+    const float s011 = corner_sdf<VR>(m, q011, bzl + byl + ax);
+    const float s111 = corner_sdf<VR>(m, q111, bzl + byl + bxl);
     const float r0 = lerp(s000, s100, f.x), r1 = lerp(s010, s110, f.x);
     const float r2 = lerp(r0, r1, f.y);
     const float r0b = lerp(s001, s101, f.x), r1b = lerp(s011, s111, f.x);
