@@ -127,7 +127,7 @@ struct MapCounters {
     // snapshot taken before insertion (read by the insert kernel only)
     int snap_M, snap_hc, snap_ep, snap_na;
     int fast;              // the parallel insertion path applies
-    unsigned int ray_next; // work counter of the pooled raycast (zeroed with the z ranges)
+    unsigned int ray_next; // tile counter of the queued raycast (zeroed with the z ranges)
 };
 
 struct NewBlock {
@@ -205,7 +205,7 @@ int launch_integrate(const MapView& m, int W, int H, const Intr& k, const DevPos
                      cudaStream_t s, int ctas_per_sm = 0);
 int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s);
 // tile bx x by threads: bx * by <= 128 (the kernel's launch bound), a multiple
-// of 32; bx = by = 0: the pooled raycast (lane refill)
+// of 32; bx = by = 0: the queued raycast (warps take 8 x 4 pixel tiles from a counter)
 int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,
                     const DevPose* pose, const int* skip, cudaStream_t s, int bx = 16, int by = 8);
 

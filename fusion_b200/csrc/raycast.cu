@@ -14,6 +14,8 @@
 // pixels: [ul, min(ul + 15, lr)].  That is the rectangle filled here.
 #include <cuda_fp16.h>
 
+#include <algorithm>
+
 #include "fb_fused.cuh"
 #include "fb_internal.h"
 
@@ -363,39 +365,51 @@ __device__ float read_sdf_interp(const MapView& m, const GridView& gv, f3 pt, En
     return lerp(r2, r3, f.z);
 }
 
-// Rendering::readNormal (RenderScene.cu:321-352)
+// Rendering::readNormal (RenderScene.cu:321-352): the six samples at
+// pt +- 1 per axis, in the reference's order, and the normal from their three
+// differences.  Offsets and differences stay in registers (a dynamically
+// indexed table of samples would live in local memory).
 template <class VR>
 __device__ bool read_normal(const MapView& m, const GridView& gv, f3 pt, EntryCache& c, const M3& Rinv, f3& n) {
     bool valid;
-    float s[6];
-    const float off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    float prev = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
     for (int q = 0; q < 6; ++q) {
-        s[q] = read_sdf_interp<VR>(m, gv, mk3(fa(pt.x, off[q][0]), fa(pt.y, off[q][1]), fa(pt.z, off[q][2])), c, valid);
-        if (isnan(s[q]) || s[q] == 1.0f || !valid) return false;
+        const float d = (q & 1) ? -1.0f : 1.0f;
+        const int a = q >> 1;
+        const f3 ps = mk3(fa(pt.x, a == 0 ? d : 0.0f), fa(pt.y, a == 1 ? d : 0.0f), fa(pt.z, a == 2 ? d : 0.0f));
+        const float sq = read_sdf_interp<VR>(m, gv, ps, c, valid);
+        if (isnan(sq) || sq == 1.0f || !valid) return false;
+        if (q & 1) {
+            const float g = fs(prev, sq);
+            gx = a == 0 ? g : gx;
+            gy = a == 1 ? g : gy;
+            gz = a == 2 ? g : gz;
+        }
+        prev = sq;
     }
-    n = normalised3(mv(Rinv, mk3(fs(s[0], s[1]), fs(s[2], s[3]), fs(s[4], s[5]))));
+    n = normalised3(mv(Rinv, mk3(gx, gy, gz)));
     return true;
 }
 
-// Rendering::operator() (RenderScene.cu:354-440)
-template <class VR>
-__device__ __forceinline__ void raycast_body(const BlockCtx& ctx, MapView m, float4* __restrict__ vmap,
-                                             float4* __restrict__ nmap, int vp, int W, int H, Intr k,
-                                             const DevPose* __restrict__ posep, const int* __restrict__ skip) {
-    if (skip && *skip) return;
-    if (m.ctr->n_tiles == 0) return;   // CreateRenderingBlocks returned false: maps untouched
-    const int x = ctx.bx * blockDim.x + threadIdx.x;
-    const int y = ctx.by * blockDim.y + threadIdx.y;
-    if (x >= W || y >= H) return;
-    const DevPose P = *posep;
+// The dense index's extent from this frame's counters (all zero when the
+// index is off: every lookup then walks the table).
+__device__ __forceinline__ GridView grid_view(const MapView& m) {
     GridView gv;
     gv.ox = m.ctr->g_o[0];
     gv.oy = m.ctr->g_o[1];
     gv.oz = m.ctr->g_o[2];
-    gv.nx = m.ctr->g_n[0];   // 0 when the index is off: every lookup walks the table
+    gv.nx = m.ctr->g_n[0];
     gv.ny = m.ctr->g_n[1];
     gv.nz = m.ctr->g_n[2];
-    const size_t o = (size_t)y * vp + x;
+    return gv;
+}
+
+// Rendering::operator() (RenderScene.cu:354-440) for pixel (x, y): writes
+// its vertex and normal (NaN where the ray finds no surface).
+template <class VR>
+__device__ __forceinline__ void raycast_pixel(const MapView& m, const GridView& gv, const DevPose& P, const Intr& k,
+                                              int x, int y, float4* __restrict__ vout_p,
+                                              float4* __restrict__ nout_p) {
     const float4 nan4 = make_float4(qnan(), qnan(), qnan(), qnan());
     float4 vout = nan4, nout = nan4;
     const int lx = (int)floorf(fd((float)x, 8.f)), ly = (int)floorf(fd((float)y, 8.f));
@@ -446,8 +460,22 @@ __device__ __forceinline__ void raycast_body(const BlockCtx& ctx, MapView m, flo
             nout = make_float4(n.x, n.y, n.z, 1.0f);
         }
     }
-    vmap[o] = vout;
-    nmap[o] = nout;
+    *vout_p = vout;
+    *nout_p = nout;
+}
+
+// One thread per pixel in CUDA blocks of the session's tile shape.
+template <class VR>
+__device__ __forceinline__ void raycast_body(const BlockCtx& ctx, MapView m, float4* __restrict__ vmap,
+                                             float4* __restrict__ nmap, int vp, int W, int H, Intr k,
+                                             const DevPose* __restrict__ posep, const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    if (m.ctr->n_tiles == 0) return;   // CreateRenderingBlocks returned false: maps untouched
+    const int x = ctx.bx * blockDim.x + threadIdx.x;
+    const int y = ctx.by * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const size_t o = (size_t)y * vp + x;
+    raycast_pixel<VR>(m, grid_view(m), *posep, k, x, y, vmap + o, nmap + o);
 }
 
 template <class VR>
@@ -462,136 +490,47 @@ __global__ void __launch_bounds__(128)
     run_part(fp, [](const BlockCtx& c, const auto&... a) { raycast_body<VR>(c, a...); });
 }
 
-// The same rays with lane refill: a persistent grid whose warps take pixels
-// from a work counter (8 x 4 pixel tiles in row-major order, 32 at a time),
-// and every lane whose ray has ended takes the next pixel at once, so the
-// lanes of a warp stay busy while their rays need different numbers of
-// march steps.  Each ray runs the same operations in the same order as in
-// k_raycast (one march step per loop turn), so every pixel is identical.
-// Measured on B200: 3.6x slower than k_raycast at 640x480 (one global atomic
-// per warp and loop turn), faster only on 160x120 images, where the
-// batched form's autotuner may pick it.
+// The same rays from a work queue: a grid of resident CTAs whose warps take
+// 8 x 4 pixel tiles (row-major tile order) from a counter, one atomic per
+// warp and tile, until every tile is taken, so a warp that drew cheap rays
+// takes more tiles instead of leaving its slot idle until the grid's last
+// CTAs end.  Every pixel runs raycast_pixel as in k_raycast: the same bits.
 template <class VR>
-__device__ __forceinline__ void raycast_pool_body(const BlockCtx&, MapView m, float4* __restrict__ vmap,
-                                                  float4* __restrict__ nmap, int vp, int W, int H, Intr k,
-                                                  const DevPose* __restrict__ posep, const int* __restrict__ skip) {
+__device__ __forceinline__ void raycast_queue_body(const BlockCtx&, MapView m, float4* __restrict__ vmap,
+                                                   float4* __restrict__ nmap, int vp, int W, int H, Intr k,
+                                                   const DevPose* __restrict__ posep,
+                                                   const int* __restrict__ skip) {
     if (skip && *skip) return;
     if (m.ctr->n_tiles == 0) return;   // CreateRenderingBlocks returned false: maps untouched
-    const DevPose P = *posep;
-    GridView gv;
-    gv.ox = m.ctr->g_o[0];
-    gv.oy = m.ctr->g_o[1];
-    gv.oz = m.ctr->g_o[2];
-    gv.nx = m.ctr->g_n[0];
-    gv.ny = m.ctr->g_n[1];
-    gv.nz = m.ctr->g_n[2];
+    const GridView gv = grid_view(m);
     const int tiles_x = (W + 7) >> 3;
-    const unsigned total = (unsigned)tiles_x * (unsigned)((H + 3) >> 2) * 32u;
-    unsigned* next = &m.ctr->ray_next;
+    const unsigned total = (unsigned)tiles_x * (unsigned)((H + 3) >> 2);
     const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    const float vinv = m.g.voxel_size_inv, stepScale = m.g.step_scale;
-    const float4 nan4 = make_float4(qnan(), qnan(), qnan(), qnan());
-    bool live = false;
-    size_t o = 0;
-    f3 result = mk3(0.f, 0.f, 0.f), dir = result;
-    float dist_s = 0.f, dist_e = 0.f, sdf = 1.0f, step = 0.f;
-    bool valid = false;
-    EntryCache c;
-    c.set = false;
     for (;;) {
-        // lanes without a ray take the next pixels (one atomic per warp)
-        const unsigned idle = __ballot_sync(0xffffffffu, !live);
-        if (idle) {
-            const int leader = __ffs(idle) - 1;
-            unsigned base = 0;
-            if (lane == leader) base = atomicAdd(next, (unsigned)__popc(idle));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (base >= total && idle == 0xffffffffu) break;
-            if (!live) {
-                const unsigned item = base + (unsigned)__popc(idle & lt);
-                const int t = (int)(item >> 5), l = (int)(item & 31u);
-                const int x = (t % tiles_x) * 8 + (l & 7), y = (t / tiles_x) * 4 + (l >> 3);
-                if (item < total && x < W && y < H) {
-                    o = (size_t)y * vp + x;
-                    const int lx = (int)floorf(fd((float)x, 8.f)), ly = (int)floorf(fd((float)y, 8.f));
-                    const float zrx = m.zmin[ly * m.zc + lx], zry = m.zmax[ly * m.zc + lx];
-                    if ((double)zry < 1e-3 || (double)zrx < 1e-3 || isnan(zrx) || isnan(zry)) {
-                        vmap[o] = nan4;
-                        nmap[o] = nan4;
-                    } else {
-                        f3 p;
-                        p.z = zrx;
-                        p.x = fm(fm(p.z, fs((float)x, k.cx)), k.invfx);
-                        p.y = fm(fm(p.z, fs((float)y, k.cy)), k.invfy);
-                        dist_s = fm(norm3(p), vinv);
-                        const f3 block_s = mul3(add3(mv(P.R, p), P.t), vinv);
-                        p.z = zry;
-                        p.x = fm(fm(p.z, fs((float)x, k.cx)), k.invfx);
-                        p.y = fm(fm(p.z, fs((float)y, k.cy)), k.invfy);
-                        dist_e = fm(norm3(p), vinv);
-                        const f3 block_e = mul3(add3(mv(P.R, p), P.t), vinv);
-                        dir = normalised3(sub3(block_e, block_s));
-                        result = block_s;
-                        sdf = 1.0f;
-                        valid = false;
-                        c.set = false;
-                        live = true;
-                    }
-                }
-            }
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(&m.ctr->ray_next, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= total) break;
+        const int x = (int)(t % (unsigned)tiles_x) * 8 + (lane & 7);
+        const int y = (int)(t / (unsigned)tiles_x) * 4 + (lane >> 3);
+        if (x < W && y < H) {
+            const size_t o = (size_t)y * vp + x;
+            raycast_pixel<VR>(m, gv, *posep, k, x, y, vmap + o, nmap + o);
         }
-        if (!live) continue;
-        // one turn of the march loop of k_raycast
-        bool end = !(dist_s < dist_e);
-        if (!end) {
-            sdf = read_sdf<VR>(m, gv, result, c, valid);
-            if (!valid) {
-                step = 8.0f;
-            } else {
-                if (sdf <= 0.1f && sdf >= -0.5f) sdf = read_sdf_interp<VR>(m, gv, result, c, valid);
-                if (sdf <= 0.0f)
-                    end = true;
-                else
-                    step = !isnan(sdf) ? fmaxf(fm(sdf, stepScale), 1.0f) : 8.0f;
-            }
-            if (!end) {
-                result = add3(result, smul3(step, dir));
-                dist_s = fa(dist_s, step);
-            }
-        }
-        if (!end) continue;
-        float4 vout = nan4, nout = nan4;
-        if (sdf <= 0.0f) {
-            step = fm(sdf, stepScale);
-            result = add3(result, smul3(step, dir));
-            sdf = read_sdf_interp<VR>(m, gv, result, c, valid);
-            step = fm(sdf, stepScale);
-            result = add3(result, smul3(step, dir));
-            f3 n;
-            if (read_normal<VR>(m, gv, result, c, P.Rinv, n)) {
-                const f3 r = mv(P.Rinv, sub3(mul3(result, m.g.voxel_size), P.t));
-                vout = make_float4(r.x, r.y, r.z, 1.0f);
-                nout = make_float4(n.x, n.y, n.z, 1.0f);
-            }
-        }
-        vmap[o] = vout;
-        nmap[o] = nout;
-        live = false;
     }
 }
 
 template <class VR>
-__global__ void __launch_bounds__(128, 8) k_raycast_pool(MapView m, float4* __restrict__ vmap,
-                                                         float4* __restrict__ nmap, int vp, int W, int H, Intr k,
-                                                         const DevPose* __restrict__ posep,
-                                                         const int* __restrict__ skip) {
-    raycast_pool_body<VR>(own_ctx(), m, vmap, nmap, vp, W, H, k, posep, skip);
+__global__ void __launch_bounds__(128) k_raycast_queue(MapView m, float4* __restrict__ vmap,
+                                                       float4* __restrict__ nmap, int vp, int W, int H, Intr k,
+                                                       const DevPose* __restrict__ posep,
+                                                       const int* __restrict__ skip) {
+    raycast_queue_body<VR>(own_ctx(), m, vmap, nmap, vp, W, H, k, posep, skip);
 }
 template <class VR>
-__global__ void __launch_bounds__(128, 8)
-    k_raycast_pool_fused(const __grid_constant__ FusedParams<ArgsOf<decltype(&k_raycast_pool<VR>)>> fp) {
-    run_part(fp, [](const BlockCtx& c, const auto&... a) { raycast_pool_body<VR>(c, a...); });
+__global__ void __launch_bounds__(128)
+    k_raycast_queue_fused(const __grid_constant__ FusedParams<ArgsOf<decltype(&k_raycast_queue<VR>)>> fp) {
+    run_part(fp, [](const BlockCtx& c, const auto&... a) { raycast_queue_body<VR>(c, a...); });
 }
 
 static int sm_count_rc() {
@@ -603,6 +542,20 @@ static int sm_count_rc() {
         if (n <= 0) n = 148;
     }
     return n;
+}
+
+// CTAs of the queued raycast resident on one SM (its register count decides).
+static int queue_ctas_per_sm(bool compact) {
+    static int n[2] = {0, 0};
+    int& v = n[compact ? 1 : 0];
+    if (!v) {
+        if (compact)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_raycast_queue<CompactVox>, 128, 0);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_raycast_queue<ExactVox>, 128, 0);
+        if (v <= 0) v = 8;
+    }
+    return v;
 }
 
 int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s) {
@@ -617,13 +570,15 @@ int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const in
 int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,
                     const DevPose* pose, const int* skip, cudaStream_t s, int bx, int by) {
     if (bx == 0 && by == 0) {
-        const int blocks = sm_count_rc() * 8;
+        // resident CTAs only (4 warps each), no more than the tiles need
+        const int tiles = ((W + 7) >> 3) * ((H + 3) >> 2);
+        const int blocks = std::min(sm_count_rc() * queue_ctas_per_sm(m.cvox != nullptr), (tiles + 3) / 4);
         if (m.cvox)
-            fb_launch(k_raycast_pool<CompactVox>, (const void*)k_raycast_pool_fused<CompactVox>, blocks, 128, 0, s, m,
-                      vmap, nmap, p, W, H, k, pose, skip);
+            fb_launch(k_raycast_queue<CompactVox>, (const void*)k_raycast_queue_fused<CompactVox>, blocks, 128, 0, s,
+                      m, vmap, nmap, p, W, H, k, pose, skip);
         else
-            fb_launch(k_raycast_pool<ExactVox>, (const void*)k_raycast_pool_fused<ExactVox>, blocks, 128, 0, s, m, vmap,
-                      nmap, p, W, H, k, pose, skip);
+            fb_launch(k_raycast_queue<ExactVox>, (const void*)k_raycast_queue_fused<ExactVox>, blocks, 128, 0, s, m,
+                      vmap, nmap, p, W, H, k, pose, skip);
         return 1;
     }
     dim3 b(bx, by), g((W + bx - 1) / bx, (H + by - 1) / by);

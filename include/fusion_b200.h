@@ -177,9 +177,9 @@ FB_API int fb_session_prepare(fb_session* s, int shared);
 FB_API int fb_session_prepare_some(fb_session* s, int shared, int max_graphs, int* remaining);
 /* The model raycast's launch shape for this session: one thread per pixel
  * in CUDA blocks of bx x by threads (bx * by <= 128 and a multiple of 32;
- * default 16 x 8), or with bx = by = 0 the pooled raycast, whose warps take
- * 8 x 4 pixel tiles from a work counter and refill every lane whose ray has
- * ended (it pays off on small images only).  Results do not depend on it
+ * default 16 x 8), or with bx = by = 0 the queued raycast, a grid of
+ * resident CTAs whose warps take 8 x 4 pixel tiles from a work counter until
+ * every tile is taken.  Results do not depend on it
  * (every pixel is traced alone, by the same operations).  Cached frame
  * graphs are rebuilt on the next frame.  No reference counterpart: a tuning
  * knob for the batched form's autotuner. */
