@@ -175,8 +175,23 @@ struct MapView {
     float4* frec;               // fusion records, 8 zc x 8 zr: {depth or NaN, normal xyz} (fuse_record), or
                                 // in the precision form one packed 16-byte word each (fuse_record_packed)
     uint32_t* fcol;             // reference form: the records' colours r | g << 8 | b << 16
+    // raycast block order (a scheduling hint; no result depends on it): each
+    // raycast warp records its duration in rc_cost[tile] (clock cycles, max
+    // over the tile's warps); the z-range pass turns the last raycast's costs
+    // into rc_order = {tile count n, then the n tiles slowest first} and
+    // clears them; a raycast of n tiles runs its blocks in that order
+    uint32_t* rc_cost;          // rc_cap
+    int* rc_order;              // 1 + rc_cap
+    int rc_cap;
     MapGeom g;
 };
+
+// Tiles of the raycast's block grid for a W x H image in bx x by blocks, and
+// the most any block shape of 32..128 threads (a multiple of 32) can need.
+inline int raycast_tiles(int W, int H, int bx, int by) {
+    return bx > 0 && by > 0 ? ((W + bx - 1) / bx) * ((H + by - 1) / by) : 0;
+}
+inline int raycast_tile_cap(int W, int H) { return W * H / 32 + W + H + 1; }
 
 constexpr int kScanChunk = 4096;
 constexpr int kMinNewBlocks = 1 << 16;
@@ -203,7 +218,10 @@ int launch_fuse_records(const MapView& m, const float* raw, int rp, const uint8_
 // block); 0: the form's default.  Results do not depend on it.
 int launch_integrate(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
                      cudaStream_t s, int ctas_per_sm = 0);
-int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s);
+// rc_tiles: tiles of the raycast that follows (raycast_tiles), whose block
+// order this pass prepares from the last raycast's costs; 0: leave it as it is.
+int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s,
+                  int rc_tiles = 0);
 // tile bx x by threads: bx * by <= 128 (the kernel's launch bound), a multiple
 // of 32; bx = by = 0: the queued raycast (warps take 8 x 4 pixel tiles from a counter)
 int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,

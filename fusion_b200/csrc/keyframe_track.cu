@@ -274,7 +274,7 @@ int issue_reloc(fb_session* s, const double* T) {
     const DevPose* pose = &s->st->cur;
     int n = 1;
     n += launch_visibility(s->map, s->W[0], s->H[0], s->K[0], pose, nullptr, st);
-    n += launch_zrange(s->map, s->K[0], pose, nullptr, st);
+    n += launch_zrange(s->map, s->K[0], pose, nullptr, st, raycast_tiles(s->W[0], s->H[0], s->rc_bx, s->rc_by));
     n += launch_raycast(s->map, N.vmap[0], N.nmap[0], s->W[0], s->W[0], s->H[0], s->K[0], pose, nullptr, st, s->rc_bx,
                         s->rc_by);
     launch_commit(s, 1, st);

@@ -43,18 +43,77 @@ __global__ void __launch_bounds__(256) k_zrange_init(MapView m, const int* __res
 }
 FB_FUSED_KERNEL(k_zrange_init, zrange_init_body, 256)
 
+// Histogram bucket of a raycast tile's cost: 16 buckets per octave (the
+// exponent and the next four bits), 0..511.
+__device__ __forceinline__ int cost_bucket(uint32_t c) {
+    if (c == 0) return 0;
+    const int msb = 31 - __clz(c);
+    const uint32_t frac = msb >= 4 ? (c >> (msb - 4)) & 15u : (c << (4 - msb)) & 15u;
+    return msb * 16 + (int)frac;
+}
+
+// The raycast's block order for its next launch of n tiles (one block of 256
+// threads): the tiles sorted by the last raycast's costs, slowest first (to
+// 1/16 octave; ties in any order), so that the longest rays start first and
+// the launch does not end waiting for a slow tile that started last.  Clears
+// the costs.  The order is a permutation of 0..n-1 whatever the costs hold.
+__device__ __forceinline__ void order_tiles(const MapView& m, int n) {
+    __shared__ int hist[512];
+    __shared__ int wsum[8];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (n > m.rc_cap) {
+        if (t == 0) m.rc_order[0] = 0;   // no order: blocks in grid order
+        return;
+    }
+    hist[t] = 0;
+    hist[t + 256] = 0;
+    __syncthreads();
+    for (int i = t; i < n; i += 256) atomicAdd(&hist[cost_bucket(m.rc_cost[i])], 1);
+    __syncthreads();
+    // bucket starts in descending bucket order: thread t owns buckets 511 - 2t
+    // and 510 - 2t (a block-wide exclusive scan of their counts)
+    const int h0 = hist[511 - 2 * t], h1 = hist[510 - 2 * t];
+    int v = h0 + h1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) wsum[w] = v;
+    __syncthreads();
+    int base = 0;
+    for (int q = 0; q < w; ++q) base += wsum[q];
+    const int excl = base + v - (h0 + h1);
+    hist[511 - 2 * t] = excl;   // every thread has read its two counts above
+    hist[510 - 2 * t] = excl + h0;
+    __syncthreads();
+    for (int i = t; i < n; i += 256) {
+        const int slot = atomicAdd(&hist[cost_bucket(m.rc_cost[i])], 1);
+        m.rc_order[1 + slot] = i;
+        m.rc_cost[i] = 0;
+    }
+    if (t == 0) m.rc_order[0] = n;
+}
+
 // Projection::projectBlock (RenderScene.cu:54-104) + the first tile's fill
-// (fillBlocks, RenderScene.cu:156-179).
+// (fillBlocks, RenderScene.cu:156-179).  With ord_n > 0 the grid's last block
+// prepares the next raycast's block order instead (order_tiles), beside the
+// projection.
 __device__ __forceinline__ void zrange_body(const BlockCtx& ctx, MapView m, Intr k, const DevPose* __restrict__ posep,
-                                            const int* __restrict__ skip) {
+                                            const int* __restrict__ skip, int ord_n) {
     if (skip && *skip) return;
+    if (ord_n > 0 && ctx.bx == ctx.gx - 1) {
+        order_tiles(m, ord_n);
+        return;
+    }
+    const int gx = ord_n > 0 ? ctx.gx - 1 : ctx.gx;
     const DevPose P = *posep;
     const int n = min(m.ctr->n_visible, m.NS);
     const int zc = m.zc, zr = m.zr;
     // box of the visible blocks (warp-reduced, then one atomic per warp)
     {
         int lo[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, hi[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
-        for (int i = ctx.bx * blockDim.x + threadIdx.x; i < n; i += ctx.gx * blockDim.x) {
+        for (int i = ctx.bx * blockDim.x + threadIdx.x; i < n; i += gx * blockDim.x) {
             const HEntry e = m.vis_blocks[i];
             lo[0] = min(lo[0], (int)e.x);
             lo[1] = min(lo[1], (int)e.y);
@@ -76,7 +135,7 @@ __device__ __forceinline__ void zrange_body(const BlockCtx& ctx, MapView m, Intr
             }
         }
     }
-    for (int i = ctx.bx * blockDim.x + threadIdx.x; i < n; i += ctx.gx * blockDim.x) {
+    for (int i = ctx.bx * blockDim.x + threadIdx.x; i < n; i += gx * blockDim.x) {
         const HEntry e = m.vis_blocks[i];
         int ulx = zc, uly = zr, lrx = -1, lry = -1;
         float zx = m.g.depth_max, zy = m.g.depth_min;
@@ -115,8 +174,8 @@ __device__ __forceinline__ void zrange_body(const BlockCtx& ctx, MapView m, Intr
 }
 
 __global__ void __launch_bounds__(256) k_zrange(MapView m, Intr k, const DevPose* __restrict__ posep,
-                                  const int* __restrict__ skip) {
-    zrange_body(own_ctx(), m, k, posep, skip);
+                                  const int* __restrict__ skip, int ord_n) {
+    zrange_body(own_ctx(), m, k, posep, skip, ord_n);
 }
 FB_FUSED_KERNEL(k_zrange, zrange_body, 256)
 
@@ -464,28 +523,49 @@ __device__ __forceinline__ void raycast_pixel(const MapView& m, const GridView& 
     *nout_p = nout;
 }
 
-// One thread per pixel in CUDA blocks of the session's tile shape.
+// One thread per pixel in CUDA blocks of the session's tile shape.  Block b
+// of the grid traces tile rc_order[1 + b] when the z-range pass ordered this
+// launch's tiles (rc_order[0] == the tile count), else tile b; each warp
+// records its duration as its tile's cost for the next order.
 template <class VR>
 __device__ __forceinline__ void raycast_body(const BlockCtx& ctx, MapView m, float4* __restrict__ vmap,
                                              float4* __restrict__ nmap, int vp, int W, int H, Intr k,
                                              const DevPose* __restrict__ posep, const int* __restrict__ skip) {
     if (skip && *skip) return;
     if (m.ctr->n_tiles == 0) return;   // CreateRenderingBlocks returned false: maps untouched
-    const int x = ctx.bx * blockDim.x + threadIdx.x;
-    const int y = ctx.by * blockDim.y + threadIdx.y;
-    if (x >= W || y >= H) return;
-    const size_t o = (size_t)y * vp + x;
-    raycast_pixel<VR>(m, grid_view(m), *posep, k, x, y, vmap + o, nmap + o);
+    // the warp's start time and tile wait in shared memory (not in registers
+    // across the ray)
+    __shared__ long long s_t0[4];
+    __shared__ int s_tile[4];
+    const int lt = threadIdx.y * blockDim.x + threadIdx.x, wq = lt >> 5;   // blockDim <= 128
+    const int nt = ctx.gx * ctx.gy, b = ctx.by * ctx.gx + ctx.bx;
+    int tile = b;
+    if (m.rc_order && nt <= m.rc_cap && m.rc_order[0] == nt) tile = m.rc_order[1 + b];
+    if ((lt & 31) == 0) {
+        s_t0[wq] = clock64();
+        s_tile[wq] = tile;
+    }
+    const int ty = tile / ctx.gx, tx = tile - ty * ctx.gx;
+    const int x = tx * blockDim.x + threadIdx.x;
+    const int y = ty * blockDim.y + threadIdx.y;
+    if (x < W && y < H) {
+        const size_t o = (size_t)y * vp + x;
+        raycast_pixel<VR>(m, grid_view(m), *posep, k, x, y, vmap + o, nmap + o);
+    }
+    if ((lt & 31) == 0 && m.rc_cost && s_tile[wq] < m.rc_cap)
+        atomicMax(&m.rc_cost[s_tile[wq]], (uint32_t)min(clock64() - s_t0[wq], 0xffffffffLL));
 }
 
+// Nine CTAs of 128 threads per SM (56 registers; the compiler's own choice
+// of 72 leaves seven, and the tail of the launch is longer).
 template <class VR>
-__global__ void __launch_bounds__(128) k_raycast(MapView m, float4* __restrict__ vmap, float4* __restrict__ nmap,
+__global__ void __launch_bounds__(128, 9) k_raycast(MapView m, float4* __restrict__ vmap, float4* __restrict__ nmap,
                                                  int vp, int W, int H, Intr k, const DevPose* __restrict__ posep,
                                                  const int* __restrict__ skip) {
     raycast_body<VR>(own_ctx(), m, vmap, nmap, vp, W, H, k, posep, skip);
 }
 template <class VR>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 9)
     k_raycast_fused(const __grid_constant__ FusedParams<ArgsOf<decltype(&k_raycast<VR>)>> fp) {
     run_part(fp, [](const BlockCtx& c, const auto&... a) { raycast_body<VR>(c, a...); });
 }
@@ -558,9 +638,13 @@ static int queue_ctas_per_sm(bool compact) {
     return v;
 }
 
-int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s) {
+int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const int* skip, cudaStream_t s,
+                  int rc_tiles) {
     fb_launch(k_zrange_init, (const void*)k_zrange_init_fused, (m.zc * m.zr + 255) / 256, 256, 0, s, m, skip);
-    fb_launch(k_zrange, (const void*)k_zrange_fused, sm_count_rc() * 2, 256, 0, s, m, k, pose, skip);
+    // one more block prepares the raycast's block order when there is one to prepare
+    const int ord_n = m.rc_order ? rc_tiles : 0;
+    fb_launch(k_zrange, (const void*)k_zrange_fused, sm_count_rc() * 2 + (ord_n > 0 ? 1 : 0), 256, 0, s, m, k, pose,
+              skip, ord_n);
     fb_launch(k_grid_prepare, (const void*)k_grid_prepare_fused, 1, 1, 0, s, m, skip);
     fb_launch(k_grid_clear, (const void*)k_grid_clear_fused, sm_count_rc() * 4, 256, 0, s, m, skip);
     fb_launch(k_grid_fill, (const void*)k_grid_fill_fused, sm_count_rc() * 4, 256, 0, s, m, skip);

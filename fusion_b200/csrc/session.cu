@@ -309,6 +309,7 @@ bool carve_session(fb_session* s, const fb_config* cfg) {
         }
         m.zc = (cfg->width + 7) / 8;
         m.zr = (cfg->height + 7) / 8;
+        m.rc_cap = raycast_tile_cap(cfg->width, cfg->height);
         m.g = make_geom(*cfg);
         ok = dalloc(s, &m.entries, (size_t)m.NB + m.NE) && dalloc(s, &m.heap, m.NS) &&
              (cfg->form == FB_FORM_PRECISION ? dalloc(s, &m.cvox, (size_t)m.NS * kCBlockBytes)
@@ -321,7 +322,8 @@ bool carve_session(fb_session* s, const fb_config* cfg) {
              dalloc(s, &m.chunk_sums, 2 * (size_t)m.nchunks) && dalloc(s, &m.zmin, (size_t)m.zc * m.zr) &&
              dalloc(s, &m.grid, (size_t)m.grid_cap) &&
              dalloc(s, &m.zmax, (size_t)m.zc * m.zr) && dalloc(s, &m.frec, (size_t)64 * m.zc * m.zr) &&
-             dalloc(s, &m.fcol, (size_t)64 * m.zc * m.zr);
+             dalloc(s, &m.fcol, (size_t)64 * m.zc * m.zr) && dalloc(s, &m.rc_cost, (size_t)m.rc_cap) &&
+             dalloc(s, &m.rc_order, (size_t)m.rc_cap + 1);
         s->ctr = m.ctr;
     }
     return ok;
@@ -331,6 +333,8 @@ int reset_session(fb_session* s) {
     launch_map_reset(s->map, s->stream);
     k_init_poses<<<1, 1, 0, s->stream>>>(s->st);
     FB_CUDA(cudaMemsetAsync(s->tickets, 0, 4 * sizeof(unsigned), s->stream));
+    FB_CUDA(cudaMemsetAsync(s->map.rc_cost, 0, (size_t)s->map.rc_cap * sizeof(uint32_t), s->stream));
+    FB_CUDA(cudaMemsetAsync(s->map.rc_order, 0, sizeof(int), s->stream));   // no order yet: blocks in grid order
     for (int f = 0; f < 2; ++f)
         for (int l = 0; l < 3; ++l) {
             size_t n = (size_t)s->W[l] * s->H[l];
@@ -452,7 +456,7 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
         }
         // Mapping::RayTrace (Mapping.cc:92-109) into the frame's level-0 maps
         launch_slot(kSlotZRange);
-        n += launch_zrange(s->map, s->K[0], pose, skip, st);
+        n += launch_zrange(s->map, s->K[0], pose, skip, st, raycast_tiles(s->W[0], s->H[0], s->rc_bx, s->rc_by));
         mark(7);
         launch_slot(kSlotRaycast);
         n += launch_raycast(s->map, N.vmap[0], N.nmap[0], s->W[0], s->W[0], s->H[0], s->K[0], pose, skip, st,
