@@ -463,61 +463,97 @@ __device__ __forceinline__ GridView grid_view(const MapView& m) {
     return gv;
 }
 
-// Rendering::operator() (RenderScene.cu:354-440) for pixel (x, y): writes
-// its vertex and normal (NaN where the ray finds no surface).
+// One ray of Rendering::operator() (RenderScene.cu:354-440), in three parts
+// that every raycast kernel runs in this order: ray_begin, ray_step until it
+// reports the end of the march loop, ray_finish.
+struct Ray {
+    f3 result, dir;
+    float dist_s, dist_e, sdf;
+};
+
+// The ray of pixel (x, y) from its depth interval; false when the pixel has
+// none (its vertex and normal are NaN).
+__device__ __forceinline__ bool ray_begin(const MapView& m, const DevPose& P, const Intr& k, int x, int y, Ray& r) {
+    const int lx = (int)floorf(fd((float)x, 8.f)), ly = (int)floorf(fd((float)y, 8.f));
+    const float zrx = m.zmin[ly * m.zc + lx], zry = m.zmax[ly * m.zc + lx];
+    if ((double)zry < 1e-3 || (double)zrx < 1e-3 || isnan(zrx) || isnan(zry)) return false;
+    const float vinv = m.g.voxel_size_inv;
+    f3 p;
+    p.z = zrx;
+    p.x = fm(fm(p.z, fs((float)x, k.cx)), k.invfx);
+    p.y = fm(fm(p.z, fs((float)y, k.cy)), k.invfy);
+    r.dist_s = fm(norm3(p), vinv);
+    const f3 block_s = mul3(add3(mv(P.R, p), P.t), vinv);
+    p.z = zry;
+    p.x = fm(fm(p.z, fs((float)x, k.cx)), k.invfx);
+    p.y = fm(fm(p.z, fs((float)y, k.cy)), k.invfy);
+    r.dist_e = fm(norm3(p), vinv);
+    const f3 block_e = mul3(add3(mv(P.R, p), P.t), vinv);
+    r.dir = normalised3(sub3(block_e, block_s));
+    r.result = block_s;
+    r.sdf = 1.0f;
+    return true;
+}
+
+// One turn of the march loop; true when the loop has ended (its condition
+// failed, or a sample at or behind the surface).
+template <class VR>
+__device__ __forceinline__ bool ray_step(const MapView& m, const GridView& gv, float stepScale, Ray& r,
+                                         EntryCache& c) {
+    if (!(r.dist_s < r.dist_e)) return true;
+    bool valid;
+    float step;
+    r.sdf = read_sdf<VR>(m, gv, r.result, c, valid);
+    if (!valid) {
+        step = 8.0f;
+    } else {
+        if (r.sdf <= 0.1f && r.sdf >= -0.5f) r.sdf = read_sdf_interp<VR>(m, gv, r.result, c, valid);
+        if (r.sdf <= 0.0f) return true;
+        step = !isnan(r.sdf) ? fmaxf(fm(r.sdf, stepScale), 1.0f) : 8.0f;
+    }
+    r.result = add3(r.result, smul3(step, r.dir));
+    r.dist_s = fa(r.dist_s, step);
+    return false;
+}
+
+// After the loop: a ray whose last sample is at or behind the surface (sdf
+// <= 0) is refined by two steps and gets its vertex and normal; every other
+// ray gives NaN.
+template <class VR>
+__device__ __forceinline__ void ray_finish(const MapView& m, const GridView& gv, const DevPose& P, float stepScale,
+                                           Ray r, EntryCache& c, float4& vout, float4& nout) {
+    const float4 nan4 = make_float4(qnan(), qnan(), qnan(), qnan());
+    vout = nan4;
+    nout = nan4;
+    if (!(r.sdf <= 0.0f)) return;
+    bool valid;
+    float step = fm(r.sdf, stepScale);
+    r.result = add3(r.result, smul3(step, r.dir));
+    r.sdf = read_sdf_interp<VR>(m, gv, r.result, c, valid);
+    step = fm(r.sdf, stepScale);
+    r.result = add3(r.result, smul3(step, r.dir));
+    f3 n;
+    if (read_normal<VR>(m, gv, r.result, c, P.Rinv, n)) {
+        const f3 q = mv(P.Rinv, sub3(mul3(r.result, m.g.voxel_size), P.t));
+        vout = make_float4(q.x, q.y, q.z, 1.0f);
+        nout = make_float4(n.x, n.y, n.z, 1.0f);
+    }
+}
+
+// The whole ray of pixel (x, y): writes its vertex and normal.
 template <class VR>
 __device__ __forceinline__ void raycast_pixel(const MapView& m, const GridView& gv, const DevPose& P, const Intr& k,
                                               int x, int y, float4* __restrict__ vout_p,
                                               float4* __restrict__ nout_p) {
-    const float4 nan4 = make_float4(qnan(), qnan(), qnan(), qnan());
-    float4 vout = nan4, nout = nan4;
-    const int lx = (int)floorf(fd((float)x, 8.f)), ly = (int)floorf(fd((float)y, 8.f));
-    const float zrx = m.zmin[ly * m.zc + lx], zry = m.zmax[ly * m.zc + lx];
-    if (!((double)zry < 1e-3 || (double)zrx < 1e-3 || isnan(zrx) || isnan(zry))) {
-        const float vinv = m.g.voxel_size_inv, stepScale = m.g.step_scale;
-        f3 p;
-        p.z = zrx;
-        p.x = fm(fm(p.z, fs((float)x, k.cx)), k.invfx);
-        p.y = fm(fm(p.z, fs((float)y, k.cy)), k.invfy);
-        float dist_s = fm(norm3(p), vinv);
-        const f3 block_s = mul3(add3(mv(P.R, p), P.t), vinv);
-        p.z = zry;
-        p.x = fm(fm(p.z, fs((float)x, k.cx)), k.invfx);
-        p.y = fm(fm(p.z, fs((float)y, k.cy)), k.invfy);
-        const float dist_e = fm(norm3(p), vinv);
-        const f3 block_e = mul3(add3(mv(P.R, p), P.t), vinv);
-        const f3 dir = normalised3(sub3(block_e, block_s));
-        f3 result = block_s;
-        float sdf = 1.0f, step;
-        bool valid = false, found = false;
+    float4 vout = make_float4(qnan(), qnan(), qnan(), qnan()), nout = vout;
+    Ray r;
+    if (ray_begin(m, P, k, x, y, r)) {
+        const float stepScale = m.g.step_scale;
         EntryCache c;
         c.set = false;
-        while (dist_s < dist_e) {
-            sdf = read_sdf<VR>(m, gv, result, c, valid);
-            if (!valid) {
-                step = 8.0f;
-            } else {
-                if (sdf <= 0.1f && sdf >= -0.5f) sdf = read_sdf_interp<VR>(m, gv, result, c, valid);
-                if (sdf <= 0.0f) break;
-                step = !isnan(sdf) ? fmaxf(fm(sdf, stepScale), 1.0f) : 8.0f;
-            }
-            result = add3(result, smul3(step, dir));
-            dist_s = fa(dist_s, step);
+        while (!ray_step<VR>(m, gv, stepScale, r, c)) {
         }
-        if (sdf <= 0.0f) {
-            step = fm(sdf, stepScale);
-            result = add3(result, smul3(step, dir));
-            sdf = read_sdf_interp<VR>(m, gv, result, c, valid);
-            step = fm(sdf, stepScale);
-            result = add3(result, smul3(step, dir));
-            found = true;
-        }
-        f3 n;
-        if (found && read_normal<VR>(m, gv, result, c, P.Rinv, n)) {
-            const f3 r = mv(P.Rinv, sub3(mul3(result, m.g.voxel_size), P.t));
-            vout = make_float4(r.x, r.y, r.z, 1.0f);
-            nout = make_float4(n.x, n.y, n.z, 1.0f);
-        }
+        ray_finish<VR>(m, gv, P, stepScale, r, c, vout, nout);
     }
     *vout_p = vout;
     *nout_p = nout;
@@ -575,6 +611,10 @@ __global__ void __launch_bounds__(128, 9)
 // warp and tile, until every tile is taken, so a warp that drew cheap rays
 // takes more tiles instead of leaving its slot idle until the grid's last
 // CTAs end.  Every pixel runs raycast_pixel as in k_raycast: the same bits.
+// (Refilling each lane whose ray has ended with a new pixel, the finished
+// rays queued so that the whole warp computes their normals together, was
+// measured 1.7x slower than k_raycast at 640x480: a warp's lanes then march
+// unrelated rays, and their voxel reads no longer fall on shared lines.)
 template <class VR>
 __device__ __forceinline__ void raycast_queue_body(const BlockCtx&, MapView m, float4* __restrict__ vmap,
                                                    float4* __restrict__ nmap, int vp, int W, int H, Intr k,
