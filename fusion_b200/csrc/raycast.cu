@@ -281,6 +281,12 @@ struct ExactVox {
     static __device__ __forceinline__ bool null(ref v) { return v == nullptr; }
     static __device__ __forceinline__ float sdf(ref v) { return v->sdf; }
     static __device__ __forceinline__ int weight(ref v) { return v->weight; }
+    // TSDF and weight with one 8-byte load
+    static __device__ __forceinline__ float sdf_w(ref v, int& w) {
+        const uint2 raw = *reinterpret_cast<const uint2*>(v);
+        w = (int)(raw.y & 0xffu);
+        return __uint_as_float(raw.x);
+    }
 };
 
 // Precision form: FP16 TSDF array, then one r, g, b, weight word per voxel.
@@ -298,6 +304,10 @@ struct CompactVox {
         return __half2float(*(const __half*)(v.blk + 2 * v.idx));
     }
     static __device__ __forceinline__ int weight(ref v) { return v.blk[c_weight(v.idx)]; }
+    static __device__ __forceinline__ float sdf_w(ref v, int& w) {
+        w = weight(v);
+        return sdf(v);
+    }
 };
 
 // FindEntry's block (DeviceMap.cu:122-135) through the dense index where it
@@ -359,8 +369,10 @@ template <class VR>
 __device__ __forceinline__ float read_sdf(const MapView& m, const GridView& gv, f3 p, EntryCache& c, bool& valid) {
     const typename VR::ref v = find_voxel<VR>(m, gv, p, c, valid);
     if (VR::null(v)) return qnan();
-    if (VR::weight(v) == 0) valid = false;
-    return VR::sdf(v);
+    int w;
+    const float sdf = VR::sdf_w(v, w);
+    if (w == 0) valid = false;
+    return sdf;
 }
 
 // One corner of a trilinear read: the voxel's TSDF in block q, NaN for a
@@ -600,8 +612,10 @@ __global__ void __launch_bounds__(128, 9) k_raycast(MapView m, float4* __restric
                                                  const int* __restrict__ skip) {
     raycast_body<VR>(own_ctx(), m, vmap, nmap, vp, W, H, k, posep, skip);
 }
+// (the fused form keeps the compiler's register count: its spills at nine
+// CTAs per SM cost more in batched steps than the occupancy gains)
 template <class VR>
-__global__ void __launch_bounds__(128, 9)
+__global__ void __launch_bounds__(128)
     k_raycast_fused(const __grid_constant__ FusedParams<ArgsOf<decltype(&k_raycast<VR>)>> fp) {
     run_part(fp, [](const BlockCtx& c, const auto&... a) { raycast_body<VR>(c, a...); });
 }
