@@ -871,21 +871,37 @@ __device__ __forceinline__ void finish_iteration(TrackState* st, unsigned int* t
     {
         const int val = threadIdx.x & 63, part = threadIdx.x >> 6;
         const int per = (NG + 3) / 4, g0 = part * per, g1 = min(NG, g0 + per);
+        // the range's values are loaded 16 at a time before any is added (one
+        // L2 round trip for the usual ten groups), then added in group order
         if constexpr (kComp) {
             // compensated FP32 over the groups; to FP64 only for the solve
             float2 t = make_float2(0.f, 0.f);
             if ((val & 31) < 29) {
                 const float2* src = val < 32 ? &st->grp_icp2[0][val] : &st->grp_rgb2[0][val - 32];
-#pragma unroll 8
-                for (int g = g0; g < g1; ++g) t = pair_add(t, __ldcg(src + (size_t)g * 32));
+                for (int g = g0; g < g1; g += 16) {
+                    float2 v[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (g + j < g1) v[j] = __ldcg(src + (size_t)(g + j) * 32);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (g + j < g1) t = pair_add(t, v[j]);
+                }
             }
             s_partc[part][val] = t;
         } else {
             double t = 0;
             if ((val & 31) < 29) {
                 const double* src = val < 32 ? &st->grp_icp[0][val] : &st->grp_rgb[0][val - 32];
-#pragma unroll 8
-                for (int g = g0; g < g1; ++g) t += __ldcg(src + (size_t)g * 32);
+                for (int g = g0; g < g1; g += 16) {
+                    double v[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (g + j < g1) v[j] = __ldcg(src + (size_t)(g + j) * 32);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (g + j < g1) t += v[j];
+                }
             }
             s_part[part][val] = t;
         }
