@@ -106,6 +106,79 @@ int launch_nmap(const float4* vmap, int vp, int W, int H, float4* nmap, int np, 
 int launch_resize(const float4* vs, const float4* ns, int sp, int SW, int SH, float4* vd, float4* nd, int dp,
                    cudaStream_t st);
 
+// One launch of a frame's preprocessing whose blocks take up to four roles,
+// each the kernel of the same name above over its own image as a grid of
+// 32 x 8 blocks (gx x gy; 0 x 0: role absent); the launch's 1-D grid holds
+// the roles' grids one after another in the order level 0, resize, pyrdown,
+// maps.  Roles in one launch must not depend on each other.
+struct Level0Args {
+    const uint16_t* depth;
+    int dpitch;
+    const uint8_t* rgb;
+    int rgbpitch, W, H;
+    float inv, cutoff;
+    float* raw;
+    int rawpitch;
+    float* filt;
+    int fpitch;
+    uint8_t* gray;
+    int gpitch;
+};
+struct ResizeArgs {
+    const float4* vs;
+    const float4* ns;
+    int sp, SW, SH;
+    float4* vd;
+    float4* nd;
+    int dp;
+};
+struct PyrArgs {
+    const float* sd;
+    int sdp;
+    const uint8_t* sg;
+    int sgp, SW, SH;
+    float* dd;
+    int ddp;
+    uint8_t* dg;
+    int dgp;
+};
+struct MapsArgs {
+    const float* depth;
+    int dp;
+    const uint8_t* gray;
+    int gp, W, H;
+    Intr k;
+    float cutoff;
+    float4* vmap;
+    int vp;
+    float4* nmap;
+    int np;
+    int16_t* dxo;
+    int16_t* dyo;
+    int sp;
+    uint8_t* rgbok;
+    FuseRecDst fr;
+};
+struct PreLaunch {
+    Level0Args l0;
+    ResizeArgs rs;
+    PyrArgs py;
+    MapsArgs mp;
+    int gx[4], gy[4];
+};
+// Role setters (same arguments as the launchers above) and the launch.
+void pre_level0(PreLaunch& P, const uint16_t* depth, int dpitch, const uint8_t* rgb, int rgbpitch, int W, int H,
+                float depth_scale, float cutoff, float* raw, int rawpitch, float* filt, int fpitch, uint8_t* gray,
+                int gpitch);
+void pre_resize(PreLaunch& P, const float4* vs, const float4* ns, int sp, int SW, int SH, float4* vd, float4* nd,
+                int dp);
+void pre_pyrdown(PreLaunch& P, const float* sd, int sdp, const uint8_t* sg, int sgp, int SW, int SH, float* dd,
+                 int ddp, uint8_t* dg, int dgp);
+void pre_maps(PreLaunch& P, const float* depth, int dp, const uint8_t* gray, int gp, int W, int H, const Intr& k,
+              float cutoff, float4* vmap, int vp, float4* nmap, int np, int16_t* dx, int16_t* dy, int sp,
+              uint8_t* rgbok, const FuseRecDst* fr);
+int launch_pre(const PreLaunch& P, cudaStream_t st);
+
 // ----------------------------------------------------------------------- map
 
 struct MapCounters {

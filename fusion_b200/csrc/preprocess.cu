@@ -248,7 +248,83 @@ __global__ void k_resize(const float4* __restrict__ vs, const float4* __restrict
 }
 FB_FUSED_KERNEL(k_resize, resize_body, 256)
 
+// A launch of up to four roles (PreLaunch): each block finds its role and
+// runs that role's body with its coordinates in the role's own grid.
+__device__ __forceinline__ void pre_body(const BlockCtx& ctx, const PreLaunch& P) {
+    int b = ctx.bx;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int n = P.gx[r] * P.gy[r];
+        if (b < n) {
+            const BlockCtx c{b % P.gx[r], b / P.gx[r], P.gx[r], P.gy[r]};
+            if (r == 0) {
+                const Level0Args& a = P.l0;
+                level0_body(c, a.depth, a.dpitch, a.rgb, a.rgbpitch, a.W, a.H, a.inv, a.cutoff, a.raw, a.rawpitch,
+                            a.filt, a.fpitch, a.gray, a.gpitch);
+            } else if (r == 1) {
+                const ResizeArgs& a = P.rs;
+                resize_body(c, a.vs, a.ns, a.sp, a.SW, a.SH, a.vd, a.nd, a.dp);
+            } else if (r == 2) {
+                const PyrArgs& a = P.py;
+                pyrdown_body(c, a.sd, a.sdp, a.sg, a.sgp, a.SW, a.SH, a.dd, a.ddp, a.dg, a.dgp);
+            } else {
+                const MapsArgs& a = P.mp;
+                maps_body(c, a.depth, a.dp, a.gray, a.gp, a.W, a.H, a.k, a.cutoff, a.vmap, a.vp, a.nmap, a.np,
+                          a.dxo, a.dyo, a.sp, a.rgbok, a.fr);
+            }
+            return;
+        }
+        b -= n;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_pre(PreLaunch P) { pre_body(own_ctx(), P); }
+FB_FUSED_KERNEL(k_pre, pre_body, 256)
+
 static inline dim3 grid2d(int W, int H, dim3 b) { return dim3((W + b.x - 1) / b.x, (H + b.y - 1) / b.y); }
+
+static void set_role(PreLaunch& P, int r, int W, int H) {
+    const dim3 g = grid2d(W, H, dim3(32, 8));
+    P.gx[r] = W > 0 && H > 0 ? (int)g.x : 0;
+    P.gy[r] = W > 0 && H > 0 ? (int)g.y : 0;
+}
+
+void pre_level0(PreLaunch& P, const uint16_t* depth, int dpitch, const uint8_t* rgb, int rgbpitch, int W, int H,
+                float depth_scale, float cutoff, float* raw, int rawpitch, float* filt, int fpitch, uint8_t* gray,
+                int gpitch) {
+    // FilterDepth passes 1.0 / depthScale computed in double (Pyrdown.cu:50)
+    P.l0 = Level0Args{depth, dpitch, rgb, rgbpitch, W, H, (float)(1.0 / (double)depth_scale), cutoff, raw,
+                      rawpitch, filt, fpitch, gray, gpitch};
+    set_role(P, 0, W, H);
+}
+
+void pre_resize(PreLaunch& P, const float4* vs, const float4* ns, int sp, int SW, int SH, float4* vd, float4* nd,
+                int dp) {
+    P.rs = ResizeArgs{vs, ns, sp, SW, SH, vd, nd, dp};
+    set_role(P, 1, SW / 2, SH / 2);
+}
+
+void pre_pyrdown(PreLaunch& P, const float* sd, int sdp, const uint8_t* sg, int sgp, int SW, int SH, float* dd,
+                 int ddp, uint8_t* dg, int dgp) {
+    P.py = PyrArgs{sd, sdp, sg, sgp, SW, SH, dd, ddp, dg, dgp};
+    set_role(P, 2, SW / 2, SH / 2);
+}
+
+void pre_maps(PreLaunch& P, const float* depth, int dp, const uint8_t* gray, int gp, int W, int H, const Intr& k,
+              float cutoff, float4* vmap, int vp, float4* nmap, int np, int16_t* dx, int16_t* dy, int sp,
+              uint8_t* rgbok, const FuseRecDst* fr) {
+    const FuseRecDst none{};
+    P.mp = MapsArgs{depth, dp, gray, gp, W, H, k, cutoff, vmap, vp, nmap, np, dx, dy, sp, rgbok, fr ? *fr : none};
+    set_role(P, 3, W, H);
+}
+
+int launch_pre(const PreLaunch& P, cudaStream_t st) {
+    int blocks = 0;
+    for (int r = 0; r < 4; ++r) blocks += P.gx[r] * P.gy[r];
+    if (blocks == 0) return 0;
+    fb_launch(k_pre, (const void*)k_pre_fused, blocks, dim3(32, 8), 0, st, P);
+    return 1;
+}
 
 // ---- launchers (pitches in elements) ----
 

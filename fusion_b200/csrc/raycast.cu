@@ -486,9 +486,11 @@ struct Ray {
 // The ray of pixel (x, y) from its depth interval; false when the pixel has
 // none (its vertex and normal are NaN).
 __device__ __forceinline__ bool ray_begin(const MapView& m, const DevPose& P, const Intr& k, int x, int y, Ray& r) {
-    const int lx = (int)floorf(fd((float)x, 8.f)), ly = (int)floorf(fd((float)y, 8.f));
+    // floor(x / 8) of a pixel coordinate (>= 0) is x >> 3; (double)z < 1e-3
+    // holds exactly when z < 0.001f (the float identities' test checks it)
+    const int lx = x >> 3, ly = y >> 3;
     const float zrx = m.zmin[ly * m.zc + lx], zry = m.zmax[ly * m.zc + lx];
-    if ((double)zry < 1e-3 || (double)zrx < 1e-3 || isnan(zrx) || isnan(zry)) return false;
+    if (zry < 0.001f || zrx < 0.001f || isnan(zrx) || isnan(zry)) return false;
     const float vinv = m.g.voxel_size_inv;
     f3 p;
     p.z = zrx;

@@ -371,28 +371,54 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
         if (s->profile) cudaEventRecord(s->ev[k], st);
     };
     if (part != 2) {
-        // Tracker::GrabFrame (Tracking.cc:236-243): LastFrame->ResizeImages ...
+        // Tracker::GrabFrame (Tracking.cc:236-243): LastFrame->ResizeImages and
+        // NextFrame->FillImages (Core/Frame.cc:59-84) in four launches whose
+        // roles do not depend on each other: {level 0, resize 0 -> 1},
+        // {pyrdown 0 -> 1, maps 0, resize 1 -> 2}, {pyrdown 1 -> 2, maps 1},
+        // {maps 2} (the resize's time is counted in the pyramid's)
         mark(0);
-        launch_slot(kSlotResize);
-        for (int l = 1; l < 3; ++l)
-            n += launch_resize(L.vmap[l - 1], L.nmap[l - 1], s->W[l - 1], s->W[l - 1], s->H[l - 1], L.vmap[l], L.nmap[l],
-                               s->W[l], st);
         *ran |= 1u << 0;
-        // ... NextFrame->FillImages (Core/Frame.cc:59-78)
         mark(1);
         launch_slot(kSlotPyramid);
-        n += launch_level0(N.depth_in, s->W[0], N.rgb, 3 * s->W[0], s->W[0], s->H[0], c.depth_scale, c.depth_cutoff,
-                           N.raw, s->W[0], N.depth[0], s->W[0], N.gray[0], s->W[0], st);
-        for (int l = 1; l < 3; ++l)
-            n += launch_pyrdown(N.depth[l - 1], s->W[l - 1], N.gray[l - 1], s->W[l - 1], s->W[l - 1], s->H[l - 1],
-                                N.depth[l], s->W[l], N.gray[l], s->W[l], st);
-        for (int l = 0; l < 3; ++l) {
+        auto maps = [&](PreLaunch& P, int l) {
             // level 0 also makes the frame's fusion records
             FuseRecDst fr{N.raw,          s->W[0],      N.rgb, 3 * s->W[0], c.depth_min, c.depth_max, s->map.frec,
                           s->map.fcol, s->map.cvox ? 1 : 0};
-            n += launch_maps(N.depth[l], s->W[l], N.gray[l], s->W[l], s->W[l], s->H[l], s->K[l], c.depth_cutoff,
-                             N.vmap[l], s->W[l], N.nmap[l], s->W[l], N.dx[l], N.dy[l], s->W[l], st, N.rgbok[l],
-                             l == 0 ? &fr : nullptr);
+            pre_maps(P, N.depth[l], s->W[l], N.gray[l], s->W[l], s->W[l], s->H[l], s->K[l], c.depth_cutoff, N.vmap[l],
+                     s->W[l], N.nmap[l], s->W[l], N.dx[l], N.dy[l], s->W[l], N.rgbok[l], l == 0 ? &fr : nullptr);
+        };
+        auto resize = [&](PreLaunch& P, int l) {
+            pre_resize(P, L.vmap[l - 1], L.nmap[l - 1], s->W[l - 1], s->W[l - 1], s->H[l - 1], L.vmap[l], L.nmap[l],
+                       s->W[l]);
+        };
+        auto pyrdown = [&](PreLaunch& P, int l) {
+            pre_pyrdown(P, N.depth[l - 1], s->W[l - 1], N.gray[l - 1], s->W[l - 1], s->W[l - 1], s->H[l - 1],
+                        N.depth[l], s->W[l], N.gray[l], s->W[l]);
+        };
+        {
+            PreLaunch P{};
+            pre_level0(P, N.depth_in, s->W[0], N.rgb, 3 * s->W[0], s->W[0], s->H[0], c.depth_scale, c.depth_cutoff,
+                       N.raw, s->W[0], N.depth[0], s->W[0], N.gray[0], s->W[0]);
+            resize(P, 1);
+            n += launch_pre(P, st);
+        }
+        {
+            PreLaunch P{};
+            pyrdown(P, 1);
+            maps(P, 0);
+            resize(P, 2);
+            n += launch_pre(P, st);
+        }
+        {
+            PreLaunch P{};
+            pyrdown(P, 2);
+            maps(P, 1);
+            n += launch_pre(P, st);
+        }
+        {
+            PreLaunch P{};
+            maps(P, 2);
+            n += launch_pre(P, st);
         }
         *ran |= 1u << 1;
         if (part == 1) return n;
