@@ -273,8 +273,10 @@ int launch_map_reset(const MapView& m, cudaStream_t s);
 // pose: device pointer; skip: device flag (nonzero: do nothing), may be null
 int launch_allocate(const MapView& m, const float* raw, int rp, int W, int H, const Intr& k, const DevPose* pose,
                      const int* skip, cudaStream_t s);
+// after_allocate: launched right after launch_allocate, whose last kernel
+// already zeroed the visible-block and rendering-rectangle counters.
 int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
-                       cudaStream_t s);
+                       cudaStream_t s, bool after_allocate = false);
 // The visible entries (at most `capacity`) in the reference's 32-byte
 // HashEntry layout at dst; the table, voxels and counters in the reference's
 // layouts (the reference form's voxels are the reference's already: the

@@ -976,10 +976,11 @@ int launch_allocate(const MapView& m, const float* raw, int rp, int W, int H, co
 }
 
 int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
-                       cudaStream_t s) {
-    fb_launch(k_reset_visible, (const void*)k_reset_visible_fused, 1, 1, 0, s, m.ctr);
+                       cudaStream_t s, bool after_allocate) {
+    // the allocation's last kernel (k_alloc_finalize) zeroes the same counters
+    if (!after_allocate) fb_launch(k_reset_visible, (const void*)k_reset_visible_fused, 1, 1, 0, s, m.ctr);
     fb_launch(k_visibility, (const void*)k_visibility_fused, sm_count() * 4, 256, 0, s, m, W, H, k, pose, skip);
-    return 2;
+    return after_allocate ? 1 : 2;
 }
 
 int launch_export_visible(const MapView& m, void* dst, int capacity, cudaStream_t s) {

@@ -186,35 +186,38 @@ FB_FUSED_KERNEL(k_zrange, zrange_body, 256)
 // hash table holds for those coordinates (one entry per block), so every
 // lookup returns the same block: a ray's samples turn one indexed load instead
 // of a bucket probe and chain walk, which also keeps a warp's lanes together.
-__device__ __forceinline__ void grid_prepare_body(const BlockCtx& ctx, MapView m, const int* __restrict__ skip) {
-    if (skip && *skip) return;
-    MapCounters* c = m.ctr;
-    long long vol = 1;
-    int n[3], o[3];
-    for (int a = 0; a < 3; ++a) {
-        o[a] = c->bmin[a] - 1;
-        n[a] = c->bmax[a] - c->bmin[a] + 3;
-        if (n[a] < 1) n[a] = 0;
-        vol *= n[a];
-    }
-    const bool on = c->bmin[0] <= c->bmax[0] && vol > 0 && vol <= m.grid_cap;
-    for (int a = 0; a < 3; ++a) {
-        c->g_o[a] = o[a];
-        c->g_n[a] = on ? n[a] : 0;
-    }
-    c->g_on = on ? 1 : 0;
-}
+//
+// The box from the z-range pass's bounds (every block of the clearing kernel
+// derives it; block 0 publishes it for the fill and the raycast).
+struct GridBox {
+    int o[3], n[3];
+    bool on;
+};
 
-__global__ void __launch_bounds__(32) k_grid_prepare(MapView m, const int* __restrict__ skip) {
-    grid_prepare_body(own_ctx(), m, skip);
+__device__ __forceinline__ GridBox grid_box(const MapView& m) {
+    const MapCounters* c = m.ctr;
+    GridBox b;
+    long long vol = 1;
+    for (int a = 0; a < 3; ++a) {
+        b.o[a] = c->bmin[a] - 1;
+        b.n[a] = c->bmax[a] - c->bmin[a] + 3;
+        if (b.n[a] < 1) b.n[a] = 0;
+        vol *= b.n[a];
+    }
+    b.on = c->bmin[0] <= c->bmax[0] && vol > 0 && vol <= m.grid_cap;
+    return b;
 }
-FB_FUSED_KERNEL(k_grid_prepare, grid_prepare_body, 32)
 
 __device__ __forceinline__ void grid_clear_body(const BlockCtx& ctx, MapView m, const int* __restrict__ skip) {
     if (skip && *skip) return;
-    const MapCounters* c = m.ctr;
-    if (!c->g_on) return;
-    const int vol = c->g_n[0] * c->g_n[1] * c->g_n[2];
+    const GridBox gb = grid_box(m);
+    if (ctx.bx == 0 && threadIdx.x < 3) {
+        m.ctr->g_o[threadIdx.x] = gb.o[threadIdx.x];
+        m.ctr->g_n[threadIdx.x] = gb.on ? gb.n[threadIdx.x] : 0;
+        if (threadIdx.x == 0) m.ctr->g_on = gb.on ? 1 : 0;
+    }
+    if (!gb.on) return;
+    const int vol = gb.n[0] * gb.n[1] * gb.n[2];
     int4* g4 = (int4*)m.grid;
     const int4 none = make_int4(-1, -1, -1, -1);
     for (int i = ctx.bx * blockDim.x + threadIdx.x; i < (vol + 3) / 4; i += ctx.gx * blockDim.x) g4[i] = none;
@@ -701,10 +704,9 @@ int launch_zrange(const MapView& m, const Intr& k, const DevPose* pose, const in
     const int ord_n = m.rc_order ? rc_tiles : 0;
     fb_launch(k_zrange, (const void*)k_zrange_fused, sm_count_rc() * 2 + (ord_n > 0 ? 1 : 0), 256, 0, s, m, k, pose,
               skip, ord_n);
-    fb_launch(k_grid_prepare, (const void*)k_grid_prepare_fused, 1, 1, 0, s, m, skip);
     fb_launch(k_grid_clear, (const void*)k_grid_clear_fused, sm_count_rc() * 4, 256, 0, s, m, skip);
     fb_launch(k_grid_fill, (const void*)k_grid_fill_fused, sm_count_rc() * 4, 256, 0, s, m, skip);
-    return 5;
+    return 4;
 }
 
 int launch_raycast(const MapView& m, float4* vmap, float4* nmap, int p, int W, int H, const Intr& k,

@@ -463,7 +463,7 @@ int issue_frame(fb_session* s, bool track, bool fuse, bool render, bool init, un
         n += launch_allocate(s->map, N.raw, s->W[0], s->W[0], s->H[0], s->K[0], pose, skip, st);
         mark(4);
         launch_slot(kSlotVisibility);
-        n += launch_visibility(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st);
+        n += launch_visibility(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st, true);
         mark(5);
         launch_slot(kSlotIntegrate);
         n += launch_integrate(s->map, s->W[0], s->H[0], s->K[0], pose, skip, st, s->integ_cps);
