@@ -201,6 +201,7 @@ struct MapCounters {
     int snap_M, snap_hc, snap_ep, snap_na;
     int fast;              // the parallel insertion path applies
     unsigned int ray_next; // tile counter of the queued raycast (zeroed with the z ranges)
+    unsigned int scan_ticket; // chunk-scan blocks done this frame (the last one resets it)
 };
 
 struct NewBlock {

@@ -13,9 +13,11 @@
 //              the map go into a per-frame open-addressing request set (CAS on
 //              64-bit keys); the first insert of a key appends it to the list
 //              of new blocks.
-//   count / scan / place / rank : a counting sort of the new blocks by bucket
-//              (per-bucket counters, a two-level scan over all buckets), then
-//              the rank of each block inside its bucket by coordinates.
+//   scan / place / rank : a counting sort of the new blocks by bucket
+//              (per-bucket counters taken by the requests, a two-level scan
+//              over all buckets whose top level runs in the last chunk block
+//              to finish), then the rank of each block inside its bucket by
+//              coordinates.
 //   insert   : each new block computes from its rank alone where the
 //              sequential insertion would put it: free-stack position, head
 //              slot or excess slot, and its chain link; the one block per
@@ -85,7 +87,9 @@ __device__ __forceinline__ void request_block(const MapView& m, int x, int y, in
                 nb.pad = 0;
                 nb.bucket = bucket_of_m(x, y, z, (uint32_t)m.NB, m.nb_mask);
                 nb.setslot = (int)h;
-                nb.j = 0;
+                // arrival order inside the bucket (any order: the rank
+                // below orders the bucket by coordinates)
+                nb.j = atomicAdd(&m.bucket_cnt[nb.bucket], 1);
                 nb.rank = 0;
                 nb.pad2 = 0;
                 m.newblk[idx] = nb;
@@ -148,25 +152,18 @@ __global__ void __launch_bounds__(256) k_alloc_requests(MapView m, const float* 
 }
 FB_FUSED_KERNEL(k_alloc_requests, alloc_requests_body, 256)
 
-__device__ __forceinline__ void alloc_count_body(const BlockCtx& ctx, MapView m) {
-    const int M = min(m.ctr->n_req, m.newcap);
-    for (int i = ctx.bx * blockDim.x + threadIdx.x; i < M; i += ctx.gx * blockDim.x)
-        m.newblk[i].j = atomicAdd(&m.bucket_cnt[m.newblk[i].bucket], 1);
-}
-
-__global__ void __launch_bounds__(256) k_alloc_count(MapView m) {
-    alloc_count_body(own_ctx(), m);
-}
-FB_FUSED_KERNEL(k_alloc_count, alloc_count_body, 256)
+__device__ __forceinline__ void scan_top_body(MapView m);
 
 // Per chunk of kScanChunk buckets: number of new blocks, and of those that go
 // to the excess list (all but the first when the bucket's head slot is empty).
+// The last block to finish then scans the chunk sums (scan_top_body).
 __device__ __forceinline__ void scan_chunks_body(const BlockCtx& ctx, MapView m) {
-    if (m.ctr->n_req == 0) return;
     __shared__ int s_c[256], s_x[256];
+    __shared__ bool s_last;
     const int base = ctx.bx * kScanChunk;
+    const bool any = m.ctr->n_req > 0;
     int c = 0, xs = 0;
-    for (int q = threadIdx.x; q < kScanChunk; q += 256) {
+    for (int q = threadIdx.x; any && q < kScanChunk; q += 256) {
         int b = base + q;
         if (b >= m.NB) break;
         int n = m.bucket_cnt[b];
@@ -189,7 +186,14 @@ __device__ __forceinline__ void scan_chunks_body(const BlockCtx& ctx, MapView m)
     if (threadIdx.x == 0) {
         m.chunk_sums[2 * ctx.bx] = s_c[0];
         m.chunk_sums[2 * ctx.bx + 1] = s_x[0];
+        __threadfence();
+        s_last = atomicAdd(&m.ctr->scan_ticket, 1u) == (unsigned)ctx.gx - 1u;
     }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) m.ctr->scan_ticket = 0;
+    scan_top_body(m);
 }
 
 __global__ void __launch_bounds__(256) k_scan_chunks(MapView m) {
@@ -197,13 +201,13 @@ __global__ void __launch_bounds__(256) k_scan_chunks(MapView m) {
 }
 FB_FUSED_KERNEL(k_scan_chunks, scan_chunks_body, 256)
 
-// Exclusive scan over the chunk sums (one block of 1024 threads, chunks in
-// order); snapshot of the counters and choice of the parallel or sequential
-// insertion path.
-__device__ __forceinline__ void scan_top_body(const BlockCtx& ctx, MapView m) {
+// Exclusive scan over the chunk sums (the 256 threads of the last chunk
+// block, chunks in order); snapshot of the counters and choice of the
+// parallel or sequential insertion path.
+__device__ __forceinline__ void scan_top_body(MapView m) {
     MapCounters* c = m.ctr;
     const int M = min(c->n_req, m.newcap);
-    __shared__ int s_a[1024], s_e[1024];
+    __shared__ int s_a[256], s_e[256];
     __shared__ int s_base_a, s_base_e;
     if (threadIdx.x == 0) {
         s_base_a = 0;
@@ -211,14 +215,14 @@ __device__ __forceinline__ void scan_top_body(const BlockCtx& ctx, MapView m) {
     }
     __syncthreads();
     if (M > 0) {
-        for (int c0 = 0; c0 < m.nchunks; c0 += 1024) {
+        for (int c0 = 0; c0 < m.nchunks; c0 += 256) {
             const int i = c0 + threadIdx.x;
-            const int a = i < m.nchunks ? m.chunk_sums[2 * i] : 0;
-            const int e = i < m.nchunks ? m.chunk_sums[2 * i + 1] : 0;
+            const int a = i < m.nchunks ? __ldcg(&m.chunk_sums[2 * i]) : 0;
+            const int e = i < m.nchunks ? __ldcg(&m.chunk_sums[2 * i + 1]) : 0;
             s_a[threadIdx.x] = a;
             s_e[threadIdx.x] = e;
             __syncthreads();
-            for (int o = 1; o < 1024; o <<= 1) {   // inclusive Hillis-Steele scan
+            for (int o = 1; o < 256; o <<= 1) {   // inclusive Hillis-Steele scan
                 int ta = threadIdx.x >= o ? s_a[threadIdx.x - o] : 0;
                 int te = threadIdx.x >= o ? s_e[threadIdx.x - o] : 0;
                 __syncthreads();
@@ -232,8 +236,8 @@ __device__ __forceinline__ void scan_top_body(const BlockCtx& ctx, MapView m) {
             }
             __syncthreads();
             if (threadIdx.x == 0) {
-                s_base_a += s_a[1023];
-                s_base_e += s_e[1023];
+                s_base_a += s_a[255];
+                s_base_e += s_e[255];
             }
             __syncthreads();
         }
@@ -252,10 +256,6 @@ __device__ __forceinline__ void scan_top_body(const BlockCtx& ctx, MapView m) {
     }
 }
 
-__global__ void __launch_bounds__(1024) k_scan_top(MapView m) {
-    scan_top_body(own_ctx(), m);
-}
-FB_FUSED_KERNEL(k_scan_top, scan_top_body, 1024)
 
 // Per chunk: exclusive scan of the per-bucket counts into segment starts and
 // excess starts.
@@ -939,6 +939,8 @@ __global__ void k_map_reset(MapView m) {
         c->err = 0;
         c->seq_path = 0;
         c->snap_M = 0;
+        c->ray_next = 0;
+        c->scan_ticket = 0;
     }
 }
 
@@ -964,15 +966,13 @@ int launch_allocate(const MapView& m, const float* raw, int rp, int W, int H, co
     dim3 b(32, 8), g((W + 31) / 32, (H + 7) / 8);
     fb_launch(k_alloc_requests, (const void*)k_alloc_requests_fused, g, b, 0, s, m, raw, rp, W, H, k, pose, skip);
     const int gs = sm_count() * 4;
-    fb_launch(k_alloc_count, (const void*)k_alloc_count_fused, gs, 256, 0, s, m);
     fb_launch(k_scan_chunks, (const void*)k_scan_chunks_fused, m.nchunks, 256, 0, s, m);
-    fb_launch(k_scan_top, (const void*)k_scan_top_fused, 1, 1024, 0, s, m);
     fb_launch(k_scan_apply, (const void*)k_scan_apply_fused, m.nchunks, 256, 0, s, m);
     fb_launch(k_alloc_place, (const void*)k_alloc_place_fused, gs, 256, 0, s, m);
     fb_launch(k_alloc_rank, (const void*)k_alloc_rank_fused, gs, 256, 0, s, m);
     fb_launch(k_alloc_insert, (const void*)k_alloc_insert_fused, gs, 256, 0, s, m);
     fb_launch(k_alloc_finalize, (const void*)k_alloc_finalize_fused, gs, 256, 0, s, m);
-    return 9;
+    return 7;
 }
 
 int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
