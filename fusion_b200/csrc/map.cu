@@ -18,7 +18,8 @@
 //              over all buckets whose top level runs in the last chunk block
 //              to finish), then the rank of each block inside its bucket by
 //              coordinates.
-//   insert   : each new block computes from its rank alone where the
+//   insert   : (also the counters after the frame and the clearing of the
+//              per-bucket counters) each new block computes from its rank alone where the
 //              sequential insertion would put it: free-stack position, head
 //              slot or excess slot, and its chain link; the one block per
 //              bucket that extends an existing chain links the old tail.  If
@@ -394,13 +395,30 @@ __device__ int create_block_seq(const MapView& m, int x, int y, int z, int& hc, 
     return -1;
 }
 
+// The insertion (parallel or sequential path), the clearing of the per-bucket
+// counters for the next frame, and the map counters after this frame: every
+// thread reads only the snapshot, so the first thread can write the counters
+// at once.
 __device__ __forceinline__ void alloc_insert_body(const BlockCtx& ctx, MapView m) {
     MapCounters* c = m.ctr;
     const int M = c->snap_M;
+    const bool fast = c->fast;
+    const int gtid = ctx.bx * blockDim.x + threadIdx.x, gstride = ctx.gx * blockDim.x;
+    if (gtid == 0) {
+        if (M > 0 && fast) {
+            c->heap_counter = c->snap_hc - M;
+            c->entry_ptr = c->snap_ep + c->excess_total;
+            c->n_alloc = c->snap_na + M;
+            c->seq_path = 0;
+        }
+        c->n_new = M;
+        c->n_req = 0;
+        c->n_visible = 0;
+        c->n_tiles = 0;
+    }
     if (M == 0) return;
     const int hc0 = c->snap_hc, ep0 = c->snap_ep, na0 = c->snap_na;
-    const int gtid = ctx.bx * blockDim.x + threadIdx.x, gstride = ctx.gx * blockDim.x;
-    if (!c->fast) {
+    if (!fast) {
         if (gtid == 0) {
             int hc = hc0, ep = ep0, holes = c->holes, na = na0;
             for (int R = 0; R < M; ++R) {
@@ -418,16 +436,23 @@ __device__ __forceinline__ void alloc_insert_body(const BlockCtx& ctx, MapView m
             c->n_alloc = na;
             c->seq_path = 1;
         }
-        for (int R = gtid; R < M; R += gstride) m.reqset[m.newblk[m.order[R]].setslot] = 0ull;
+        for (int R = gtid; R < M; R += gstride) {
+            const NewBlock& nb = m.newblk[m.order[R]];
+            m.reqset[nb.setslot] = 0ull;
+            m.bucket_cnt[nb.bucket] = 0;
+        }
         return;
     }
     for (int R = gtid; R < M; R += gstride) {
         const int i = m.order[R];
         const NewBlock nb = m.newblk[i];
         const int b = (int)nb.bucket;
-        const int s = m.bucket_start[b], n = m.bucket_cnt[b], bx = m.bucket_x[b];
+        const int s = m.bucket_start[b], bx = m.bucket_x[b];
         const int he = bx & 1, xs = bx >> 1;
         const int r = R - s;
+        // the bucket's blocks are consecutive in canonical order: another
+        // follows this one exactly when the next block has the same bucket
+        const bool more = R + 1 < M && (int)m.newblk[m.order[R + 1]].bucket == b;
         HEntry e;
         e.x = nb.x;
         e.y = nb.y;
@@ -437,12 +462,12 @@ __device__ __forceinline__ void alloc_insert_body(const BlockCtx& ctx, MapView m
         int slot;
         if (he && r == 0) {
             slot = b;
-            e.offset = n > 1 ? ep0 + xs : 0;
+            e.offset = more ? ep0 + xs : 0;
         } else {
             const int q = r - he;                 // rank among this bucket's excess blocks
             const int off = ep0 + xs + q;
             slot = m.NB + off - 1;
-            e.offset = r + 1 < n ? off + 1 : 0;
+            e.offset = more ? off + 1 : 0;
             if (q == 0 && !he) {
                 // link the tail of the existing chain (CreateBlock's e->offset = offset)
                 int t = b;
@@ -455,6 +480,7 @@ __device__ __forceinline__ void alloc_insert_body(const BlockCtx& ctx, MapView m
         m.entries[slot] = e;
         m.alloc_list[na0 + R] = slot;
         m.reqset[nb.setslot] = 0ull;
+        m.bucket_cnt[b] = 0;
     }
 }
 
@@ -463,29 +489,6 @@ __global__ void __launch_bounds__(256) k_alloc_insert(MapView m) {
 }
 FB_FUSED_KERNEL(k_alloc_insert, alloc_insert_body, 256)
 
-__device__ __forceinline__ void alloc_finalize_body(const BlockCtx& ctx, MapView m) {
-    MapCounters* c = m.ctr;
-    const int M = c->snap_M;
-    for (int i = ctx.bx * blockDim.x + threadIdx.x; i < M; i += ctx.gx * blockDim.x)
-        m.bucket_cnt[m.newblk[i].bucket] = 0;
-    if (ctx.bx == 0 && threadIdx.x == 0) {
-        if (M > 0 && c->fast) {
-            c->heap_counter = c->snap_hc - M;
-            c->entry_ptr = c->snap_ep + c->excess_total;
-            c->n_alloc = c->snap_na + M;
-            c->seq_path = 0;
-        }
-        c->n_new = M;
-        c->n_req = 0;
-        c->n_visible = 0;
-        c->n_tiles = 0;
-    }
-}
-
-__global__ void __launch_bounds__(256) k_alloc_finalize(MapView m) {
-    alloc_finalize_body(own_ctx(), m);
-}
-FB_FUSED_KERNEL(k_alloc_finalize, alloc_finalize_body, 256)
 
 // ---------------------------------------------------------------- visibility
 
@@ -971,13 +974,12 @@ int launch_allocate(const MapView& m, const float* raw, int rp, int W, int H, co
     fb_launch(k_alloc_place, (const void*)k_alloc_place_fused, gs, 256, 0, s, m);
     fb_launch(k_alloc_rank, (const void*)k_alloc_rank_fused, gs, 256, 0, s, m);
     fb_launch(k_alloc_insert, (const void*)k_alloc_insert_fused, gs, 256, 0, s, m);
-    fb_launch(k_alloc_finalize, (const void*)k_alloc_finalize_fused, gs, 256, 0, s, m);
-    return 7;
+    return 6;
 }
 
 int launch_visibility(const MapView& m, int W, int H, const Intr& k, const DevPose* pose, const int* skip,
                        cudaStream_t s, bool after_allocate) {
-    // the allocation's last kernel (k_alloc_finalize) zeroes the same counters
+    // the allocation's last kernel (k_alloc_insert) zeroes the same counters
     if (!after_allocate) fb_launch(k_reset_visible, (const void*)k_reset_visible_fused, 1, 1, 0, s, m.ctr);
     fb_launch(k_visibility, (const void*)k_visibility_fused, sm_count() * 4, 256, 0, s, m, W, H, k, pose, skip);
     return after_allocate ? 1 : 2;
