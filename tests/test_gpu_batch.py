@@ -138,10 +138,34 @@ def test_raycast_tile_does_not_change_results(frames):
     base, _ = _batched(frames, LOCKSTEP, 0)
     tiled, _ = _batched(frames, LOCKSTEP, 0, tiles=[(0, 0), (32, 4), (8, 8)])
     assert tiled == base
-    # fused steps: sessions with different tiles (and the lane-refill
-    # raycast) run as separate fused raycast launches
+    # fused steps: sessions with different tiles (and the queued raycast)
+    # run as separate fused raycast launches
     fused, _ = _batched(frames, LOCKSTEP, 2, tiles=[(0, 0), (32, 4), (8, 8)])
     assert fused == base
+
+
+def test_raycast_tile_change_between_frames_changes_no_result(frames):
+    """The raycast dispatches its blocks in the order the z-range pass
+    prepared from the last raycast's per-tile costs.  A session whose tile
+    changes every frame (so each order comes from another tile grid's costs)
+    gives the same poses, counts, map and final raycast maps as one that keeps
+    the default tile."""
+    from fusion_b200 import Session
+    from fusion_b200.batch import set_raycast_tile
+    d, c = frames[2]
+    out = []
+    for tiles in ([(16, 8)] * N_FRAMES, [(16, 8), (8, 8), (32, 4), (0, 0), (16, 8), (8, 16)]):
+        s = Session(_config(2))
+        rows = []
+        for k in range(N_FRAMES):
+            set_raycast_tile(s, *tiles[k])
+            rows.append(_row(s.grab(d[k], c[k])))
+        maps = [s.level(which, 0)[key].tobytes() for which in (0, 1) for key in ("vmap", "nmap")]
+        out.append((rows, _map_digest(s), maps))
+        s.close()
+    assert out[0][0] == out[1][0]
+    assert out[0][1] == out[1][1]
+    assert out[0][2] == out[1][2]
 
 
 FORMS = [1, 0, 1, 0, 0]   # precision and reference forms mixed in one step
