@@ -388,11 +388,13 @@ __device__ __forceinline__ void add_products(const float row[7], float acc[29]) 
 // gathers of two entries overlap (the clustered forms, with registers to
 // spare; the 64-register group forms add the rows one at a time,
 // add_segment_rows_seq: 2 % faster there, the same sums).
+// `a`: the fetch of entry `lane` (when lane < n), issued by the caller before
+// the robust scale is known.
 __device__ __forceinline__ void add_segment_rows(const TrackLevel& L, const DevPose& cur, const DevPose& last,
-                                                 float sigma, const int2* seg, int n, int lane, float acc[29]) {
+                                                 float sigma, const int2* seg, int n, int lane, float acc[29],
+                                                 RgbIn a) {
     int i = lane;
     if (i >= n) return;
-    RgbIn a = rgb_fetch_entry(L, seg[i]);
     for (; i < n; i += 32) {
         RgbIn b = a;
         if (i + 32 < n) b = rgb_fetch_entry(L, seg[i + 32]);
@@ -748,6 +750,8 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     int p = blockIdx.x * 256 + threadIdx.x;
     PixelWalk pw(p, G * 256, L.W);
     if (st->failed) return;   // uniform over the grid: written by an earlier kernel
+    // the pose loads are in flight while the first chunks are staged
+    const DevPose cur = st->cur, last = st->last;
     cg::cluster_group cl = cg::this_cluster();
     __shared__ float sm[8 * 32];
     __shared__ long long smll[32];
@@ -761,7 +765,6 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
         for (int c = 0; c < 2 && c < iters && base + c * G * 256 < N; ++c) stage_chunk(stg, c, L, base + c * G * 256, N);
     }
     __syncthreads();
-    const DevPose cur = st->cur, last = st->last;
     float acc[29];
 #pragma unroll
     for (int k = 0; k < 29; ++k) acc[k] = 0.f;
@@ -977,6 +980,13 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
         }
     }
     if (st->failed) return;
+    // the first row's inputs (list entry, then its gathers) are loaded while
+    // the robust scale is reduced: neither needs the other
+    const int gw = blockIdx.x * kTrackWarps + wid;
+    const int2* seg = list + (size_t)gw * seg_size;
+    const int nseg = counts[gw];
+    RgbIn first{};
+    if (lane < nseg) first = rgb_fetch_entry(L, seg[lane]);
     const DevPose cur = st->cur, last = st->last;
     // sigma = sqrt((float) sum / count) (Reduction.cu:606-608); every warp
     // adds the group counts itself (integers: exact in any order)
@@ -994,8 +1004,7 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     float acc[29];
 #pragma unroll
     for (int k = 0; k < 29; ++k) acc[k] = 0.f;
-    const int gw = blockIdx.x * kTrackWarps + wid;
-    add_segment_rows(L, cur, last, sigma, list + (size_t)gw * seg_size, counts[gw], lane, acc);
+    add_segment_rows(L, cur, last, sigma, seg, nseg, lane, acc, first);
     const float bsum = block_sum29(acc, sm);
     if (wid == 0) s_rgb[lane] = lane < 29 ? bsum : 0.f;
     const int grp = blockIdx.x / kTrackCluster;
