@@ -148,8 +148,10 @@ FB_API int fb_stage_frame(fb_session* s, const uint16_t* depth, size_t depth_pit
 /* Tracing (the reference has none; Utility/StopWatch.h is never called):
  * with profiling on, every frame records CUDA events around its stages and
  * accumulates device milliseconds per stage: 0 resize of the last frame's
- * maps, 1 pyramid, 2 tracking, 3 block allocation, 4 visibility,
- * 5 integration, 6 z ranges, 7 raycast.  Switching it on resets the sums. */
+ * maps (its kernels run inside the pyramid's launches, so its own time is
+ * only the events'), 1 pyramid and resize, 2 tracking, 3 block allocation,
+ * 4 visibility, 5 integration, 6 z ranges, 7 raycast.  Switching it on
+ * resets the sums. */
 FB_API int fb_session_set_profiling(fb_session* s, int on);
 FB_API int fb_session_stage_times(fb_session* s, double* ms, uint64_t* calls, int n);
 /* Frames run as captured CUDA graphs (default on; one capture per tracker
