@@ -66,7 +66,7 @@ int track_grid(int n);
 int track_cluster_grid(int n);   // track_grid rounded up to whole clusters
 int launch_track_begin(TrackState* st, cudaStream_t s);
 // residual: per-warp compact segments of photometric correspondences
-// (int2: pixel, packed last pixel + difference), capacity track_list_capacity;
+// (int2: the pixel's Sobel derivatives dx | dy << 16, packed last pixel + difference), capacity track_list_capacity;
 // counts: entries per segment (kTrackMaxBlocks * kTrackWarps ints)
 // shared_gpu: the instance with four resident blocks per SM (other sessions'
 // kernels run beside it); same results as the two-block instance

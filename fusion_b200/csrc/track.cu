@@ -58,13 +58,12 @@ __device__ __forceinline__ float below_1em6() { return __int_as_float(0x358637be
 // (u, v) and the gray difference d (-254..255, as d + 255 in 1..510):
 // v << 21 | u << 9 | (d + 255).  Images are at most 4096 x 2048; the low 9
 // bits are never all ones, so -1 (all ones) marks "no correspondence".
-// Pixels of the correspondence lists are packed as y << 12 | x.
+// A correspondence list entry is {the pixel's Sobel derivatives (uint16) dx | dy << 16, pack_corr}.
 __device__ __forceinline__ int pack_corr(int u, int v, int d255) {
     return (int)(((unsigned)v << 21) | ((unsigned)u << 9) | (unsigned)d255);
 }
 __device__ __forceinline__ int corr_u(int c) { return (int)(((unsigned)c >> 9) & 4095u); }
 __device__ __forceinline__ int corr_v(int c) { return (int)((unsigned)c >> 21); }
-__device__ __forceinline__ int pack_xy(int x, int y) { return (y << 12) | x; }
 
 // ICPReduce::searchPoint + getRow (Reduction.cu:227-286).  Returns false when
 // the pixel has no correspondence.  Decisions use the order-exact float ops.
@@ -159,9 +158,16 @@ __device__ __forceinline__ RgbIn rgb_fetch(const TrackLevel& L, int x, int y, in
     return in;
 }
 
-// The fetch of correspondence list entry e (pixel y << 12 | x, packed value).
+// The fetch of correspondence list entry e (the pixel's derivatives
+// (uint16) dx | dy << 16, packed value): only the last vertex at the
+// correspondence is gathered.
 __device__ __forceinline__ RgbIn rgb_fetch_entry(const TrackLevel& L, int2 e) {
-    return rgb_fetch(L, e.x & 4095, e.x >> 12, e.y);
+    RgbIn in;
+    in.vlast = L.vlast[corr_v(e.y) * L.vp + corr_u(e.y)];
+    in.dx = (int)(int16_t)(e.x & 0xffff);
+    in.dy = e.x >> 16;
+    in.packed = e.y;
+    return in;
 }
 
 // RGBReduction::GetRow (Reduction.cu:471-508) from fetched inputs.
@@ -203,40 +209,23 @@ struct PixelIn {
     float3 nc;      // current normal (xyz)
     int ok;         // photometric eligibility (border, window, gradient)
     int gc;         // current gray value
-};
-
-// Pixel coordinates of a strided pixel walk without divisions: the walk
-// starts at linear pixel p and steps by S pixels (S = SY rows + SX columns).
-struct PixelWalk {
-    int x, y, sx, sy, W;
-    __device__ __forceinline__ PixelWalk(int p, int S, int W_) : W(W_) {
-        y = p / W;
-        x = p - y * W;
-        sy = S / W;
-        sx = S - sy * W;
-    }
-    __device__ __forceinline__ void next(int& nx, int& ny) const {
-        nx = x + sx;
-        ny = y + sy;
-        if (nx >= W) {
-            nx -= W;
-            ++ny;
-        }
-    }
-    __device__ __forceinline__ void step() { next(x, y); }
+    int dxy;        // Sobel derivatives: (uint16) dx | dy << 16
 };
 
 // Pass A's current-frame inputs staged in shared memory by bulk copies
 // (cp.async.bulk, this GPU's own memory, no multicast).  A chunk is one
 // logical block's 256 consecutive pixels of one pass over the image (the
 // frame buffers have pitch == width, so a chunk is one contiguous range of
-// each map): vertices and normals (4 KB each), photometric eligibility and
-// gray (256 B each, rounded up to 16 B at the image's end, inside the
+// each map): vertices and normals (4 KB each), the Sobel derivatives
+// (512 B each), photometric eligibility and gray (256 B each; the derivative
+// and byte rows are rounded up to 16 B at the image's end, inside the
 // allocations, which are 256-byte multiples).  Two buffers: chunk c + 2 is
 // copied while chunk c + 1 is processed.
 struct PixelStage {
     float4 v[2][256];
     float4 n[2][256];
+    int16_t dx[2][256];
+    int16_t dy[2][256];
     uint8_t ok[2][256];
     uint8_t g[2][256];
     uint64_t bar[2];
@@ -247,10 +236,13 @@ struct PixelStage {
 __device__ __forceinline__ void stage_chunk(PixelStage& S, int buf, const TrackLevel& L, int start, int N) {
     const int cnt = min(256, N - start);
     const uint32_t b16 = (uint32_t)cnt * 16u, b1 = ((uint32_t)cnt + 15u) & ~15u;
+    const uint32_t b2 = ((uint32_t)cnt * 2u + 15u) & ~15u;
     fence_proxy_async_smem();
-    mbar_arrive_expect_tx(&S.bar[buf], 2u * b16 + 2u * b1);
+    mbar_arrive_expect_tx(&S.bar[buf], 2u * b16 + 2u * b2 + 2u * b1);
     bulk_copy_g2s(S.v[buf], L.vcurr + start, b16, &S.bar[buf]);
     bulk_copy_g2s(S.n[buf], L.ncurr + start, b16, &S.bar[buf]);
+    bulk_copy_g2s(S.dx[buf], L.dx + start, b2, &S.bar[buf]);
+    bulk_copy_g2s(S.dy[buf], L.dy + start, b2, &S.bar[buf]);
     bulk_copy_g2s(S.ok[buf], L.rgbok + start, b1, &S.bar[buf]);
     bulk_copy_g2s(S.g[buf], L.gcurr + start, b1, &S.bar[buf]);
 }
@@ -302,6 +294,7 @@ __device__ __forceinline__ PixelIn staged_pixel(const PixelStage& S, int buf, in
     in.nc = make_float3(n.x, n.y, n.z);
     in.ok = S.ok[buf][t];
     in.gc = S.g[buf][t];
+    in.dxy = (int)(uint16_t)S.dx[buf][t] | ((int)S.dy[buf][t] << 16);
     return in;
 }
 
@@ -748,7 +741,6 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
     const int N = L.W * L.H;
     const int G = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int p = blockIdx.x * 256 + threadIdx.x;
-    PixelWalk pw(p, G * 256, L.W);
     if (st->failed) return;   // uniform over the grid: written by an earlier kernel
     // the pose loads are in flight while the first chunks are staged
     const DevPose cur = st->cur, last = st->last;
@@ -785,8 +777,6 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
         __syncthreads();   // buffer `buf` is read: chunk k + 2 may overwrite it
         if (threadIdx.x == 0 && k + 2 < iters && base + (k + 2) * G * 256 < N)
             stage_chunk(stg, buf, L, base + (k + 2) * G * 256, N);
-        const int px = pw.x, py = pw.y;
-        pw.step();
         int r = -1;
         if (p < N) {
             float row[7];
@@ -798,7 +788,7 @@ __global__ void __cluster_dims__(kTrackCluster, 1, 1) __launch_bounds__(256, kMi
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, r != -1);
-        if (r != -1) seg[run + __popc(m & lt)] = make_int2(pack_xy(px, py), r);
+        if (r != -1) seg[run + __popc(m & lt)] = make_int2(in.dxy, r);
         run += __popc(m);
     }
     if (lane == 0) counts[gw] = run;
@@ -1081,7 +1071,6 @@ __device__ __forceinline__ void track_a_grp_body(const BlockCtx& ctx, TrackLevel
     for (int r = 0; r < kTrackCluster; ++r) {
         const int b = g * kTrackCluster + r;
         int p = b * 256 + threadIdx.x;
-        PixelWalk pw(p, G * 256, L.W);
         float acc[29];
 #pragma unroll
         for (int k = 0; k < 29; ++k) acc[k] = 0.f;
@@ -1105,8 +1094,6 @@ __device__ __forceinline__ void track_a_grp_body(const BlockCtx& ctx, TrackLevel
                 ++prod.k;
                 prod.settle(ctx.bx, gpc, NG, iters, G * 256, N);
             }
-            const int px = pw.x, py = pw.y;
-            pw.step();
             int rr = -1;
             if (p < N) {
                 float row[7];
@@ -1118,7 +1105,7 @@ __device__ __forceinline__ void track_a_grp_body(const BlockCtx& ctx, TrackLevel
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, rr != -1);
-            if (rr != -1) seg[run + __popc(m & lt)] = make_int2(pack_xy(px, py), rr);
+            if (rr != -1) seg[run + __popc(m & lt)] = make_int2(in.dxy, rr);
             run += __popc(m);
         }
         if (lane == 0) counts[gw] = run;
